@@ -1,0 +1,278 @@
+/*
+ * rtrace_gpu.h -- C ABI of the B200 render path for SeaRyanC/rtrace scenes.
+ *
+ * The reference renders through the Rust API `Renderer::render(&self,
+ * &Scene) -> Result<RgbImage, Box<dyn Error>>` (src/renderer.rs:120) and
+ * `Renderer::render_to_file` (src/renderer.rs:914).  This header is what a
+ * Rust (or any C-FFI) host binds to replace that body: scenes are loaded
+ * once into a device-resident handle, and each render call takes the
+ * `Renderer` fields (src/renderer.rs:37-47) and fills a caller-owned RGB8
+ * buffer with the bytes `create_image_from_data` (src/renderer.rs:899-912)
+ * would produce.
+ *
+ * Conventions
+ *   - Every entry point returns an rt_status; nothing throws across the ABI.
+ *     The message of the last failure on a context is rt_last_error(ctx).
+ *   - Caller buffers are borrowed for the duration of the call; device
+ *     memory belongs to the context (or to the scene handle).
+ *   - A context owns one CUDA stream.  Calls on one context must not
+ *     overlap; use one context per host thread for concurrency (render
+ *     calls are re-entrant in the reference: src/renderer.rs:120 takes
+ *     &self and builds its world per call).
+ */
+#ifndef RTRACE_GPU_H
+#define RTRACE_GPU_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* Status codes.  The reference reports errors as strings inside a
+ * Result; RT_ERR_SCENE covers Scene::from_json_file/from_json_str failures
+ * (src/scene.rs:462-505, src/mesh.rs:751-1003) and RT_ERR_RENDER covers the
+ * errors Renderer::render returns: "Samples must be greater than 0"
+ * (src/renderer.rs:122-124), "Field of view must be between 0 and 180
+ * degrees" (src/camera.rs:115-117), "Unsupported camera type: ..."
+ * (src/camera.rs:62), "Invalid hex color..." (src/scene.rs:15-30) and the
+ * panics of rand's gen_range on an empty range (a disk light of zero or
+ * negative diameter).  The remaining codes are GPU-side failures the
+ * reference cannot have. */
+typedef enum rt_status {
+  RT_OK = 0,
+  RT_ERR_INVALID_ARGUMENT = 1,
+  RT_ERR_SCENE = 2,
+  RT_ERR_RENDER = 3,
+  RT_ERR_CUDA = 4,
+  RT_ERR_OUT_OF_MEMORY = 5,
+  RT_ERR_DEVICE_WATCHDOG = 6, /* a bounded device loop ran out of iterations */
+  RT_ERR_IO = 7
+} rt_status;
+
+/* AntiAliasingMode (src/renderer.rs:16-24). */
+typedef enum rt_aa_mode {
+  RT_AA_NO_JITTER = 0,
+  RT_AA_QUINCUNX = 1,
+  RT_AA_STOCHASTIC = 2
+} rt_aa_mode;
+
+typedef struct rt_ctx rt_ctx;     /* device, stream and scratch buffers */
+typedef struct rt_scene rt_scene; /* device-resident flattened world */
+
+/* OutlineConfig (src/outline.rs:5-31).  Applied only in the no-jitter and
+ * stochastic modes, as src/renderer.rs:409-410 ignores it in quincunx. */
+typedef struct rt_outline_config {
+  int32_t enabled;
+  int32_t use_8_neighbors;
+  double depth_weight;
+  double normal_weight;
+  double threshold;
+  double edge_color[3];
+  double line_thickness;
+} rt_outline_config;
+
+/* Renderer fields (src/renderer.rs:37-47).  thread_count has no device
+ * meaning and is not carried.  seed: `None` is rendered as 0, exactly as
+ * `self.seed.unwrap_or(0)` does. */
+typedef struct rt_render_params {
+  uint32_t width;
+  uint32_t height;
+  int32_t max_depth;
+  int32_t use_kdtree;
+  uint32_t samples;
+  int32_t anti_aliasing_mode; /* rt_aa_mode */
+  uint64_t seed;
+  rt_outline_config outline;
+} rt_render_params;
+
+/* Counters of one render.  Rays are counted the way the reference casts
+ * them: primary (one per camera sample; quincunx casts W*H centre rays and
+ * (W+1)*(H+1) corner rays), reflection (one per recursive ray_color call)
+ * and shadow (one per World::hit issued by a light). */
+typedef struct rt_stats {
+  uint64_t primary_rays;
+  uint64_t reflection_rays;
+  uint64_t shadow_rays;
+  uint64_t reserved[5];
+  double device_ms; /* CUDA-event time of the device pipeline */
+  double total_ms;  /* host wall time of the whole call */
+} rt_stats;
+
+/* ------------------------------------------------------------------ */
+/* Flattened scene description, for hosts that build their own world   */
+/* (the reference's World build, src/renderer.rs:138-317, done by the  */
+/* caller).  All pointers are borrowed during rt_scene_upload only.     */
+/* ------------------------------------------------------------------ */
+
+/* scene::Camera (src/scene.rs:33-46).  kind is the JSON string. */
+typedef struct rt_camera_config {
+  char kind[32];
+  double position[3];
+  double target[3];
+  double up[3];
+  double width;
+  double height;
+  int32_t has_fov;
+  int32_t has_grid_pitch;
+  int32_t has_grid_thickness;
+  int32_t grid_color_state; /* 0 absent, 1 parsed, 2 unparsable (render error) */
+  double fov;
+  double grid_pitch;
+  double grid_thickness;
+  double grid_color[3];
+} rt_camera_config;
+
+/* scene::Material (src/scene.rs:66-89) with its colours already parsed the
+ * way phong_lighting/apply_texture parse them (src/lighting.rs:9-54,
+ * 229-248). */
+typedef struct rt_material_desc {
+  double color[3];
+  double ambient, diffuse, specular, shininess;
+  int32_t has_reflectivity;
+  int32_t texture; /* 0 none, 1 grid, 2 checkerboard */
+  double reflectivity;
+  double grid_line_color[3]; /* hex_to_color(line_color).unwrap_or(black) */
+  double grid_line_width;
+  double grid_cell_size;
+  double checker_color[3]; /* material_b colour, unwrap_or(white) */
+  double checker_ambient, checker_diffuse, checker_specular, checker_shininess;
+} rt_material_desc;
+
+typedef enum rt_object_kind {
+  RT_OBJ_SPHERE = 0,
+  RT_OBJ_PLANE = 1,
+  RT_OBJ_CUBE = 2,
+  RT_OBJ_MESH = 3
+} rt_object_kind;
+
+/* One World entry in scene order (src/ray.rs:683-712), primitives already
+ * transformed as src/renderer.rs:141-310 does. */
+typedef struct rt_object_desc {
+  int32_t kind;          /* rt_object_kind */
+  int32_t material;      /* material index (the object's scene index) */
+  double a[3];           /* sphere/cube centre, plane point */
+  double b[3];           /* plane normal (normalised), cube size */
+  double radius;         /* sphere radius (after max column scale) */
+  int32_t has_transform; /* cube: transform[] holds its matrix */
+  int32_t mesh;          /* mesh: index into rt_scene_desc.meshes */
+  double transform[16];  /* cube local-to-world matrix, row-major */
+} rt_object_desc;
+
+/* KdNode (src/mesh.rs:41-55) in preorder; the left child of an internal
+ * node is the next node. */
+typedef struct rt_kd_node_desc {
+  int32_t axis;  /* 0..2 internal node, -1 leaf */
+  int32_t right; /* internal: index of the right child */
+  int32_t first; /* leaf: first entry in tri_index */
+  int32_t count; /* leaf: number of entries */
+  double split;
+  double bounds_min[3];
+  double bounds_max[3];
+} rt_kd_node_desc;
+
+/* Mesh (src/mesh.rs:730-1050) after its transform, with its k-d tree. */
+typedef struct rt_mesh_desc {
+  const double* vertices; /* 9 doubles per triangle: v0, v1, v2 */
+  int64_t n_triangles;
+  double bounds_min[3];
+  double bounds_max[3];
+  const rt_kd_node_desc* nodes; /* may be NULL when the mesh is empty */
+  int64_t n_nodes;
+  const int32_t* tri_index; /* leaf triangle lists, leaf order */
+  int64_t n_tri_index;
+} rt_mesh_desc;
+
+/* scene::Light (src/scene.rs:347-353), colour parsed unwrap_or(white). */
+typedef struct rt_light_desc {
+  double position[3];
+  double color[3];
+  double intensity;
+  int32_t has_diameter;
+  int32_t pad;
+  double diameter;
+} rt_light_desc;
+
+typedef struct rt_scene_desc {
+  rt_camera_config camera;
+  const rt_object_desc* objects;
+  int32_t n_objects;
+  int32_t n_materials;
+  const rt_material_desc* materials;
+  const rt_light_desc* lights;
+  int32_t n_lights;
+  int32_t n_meshes;
+  const rt_mesh_desc* meshes;
+  double ambient_color[3]; /* unwrap_or(white) */
+  double ambient_intensity;
+  int32_t has_fog;
+  int32_t has_outline; /* scene_settings.outline present and enabled */
+  double fog_color[3]; /* unwrap_or(0.5 grey) */
+  double fog_density, fog_start, fog_end;
+  double background[3];
+  rt_outline_config outline; /* Scene::get_outline_config (src/scene.rs:515-534) */
+  /* First error Renderer::render would raise while building its world
+   * (an unparsable material or background colour), or NULL. */
+  const char* render_error;
+} rt_scene_desc;
+
+/* ------------------------------------------------------------------ */
+/* Entry points                                                         */
+/* ------------------------------------------------------------------ */
+
+/* Creates a context on CUDA device `device`. */
+rt_status rt_ctx_create(int device, rt_ctx** out);
+void rt_ctx_destroy(rt_ctx* ctx);
+/* Message of the last failure on ctx ("" if none).  Valid until the next
+ * call on ctx.  rt_last_error(NULL) reports failures of rt_ctx_create. */
+const char* rt_last_error(const rt_ctx* ctx);
+
+/* Scene::from_json_file (src/scene.rs:462-470): parse, load STL meshes
+ * relative to the file's directory, transform, build k-d trees, upload. */
+rt_status rt_scene_load_json_file(rt_ctx* ctx, const char* path, rt_scene** out);
+/* Scene::from_json_str (src/scene.rs:473-480): meshes relative to ".". */
+rt_status rt_scene_load_json_str(rt_ctx* ctx, const char* json, rt_scene** out);
+/* Uploads a world the caller flattened itself. */
+rt_status rt_scene_upload(rt_ctx* ctx, const rt_scene_desc* desc, rt_scene** out);
+/* Scene::get_outline_config (src/scene.rs:515-534) of a loaded scene;
+ * *enabled = 0 when the scene has none. */
+rt_status rt_scene_outline_config(rt_ctx* ctx, const rt_scene* scene, rt_outline_config* out);
+/* Camera aspect (camera.width / camera.height) used by the CLI and the
+ * Node bindings to size images from a diagonal (cli/src/main.rs:339-350). */
+rt_status rt_scene_camera_aspect(rt_ctx* ctx, const rt_scene* scene, double* out);
+void rt_scene_free(rt_scene* scene);
+
+/* Renderer::render (src/renderer.rs:120-382).  rgb_out receives
+ * width*height*3 bytes, row-major, top row first.  out_on_device != 0 means
+ * rgb_out is a device pointer on the context's device.  stats may be NULL. */
+rt_status rt_render(rt_ctx* ctx, const rt_scene* scene, const rt_render_params* params, uint8_t* rgb_out,
+                    int out_on_device, rt_stats* stats);
+
+/* Same as rt_render but also returns the pre-quantisation colours
+ * (width*height*3 doubles, host memory).  Used by parity tests. */
+rt_status rt_render_linear(rt_ctx* ctx, const rt_scene* scene, const rt_render_params* params, uint8_t* rgb_out,
+                           double* linear_out, rt_stats* stats);
+
+/* ------------------------------------------------------------------ */
+/* Device unit entry points used by the parity tests                   */
+/* ------------------------------------------------------------------ */
+
+/* The first n_words u32 outputs of rand's StdRng::seed_from_u64(seed[i])
+ * (rand 0.8 / rand_chacha 0.3 ChaCha12, rand_core 0.6 PCG32 seeding) for
+ * each of n seeds, generated on the device.  out: n * n_words, host. */
+rt_status rt_debug_stdrng_u32(rt_ctx* ctx, const uint64_t* seeds, int64_t n, int32_t n_words, uint32_t* out);
+/* The 16 (dx, dy) disk offsets of one area-light shading point
+ * (src/lighting.rs:57-66, 170-173) for each light seed; out: n * 32. */
+rt_status rt_debug_disk_offsets(rt_ctx* ctx, const uint64_t* light_seeds, int64_t n, double radius, double* out);
+/* MeshObject::hit (src/ray.rs:614-675) of mesh `mesh_object` of a loaded
+ * scene for n rays (6 doubles each: origin, direction).  out: 8 doubles per
+ * ray [hit, t, point xyz, normal xyz]. */
+rt_status rt_debug_mesh_hit(rt_ctx* ctx, const rt_scene* scene, int32_t object_index, int32_t use_kdtree,
+                            const double* rays, int64_t n, double t_min, double t_max, double* out);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* RTRACE_GPU_H */

@@ -1,0 +1,292 @@
+"""B200 render path for SeaRyanC/rtrace scenes.
+
+The Python surface mirrors the reference crate's public API
+(src/lib.rs re-exports): ``Scene.from_json_file`` / ``Scene.from_json_str``
+(src/scene.rs:462-480), ``Renderer`` with its fields and constructors
+(src/renderer.rs:37-118), ``AntiAliasingMode`` (src/renderer.rs:16-24),
+``OutlineConfig`` (src/outline.rs:5-31) and ``Renderer.render`` /
+``Renderer.render_to_file`` (src/renderer.rs:120, 914).  Rendering runs on
+the GPU through the C ABI in include/rtrace_gpu.h; there is no CPU path.
+Errors the reference returns as ``Err(String)`` raise ``RenderError`` /
+``SceneError`` with the reference's message.
+"""
+import ctypes
+import enum
+import threading
+from dataclasses import dataclass, field
+
+import numpy as np
+
+from . import _capi
+
+__all__ = [
+    "AntiAliasingMode", "OutlineConfig", "Scene", "Renderer", "RtraceError", "SceneError",
+    "RenderError", "DeviceError", "Context", "RenderStats", "default_context", "write_png",
+]
+
+
+class RtraceError(Exception):
+    """Base class; ``status`` is the rt_status code."""
+
+    def __init__(self, status, message):
+        super().__init__(message)
+        self.status = status
+
+
+class SceneError(RtraceError):
+    """Scene::from_json_* failures (JSON, STL, I/O)."""
+
+
+class RenderError(RtraceError):
+    """Errors Renderer::render returns (samples, camera, colours, ranges)."""
+
+
+class DeviceError(RtraceError):
+    """CUDA, memory or device-watchdog failures."""
+
+
+def _raise(status, ctx_handle):
+    msg = _capi.lib().rt_last_error(ctx_handle)
+    msg = msg.decode("utf-8", "replace") if msg else _capi.STATUS_NAMES.get(status, str(status))
+    if status in (_capi.RT_ERR_SCENE, _capi.RT_ERR_IO):
+        raise SceneError(status, msg)
+    if status == _capi.RT_ERR_RENDER:
+        raise RenderError(status, msg)
+    if status == _capi.RT_ERR_INVALID_ARGUMENT:
+        raise ValueError(msg)
+    raise DeviceError(status, msg)
+
+
+class AntiAliasingMode(enum.IntEnum):
+    """src/renderer.rs:16-24"""
+    NoJitter = 0
+    Quincunx = 1
+    Stochastic = 2
+
+
+@dataclass
+class OutlineConfig:
+    """src/outline.rs:5-31 (defaults from OutlineConfig::default)."""
+    depth_weight: float = 1.0
+    normal_weight: float = 1.0
+    threshold: float = 0.1
+    edge_color: tuple = (0.0, 0.0, 0.0)
+    use_8_neighbors: bool = False
+    line_thickness: float = 1.0
+
+
+@dataclass
+class RenderStats:
+    primary_rays: int = 0
+    reflection_rays: int = 0
+    shadow_rays: int = 0
+    device_ms: float = 0.0
+    total_ms: float = 0.0
+
+    @property
+    def rays(self):
+        return self.primary_rays + self.reflection_rays + self.shadow_rays
+
+
+class Context:
+    """One CUDA device and stream (rt_ctx).  Not shared between threads."""
+
+    def __init__(self, device=0):
+        L = _capi.lib()
+        h = ctypes.c_void_p()
+        st = L.rt_ctx_create(int(device), ctypes.byref(h))
+        if st != _capi.RT_OK:
+            _raise(st, None)
+        self.handle = h
+        self.device = device
+
+    def close(self):
+        if self.handle:
+            _capi.lib().rt_ctx_destroy(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+_tls = threading.local()
+
+
+def default_context(device=0):
+    """The calling thread's context for `device` (created on first use)."""
+    ctxs = getattr(_tls, "ctxs", None)
+    if ctxs is None:
+        ctxs = _tls.ctxs = {}
+    if device not in ctxs:
+        ctxs[device] = Context(device)
+    return ctxs[device]
+
+
+class Scene:
+    """A scene uploaded to the device (rt_scene)."""
+
+    def __init__(self, handle, ctx):
+        self._handle = handle
+        self._ctx = ctx
+
+    @classmethod
+    def from_json_file(cls, path, ctx=None):
+        """Scene::from_json_file: meshes resolve against the file's directory."""
+        ctx = ctx or default_context()
+        h = ctypes.c_void_p()
+        st = _capi.lib().rt_scene_load_json_file(ctx.handle, str(path).encode(), ctypes.byref(h))
+        if st != _capi.RT_OK:
+            _raise(st, ctx.handle)
+        return cls(h, ctx)
+
+    @classmethod
+    def from_json_str(cls, text, ctx=None):
+        """Scene::from_json_str: meshes resolve against the current directory."""
+        ctx = ctx or default_context()
+        h = ctypes.c_void_p()
+        st = _capi.lib().rt_scene_load_json_str(ctx.handle, text.encode(), ctypes.byref(h))
+        if st != _capi.RT_OK:
+            _raise(st, ctx.handle)
+        return cls(h, ctx)
+
+    def get_outline_config(self):
+        """Scene::get_outline_config (src/scene.rs:515-534): None or OutlineConfig."""
+        oc = _capi.rt_outline_config()
+        st = _capi.lib().rt_scene_outline_config(self._ctx.handle, self._handle, ctypes.byref(oc))
+        if st != _capi.RT_OK:
+            _raise(st, self._ctx.handle)
+        if not oc.enabled:
+            return None
+        return OutlineConfig(oc.depth_weight, oc.normal_weight, oc.threshold, tuple(oc.edge_color),
+                             bool(oc.use_8_neighbors), oc.line_thickness)
+
+    @property
+    def camera_aspect(self):
+        v = ctypes.c_double()
+        st = _capi.lib().rt_scene_camera_aspect(self._ctx.handle, self._handle, ctypes.byref(v))
+        if st != _capi.RT_OK:
+            _raise(st, self._ctx.handle)
+        return v.value
+
+    def close(self):
+        if self._handle:
+            _capi.lib().rt_scene_free(self._handle)
+            self._handle = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class Renderer:
+    """src/renderer.rs:37-118.  thread_count is accepted and ignored."""
+
+    def __init__(self, width, height):
+        self.width = int(width)
+        self.height = int(height)
+        self.max_depth = 10
+        self.use_kdtree = True
+        self.thread_count = None
+        self.samples = 1
+        self.anti_aliasing_mode = AntiAliasingMode.Quincunx
+        self.seed = 0
+        self.outline_config = None
+        self.last_stats = RenderStats()
+
+    @classmethod
+    def new(cls, width, height):
+        return cls(width, height)
+
+    @classmethod
+    def new_brute_force(cls, width, height):
+        r = cls(width, height)
+        r.use_kdtree = False
+        return r
+
+    @classmethod
+    def new_with_threads(cls, width, height, thread_count):
+        r = cls(width, height)
+        r.thread_count = thread_count
+        return r
+
+    @classmethod
+    def new_with_options(cls, width, height, use_kdtree, thread_count):
+        r = cls(width, height)
+        r.use_kdtree = bool(use_kdtree)
+        r.thread_count = thread_count
+        return r
+
+    def with_outline_detection(self, config):
+        self.outline_config = config
+        return self
+
+    def _params(self):
+        p = _capi.rt_render_params()
+        p.width = self.width
+        p.height = self.height
+        p.max_depth = int(self.max_depth)
+        p.use_kdtree = 1 if self.use_kdtree else 0
+        p.samples = int(self.samples)
+        p.anti_aliasing_mode = int(self.anti_aliasing_mode)
+        p.seed = int(self.seed or 0) & 0xFFFFFFFFFFFFFFFF
+        oc = self.outline_config
+        if oc is not None:
+            p.outline.enabled = 1
+            p.outline.use_8_neighbors = 1 if oc.use_8_neighbors else 0
+            p.outline.depth_weight = oc.depth_weight
+            p.outline.normal_weight = oc.normal_weight
+            p.outline.threshold = oc.threshold
+            for k in range(3):
+                p.outline.edge_color[k] = oc.edge_color[k]
+            p.outline.line_thickness = oc.line_thickness
+        return p
+
+    def render(self, scene, out=None, linear=False):
+        """Renderer::render: returns an (height, width, 3) uint8 array.
+
+        With linear=True also returns the float64 colours before
+        quantisation (parity tests)."""
+        p = self._params()
+        img = out if out is not None else np.empty((self.height, self.width, 3), np.uint8)
+        st = _capi.rt_stats()
+        L = _capi.lib()
+        ctxh = scene._ctx.handle
+        if linear:
+            lin = np.empty((self.height, self.width, 3), np.float64)
+            code = L.rt_render_linear(ctxh, scene._handle, ctypes.byref(p), img.ctypes.data, lin.ctypes.data,
+                                      ctypes.byref(st))
+        else:
+            code = L.rt_render(ctxh, scene._handle, ctypes.byref(p), img.ctypes.data, 0, ctypes.byref(st))
+        if code != _capi.RT_OK:
+            _raise(code, ctxh)
+        self.last_stats = RenderStats(st.primary_rays, st.reflection_rays, st.shadow_rays, st.device_ms,
+                                      st.total_ms)
+        return (img, lin) if linear else img
+
+    def render_to_file(self, scene, output_path):
+        """Renderer::render_to_file: renders and writes a PNG."""
+        write_png(output_path, self.render(scene))
+
+
+def write_png(path, img):
+    """Writes an (H, W, 3) uint8 array as an 8-bit RGB PNG."""
+    import struct
+    import zlib
+    img = np.ascontiguousarray(img, dtype=np.uint8)
+    h, w, _ = img.shape
+    raw = np.zeros((h, 1 + 3 * w), np.uint8)
+    raw[:, 1:] = img.reshape(h, 3 * w)
+
+    def chunk(tag, data):
+        c = struct.pack(">I", len(data)) + tag + data
+        return c + struct.pack(">I", zlib.crc32(tag + data) & 0xFFFFFFFF)
+
+    png = b"\x89PNG\r\n\x1a\n" + chunk(b"IHDR", struct.pack(">IIBBBBB", w, h, 8, 2, 0, 0, 0))
+    png += chunk(b"IDAT", zlib.compress(raw.tobytes(), 6)) + chunk(b"IEND", b"")
+    with open(path, "wb") as f:
+        f.write(png)

@@ -1,0 +1,107 @@
+"""ctypes bindings of include/rtrace_gpu.h.
+
+The library is the in-tree ``rtrace_b200/_lib/librtrace_b200.so``; importing
+this module fails loudly when it is missing (there is no CPU fallback).
+"""
+import ctypes
+import os
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, "_lib", "librtrace_b200.so")
+
+RT_OK = 0
+RT_ERR_INVALID_ARGUMENT = 1
+RT_ERR_SCENE = 2
+RT_ERR_RENDER = 3
+RT_ERR_CUDA = 4
+RT_ERR_OUT_OF_MEMORY = 5
+RT_ERR_DEVICE_WATCHDOG = 6
+RT_ERR_IO = 7
+
+STATUS_NAMES = {
+    RT_OK: "RT_OK",
+    RT_ERR_INVALID_ARGUMENT: "RT_ERR_INVALID_ARGUMENT",
+    RT_ERR_SCENE: "RT_ERR_SCENE",
+    RT_ERR_RENDER: "RT_ERR_RENDER",
+    RT_ERR_CUDA: "RT_ERR_CUDA",
+    RT_ERR_OUT_OF_MEMORY: "RT_ERR_OUT_OF_MEMORY",
+    RT_ERR_DEVICE_WATCHDOG: "RT_ERR_DEVICE_WATCHDOG",
+    RT_ERR_IO: "RT_ERR_IO",
+}
+
+
+class rt_outline_config(ctypes.Structure):
+    _fields_ = [
+        ("enabled", ctypes.c_int32),
+        ("use_8_neighbors", ctypes.c_int32),
+        ("depth_weight", ctypes.c_double),
+        ("normal_weight", ctypes.c_double),
+        ("threshold", ctypes.c_double),
+        ("edge_color", ctypes.c_double * 3),
+        ("line_thickness", ctypes.c_double),
+    ]
+
+
+class rt_render_params(ctypes.Structure):
+    _fields_ = [
+        ("width", ctypes.c_uint32),
+        ("height", ctypes.c_uint32),
+        ("max_depth", ctypes.c_int32),
+        ("use_kdtree", ctypes.c_int32),
+        ("samples", ctypes.c_uint32),
+        ("anti_aliasing_mode", ctypes.c_int32),
+        ("seed", ctypes.c_uint64),
+        ("outline", rt_outline_config),
+    ]
+
+
+class rt_stats(ctypes.Structure):
+    _fields_ = [
+        ("primary_rays", ctypes.c_uint64),
+        ("reflection_rays", ctypes.c_uint64),
+        ("shadow_rays", ctypes.c_uint64),
+        ("reserved", ctypes.c_uint64 * 5),
+        ("device_ms", ctypes.c_double),
+        ("total_ms", ctypes.c_double),
+    ]
+
+
+_vp = ctypes.c_void_p
+_lib = None
+
+
+def lib():
+    """Loads the CUDA library (once); raises if it has not been built."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(LIB_PATH):
+        raise ImportError(
+            "rtrace_b200 CUDA library not found at %s; build it with "
+            "`python -m rtrace_b200.build` (nvcc, sm_100a)" % LIB_PATH)
+    L = ctypes.CDLL(LIB_PATH)
+    sig = {
+        "rt_ctx_create": (ctypes.c_int, [ctypes.c_int, ctypes.POINTER(_vp)]),
+        "rt_ctx_destroy": (None, [_vp]),
+        "rt_last_error": (ctypes.c_char_p, [_vp]),
+        "rt_scene_load_json_file": (ctypes.c_int, [_vp, ctypes.c_char_p, ctypes.POINTER(_vp)]),
+        "rt_scene_load_json_str": (ctypes.c_int, [_vp, ctypes.c_char_p, ctypes.POINTER(_vp)]),
+        "rt_scene_upload": (ctypes.c_int, [_vp, _vp, ctypes.POINTER(_vp)]),
+        "rt_scene_outline_config": (ctypes.c_int, [_vp, _vp, ctypes.POINTER(rt_outline_config)]),
+        "rt_scene_camera_aspect": (ctypes.c_int, [_vp, _vp, ctypes.POINTER(ctypes.c_double)]),
+        "rt_scene_free": (None, [_vp]),
+        "rt_render": (ctypes.c_int, [_vp, _vp, ctypes.POINTER(rt_render_params), _vp, ctypes.c_int,
+                                     ctypes.POINTER(rt_stats)]),
+        "rt_render_linear": (ctypes.c_int, [_vp, _vp, ctypes.POINTER(rt_render_params), _vp, _vp,
+                                            ctypes.POINTER(rt_stats)]),
+        "rt_debug_stdrng_u32": (ctypes.c_int, [_vp, _vp, ctypes.c_int64, ctypes.c_int32, _vp]),
+        "rt_debug_disk_offsets": (ctypes.c_int, [_vp, _vp, ctypes.c_int64, ctypes.c_double, _vp]),
+        "rt_debug_mesh_hit": (ctypes.c_int, [_vp, _vp, ctypes.c_int32, ctypes.c_int32, _vp, ctypes.c_int64,
+                                             ctypes.c_double, ctypes.c_double, _vp]),
+    }
+    for name, (res, args) in sig.items():
+        f = getattr(L, name)
+        f.restype = res
+        f.argtypes = args
+    _lib = L
+    return L

@@ -1,0 +1,161 @@
+"""Parity of the CUDA render path with the reference (golden renders) and
+with the CPU oracle, through the C ABI.  Integer/byte outputs (RNG words,
+RGB8 pixels) must be bit-exact, and so must the traversal's t / point /
+normal (pure + - * / sqrt, which the device rounds exactly like the
+reference's CPU code).  The double-precision colours before quantisation
+may differ in the last bits where the reference calls a transcendental
+function: CUDA's pow/exp/sin/cos are within 2 ulp of glibc's, so those are
+compared with a relative tolerance of LINEAR_RTOL."""
+import hashlib
+import json
+import os
+
+import numpy as np
+import pytest
+
+import rtrace_b200 as rt
+from rtrace_b200 import workloads
+from tests import oracle_lib
+
+pytestmark = pytest.mark.gpu
+
+LINEAR_RTOL = 1e-13  # a few ulp of a colour channel in [0, 1]
+
+GOLD = json.load(open(os.path.join(oracle_lib.GOLDEN, "images.json")))
+AA = {"no-jitter": rt.AntiAliasingMode.NoJitter, "quincunx": rt.AntiAliasingMode.Quincunx,
+      "stochastic": rt.AntiAliasingMode.Stochastic}
+
+
+def gpu_render(scene_path, w, h, aa="quincunx", samples=1, outline=False, max_depth=10, seed=0, use_kdtree=True,
+               linear=False):
+    sc = rt.Scene.from_json_file(scene_path)
+    r = rt.Renderer(w, h)
+    r.anti_aliasing_mode = AA[aa]
+    r.samples = samples
+    r.max_depth = max_depth
+    r.seed = seed
+    r.use_kdtree = use_kdtree
+    if outline:
+        r.outline_config = sc.get_outline_config()
+    out = r.render(sc, linear=linear)
+    return out, r.last_stats
+
+
+@pytest.mark.parametrize("case", GOLD, ids=[c["image"] for c in GOLD])
+def test_gpu_matches_reference_render(gpu_ctx, case):
+    img, _ = gpu_render(os.path.join(oracle_lib.SCENES, case["scene"]), case["width"], case["height"],
+                        case["anti_aliasing"], case["samples"], case["outline"])
+    if hashlib.sha256(img.tobytes()).hexdigest() != case["sha256_rgb"]:
+        ref = oracle_lib.render(os.path.join(oracle_lib.SCENES, case["scene"]), width=case["width"],
+                                height=case["height"], aa=case["anti_aliasing"], samples=case["samples"],
+                                outline=case["outline"])
+        d = np.abs(img.astype(int) - ref.astype(int)).max(2)
+        pytest.fail("differs from the reference render: %d pixels, max %d" % ((d > 0).sum(), d.max()))
+
+
+def test_device_stdrng_words(gpu_ctx):
+    import ctypes
+    rng = np.random.default_rng(3)
+    seeds = np.concatenate([np.array([0, 1, 42, 2 ** 64 - 1], np.uint64),
+                            rng.integers(0, 2 ** 63, 500, dtype=np.uint64)])
+    out = np.zeros((len(seeds), 150), np.uint32)
+    st = rt._capi.lib().rt_debug_stdrng_u32(gpu_ctx.handle, seeds.ctypes.data, len(seeds), 150, out.ctypes.data)
+    assert st == 0
+    for i, s in enumerate(seeds):
+        assert np.array_equal(out[i], oracle_lib.stdrng_u32(int(s), 150)), int(s)
+
+
+@pytest.mark.parametrize("radius", [1.0, 0.37, 12.5])
+def test_device_disk_samples(gpu_ctx, radius):
+    rng = np.random.default_rng(5)
+    seeds = rng.integers(0, 2 ** 63, 400, dtype=np.uint64)
+    out = np.zeros((len(seeds), 32), np.float64)
+    st = rt._capi.lib().rt_debug_disk_offsets(gpu_ctx.handle, seeds.ctypes.data, len(seeds), radius, out.ctypes.data)
+    assert st == 0
+    for i, s in enumerate(seeds):
+        assert np.array_equal(out[i], oracle_lib.disk_offsets(int(s), radius))
+
+
+@pytest.mark.parametrize("use_kd", [True, False])
+def test_kd_traversal_matches_oracle(gpu_ctx, tmp_path, use_kd):
+    from tests.kd_rays import plus_rays
+    stl = os.path.join(oracle_lib.SCENES, "plus.stl")
+    scene = {"camera": {"kind": "ortho", "position": [0, -5, 0], "target": [0, 0, 0], "up": [0, 0, 1],
+                        "width": 1, "height": 1},
+             "objects": [{"kind": "mesh", "filename": stl, "material": {"color": "#FFFFFF", "ambient": 0.1,
+                                                                       "diffuse": 0.7, "specular": 0.3,
+                                                                       "shininess": 32}}],
+             "lights": [], "scene_settings": {"ambient_illumination": {"color": "#FFFFFF", "intensity": 0.1}}}
+    sc = rt.Scene.from_json_str(json.dumps(scene))
+    rays = plus_rays(stl, extra_random=3000)
+    out = np.zeros((len(rays), 8))
+    st = rt._capi.lib().rt_debug_mesh_hit(gpu_ctx.handle, sc._handle, 0, 1 if use_kd else 0, rays.ctypes.data,
+                                          len(rays), 0.001, float("inf"), out.ctypes.data)
+    assert st == 0
+    ref = oracle_lib.mesh_hit(stl, rays, use_kdtree=use_kd)
+    assert np.array_equal(out, ref)
+
+
+def _synthetic_scenes(tmp):
+    d = str(tmp)
+    paths = {"sphere_grid": workloads.write_scene(d, "sphere_grid.json", workloads.sphere_grid_scene()),
+             "icosphere": workloads.make_noisy_icosphere(d, level=3, seed=5),
+             "rings": workloads.write_scene(d, "rings.json", workloads.ring_spheres_scene(seed=1, n_rings=3,
+                                                                                         per_ring=15))}
+    # area light + reflections + cube + checkerboard + transforms
+    s = json.load(open(os.path.join(oracle_lib.SCENES, "checkerboard-advanced.json")))
+    s["lights"].append({"position": [1, -2, 4], "color": "#FFEEDD", "intensity": 0.7, "diameter": 1.5})
+    s["objects"].append({"kind": "cube", "center": [1, 1, 0.5], "size": [1, 2, 0.5],
+                         "transform": ["rotate(10, 20, 30)", "scale(1, 2, 1)", "translate(0.5, 0, 0)"],
+                         "material": {"color": "#33AA77", "ambient": 0.1, "diffuse": 0.7, "specular": 0.3,
+                                      "shininess": 16, "reflectivity": 0.4}})
+    paths["mixed"] = workloads.write_scene(d, "mixed.json", s)
+    return paths
+
+
+@pytest.mark.parametrize("aa,samples", [("quincunx", 1), ("no-jitter", 1), ("no-jitter", 3), ("stochastic", 1),
+                                        ("stochastic", 4)])
+def test_modes_match_oracle(gpu_ctx, tmp_path, aa, samples):
+    for name, path in _synthetic_scenes(tmp_path).items():
+        outline = name == "icosphere" and aa != "quincunx"
+        (img, lin), st = gpu_render(path, 71, 43, aa, samples, outline=outline, linear=True)
+        ref, rlin, cnt = oracle_lib.render(path, width=71, height=43, aa=aa, samples=samples, outline=outline,
+                                           linear=True, counts=True)
+        assert np.array_equal(img, ref), (name, int((img != ref).any(2).sum()))
+        assert np.allclose(lin, rlin, rtol=LINEAR_RTOL, atol=1e-15), (name, float(np.abs(lin - rlin).max()))
+        assert (st.primary_rays, st.reflection_rays, st.shadow_rays) == (int(cnt[0]), int(cnt[1]), int(cnt[2])), name
+
+
+def test_brute_force_and_seed(gpu_ctx, tmp_path):
+    path = _synthetic_scenes(tmp_path)["icosphere"]
+    for kd in (True, False):
+        img, _ = gpu_render(path, 40, 30, "stochastic", 2, seed=12345, use_kdtree=kd)
+        ref = oracle_lib.render(path, width=40, height=30, aa="stochastic", samples=2, seed=12345, use_kdtree=kd)
+        assert np.array_equal(img, ref)
+
+
+def test_depth_limits(gpu_ctx, tmp_path):
+    path = _synthetic_scenes(tmp_path)["mixed"]
+    for depth in (0, 1, 2, 3):
+        img, _ = gpu_render(path, 33, 21, "no-jitter", 1, max_depth=depth)
+        ref = oracle_lib.render(path, width=33, height=21, aa="no-jitter", max_depth=depth)
+        assert np.array_equal(img, ref), depth
+
+
+def test_render_errors(gpu_ctx):
+    scene = json.load(open(os.path.join(oracle_lib.SCENES, "object-sphere.json")))
+    sc = rt.Scene.from_json_str(json.dumps(scene))
+    r = rt.Renderer(10, 10)
+    r.samples = 0
+    with pytest.raises(rt.RenderError, match="Samples must be greater than 0"):
+        r.render(sc)
+    for mut, msg in [(lambda s: s["camera"].__setitem__("kind", "fisheye"), "Unsupported camera type: fisheye"),
+                     (lambda s: s["camera"].update(kind="perspective", fov=0), "Field of view"),
+                     (lambda s: s["objects"][0]["material"].__setitem__("color", "#12345"), "Invalid hex color"),
+                     (lambda s: s["lights"][0].__setitem__("diameter", 0.0), "cannot sample empty range")]:
+        s2 = json.loads(json.dumps(scene))
+        mut(s2)
+        with pytest.raises(rt.RenderError, match=msg):
+            rt.Renderer(10, 10).render(rt.Scene.from_json_str(json.dumps(s2)))
+    with pytest.raises(rt.SceneError):
+        rt.Scene.from_json_str("{\"camera\": 3}")
