@@ -1,0 +1,344 @@
+"""Throughput of the B200 render path on the mesh workload at 1080p.
+
+Workload (one step = one render of one frame): the noisy-icosphere mesh
+scene (level-6 icosphere, 81,920 triangles, f32 vertices displaced +-5% by
+seeded value noise; reflective grid plane; one disk light of diameter 2,
+16 samples per shading point; fog start 5 / end 50 / density 0.05; outline
+on; 50-degree perspective camera) at 1920x1080, max depth 10, seed 0.  The
+scene enables outlines, so anti-aliasing is no-jitter, which is the mode the
+reference CLI switches to for outlined scenes (cli/src/main.rs:364-376).
+
+Metric: Mrays/s, counting every ray the reference would cast (primary +
+reflection + shadow), and ms per frame.  `value` is the device-timed
+pipeline with the scene resident; `e2e` is the same metric through the
+public API with host buffers: each step uploads the host-side scene, renders
+into pinned host memory and frees the device scene.
+
+N > 1 GPUs: one process per GPU, each rendering its own copy of the frame
+(replicas, weak scaling); no collective touches the data path.
+
+--impl reference times the CPU restatement of the reference (oracle/,
+std::thread over pixels like the reference's rayon loop) on this host's
+cores, on bounded row bands of the same frame.
+"""
+import argparse
+import ctypes
+import json
+import math
+import os
+import signal
+import subprocess
+import sys
+import tempfile
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "Mrays/s & ms/frame at 1080p, learned vs plain shadows at ≥40 dB PSNR, 1 B200"
+W, H = 1920, 1080
+WORKLOAD = "noisy_icosphere_l6_1080p"
+PEAKS = os.path.join(ROOT, "MEASURED_PEAKS.json")
+TRAFFIC_FILE = os.path.join(ROOT, "profiles", "k_shadow_noisy_icosphere_1080p.md")
+
+# Algorithmic bytes per unit of work of the any-hit (shadow) kernel: every
+# shadow ray reads its direction and distance (32 B) and its hit's origin
+# (24 B) and writes one visibility byte; each BVH node visit reads one node
+# (112 B), each triangle test one triangle record (80 B), each sphere test
+# one sphere (40 B), each verification unit one 16-byte k-d record.
+B_RAY, B_NODE, B_TRI, B_SPH, B_VERIFY = 57, 112, 80, 40, 16
+# FP64 operations per unit (adds, multiplies, divisions and square roots of
+# the restated reference formulas): box pair 36, Moller-Trumbore 40,
+# sphere test 22, verification unit 2.
+F_NODE, F_TRI, F_SPH, F_VERIFY = 36, 40, 22, 2
+
+
+def env_int(name, default):
+    try:
+        return int(os.environ.get(name, default))
+    except ValueError:
+        return default
+
+
+def make_workload(directory):
+    from rtrace_b200 import workloads
+    return workloads.make_noisy_icosphere(directory, level=6, seed=7, outline=True)
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled every 200 ms."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index):
+        self.path = tempfile.mktemp(prefix="rtb_clocks_", suffix=".csv")
+        self.proc = None
+        try:
+            self.fh = open(self.path, "w")
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(gpu_index), "--query-gpu=" + self.FIELDS, "--format=csv,noheader,nounits",
+                 "-lms", "200"], stdout=self.fh, stderr=subprocess.DEVNULL)
+        except (OSError, FileNotFoundError):
+            self.proc = None
+
+    def stop(self):
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.send_signal(signal.SIGTERM)
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        self.fh.close()
+        sm, smax, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in open(self.path):
+            parts = [p.strip() for p in line.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                smax = float(parts[2])
+            except ValueError:
+                continue
+            for n, v in zip(names, parts[5:9]):
+                if v.lower().startswith("active"):
+                    reasons.add(n)
+        os.unlink(self.path)
+        sm.sort()
+        return {"sm_mhz": sm[len(sm) // 2] if sm else None, "sm_max_mhz": smax, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def read_traffic():
+    """Per-launch DRAM bytes of the shadow kernel from the committed ncu summary."""
+    try:
+        for line in open(TRAFFIC_FILE):
+            if line.startswith("traffic_bytes_per_frame:"):
+                return float(line.split(":", 1)[1])
+    except OSError:
+        pass
+    return None
+
+
+def cpu_baseline(scene_path, budget_s, threads, kind_outline=True):
+    """Mrays/s of the CPU restatement of the reference on a row band."""
+    from tests import oracle_lib
+    import numpy as np
+    L = oracle_lib.load()
+    err = ctypes.create_string_buffer(512)
+
+    def band(y0, y1):
+        out = np.zeros((H, W, 3), np.uint8)
+        cnt = np.zeros(6, np.uint64)
+        t = time.perf_counter()
+        rc = L.oracle_render_rows(scene_path.encode(), None, W, H, 0, 1, 10, 0, 1, 1 if kind_outline else 0,
+                                  threads, y0, y1, out.ctypes.data, None, cnt.ctypes.data, err, 512)
+        if rc:
+            raise RuntimeError(err.value.decode())
+        return time.perf_counter() - t, int(cnt[0] + cnt[1] + cnt[2])
+
+    mid = H // 2
+    dt, rays = band(mid, mid + 2)  # calibration
+    per_row = max(dt / 2.0, 1e-4)
+    rows = int(max(2, min(H, budget_s / per_row)))
+    y0 = max(0, mid - rows // 2)
+    dt, rays = band(y0, y0 + rows)
+    return {"value": rays / dt / 1e6, "unit": "Mrays/s", "cores": threads, "kind": "port",
+            "sample": "rows %d-%d of the %dx%d frame (%d rays, %.1f s), CPU restatement of the reference, "
+                      "%d threads" % (y0, y0 + rows, W, H, rays, dt, threads),
+            "rays": rays, "seconds": dt}
+
+
+def run_reference(args, rank, world):
+    if rank != 0:
+        return 0
+    d = tempfile.mkdtemp(prefix="rtb_ref_")
+    path = make_workload(d)
+    threads = os.cpu_count() or 1
+    # each step: a row band sized so that warm-up + steps take ~2 minutes
+    per_step = max(2.0, 120.0 / max(1, args.steps + args.warmup))
+    for _ in range(args.warmup):
+        cpu_baseline(path, min(per_step, 5.0), threads)
+    tot_rays, tot_s, samples = 0, 0.0, []
+    for _ in range(args.steps):
+        r = cpu_baseline(path, per_step, threads)
+        tot_rays += r["rays"]
+        tot_s += r["seconds"]
+        samples.append(r["sample"])
+    value = tot_rays / tot_s / 1e6
+    line = {
+        "impl": "reference", "metric": METRIC, "value": value, "unit": "Mrays/s", "n_gpus": args.gpus,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * tot_s / args.steps,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": WORKLOAD, "width": W, "height": H, "anti_aliasing": "no-jitter", "samples": 1,
+                   "max_depth": 10, "outline": True, "step": "row band of the frame, CPU"},
+        "cpu_baseline": {"value": value, "unit": "Mrays/s", "cores": threads, "kind": "port",
+                         "sample": "; ".join(samples[:2]) + ("; ..." if len(samples) > 2 else "")},
+        "e2e": {"value": value, "unit": "Mrays/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def main():
+    ap = argparse.ArgumentParser(description=__doc__.splitlines()[0])
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--cpu-seconds", type=float, default=15.0)
+    args = ap.parse_args()
+    args.warmup = max(3, args.warmup)
+    rank, world, local = env_int("RANK", 0), env_int("WORLD_SIZE", 1), env_int("LOCAL_RANK", 0)
+    if args.impl == "reference":
+        return run_reference(args, rank, world)
+
+    import numpy as np
+    import torch
+    import torch.distributed as dist
+    from datetime import timedelta
+
+    import rtrace_b200 as rt
+    from rtrace_b200 import _capi
+
+    if world > 1:
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=timedelta(seconds=300))
+    dev = torch.device("cuda", local)
+    d = tempfile.mkdtemp(prefix="rtb_bench_%d_" % rank)
+    path = make_workload(d)
+
+    ctx = rt.Context(local)
+    scene = rt.Scene.from_json_file(path, ctx)
+    r = rt.Renderer(W, H)
+    r.anti_aliasing_mode = rt.AntiAliasingMode.NoJitter
+    r.outline_config = scene.get_outline_config()
+    out = torch.empty(W * H * 3, dtype=torch.uint8, device=dev)
+    flush = torch.empty(512 * 1024 * 1024, dtype=torch.uint8, device=dev)  # > L2 (126 MB)
+
+    for _ in range(args.warmup):
+        r.render(scene, device_ptr=out.data_ptr())
+    # profiling render (not timed): stage times and work counters
+    r.flags = _capi.RT_FLAG_STAGE_TIMES | _capi.RT_FLAG_COUNT_WORK
+    r.render(scene, device_ptr=out.data_ptr())
+    prof = r.last_stats
+    r.flags = 0
+
+    clocks = ClockSampler(local)
+    if world > 1:
+        dist.barrier()
+    torch.cuda.synchronize(dev)
+    dev_ms, rays, launches = 0.0, 0, 0
+    wall0 = time.perf_counter()
+    for _ in range(args.steps):
+        flush.zero_()
+        torch.cuda.synchronize(dev)
+        r.render(scene, device_ptr=out.data_ptr())
+        st = r.last_stats
+        dev_ms += st.device_ms
+        rays += st.rays
+        launches += st.kernel_launches
+    torch.cuda.synchronize(dev)
+    if world > 1:
+        dist.barrier()
+    wall_s = time.perf_counter() - wall0
+    clk = clocks.stop()
+
+    # end to end through the public API: upload the host scene, render into
+    # pinned host memory, free
+    host = rt.HostScene.from_json_file(path)
+    pinned = torch.empty((H, W, 3), dtype=torch.uint8, pin_memory=True)
+    pin_np = pinned.numpy()
+    for _ in range(2):
+        sc = rt.Scene.upload(host, ctx)
+        r.render(sc, out=pin_np)
+        sc.close()
+    e2e_s, e2e_rays, h2d = 0.0, 0, 0
+    if world > 1:
+        dist.barrier()
+    for _ in range(args.steps):
+        t = time.perf_counter()
+        sc = rt.Scene.upload(host, ctx)
+        r.render(sc, out=pin_np)
+        h2d = sc.device_bytes
+        sc.close()
+        e2e_s += time.perf_counter() - t
+        e2e_rays += r.last_stats.rays
+
+    # max over ranks of the device time, sum of the work
+    t = torch.tensor([dev_ms, e2e_s], dtype=torch.float64, device=dev)
+    n = torch.tensor([float(rays), float(e2e_rays)], dtype=torch.float64, device=dev)
+    if world > 1:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        dist.all_reduce(n, op=dist.ReduceOp.SUM)
+    dev_ms_max, e2e_s_max = float(t[0]), float(t[1])
+    rays_all, e2e_rays_all = float(n[0]), float(n[1])
+    value = rays_all / (dev_ms_max * 1e-3) / 1e6
+    e2e_value = e2e_rays_all / e2e_s_max / 1e6
+
+    if rank == 0:
+        # roofline of the dominant kernel (the shadow any-hit kernel)
+        stages = prof.stage_ms
+        dom = max(stages, key=lambda k: stages[k])
+        w = prof.work
+        sh_bytes = (prof.shadow_rays * B_RAY + w["shadow_nodes"] * B_NODE + w["shadow_triangles"] * B_TRI +
+                    w["shadow_spheres"] * B_SPH + w["shadow_verifications"] * B_VERIFY)
+        sh_flops = (w["shadow_nodes"] * F_NODE + w["shadow_triangles"] * F_TRI + w["shadow_spheres"] * F_SPH +
+                    w["shadow_verifications"] * F_VERIFY)
+        sh_s = stages["shadow"] * 1e-3
+        try:
+            peaks = json.load(open(PEAKS))
+            hbm, peak_src = float(peaks["hbm_gbs"]), "measured"
+        except (OSError, KeyError, ValueError):
+            hbm, peak_src = 6650.0, "fallback"
+        fp64 = rt.fp64_rate(ctx)
+        achieved = sh_bytes / sh_s / 1e9 if sh_s > 0 else None
+        roofline = {"kernel": "k_shadow", "bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s",
+                    "frac": achieved / hbm if achieved else None, "peak_source": peak_src,
+                    "traffic": read_traffic(), "traffic_unit": "bytes per frame (all k_shadow launches)",
+                    "algorithmic_bytes_per_frame": sh_bytes, "kernel_ms_per_frame": stages["shadow"],
+                    "dominant_stage": dom,
+                    "fp64": {"achieved_gops": sh_flops / sh_s / 1e9 if sh_s > 0 else None,
+                             "peak_gops": fp64, "peak_source": "measured FP64 add/mul issue rate (k_fp64_rate)",
+                             "frac": (sh_flops / sh_s / 1e9) / fp64 if sh_s > 0 and fp64 else None}}
+        cpu = None
+        if world == 1 and not args.no_cpu_baseline:
+            try:
+                cpu = cpu_baseline(path, args.cpu_seconds, os.cpu_count() or 1)
+                cpu.pop("rays", None)
+                cpu.pop("seconds", None)
+            except Exception as e:  # the oracle is test infrastructure; report, do not fail
+                cpu = {"value": None, "unit": "Mrays/s", "cores": os.cpu_count(), "kind": "port",
+                       "sample": "failed: %s" % e}
+        line = {
+            "metric": METRIC, "value": value, "unit": "Mrays/s", "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": dev_ms_max / args.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": WORKLOAD, "width": W, "height": H, "anti_aliasing": "no-jitter (outline on)",
+                       "samples": 1, "max_depth": 10, "seed": 0, "triangles": 81920,
+                       "rays_per_frame": rays_all / world / args.steps, "l2": "flushed (512 MB write) before each step",
+                       "parallelism": "replicas" if world > 1 else "single"},
+            "ms_per_frame": dev_ms_max / args.steps,
+            "wall_ms_per_step": 1e3 * wall_s / args.steps,
+            "gpu_launches": launches,
+            "e2e": {"value": e2e_value, "unit": "Mrays/s", "ms_per_frame": 1e3 * e2e_s_max / args.steps,
+                    "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": W * H * 3},
+            "roofline": roofline,
+            "stage_ms": {k: round(v, 4) for k, v in stages.items()},
+            "work_per_frame": w,
+            "cpu_baseline": cpu,
+            "clocks": clk,
+        }
+        print(json.dumps(line), flush=True)
+    if world > 1:
+        dist.barrier()
+        dist.destroy_process_group()
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -75,7 +75,7 @@ typedef struct rt_outline_config {
 
 /* Renderer fields (src/renderer.rs:37-47).  thread_count has no device
  * meaning and is not carried.  seed: `None` is rendered as 0, exactly as
- * `self.seed.unwrap_or(0)` does. */
+ * `self.seed.unwrap_or(0)` does.  flags: RT_FLAG_* (profiling only). */
 typedef struct rt_render_params {
   uint32_t width;
   uint32_t height;
@@ -85,7 +85,18 @@ typedef struct rt_render_params {
   int32_t anti_aliasing_mode; /* rt_aa_mode */
   uint64_t seed;
   rt_outline_config outline;
+  uint32_t flags;
+  uint32_t reserved;
 } rt_render_params;
+
+/* Profiling flags: per-stage CUDA-event times, and device work counters
+ * (node visits, primitive tests).  Both slow the render slightly. */
+#define RT_FLAG_STAGE_TIMES 1u
+#define RT_FLAG_COUNT_WORK 2u
+
+/* Stages reported in rt_stats.stage_ms */
+enum { RT_STAGE_RAYGEN = 0, RT_STAGE_TRACE = 1, RT_STAGE_EMIT = 2, RT_STAGE_SHADOW = 3, RT_STAGE_RESOLVE = 4,
+       RT_STAGE_FOLD = 5, RT_STAGE_POST = 6, RT_STAGE_COUNT = 8 };
 
 /* Counters of one render.  Rays are counted the way the reference casts
  * them: primary (one per camera sample; quincunx casts W*H centre rays and
@@ -95,9 +106,17 @@ typedef struct rt_stats {
   uint64_t primary_rays;
   uint64_t reflection_rays;
   uint64_t shadow_rays;
-  uint64_t reserved[5];
+  uint64_t hits;            /* closest-hit queries that hit an object */
+  /* RT_FLAG_COUNT_WORK: work of the closest-hit (trace) and shadow (any-hit)
+   * kernels: acceleration nodes visited, triangle and sphere tests, and
+   * reference-leaf verifications of mesh candidates */
+  uint64_t trace_nodes, trace_triangles, trace_spheres, trace_verifications;
+  uint64_t shadow_nodes, shadow_triangles, shadow_spheres, shadow_verifications;
+  uint32_t kernel_launches; /* kernels this render launched */
+  uint32_t reserved;
   double device_ms; /* CUDA-event time of the device pipeline */
   double total_ms;  /* host wall time of the whole call */
+  double stage_ms[RT_STAGE_COUNT]; /* RT_FLAG_STAGE_TIMES */
 } rt_stats;
 
 /* ------------------------------------------------------------------ */
@@ -243,6 +262,19 @@ rt_status rt_scene_outline_config(rt_ctx* ctx, const rt_scene* scene, rt_outline
 rt_status rt_scene_camera_aspect(rt_ctx* ctx, const rt_scene* scene, double* out);
 void rt_scene_free(rt_scene* scene);
 
+/* Host-side scene: Scene::from_json_file / from_json_str parsed, meshes
+ * loaded and transformed and k-d trees built, with nothing on the device
+ * yet.  rt_host_scene_desc exposes the flattened description that
+ * rt_scene_upload takes (valid until rt_host_scene_free).  Errors are
+ * reported through rt_last_error(NULL). */
+typedef struct rt_host_scene rt_host_scene;
+rt_status rt_host_scene_load_json_file(const char* path, rt_host_scene** out);
+rt_status rt_host_scene_load_json_str(const char* json, rt_host_scene** out);
+const rt_scene_desc* rt_host_scene_desc(const rt_host_scene* hs);
+void rt_host_scene_free(rt_host_scene* hs);
+/* Bytes rt_scene_upload copied to the device for this scene. */
+rt_status rt_scene_device_bytes(rt_ctx* ctx, const rt_scene* scene, uint64_t* out);
+
 /* Renderer::render (src/renderer.rs:120-382).  rgb_out receives
  * width*height*3 bytes, row-major, top row first.  out_on_device != 0 means
  * rgb_out is a device pointer on the context's device.  stats may be NULL. */
@@ -265,6 +297,9 @@ rt_status rt_debug_stdrng_u32(rt_ctx* ctx, const uint64_t* seeds, int64_t n, int
 /* The 16 (dx, dy) disk offsets of one area-light shading point
  * (src/lighting.rs:57-66, 170-173) for each light seed; out: n * 32. */
 rt_status rt_debug_disk_offsets(rt_ctx* ctx, const uint64_t* light_seeds, int64_t n, double radius, double* out);
+/* Measured issue rate of separate FP64 add and multiply instructions (the
+ * operations the render path uses; it never fuses them), in Gop/s. */
+rt_status rt_debug_fp64_rate(rt_ctx* ctx, double* gops);
 /* MeshObject::hit (src/ray.rs:614-675) of mesh `mesh_object` of a loaded
  * scene for n rays (6 doubles each: origin, direction).  out: 8 doubles per
  * ray [hit, t, point xyz, normal xyz]. */

@@ -1285,6 +1285,22 @@ static Hit make_hit(V3 p, V3 outward, double t, const Ray& r, size_t mi) {
 struct Counters {
   std::atomic<uint64_t> primary{0}, reflection{0}, shadow{0}, kd_visits{0}, tri_tests{0}, sphere_tests{0};
 };
+// Per-thread tallies, added into the shared Counters when a worker finishes
+// (keeps the timed CPU baseline free of atomic contention).
+struct LocalCounts {
+  uint64_t primary = 0, reflection = 0, shadow = 0, kd_visits = 0, tri_tests = 0, sphere_tests = 0;
+};
+static thread_local LocalCounts tlc;
+static void flush_counts(Counters* c) {
+  if (!c) return;
+  c->primary += tlc.primary;
+  c->reflection += tlc.reflection;
+  c->shadow += tlc.shadow;
+  c->kd_visits += tlc.kd_visits;
+  c->tri_tests += tlc.tri_tests;
+  c->sphere_tests += tlc.sphere_tests;
+  tlc = LocalCounts();
+}
 
 struct Object {
   size_t mi;
@@ -1296,7 +1312,7 @@ struct Sphere : Object {  // src/ray.rs:88-120
   V3 c;
   double r;
   bool hit(const Ray& ray, double tmin, double tmax, Hit* h, Counters* ct) const override {
-    if (ct) ct->sphere_tests++;
+    if (ct) tlc.sphere_tests++;
     V3 oc = ray.o - c;
     double a = dot(ray.d, ray.d);
     double hb = dot(oc, ray.d);
@@ -1446,7 +1462,7 @@ struct MeshObj : Object {  // src/ray.rs:498-680
     double closest = tmax;
     auto visit = [&](const std::vector<size_t>& idx) {
       for (size_t ti : idx) {
-        if (ct) ct->tri_tests++;
+        if (ct) tlc.tri_tests++;
         double t, u, v;
         V3 n;
         if (tri(r, mesh->tris[ti], tmin, closest, &t, &n, &u, &v)) {
@@ -1465,7 +1481,7 @@ struct MeshObj : Object {  // src/ray.rs:498-680
       if (mesh->kd.root) {
         uint64_t visits = 0;
         mesh->kd.traverse(mesh->kd.root.get(), r.o, r.d, visit, ct ? &visits : nullptr);
-        if (ct) ct->kd_visits += visits;
+        if (ct) tlc.kd_visits += visits;
       }
     } else {
       std::vector<size_t> all(mesh->tris.size());
@@ -1632,7 +1648,7 @@ static ShadeMat effective_material(const Material& m, const Hit& h) {
 }
 
 static bool shadowed(const Ctx& c, V3 origin, V3 dir, double dist) {
-  if (c.ct) c.ct->shadow++;
+  if (c.ct) tlc.shadow++;
   Ray sr(origin, dir);
   Hit tmp;
   return c.world->hit(sr, 0.001, dist, &tmp, c.ct);
@@ -1748,7 +1764,7 @@ static V3 ray_color(const Ctx& c, const Ray& r, int depth, uint64_t seed, bool* 
         V3 vd = normalize(c.cam_pos - h.point);
         V3 rd = reflect(-vd, h.normal);
         Ray rr(h.point + 0.001 * h.normal, rd);
-        if (c.ct) c.ct->reflection++;
+        if (c.ct) tlc.reflection++;
         V3 rc = ray_color(c, rr, depth - 1, seed, nullptr, nullptr, nullptr);
         color = color * (1.0 - refl) + rc * refl;
       }
@@ -1860,6 +1876,7 @@ struct RenderOpts {
   uint64_t seed = 0;
   bool outline = false;  // apply the scene's outline settings
   int threads = 1;
+  uint32_t y0 = 0, y1 = UINT32_MAX;  // render only rows [y0, y1) (CPU baseline samples)
 };
 
 static void build_world(const Scene& s, bool use_kd, World* w, std::vector<const Material*>* mats) {
@@ -1932,9 +1949,10 @@ static void build_world(const Scene& s, bool use_kd, World* w, std::vector<const
 }
 
 template <class F>
-static void parallel_for(size_t n, int threads, F&& fn) {
+static void parallel_for(size_t n, int threads, F&& fn, Counters* ct) {
   if (threads <= 1) {
     for (size_t i = 0; i < n; i++) fn(i);
+    flush_counts(ct);
     return;
   }
   std::atomic<size_t> next{0};
@@ -1954,6 +1972,7 @@ static void parallel_for(size_t n, int threads, F&& fn) {
         if (!eptr) eptr = std::current_exception();
         next.store(n);
       }
+      flush_counts(ct);
     });
   for (auto& t : th) t.join();
   if (eptr) std::rethrow_exception(eptr);
@@ -2004,7 +2023,7 @@ static void render(const Scene& s, const RenderOpts& o, std::vector<V3>* out, Co
       double cv = rclamp(1.0 - (double)cy * ph, 0.0, 1.0);
       Ray r = get_ray(cam, cu, cv);
       uint64_t seed = o.seed * GOLD + (uint64_t)cx + (uint64_t)cy * 0x85EBCA6BULL;
-      if (ct) ct->primary++;
+      if (ct) tlc.primary++;
       V3 col = ray_color(c, r, o.max_depth, seed, nullptr, nullptr, nullptr);
       {
         std::lock_guard<std::mutex> g(mu);
@@ -2012,18 +2031,21 @@ static void render(const Scene& s, const RenderOpts& o, std::vector<V3>* out, Co
       }
       return col;
     };
-    parallel_for((size_t)W * H, o.threads, [&](size_t i) {
+    uint32_t ya = std::min(o.y0, H), yb = std::min(o.y1, H);
+    size_t base = (size_t)ya * W;
+    parallel_for((size_t)W * (yb - ya), o.threads, [&](size_t k) {
+      size_t i = base + k;
       uint32_t x = (uint32_t)(i % W), y = (uint32_t)(i / W);
       double u = ((double)x + 0.5) * pw;
       double v = 1.0 - ((double)y + 0.5) * ph;
       Ray r = get_ray(cam, u, v);
       uint64_t seed = o.seed * GOLD + (uint64_t)x * 0x85EBCA6BULL + (uint64_t)y * 0xC2B2AE35ULL + 0x12345678ULL;
-      if (ct) ct->primary++;
+      if (ct) tlc.primary++;
       V3 cc = ray_color(c, r, o.max_depth, seed, nullptr, nullptr, nullptr);
       V3 k0 = corner(x, y), k1 = corner(x + 1, y), k2 = corner(x, y + 1), k3 = corner(x + 1, y + 1);
       V3 tot = cc + k0 + k1 + k2 + k3;
       (*out)[i] = tot / 5.0;
-    });
+    }, ct);
   } else {  // render_standard[_with_outline] (src/renderer.rs:445-749)
     Ctx cc = c;
     cc.cam = &cam;
@@ -2031,7 +2053,10 @@ static void render(const Scene& s, const RenderOpts& o, std::vector<V3>* out, Co
     std::vector<double> depth(outline ? (size_t)W * H : 0, 0.0);
     std::vector<V3> nrm(outline ? (size_t)W * H : 0, v3(0, 0, 0));
     double pwid = 1.0 / (double)(uint32_t)(W - 1), phei = 1.0 / (double)(uint32_t)(H - 1);
-    parallel_for((size_t)W * H, o.threads, [&](size_t i) {
+    uint32_t ya = std::min(o.y0, H), yb = std::min(o.y1, H);
+    size_t base = (size_t)ya * W;
+    parallel_for((size_t)W * (yb - ya), o.threads, [&](size_t k) {
+      size_t i = base + k;
       uint32_t x = (uint32_t)(i % W), y = (uint32_t)(i / W);
       double pu = (double)x / (double)(uint32_t)(W - 1);
       double pv = (double)(uint32_t)(H - 1 - y) / (double)(uint32_t)(H - 1);
@@ -2063,7 +2088,7 @@ static void render(const Scene& s, const RenderOpts& o, std::vector<V3>* out, Co
         }
         Ray r = get_ray(cam, su, sv);
         uint64_t sseed = pseed + (uint64_t)sidx * 0x1F845FEDULL;
-        if (ct) ct->primary++;
+        if (ct) tlc.primary++;
         bool hd = false;
         double d = 0;
         V3 n;
@@ -2075,8 +2100,8 @@ static void render(const Scene& s, const RenderOpts& o, std::vector<V3>* out, Co
       }
       (*out)[i] = tot / (double)o.samples;
       if (outline && have) { valid[i] = 1; depth[i] = pd; nrm[i] = pn; }
-    });
-    if (outline) apply_outline(*out, valid, depth, nrm, W, H, ocfg);
+    }, ct);
+    if (outline && ya == 0 && yb == H) apply_outline(*out, valid, depth, nrm, W, H, ocfg);
   }
 }
 
@@ -2114,9 +2139,26 @@ extern "C" {
 // Returns 0 on success, 1 on a reference-side error (message in err).
 // counts (nullable) receives [primary, reflection, shadow, kd_visits,
 // triangle_tests, sphere_tests].
+int oracle_render_rows(const char* scene_path, const char* scene_json, uint32_t width, uint32_t height, int aa,
+                       uint32_t samples, int max_depth, uint64_t seed, int use_kdtree, int outline, int threads,
+                       uint32_t y0, uint32_t y1, uint8_t* out_rgb, double* out_linear, uint64_t* counts, char* err,
+                       int err_len);
+
 int oracle_render(const char* scene_path, const char* scene_json, uint32_t width, uint32_t height, int aa,
                   uint32_t samples, int max_depth, uint64_t seed, int use_kdtree, int outline, int threads,
                   uint8_t* out_rgb, double* out_linear, uint64_t* counts, char* err, int err_len) {
+  return oracle_render_rows(scene_path, scene_json, width, height, aa, samples, max_depth, seed, use_kdtree, outline,
+                            threads, 0, UINT32_MAX, out_rgb, out_linear, counts, err, err_len);
+}
+
+// As oracle_render, restricted to image rows [y0, y1): the pixels of other
+// rows stay black and the outline pass (which needs whole-image buffers) is
+// skipped unless the band is the whole image.  Used to time bounded samples
+// of a frame for the CPU baseline.
+int oracle_render_rows(const char* scene_path, const char* scene_json, uint32_t width, uint32_t height, int aa,
+                       uint32_t samples, int max_depth, uint64_t seed, int use_kdtree, int outline, int threads,
+                       uint32_t y0, uint32_t y1, uint8_t* out_rgb, double* out_linear, uint64_t* counts, char* err,
+                       int err_len) {
   using namespace orc;
   try {
     Scene s = scene_path ? parse_scene(read_file(scene_path), dir_of(scene_path))
@@ -2131,6 +2173,8 @@ int oracle_render(const char* scene_path, const char* scene_json, uint32_t width
     o.use_kdtree = use_kdtree != 0;
     o.outline = outline != 0 && aa != 1;
     o.threads = threads;
+    o.y0 = y0;
+    o.y1 = y1;
     std::vector<V3> img;
     Counters ct;
     render(s, o, &img, counts ? &ct : nullptr);

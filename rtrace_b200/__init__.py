@@ -21,7 +21,8 @@ from . import _capi
 
 __all__ = [
     "AntiAliasingMode", "OutlineConfig", "Scene", "Renderer", "RtraceError", "SceneError",
-    "RenderError", "DeviceError", "Context", "RenderStats", "default_context", "write_png",
+    "RenderError", "DeviceError", "Context", "RenderStats", "default_context", "write_png", "HostScene",
+    "fp64_rate",
 ]
 
 
@@ -82,10 +83,23 @@ class RenderStats:
     shadow_rays: int = 0
     device_ms: float = 0.0
     total_ms: float = 0.0
+    hits: int = 0
+    kernel_launches: int = 0
+    stage_ms: dict = field(default_factory=dict)
+    work: dict = field(default_factory=dict)
 
     @property
     def rays(self):
         return self.primary_rays + self.reflection_rays + self.shadow_rays
+
+    @classmethod
+    def from_c(cls, st):
+        work = {k: int(getattr(st, k)) for k in (
+            "trace_nodes", "trace_triangles", "trace_spheres", "trace_verifications", "shadow_nodes",
+            "shadow_triangles", "shadow_spheres", "shadow_verifications")}
+        stages = {name: float(st.stage_ms[i]) for i, name in enumerate(_capi.STAGES)}
+        return cls(int(st.primary_rays), int(st.reflection_rays), int(st.shadow_rays), float(st.device_ms),
+                   float(st.total_ms), int(st.hits), int(st.kernel_launches), stages, work)
 
 
 class Context:
@@ -163,6 +177,25 @@ class Scene:
         return OutlineConfig(oc.depth_weight, oc.normal_weight, oc.threshold, tuple(oc.edge_color),
                              bool(oc.use_8_neighbors), oc.line_thickness)
 
+    @classmethod
+    def upload(cls, host_scene, ctx=None):
+        """Uploads a HostScene (rt_scene_upload)."""
+        ctx = ctx or default_context()
+        h = ctypes.c_void_p()
+        L = _capi.lib()
+        st = L.rt_scene_upload(ctx.handle, L.rt_host_scene_desc(host_scene.handle), ctypes.byref(h))
+        if st != _capi.RT_OK:
+            _raise(st, ctx.handle)
+        return cls(h, ctx)
+
+    @property
+    def device_bytes(self):
+        v = ctypes.c_uint64()
+        st = _capi.lib().rt_scene_device_bytes(self._ctx.handle, self._handle, ctypes.byref(v))
+        if st != _capi.RT_OK:
+            _raise(st, self._ctx.handle)
+        return int(v.value)
+
     @property
     def camera_aspect(self):
         v = ctypes.c_double()
@@ -183,6 +216,52 @@ class Scene:
             pass
 
 
+class HostScene:
+    """A parsed scene held in host memory only (rt_host_scene): JSON and STL
+    parsed, primitives transformed, k-d trees built.  Scene.upload() puts it
+    on a device."""
+
+    def __init__(self, handle):
+        self.handle = handle
+
+    @classmethod
+    def from_json_file(cls, path):
+        h = ctypes.c_void_p()
+        st = _capi.lib().rt_host_scene_load_json_file(str(path).encode(), ctypes.byref(h))
+        if st != _capi.RT_OK:
+            _raise(st, None)
+        return cls(h)
+
+    @classmethod
+    def from_json_str(cls, text):
+        h = ctypes.c_void_p()
+        st = _capi.lib().rt_host_scene_load_json_str(text.encode(), ctypes.byref(h))
+        if st != _capi.RT_OK:
+            _raise(st, None)
+        return cls(h)
+
+    def close(self):
+        if self.handle:
+            _capi.lib().rt_host_scene_free(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def fp64_rate(ctx=None):
+    """Measured FP64 add/multiply issue rate of the device, Gop/s."""
+    ctx = ctx or default_context()
+    v = ctypes.c_double()
+    st = _capi.lib().rt_debug_fp64_rate(ctx.handle, ctypes.byref(v))
+    if st != _capi.RT_OK:
+        _raise(st, ctx.handle)
+    return v.value
+
+
 class Renderer:
     """src/renderer.rs:37-118.  thread_count is accepted and ignored."""
 
@@ -196,6 +275,7 @@ class Renderer:
         self.anti_aliasing_mode = AntiAliasingMode.Quincunx
         self.seed = 0
         self.outline_config = None
+        self.flags = 0  # rtrace_b200._capi.RT_FLAG_* (profiling)
         self.last_stats = RenderStats()
 
     @classmethod
@@ -234,6 +314,7 @@ class Renderer:
         p.samples = int(self.samples)
         p.anti_aliasing_mode = int(self.anti_aliasing_mode)
         p.seed = int(self.seed or 0) & 0xFFFFFFFFFFFFFFFF
+        p.flags = int(self.flags)
         oc = self.outline_config
         if oc is not None:
             p.outline.enabled = 1
@@ -246,16 +327,24 @@ class Renderer:
             p.outline.line_thickness = oc.line_thickness
         return p
 
-    def render(self, scene, out=None, linear=False):
+    def render(self, scene, out=None, linear=False, device_ptr=None):
         """Renderer::render: returns an (height, width, 3) uint8 array.
 
-        With linear=True also returns the float64 colours before
-        quantisation (parity tests)."""
+        out: a C-contiguous host uint8 array to fill.  device_ptr: write the
+        image to this device address instead (width*height*3 bytes on the
+        scene's device); returns None.  linear=True also returns the float64
+        colours before quantisation (parity tests)."""
         p = self._params()
-        img = out if out is not None else np.empty((self.height, self.width, 3), np.uint8)
         st = _capi.rt_stats()
         L = _capi.lib()
         ctxh = scene._ctx.handle
+        if device_ptr is not None:
+            code = L.rt_render(ctxh, scene._handle, ctypes.byref(p), int(device_ptr), 1, ctypes.byref(st))
+            if code != _capi.RT_OK:
+                _raise(code, ctxh)
+            self.last_stats = RenderStats.from_c(st)
+            return None
+        img = out if out is not None else np.empty((self.height, self.width, 3), np.uint8)
         if linear:
             lin = np.empty((self.height, self.width, 3), np.float64)
             code = L.rt_render_linear(ctxh, scene._handle, ctypes.byref(p), img.ctypes.data, lin.ctypes.data,
@@ -264,8 +353,7 @@ class Renderer:
             code = L.rt_render(ctxh, scene._handle, ctypes.byref(p), img.ctypes.data, 0, ctypes.byref(st))
         if code != _capi.RT_OK:
             _raise(code, ctxh)
-        self.last_stats = RenderStats(st.primary_rays, st.reflection_rays, st.shadow_rays, st.device_ms,
-                                      st.total_ms)
+        self.last_stats = RenderStats.from_c(st)
         return (img, lin) if linear else img
 
     def render_to_file(self, scene, output_path):

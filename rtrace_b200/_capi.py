@@ -52,7 +52,14 @@ class rt_render_params(ctypes.Structure):
         ("anti_aliasing_mode", ctypes.c_int32),
         ("seed", ctypes.c_uint64),
         ("outline", rt_outline_config),
+        ("flags", ctypes.c_uint32),
+        ("reserved", ctypes.c_uint32),
     ]
+
+
+RT_FLAG_STAGE_TIMES = 1
+RT_FLAG_COUNT_WORK = 2
+STAGES = ["raygen", "trace", "emit", "shadow", "resolve", "fold", "post", "other"]
 
 
 class rt_stats(ctypes.Structure):
@@ -60,9 +67,20 @@ class rt_stats(ctypes.Structure):
         ("primary_rays", ctypes.c_uint64),
         ("reflection_rays", ctypes.c_uint64),
         ("shadow_rays", ctypes.c_uint64),
-        ("reserved", ctypes.c_uint64 * 5),
+        ("hits", ctypes.c_uint64),
+        ("trace_nodes", ctypes.c_uint64),
+        ("trace_triangles", ctypes.c_uint64),
+        ("trace_spheres", ctypes.c_uint64),
+        ("trace_verifications", ctypes.c_uint64),
+        ("shadow_nodes", ctypes.c_uint64),
+        ("shadow_triangles", ctypes.c_uint64),
+        ("shadow_spheres", ctypes.c_uint64),
+        ("shadow_verifications", ctypes.c_uint64),
+        ("kernel_launches", ctypes.c_uint32),
+        ("reserved", ctypes.c_uint32),
         ("device_ms", ctypes.c_double),
         ("total_ms", ctypes.c_double),
+        ("stage_ms", ctypes.c_double * 8),
     ]
 
 
@@ -94,6 +112,12 @@ def lib():
                                      ctypes.POINTER(rt_stats)]),
         "rt_render_linear": (ctypes.c_int, [_vp, _vp, ctypes.POINTER(rt_render_params), _vp, _vp,
                                             ctypes.POINTER(rt_stats)]),
+        "rt_host_scene_load_json_file": (ctypes.c_int, [ctypes.c_char_p, ctypes.POINTER(_vp)]),
+        "rt_host_scene_load_json_str": (ctypes.c_int, [ctypes.c_char_p, ctypes.POINTER(_vp)]),
+        "rt_host_scene_desc": (_vp, [_vp]),
+        "rt_host_scene_free": (None, [_vp]),
+        "rt_scene_device_bytes": (ctypes.c_int, [_vp, _vp, ctypes.POINTER(ctypes.c_uint64)]),
+        "rt_debug_fp64_rate": (ctypes.c_int, [_vp, ctypes.POINTER(ctypes.c_double)]),
         "rt_debug_stdrng_u32": (ctypes.c_int, [_vp, _vp, ctypes.c_int64, ctypes.c_int32, _vp]),
         "rt_debug_disk_offsets": (ctypes.c_int, [_vp, _vp, ctypes.c_int64, ctypes.c_double, _vp]),
         "rt_debug_mesh_hit": (ctypes.c_int, [_vp, _vp, ctypes.c_int32, ctypes.c_int32, _vp, ctypes.c_int64,

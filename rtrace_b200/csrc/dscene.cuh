@@ -1,6 +1,29 @@
 // Device-resident scene layout and the intersection routines of the render
-// path.  Each routine restates one reference function in the same IEEE
-// operation order; see the comments for the reference lines.
+// path.  Each primitive test restates one reference function in the same
+// IEEE operation order; see the comments for the reference lines.
+//
+// Acceleration.  The reference tests objects in scene order
+// (World::hit, src/ray.rs:699-711) and walks each mesh's k-d tree without
+// t-interval pruning (src/mesh.rs:399-465).  The device reaches the same
+// answers faster:
+//   * Meshes: a BVH over the mesh's triangles proposes candidates; a
+//     candidate counts only if the reference's traversal would have tested
+//     it, i.e. if one of the k-d leaves holding it is visited by the
+//     reference's rules (near child always, far child iff t_split >= 0,
+//     one side for axis-parallel rays, then the leaf's slab test).  Among
+//     equal-t candidates the one the reference's depth-first walk meets
+//     first wins (the strict `t < closest` test keeps the first).  When
+//     verification cannot settle a closest-hit query (more ties than the
+//     buffer holds, or no minimal candidate is visited), the exact k-d walk
+//     runs instead.
+//   * Runs of consecutive spheres: a BVH over the run.  Spheres accept
+//     `root <= closest`, so the sequential scan's result is the minimal
+//     accepted t with ties resolved to the latest sphere; the group search
+//     returns exactly that.
+//   * Shadow rays only ask `world.hit(..).is_some()`; every per-object
+//     test is monotone in t_max, so any accepting object suffices.
+// Boxes are padded and pruning uses a relative margin, so a box never
+// rejects a primitive the exact test would accept.
 #pragma once
 
 #include "dmath.cuh"
@@ -11,17 +34,16 @@ namespace rtb {
 #define RTB_INF __longlong_as_double(0x7ff0000000000000LL)
 #endif
 
-enum { OBJ_SPHERE = 0, OBJ_PLANE = 1, OBJ_CUBE = 2, OBJ_MESH = 3 };
+enum { OBJ_SPHERE = 0, OBJ_PLANE = 1, OBJ_CUBE = 2, OBJ_MESH = 3, OBJ_SPHERE_GROUP = 4 };
 
 // Device error flags (bitmask in DFrame::err)
 enum { ERR_WATCHDOG = 1, ERR_EMPTY_RANGE = 2, ERR_STACK = 4, ERR_RANGE_OVERFLOW = 8 };
 
-// k-d tree pruning margin.  A triangle whose Moller-Trumbore t is below the
-// current closest t lies inside its leaf's bounds, so the leaf's slab entry
-// cannot exceed that t by more than the rounding of the two computations;
-// nodes are skipped only when their entry exceeds closest * (1 + REL) + ABS.
+// Pruning: a box is skipped only when its entry exceeds t * REL + ABS.
 #define RTB_PRUNE_REL 1.000001
 #define RTB_PRUNE_ABS 1e-9
+#define RTB_STACK 64
+#define RTB_TIES 8
 
 struct DCube {
   double c[3], half[3];
@@ -32,19 +54,35 @@ struct DCube {
   int pad;
 };
 
-// One mesh.  Nodes: 4 double2 each = (bmin.x, bmin.y) (bmin.z, bmax.x)
-// (bmax.y, bmax.z) (split, meta); meta = int2{a, b}: internal a = right
-// child, b = axis; leaf a = first entry, b = -1 - count.  Entries (leaf
-// order, duplicated like the reference's index lists): 5 double2 =
-// v0, e1 = v1 - v0, e2 = v2 - v0, meta int2{triangle index, degenerate}.
+// BVH node: 7 double2 = lmin, lmax, rmin, rmax (12 doubles) + int4
+// {lidx, lcnt, ridx, rcnt} (cnt > 0 leaf range, 0 internal node, < 0 empty).
+// Triangle records: 5 double2 = v0, e1 = v1 - v0, e2 = v2 - v0,
+// meta = int2{triangle index, degenerate}.
+// k-d nodes: 4 double2 = (bmin.x, bmin.y) (bmin.z, bmax.x) (bmax.y, bmax.z)
+// (split, int2 meta): internal {right child, axis}, leaf {first, -1-count}.
 struct DMesh {
   double bmin[3], bmax[3];
-  const double2* nodes;
-  const double2* entries;
-  const double2* brute;    // same entry layout, original triangle order
+  const double2* bvh;      // triangle BVH nodes
+  const double2* btris;    // triangle records in BVH leaf order
+  const double2* brute;    // triangle records in original order
   const double4* normals;  // normalize(e1 x e2) per triangle
+  const double2* nodes;    // reference k-d tree, preorder
+  const double2* entries;  // k-d leaf entries (triangle records), leaf order
+  const int2* leaf_path;   // per k-d node: {path bits (bit k: right at depth k), depth}
+  const int* occ_off;      // per triangle: occurrences [occ_off[t], occ_off[t+1])
+  const int2* occ;         // {k-d leaf node, position in the leaf}
   int n_nodes;
   int n_tris;
+};
+
+// A run of consecutive spheres [first_obj, first_obj + count) in the World.
+struct DSphGroup {
+  const double2* bvh;  // BVH nodes over the run; leaves index `order`
+  const int* order;    // BVH position -> position in the run
+  int first_sphere;    // index of the run's first sphere in DScene::sph
+  int first_obj;       // World index of the run's first sphere
+  int count;
+  int pad;
 };
 
 struct DMat {
@@ -69,13 +107,15 @@ struct DLight {
 };
 
 struct DScene {
-  int n_obj;
+  int n_obj;  // entries of `obj` (a sphere group is one entry)
   int n_lights;
-  const int4* obj;  // {kind, index in its kind array, material, 0}
-  const double* sph;  // 5 per sphere: cx cy cz r r*r
-  const double* pln;  // 12 per plane: p, n, u axis, v axis
+  const int4* obj;     // {kind, index in its kind array, material, World index}
+  const double* sph;   // 5 per sphere: cx cy cz r r*r
+  const int* sph_mat;  // per sphere: material index
+  const double* pln;   // 12 per plane: p, n, u axis, v axis
   const DCube* cub;
   const DMesh* mesh;
+  const DSphGroup* grp;
   const DMat* mat;
   const DLight* lights;
   double amb_color[3];
@@ -95,12 +135,17 @@ struct DCam {
   int grid;
 };
 
+// Work counters (profiling renders only).
+struct Work {
+  unsigned long long nodes, tris, spheres, verify;
+};
+
 // Per-ray constants shared by all object tests.
 struct RayC {
   V3 o, d;
-  double dd;       // d.d (sphere `a`)
-  V3 inv;          // 1/d per axis
-  int par;         // bit a: |d[a]| < 1e-9 (k-d slabs treat the axis as parallel)
+  double dd;  // d.d (sphere `a`)
+  V3 inv;     // 1/d per axis
+  int par;    // bit a: |d[a]| < 1e-9 (k-d slabs treat the axis as parallel)
 };
 __device__ __forceinline__ RayC make_rayc(V3 o, V3 d) {
   RayC r;
@@ -196,7 +241,7 @@ __device__ __forceinline__ bool mesh_bounds(const DMesh& M, const RayC& r, doubl
 }
 
 // MeshObject::intersect_triangle (src/ray.rs:527-583) up to the acceptance
-// test; the normal is looked up afterwards for the winning entry.
+// test; the normal is looked up afterwards for the winning triangle.
 __device__ __forceinline__ bool tri_t(const double2* E, const RayC& r, double tmin, double tmax, double* t) {
   double2 q0 = __ldg(E + 0), q1 = __ldg(E + 1), q2 = __ldg(E + 2), q3 = __ldg(E + 3), q4 = __ldg(E + 4);
   V3 v0 = mk(q0.x, q0.y, q1.x);
@@ -249,38 +294,96 @@ __device__ __forceinline__ bool kd_slab(const double2* N, const RayC& r, double*
   return th >= 0.0;
 }
 
-// MeshObject::hit with KdTree::traverse (src/ray.rs:614-649,
-// src/mesh.rs:399-465).  Leaves are visited in the reference's order; a
-// subtree is skipped when its bounds fail the reference's slab test (its
-// leaves would all fail it) or start beyond the current closest t (none of
-// its triangles can win the strict `t < closest` test).  any = true stops
-// at the first accepted triangle (shadow rays only ask is_some()).
-template <bool ANY>
-__device__ __forceinline__ bool mesh_trace(const DMesh& M, const RayC& r, double tmin, double& closest, int& best,
-                                           bool use_kd, int* err) {
-  if (!mesh_bounds(M, r, tmin, closest)) return false;
-  bool found = false;
-  if (!use_kd) {
-    for (int i = 0; i < M.n_tris; i++) {
-      double t;
-      if (tri_t(M.brute + 5 * (size_t)i, r, tmin, closest, &t)) {
-        if (t < closest) {
-          closest = t;
-          best = i;
-          found = true;
-          if (ANY) return true;
-        }
-      }
+// Ray/box entry for BVH culling (padded boxes; not a reference test).
+__device__ __forceinline__ bool box_hit(const double* mn, const double* mx, const RayC& r, double tmax,
+                                        double* te) {
+  double tl = -RTB_INF, th = RTB_INF;
+#pragma unroll
+  for (int a = 0; a < 3; a++) {
+    double o = r.o[a];
+    if (r.d[a] == 0.0) {
+      if (o < mn[a] || o > mx[a]) return false;
+    } else {
+      double inv = r.inv[a];
+      double t0 = (mn[a] - o) * inv;
+      double t1 = (mx[a] - o) * inv;
+      tl = rmax(tl, rmin(t0, t1));
+      th = rmin(th, rmax(t0, t1));
     }
-    return found;
   }
+  *te = tl;
+  return tl <= th && th >= 0.0 && !(tl > tmax * RTB_PRUNE_REL + RTB_PRUNE_ABS);
+}
+
+// Whether the reference's traversal tests k-d leaf `leaf` for this ray
+// (src/mesh.rs:399-465, leaf test :411); *key orders visited leaves in the
+// reference's depth-first visiting order (bit 31-k: far child at depth k).
+__device__ __forceinline__ bool kd_leaf_visited(const DMesh& M, const RayC& r, int leaf, unsigned* key) {
+  int2 lp = __ldg(M.leaf_path + leaf);
+  unsigned path = (unsigned)lp.x;
+  int depth = lp.y;
+  int node = 0;
+  unsigned k_out = 0;
+  for (int k = 0; k < depth; k++) {
+    double2 n3 = __ldg(M.nodes + 4 * (size_t)node + 3);
+    int right = lo32(n3.y), axis = hi32(n3.y);
+    double split = n3.x;
+    bool go_right = (path >> k) & 1u;
+    double op = r.o[axis];
+    bool left_side = op <= split;
+    if (r.par & (1 << axis)) {
+      if (go_right == left_side) return false;  // only the origin's side
+    } else if (go_right == left_side) {         // far child: needs t_split >= 0
+      double ts = (split - op) / r.d[axis];
+      if (!(ts >= 0.0)) return false;
+      k_out |= 1u << (31 - k);
+    }
+    node = go_right ? right : node + 1;
+  }
+  double te;
+  if (!kd_slab(M.nodes + 4 * (size_t)node, r, &te)) return false;
+  *key = k_out;
+  return true;
+}
+
+// The reference's first test of triangle `tri` for this ray: the smallest
+// (leaf key, position) over the visited leaves holding it.
+__device__ __forceinline__ bool tri_first_visit(const DMesh& M, const RayC& r, int tri, unsigned long long* order,
+                                                Work* w) {
+  int b = __ldg(M.occ_off + tri), e = __ldg(M.occ_off + tri + 1);
+  bool any = false;
+  unsigned long long best = ~0ULL;
+  for (int k = b; k < e; k++) {
+    int2 oc = __ldg(M.occ + k);
+    // work unit: one 16-byte read (occurrence, each ancestor's split record,
+    // and three for the leaf box)
+    if (w) w->verify += 4 + (unsigned)__ldg(M.leaf_path + oc.x).y;
+    unsigned key;
+    if (kd_leaf_visited(M, r, oc.x, &key)) {
+      unsigned long long o = ((unsigned long long)key << 32) | (unsigned)oc.y;
+      if (o < best) best = o;
+      any = true;
+    }
+  }
+  *order = best;
+  return any;
+}
+
+// The exact reference k-d walk (MeshObject::hit with KdTree::traverse,
+// src/ray.rs:614-649, src/mesh.rs:399-465) with exact subtree culling by
+// node bounds and closest-t pruning.  Returns the winning triangle index.
+template <bool ANY>
+__device__ bool mesh_kd_walk(const DMesh& M, const RayC& r, double tmin, double& closest, int& best_tri, int* err,
+                             Work* w) {
   if (M.n_nodes == 0) return false;
-  int stack[32];
+  bool found = false;
+  int stack[RTB_STACK];
   int sp = 0;
   int node = 0;
   for (;;) {
     const double2* N = M.nodes + 4 * (size_t)node;
     double te;
+    if (w) w->nodes++;
     bool visit = kd_slab(N, r, &te) && !(te > closest * RTB_PRUNE_REL + RTB_PRUNE_ABS);
     if (visit) {
       double2 n3 = __ldg(N + 3);
@@ -290,34 +393,27 @@ __device__ __forceinline__ bool mesh_trace(const DMesh& M, const RayC& r, double
         for (int k = 0; k < cnt; k++) {
           double t;
           const double2* E = M.entries + 5 * (size_t)(first + k);
-          if (tri_t(E, r, tmin, closest, &t)) {
-            if (t < closest) {
-              closest = t;
-              best = first + k;
-              found = true;
-              if (ANY) return true;
-            }
+          if (w) w->tris++;
+          if (tri_t(E, r, tmin, closest, &t) && t < closest) {
+            closest = t;
+            best_tri = lo32(__ldg(E + 4).y);
+            found = true;
+            if (ANY) return true;
           }
         }
       } else {
         int axis = mb;
         double split = n3.x;
         double op = r.o[axis];
-        int near_c, far_c;
-        if (op <= split) {
-          near_c = node + 1;
-          far_c = ma;
-        } else {
-          near_c = ma;
-          far_c = node + 1;
-        }
+        int near_c = op <= split ? node + 1 : ma;
+        int far_c = op <= split ? ma : node + 1;
         if (r.par & (1 << axis)) {
           node = near_c;
           continue;
         }
         double ts = (split - op) / r.d[axis];
         if (ts >= 0.0) {
-          if (sp >= 32) {
+          if (sp >= RTB_STACK) {
             atomicOr(err, ERR_STACK);
             return found;
           }
@@ -333,43 +429,264 @@ __device__ __forceinline__ bool mesh_trace(const DMesh& M, const RayC& r, double
   return found;
 }
 
+// Loads one BVH node: child boxes and child references.
+struct BNode {
+  double lmn[3], lmx[3], rmn[3], rmx[3];
+  int lidx, lcnt, ridx, rcnt;
+};
+__device__ __forceinline__ BNode load_bnode(const double2* base, int node) {
+  const double2* N = base + 7 * (size_t)node;
+  double2 b0 = __ldg(N + 0), b1 = __ldg(N + 1), b2 = __ldg(N + 2), b3 = __ldg(N + 3), b4 = __ldg(N + 4),
+          b5 = __ldg(N + 5), b6 = __ldg(N + 6);
+  BNode n;
+  n.lmn[0] = b0.x; n.lmn[1] = b0.y; n.lmn[2] = b1.x;
+  n.lmx[0] = b1.y; n.lmx[1] = b2.x; n.lmx[2] = b2.y;
+  n.rmn[0] = b3.x; n.rmn[1] = b3.y; n.rmn[2] = b4.x;
+  n.rmx[0] = b4.y; n.rmx[1] = b5.x; n.rmx[2] = b5.y;
+  n.lidx = lo32(b6.x);
+  n.lcnt = hi32(b6.x);
+  n.ridx = lo32(b6.y);
+  n.rcnt = hi32(b6.y);
+  return n;
+}
+
+// Generic BVH walk.  visit_leaf(first, count) tests a leaf's primitives and
+// returns true to stop; bound() is the current pruning t.  Children are
+// visited nearest first.
+template <class Leaf, class Bound>
+__device__ __forceinline__ bool bvh_walk(const double2* bvh, const RayC& r, Leaf visit_leaf, Bound bound, int* err,
+                                         Work* w) {
+  int stack[RTB_STACK];
+  int sp = 0;
+  int node = 0;
+  for (;;) {
+    BNode n = load_bnode(bvh, node);
+    if (w) w->nodes++;
+    double tl = 0, tr = 0;
+    double b = bound();
+    bool hl = n.lcnt >= 0 && box_hit(n.lmn, n.lmx, r, b, &tl);
+    bool hr = n.rcnt >= 0 && box_hit(n.rmn, n.rmx, r, b, &tr);
+    bool swap = hl && hr && tr < tl;
+    int aidx = swap ? n.ridx : n.lidx, acnt = swap ? n.rcnt : n.lcnt;
+    int bidx = swap ? n.lidx : n.ridx, bcnt = swap ? n.lcnt : n.rcnt;
+    bool ha = swap ? hr : hl, hb = swap ? hl : hr;
+    int next = -1;
+    if (ha) {
+      if (acnt > 0) {
+        if (visit_leaf(aidx, acnt)) return true;
+      } else {
+        next = aidx;
+      }
+    }
+    if (hb) {
+      if (bcnt > 0) {
+        if (visit_leaf(bidx, bcnt)) return true;
+      } else if (next < 0) {
+        next = bidx;
+      } else {
+        if (sp >= RTB_STACK) {
+          atomicOr(err, ERR_STACK);
+          return false;
+        }
+        stack[sp++] = bidx;
+      }
+    }
+    if (next >= 0) {
+      node = next;
+      continue;
+    }
+    if (sp == 0) return false;
+    node = stack[--sp];
+  }
+}
+
+// Closest hit on a mesh (MeshObject::hit, src/ray.rs:614-675).  On entry
+// `closest` is the World's closest-so-far; on a hit it becomes the hit's t
+// and best_tri the winning triangle (original index).
+__device__ bool mesh_closest(const DMesh& M, const RayC& r, double tmin, double& closest, int& best_tri,
+                             bool use_kd, int* err, Work* w) {
+  if (!mesh_bounds(M, r, tmin, closest)) return false;
+  const double cin = closest;
+  double bt = closest;
+  bool have = false;
+  int ties[RTB_TIES];
+  int nt = 0;
+  bool overflow = false;
+  bvh_walk(
+      M.bvh, r,
+      [&](int first, int cnt) {
+        for (int k = 0; k < cnt; k++) {
+          const double2* E = M.btris + 5 * (size_t)(first + k);
+          double t;
+          if (w) w->tris++;
+          if (tri_t(E, r, tmin, cin, &t)) {
+            int tri = lo32(__ldg(E + 4).y);
+            if (!have || t < bt) {
+              bt = t;
+              have = true;
+              nt = 0;
+              ties[nt++] = tri;
+              overflow = false;
+            } else if (t == bt) {
+              if (nt < RTB_TIES) ties[nt++] = tri;
+              else overflow = true;
+            }
+          }
+        }
+        return false;
+      },
+      [&]() { return bt; }, err, w);
+  // No triangle meets t in (tmin, closest): the reference finds none either.
+  if (!have) return false;
+  if (!use_kd) {
+    // brute force tests in original order: lowest index among the minimal t
+    int bi = ties[0];
+    for (int k = 1; k < nt; k++) bi = min(bi, ties[k]);
+    if (overflow) {
+      for (int i = 0; i < M.n_tris; i++) {
+        double t;
+        if (tri_t(M.brute + 5 * (size_t)i, r, tmin, cin, &t) && t == bt) {
+          bi = i;
+          break;
+        }
+      }
+    }
+    closest = bt;
+    best_tri = bi;
+    return true;
+  }
+  if (!overflow) {
+    unsigned long long bo = ~0ULL;
+    int bi = -1;
+    for (int k = 0; k < nt; k++) {
+      unsigned long long o;
+      if (tri_first_visit(M, r, ties[k], &o, w) && o < bo) {
+        bo = o;
+        bi = ties[k];
+      }
+    }
+    if (bi >= 0) {
+      closest = bt;
+      best_tri = bi;
+      return true;
+    }
+  }
+  // The reference does not test the nearest triangle (or too many tie):
+  // answer with the reference's own walk.
+  return mesh_kd_walk<false>(M, r, tmin, closest, best_tri, err, w);
+}
+
+// world.hit(..).is_some() restricted to one mesh: a triangle accepted in
+// (tmin, tmax) that the reference's traversal would test.
+__device__ bool mesh_any(const DMesh& M, const RayC& r, double tmin, double tmax, bool use_kd, int* err, Work* w) {
+  if (!mesh_bounds(M, r, tmin, tmax)) return false;
+  return bvh_walk(
+      M.bvh, r,
+      [&](int first, int cnt) {
+        for (int k = 0; k < cnt; k++) {
+          const double2* E = M.btris + 5 * (size_t)(first + k);
+          double t;
+          if (w) w->tris++;
+          if (tri_t(E, r, tmin, tmax, &t)) {
+            if (!use_kd) return true;
+            unsigned long long o;
+            if (tri_first_visit(M, r, lo32(__ldg(E + 4).y), &o, w)) return true;
+          }
+        }
+        return false;
+      },
+      [&]() { return tmax; }, err, w);
+}
+
+// A run of spheres: minimal accepted root, ties to the latest sphere.  On
+// entry `closest` is the World's closest-so-far (an inclusive bound, as
+// Sphere::hit accepts root == t_max).
+template <bool ANY>
+__device__ bool group_hit(const DScene& S, const DSphGroup& G, const RayC& r, double tmin, double& closest,
+                          int& best, int* err, Work* w) {
+  bool have = false;
+  double bt = closest;
+  int bi = -1;
+  bool stop = bvh_walk(
+      G.bvh, r,
+      [&](int first, int cnt) {
+        for (int k = 0; k < cnt; k++) {
+          int sidx = __ldg(G.order + first + k);  // position in the run
+          double t;
+          if (w) w->spheres++;
+          if (sphere_t(S.sph + 5 * (size_t)(G.first_sphere + sidx), r, tmin, bt, &t)) {
+            if (ANY) {
+              bi = sidx;
+              bt = t;
+              return true;
+            }
+            if (!have || t < bt || sidx > bi) {
+              bt = t;
+              bi = sidx;
+              have = true;
+            }
+          }
+        }
+        return false;
+      },
+      [&]() { return bt; }, err, w);
+  if (ANY) {
+    if (!stop) return false;
+    best = bi;
+    closest = bt;
+    return true;
+  }
+  if (!have) return false;
+  closest = bt;
+  best = bi;
+  return true;
+}
+
 struct WHit {
-  int obj;   // scene object index, -1 = miss
-  int aux;   // mesh entry / cube axis
+  int obj;  // World index of the winner, -1 = miss
+  int aux;  // mesh triangle / cube axis
   double t;
+  int ent;  // entry of DScene::obj that produced the hit
 };
 
 // World::hit (src/ray.rs:699-711): scene order, closest narrowing
-__device__ __forceinline__ WHit world_closest(const DScene& S, const RayC& r, double tmin, bool use_kd, int* err) {
+__device__ __forceinline__ WHit world_closest(const DScene& S, const RayC& r, double tmin, bool use_kd, int* err,
+                                             Work* w) {
   double closest = RTB_INF;
-  WHit h{-1, 0, 0.0};
+  WHit h{-1, 0, 0.0, -1};
   for (int i = 0; i < S.n_obj; i++) {
     int4 ob = __ldg(S.obj + i);
     double t;
     switch (ob.x) {
       case OBJ_SPHERE:
-        if (sphere_t(S.sph + 5 * ob.y, r, tmin, closest, &t)) {
+        if (w) w->spheres++;
+        if (sphere_t(S.sph + 5 * (size_t)ob.y, r, tmin, closest, &t)) {
           closest = t;
-          h = WHit{i, 0, t};
+          h = WHit{ob.w, 0, t, i};
         }
         break;
       case OBJ_PLANE:
-        if (plane_t(S.pln + 12 * ob.y, r, tmin, closest, &t)) {
+        if (plane_t(S.pln + 12 * (size_t)ob.y, r, tmin, closest, &t)) {
           closest = t;
-          h = WHit{i, 0, t};
+          h = WHit{ob.w, 0, t, i};
         }
         break;
       case OBJ_CUBE: {
         int ax;
         if (cube_t(S.cub[ob.y], r, tmin, closest, &t, &ax)) {
           closest = t;
-          h = WHit{i, ax, t};
+          h = WHit{ob.w, ax, t, i};
         }
         break;
       }
+      case OBJ_MESH: {
+        int tri = -1;
+        if (mesh_closest(S.mesh[ob.y], r, tmin, closest, tri, use_kd, err, w)) h = WHit{ob.w, tri, closest, i};
+        break;
+      }
       default: {
-        int best = -1;
-        if (mesh_trace<false>(S.mesh[ob.y], r, tmin, closest, best, use_kd, err)) h = WHit{i, best, closest};
+        int k = -1;
+        if (group_hit<false>(S, S.grp[ob.y], r, tmin, closest, k, err, w)) h = WHit{ob.w + k, 0, closest, i};
         break;
       }
     }
@@ -377,29 +694,32 @@ __device__ __forceinline__ WHit world_closest(const DScene& S, const RayC& r, do
   return h;
 }
 
-// world.hit(ray, t_min, t_max).is_some(): true iff some object hits with
-// t_max fixed (the per-object tests are monotone in t_max), in any order.
+// world.hit(ray, t_min, t_max).is_some()
 __device__ __forceinline__ bool world_any(const DScene& S, const RayC& r, double tmin, double tmax, bool use_kd,
-                                          int* err) {
+                                          int* err, Work* w) {
   for (int i = 0; i < S.n_obj; i++) {
     int4 ob = __ldg(S.obj + i);
     double t;
     switch (ob.x) {
       case OBJ_SPHERE:
-        if (sphere_t(S.sph + 5 * ob.y, r, tmin, tmax, &t)) return true;
+        if (w) w->spheres++;
+        if (sphere_t(S.sph + 5 * (size_t)ob.y, r, tmin, tmax, &t)) return true;
         break;
       case OBJ_PLANE:
-        if (plane_t(S.pln + 12 * ob.y, r, tmin, tmax, &t)) return true;
+        if (plane_t(S.pln + 12 * (size_t)ob.y, r, tmin, tmax, &t)) return true;
         break;
       case OBJ_CUBE: {
         int ax;
         if (cube_t(S.cub[ob.y], r, tmin, tmax, &t, &ax)) return true;
         break;
       }
+      case OBJ_MESH:
+        if (mesh_any(S.mesh[ob.y], r, tmin, tmax, use_kd, err, w)) return true;
+        break;
       default: {
         double c = tmax;
-        int best;
-        if (mesh_trace<true>(S.mesh[ob.y], r, tmin, c, best, use_kd, err)) return true;
+        int k;
+        if (group_hit<true>(S, S.grp[ob.y], r, tmin, c, k, err, w)) return true;
         break;
       }
     }
@@ -420,24 +740,27 @@ __device__ __forceinline__ V3 face_normal(V3 d, V3 outward) {
   return front ? normalize(outward) : normalize(-outward);
 }
 
-// Rebuilds the winning object's HitRecord from (object, aux, t).
-__device__ __forceinline__ HitRec finalize_hit(const DScene& S, const RayC& r, const WHit& w, bool use_kd) {
+// Rebuilds the winning object's HitRecord from (entry, aux, t).
+__device__ __forceinline__ HitRec finalize_hit(const DScene& S, const RayC& r, const WHit& w) {
   HitRec h;
-  int4 ob = __ldg(S.obj + w.obj);
+  int4 ob = __ldg(S.obj + w.ent);
   h.mat = ob.z;
   h.has_uv = 0;
   h.u = h.v = 0.0;
   double t = w.t;
   switch (ob.x) {
-    case OBJ_SPHERE: {
-      const double* s = S.sph + 5 * ob.y;
+    case OBJ_SPHERE:
+    case OBJ_SPHERE_GROUP: {
+      int si = ob.x == OBJ_SPHERE ? ob.y : S.grp[ob.y].first_sphere + (w.obj - ob.w);
+      const double* s = S.sph + 5 * (size_t)si;
+      if (ob.x == OBJ_SPHERE_GROUP) h.mat = S.sph_mat[si];
       V3 c = mk(s[0], s[1], s[2]);
       h.p = r.o + t * r.d;
       h.n = face_normal(r.d, (h.p - c) / s[3]);
       break;
     }
     case OBJ_PLANE: {
-      const double* p = S.pln + 12 * ob.y;
+      const double* p = S.pln + 12 * (size_t)ob.y;
       V3 n = mk(p[3], p[4], p[5]);
       h.p = r.o + t * r.d;
       h.n = face_normal(r.d, n);
@@ -463,10 +786,9 @@ __device__ __forceinline__ HitRec finalize_hit(const DScene& S, const RayC& r, c
     }
     default: {
       const DMesh& M = S.mesh[ob.y];
-      const double2* E = (use_kd ? M.entries : M.brute) + 5 * (size_t)w.aux;
+      const double2* E = M.brute + 5 * (size_t)w.aux;
       double2 q0 = E[0], q1 = E[1], q2 = E[2], q3 = E[3], q4 = E[4];
       V3 v0 = mk(q0.x, q0.y, q1.x), e1 = mk(q1.y, q2.x, q2.y), e2 = mk(q3.x, q3.y, q4.x);
-      int tri = lo32(q4.y);
       V3 hh = cross(r.d, e2);
       double a = dot(e1, hh);
       double f = 1.0 / a;
@@ -474,7 +796,7 @@ __device__ __forceinline__ HitRec finalize_hit(const DScene& S, const RayC& r, c
       double u = f * dot(s, hh);
       V3 q = cross(s, e1);
       double v = f * dot(r.d, q);
-      double4 nn = M.normals[tri];
+      double4 nn = M.normals[w.aux];
       V3 n = mk(nn.x, nn.y, nn.z);
       if (a < 0.0) n = -n;
       h.p = r.o + t * r.d;

@@ -1,0 +1,808 @@
+// Wavefront kernels of one render.  Per reflection depth (queue level):
+//   k_trace    closest hit per queued ray (World::hit, src/ray.rs:699);
+//              misses get their background/grid colour here, hits are
+//              compacted into the level's hit list (warp ballot + one atomic
+//              per warp)
+//   k_emit     per hit: effective material, light sampling (point lights:
+//              one ray; disk lights: 16 ChaCha12-driven disk samples) and
+//              each shadow ray's would-be contribution
+//   k_shadow   one any-hit query per shadow ray
+//   k_resolve  per hit: ambient + visible contributions in the reference's
+//              summation order, fog, and the reflection ray, appended to
+//              the next level's queue (warp ballot + one atomic per warp)
+// then, deepest level first, k_fold blends reflections into their parents
+// (src/lighting.rs:469-493), and k_pixels/k_outline_* produce the image.
+#pragma once
+
+#include "dscene.cuh"
+
+namespace rtb {
+
+struct RayBuf {
+  double *ox, *oy, *oz, *dx, *dy, *dz;
+  uint64_t* seed;
+};
+struct LevelBuf {
+  double *r, *g, *b, *refl;
+  int* child;
+};
+struct ShadowBuf {
+  double *dx, *dy, *dz, *dist;  // per shadow ray
+  double *cr, *cg, *cb;         // contribution if visible
+  unsigned char* vis;
+  double *ox, *oy, *oz;         // per hit: shadow-ray origin p + 0.001 n
+};
+
+#define RTB_MAX_LEVELS 64
+
+struct DFrame {
+  DScene S;
+  DCam C;
+  int W, H, S_per_px, aa, max_depth, use_kd, outline, camera_mode;
+  uint64_t seed;
+  long long n_primary;
+  long long n_corner;  // quincunx corner rays, (W+1)(H+1)
+  RayBuf q[2];
+  int* hobj;  // per queued ray: World index of the hit, -1 miss
+  int* haux;
+  int* hent;
+  double* ht;
+  int* hit_ray;  // per hit slot: queued ray index
+  LevelBuf* levels;  // device array [max_depth]
+  int* counts;       // device: [0, L] queue sizes, [L+1 ..] hit counts per level
+  int* nhits;        // device [max_depth]
+  ShadowBuf sh;
+  long long chunk_hits;  // hits whose shadow rays fit the shadow buffer at once
+  // per primary ray outline data
+  double *pdepth, *pnx, *pny, *pnz;
+  unsigned char* phit;
+  // per pixel
+  double *cr, *cg, *cb;
+  double *dep, *nx, *ny, *nz;
+  unsigned char* valid;
+  double* mask;
+  unsigned char* rgb;
+  double* linear;  // optional pixel colours (3 per pixel) before quantisation
+  unsigned long long* stats;  // [2..5] trace work, [6..9] shadow work (nodes, tris, spheres, verify)
+  int* err;
+  double o_wd, o_wn, o_thr, o_color[3], o_thick;
+  int o_use8, o_radius;
+};
+
+__device__ __forceinline__ int warp_alloc(int* counter, bool want) {
+  unsigned m = __ballot_sync(0xffffffffu, want);
+  int lane = threadIdx.x & 31;
+  int base = 0;
+  if (m) {
+    int leader = __ffs(m) - 1;
+    if (lane == leader) base = atomicAdd(counter, __popc(m));
+    base = __shfl_sync(0xffffffffu, base, leader);
+  }
+  return want ? base + __popc(m & ((1u << lane) - 1u)) : -1;
+}
+
+__device__ __forceinline__ void warp_sum_add(unsigned long long* ctr, unsigned long long v) {
+  for (int off = 16; off > 0; off >>= 1) v += __shfl_down_sync(0xffffffffu, v, off);
+  if ((threadIdx.x & 31) == 0 && v) atomicAdd(ctr, v);
+}
+
+// slot 0: trace counters (stats[2..5]), 1: shadow counters (stats[6..9])
+__device__ __forceinline__ void flush_work(const DFrame& F, const Work& w, int slot) {
+  unsigned long long* b = F.stats + 2 + 4 * slot;
+  warp_sum_add(b + 0, w.nodes);
+  warp_sum_add(b + 1, w.tris);
+  warp_sum_add(b + 2, w.spheres);
+  warp_sum_add(b + 3, w.verify);
+}
+
+// --------------------------------------------------------------------------
+// Camera rays
+// --------------------------------------------------------------------------
+// Camera::get_ray (src/camera.rs:155-167) followed by Ray::new's normalise
+__device__ __forceinline__ void camera_ray(const DCam& c, double u, double v, V3* o, V3* d) {
+  V3 vp = ld3(c.llc) + u * ld3(c.hor) + v * ld3(c.ver);
+  if (c.persp) {
+    V3 dir = normalize(vp - ld3(c.origin));
+    *o = ld3(c.origin);
+    *d = normalize(dir);
+  } else {
+    *o = vp;
+    *d = normalize(ld3(c.vdir));
+  }
+}
+
+__global__ void k_raygen(DFrame F) {
+  const uint64_t GOLD = 0x9E3779B97F4A7C15ULL;
+  long long n = F.n_primary;
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
+    double u, v;
+    uint64_t seed;
+    if (F.aa == RT_AA_QUINCUNX) {
+      // render_quincunx (src/renderer.rs:752-897)
+      double pw = 1.0 / (double)F.W, ph = 1.0 / (double)F.H;
+      if (i < F.n_corner) {
+        unsigned cx = (unsigned)(i % (F.W + 1)), cy = (unsigned)(i / (F.W + 1));
+        u = rclamp((double)cx * pw, 0.0, 1.0);
+        v = rclamp(1.0 - (double)cy * ph, 0.0, 1.0);
+        seed = F.seed * GOLD + (uint64_t)cx + (uint64_t)cy * 0x85EBCA6BULL;
+      } else {
+        long long j = i - F.n_corner;
+        unsigned x = (unsigned)(j % F.W), y = (unsigned)(j / F.W);
+        u = ((double)x + 0.5) * pw;
+        v = 1.0 - ((double)y + 0.5) * ph;
+        seed = F.seed * GOLD + (uint64_t)x * 0x85EBCA6BULL + (uint64_t)y * 0xC2B2AE35ULL + 0x12345678ULL;
+      }
+    } else {
+      // render_standard (src/renderer.rs:445-584)
+      long long pix = i / F.S_per_px;
+      unsigned s = (unsigned)(i % F.S_per_px);
+      unsigned x = (unsigned)(pix % F.W), y = (unsigned)(pix / F.W);
+      double wm1 = (double)(unsigned)(F.W - 1), hm1 = (double)(unsigned)(F.H - 1);
+      double pu = (double)x / wm1;
+      double pv = (double)(unsigned)(F.H - 1 - y) / hm1;
+      double pwid = 1.0 / wm1, phei = 1.0 / hm1;
+      uint64_t pseed = F.seed * GOLD + (uint64_t)x * 0x85EBCA6BULL + (uint64_t)y * 0xC2B2AE35ULL;
+      seed = pseed + (uint64_t)s * 0x1F845FEDULL;
+      if (F.aa == RT_AA_NO_JITTER) {
+        u = pu;
+        v = pv;
+      } else {
+        // The pixel's StdRng stream: sample s draws u64 number 2s and 2s+1
+        // (samples == 1: numbers 0 and 1), i.e. words 4s..4s+3, which sit in
+        // ChaCha block s / 4.
+        uint32_t key[8], blk[16];
+        pcg32_key(pseed, key);
+        chacha_block(key, (uint64_t)(s >> 2), 6, blk);
+        int w0 = 4 * (s & 3);
+        uint64_t r0 = ((uint64_t)blk[w0 + 1] << 32) | blk[w0];
+        uint64_t r1 = ((uint64_t)blk[w0 + 3] << 32) | blk[w0 + 2];
+        const double scale = 1.0 / 9007199254740992.0;
+        double f0 = scale * (double)(r0 >> 11), f1 = scale * (double)(r1 >> 11);
+        if (F.S_per_px == 1) {
+          double ju = f0 - 0.5, jv = f1 - 0.5;
+          u = pu + ju * pwid;
+          v = pv + jv * phei;
+        } else {
+          const double PI = 3.141592653589793;
+          double ang = 2.0 * PI * (double)s / (double)F.S_per_px;
+          double phase = f0 * 2.0 * PI;
+          double ra = ang + phase;
+          double rad = 0.5 * f1;
+          double ju = rad * cos(ra), jv = rad * sin(ra);
+          u = pu + ju * pwid;
+          v = pv + jv * phei;
+        }
+      }
+    }
+    V3 o, d;
+    camera_ray(F.C, u, v, &o, &d);
+    RayBuf q = F.q[0];
+    q.ox[i] = o.x;
+    q.oy[i] = o.y;
+    q.oz[i] = o.z;
+    q.dx[i] = d.x;
+    q.dy[i] = d.y;
+    q.dz[i] = d.z;
+    q.seed[i] = seed;
+  }
+}
+
+// --------------------------------------------------------------------------
+// Closest hit + hit compaction; misses resolve to their background here
+// --------------------------------------------------------------------------
+template <bool COUNT>
+__global__ void __launch_bounds__(128) k_trace(DFrame F, int level) {
+  int n = F.counts[level];
+  RayBuf q = F.q[level & 1];
+  LevelBuf L = F.levels[level];
+  int stride = gridDim.x * blockDim.x;
+  Work w{0, 0, 0, 0};
+  for (int base = blockIdx.x * blockDim.x; base < n; base += stride) {
+    int i = base + threadIdx.x;
+    bool active = i < n;
+    bool hit = false;
+    WHit h{-1, 0, 0.0, -1};
+    if (active) {
+      V3 o = mk(q.ox[i], q.oy[i], q.oz[i]);
+      V3 d = mk(q.dx[i], q.dy[i], q.dz[i]);
+      RayC r = make_rayc(o, d);
+      h = world_closest(F.S, r, 0.001, F.use_kd != 0, F.err, COUNT ? &w : nullptr);
+      hit = h.obj >= 0;
+      if (!hit) {
+        // ray_color_with_camera / ray_color miss branch (src/lighting.rs:497-505)
+        V3 g;
+        V3 c = (F.camera_mode && grid_color(F.C, o, d, &g)) ? g : ld3(F.S.bg);
+        L.r[i] = c.x;
+        L.g[i] = c.y;
+        L.b[i] = c.z;
+        L.refl[i] = 0.0;
+        L.child[i] = -1;
+        if (level == 0 && F.outline) F.phit[i] = 0;
+      }
+    }
+    int slot = warp_alloc(&F.nhits[level], hit);
+    if (hit) {
+      F.hobj[slot] = h.obj;
+      F.haux[slot] = h.aux;
+      F.hent[slot] = h.ent;
+      F.ht[slot] = h.t;
+      F.hit_ray[slot] = i;
+    }
+  }
+  if (COUNT) flush_work(F, w, 0);
+}
+
+// --------------------------------------------------------------------------
+// Shading
+// --------------------------------------------------------------------------
+struct SMat {
+  V3 c;
+  double ka, kd, ks, shin;
+};
+
+// apply_texture (src/lighting.rs:9-54) + the colour parse of phong_lighting
+__device__ __forceinline__ SMat effective_material(const DMat& m, const HitRec& h) {
+  SMat s;
+  s.c = ld3(m.color);
+  s.ka = m.ambient;
+  s.kd = m.diffuse;
+  s.ks = m.specular;
+  s.shin = m.shininess;
+  if (h.has_uv) {
+    if (m.texture == 1) {
+      double um = fabs(rfract(h.u / m.cell_size));
+      double vm = fabs(rfract(h.v / m.cell_size));
+      double hw = m.half_width;
+      bool onu = um <= hw || um >= (1.0 - hw);
+      bool onv = vm <= hw || vm >= (1.0 - hw);
+      if (onu || onv) s.c = ld3(m.grid_color);
+    } else if (m.texture == 2) {
+      int32_t cu = sat_i32(floor(h.u)), cv = sat_i32(floor(h.v));
+      int32_t sum = (int32_t)((uint32_t)cu + (uint32_t)cv);
+      if (sum % 2 != 0) {
+        s.c = ld3(m.cb_color);
+        s.ka = m.cb_ambient;
+        s.kd = m.cb_diffuse;
+        s.ks = m.cb_specular;
+        s.shin = m.cb_shininess;
+      }
+    }
+  }
+  return s;
+}
+
+// diffuse + specular of one light sample (src/lighting.rs:124-141, 191-208)
+__device__ __forceinline__ V3 light_term(const SMat& m, const HitRec& h, V3 ldir, V3 lc, double li, V3 view) {
+  double ds = rmax(dot(h.n, ldir), 0.0);
+  V3 diffuse = m.kd * ds * li * cmul(lc, m.c);
+  V3 spec = mk(0.0, 0.0, 0.0);
+  if (ds > 0.0) {
+    V3 rd = reflect(-ldir, h.n);
+    double ss = pow(rmax(dot(view, rd), 0.0), m.shin);
+    spec = m.ks * ss * li * lc;
+  }
+  return diffuse + spec;
+}
+
+__device__ __forceinline__ HitRec load_hit(const DFrame& F, int level, int h, RayC* rc, uint64_t* seed) {
+  RayBuf q = F.q[level & 1];
+  int i = F.hit_ray[h];
+  V3 o = mk(q.ox[i], q.oy[i], q.oz[i]);
+  V3 d = mk(q.dx[i], q.dy[i], q.dz[i]);
+  *seed = q.seed[i];
+  *rc = make_rayc(o, d);
+  WHit w{F.hobj[h], F.haux[h], F.ht[h], F.hent[h]};
+  return finalize_hit(F.S, *rc, w);
+}
+
+// Light sampling for hits [c0, c1) of the level's hit list.
+__global__ void __launch_bounds__(128) k_emit(DFrame F, int level, long long c0) {
+  const DScene& S = F.S;
+  long long nh = F.nhits[level];
+  long long c1 = c0 + F.chunk_hits < nh ? c0 + F.chunk_hits : nh;
+  const int K = S.shadow_per_hit;
+  V3 campos = ld3(F.C.campos);
+  for (long long h = c0 + blockIdx.x * (long long)blockDim.x + threadIdx.x; h < c1;
+       h += (long long)gridDim.x * blockDim.x) {
+    RayC rc;
+    uint64_t seed;
+    HitRec hr = load_hit(F, level, (int)h, &rc, &seed);
+    SMat m = effective_material(S.mat[hr.mat], hr);
+    V3 view = normalize(campos - hr.p);
+    V3 so = hr.p + 0.001 * hr.n;
+    long long hl = h - c0;
+    F.sh.ox[hl] = so.x;
+    F.sh.oy[hl] = so.y;
+    F.sh.oz[hl] = so.z;
+    long long s = hl * K;
+    for (int li = 0; li < S.n_lights; li++) {
+      const DLight& L0 = S.lights[li];
+      V3 lp = ld3(L0.pos), lc = ld3(L0.color);
+      if (!L0.disk) {
+        // calculate_point_light_contribution (src/lighting.rs:100-142)
+        V3 ldir = normalize(lp - hr.p);
+        double dist = norm(lp - hr.p);
+        V3 sd = normalize(ldir);  // Ray::new
+        V3 c = light_term(m, hr, ldir, lc, L0.intensity, view);
+        F.sh.dx[s] = sd.x;
+        F.sh.dy[s] = sd.y;
+        F.sh.dz[s] = sd.z;
+        F.sh.dist[s] = dist;
+        F.sh.cr[s] = c.x;
+        F.sh.cg[s] = c.y;
+        F.sh.cb[s] = c.z;
+        s++;
+      } else {
+        // calculate_diffuse_light_contribution (src/lighting.rs:145-217),
+        // sample_disk_light_point (:69-97), sample_disk_point (:57-66)
+        uint64_t ls = seed * 0x9E3779B97F4A7C15ULL + sat_u64(hr.p.x * 1000.0) * 0x85EBCA6BULL +
+                      sat_u64(hr.p.y * 1000.0) * 0xC2B2AE35ULL + sat_u64(hr.p.z * 1000.0) * 0x6C8E9CF5ULL;
+        StdRng rng;
+        rng.init(ls);
+        double radius = L0.diameter / 2.0;
+        // gen_range(-radius..radius) panics on an empty or infinite range
+        bool ok = -radius < radius;
+        if (!ok) atomicOr(F.err, ERR_EMPTY_RANGE);
+        if (ok && !isfinite(radius - -radius)) {
+          atomicOr(F.err, ERR_RANGE_OVERFLOW);
+          ok = false;
+        }
+        V3 cdir = normalize(lp - hr.p);
+        V3 up = fabs(cdir.x) < 0.9 ? mk(1.0, 0.0, 0.0) : mk(0.0, 1.0, 0.0);
+        V3 bu = normalize(cross(up, cdir));
+        V3 bv = normalize(cross(cdir, bu));
+        for (int smp = 0; smp < 16; smp++, s++) {
+          double dx = 0.0, dy = 0.0;
+          if (ok) {
+            for (int it = 0;; it++) {
+              if (it >= 4096 || !rng.range(-radius, radius, &dx) || !rng.range(-radius, radius, &dy)) {
+                atomicOr(F.err, ERR_WATCHDOG);
+                ok = false;
+                break;
+              }
+              if (dx * dx + dy * dy <= radius * radius) break;
+            }
+          }
+          V3 sp = lp + dx * bu + dy * bv;
+          V3 sdir = normalize(sp - hr.p);
+          double dist = norm(sp - hr.p);
+          V3 sd = normalize(sdir);
+          V3 c = light_term(m, hr, sdir, lc, L0.intensity, view);
+          F.sh.dx[s] = sd.x;
+          F.sh.dy[s] = sd.y;
+          F.sh.dz[s] = sd.z;
+          F.sh.dist[s] = ok ? dist : -1.0;  // -1: never traced
+          F.sh.cr[s] = c.x;
+          F.sh.cg[s] = c.y;
+          F.sh.cb[s] = c.z;
+        }
+      }
+    }
+  }
+}
+
+// world.hit(&shadow_ray, 0.001, distance).is_some() per shadow ray
+template <bool COUNT>
+__global__ void __launch_bounds__(128) k_shadow(DFrame F, int level, long long c0) {
+  long long nh = F.nhits[level];
+  long long c1 = c0 + F.chunk_hits < nh ? c0 + F.chunk_hits : nh;
+  const int K = F.S.shadow_per_hit;
+  long long ns = c1 > c0 ? (c1 - c0) * K : 0;
+  Work w{0, 0, 0, 0};
+  for (long long s = blockIdx.x * (long long)blockDim.x + threadIdx.x; s < ns; s += (long long)gridDim.x * blockDim.x) {
+    long long hl = s / K;
+    double dist = F.sh.dist[s];
+    unsigned char vis = 0;
+    if (dist >= 0.0 || dist != dist) {
+      RayC r = make_rayc(mk(F.sh.ox[hl], F.sh.oy[hl], F.sh.oz[hl]), mk(F.sh.dx[s], F.sh.dy[s], F.sh.dz[s]));
+      vis = world_any(F.S, r, 0.001, dist, F.use_kd != 0, F.err, COUNT ? &w : nullptr) ? 0 : 1;
+    }
+    F.sh.vis[s] = vis;
+  }
+  if (COUNT) flush_work(F, w, 1);
+}
+
+// phong_lighting's sum, fog and the reflection ray (src/lighting.rs:220-288,
+// 297-319, 437-496) for hits [c0, c1).
+__global__ void __launch_bounds__(128) k_resolve(DFrame F, int level, long long c0) {
+  const DScene& S = F.S;
+  long long nh = F.nhits[level];
+  long long c1 = c0 + F.chunk_hits < nh ? c0 + F.chunk_hits : nh;
+  const int K = S.shadow_per_hit;
+  RayBuf qn = F.q[(level + 1) & 1];
+  LevelBuf L = F.levels[level];
+  bool can_reflect = (F.max_depth - level) > 1;
+  V3 campos = ld3(F.C.campos);
+  long long stride = (long long)gridDim.x * blockDim.x;
+  for (long long base = c0 + blockIdx.x * (long long)blockDim.x; base < c1; base += stride) {
+    long long h = base + threadIdx.x;
+    bool active = h < c1;
+    bool emit = false;
+    V3 ro = mk(0, 0, 0), rd = mk(0, 0, 0);
+    uint64_t seed = 0;
+    int i = -1;
+    V3 color = mk(0.0, 0.0, 0.0);
+    double refl = 0.0;
+    if (active) {
+      RayC rc;
+      HitRec hr = load_hit(F, level, (int)h, &rc, &seed);
+      i = F.hit_ray[h];
+      const DMat& mat = S.mat[hr.mat];
+      SMat m = effective_material(mat, hr);
+      color = m.ka * S.amb_int * cmul(ld3(S.amb_color), m.c);
+      long long s = (h - c0) * K;
+      for (int li = 0; li < S.n_lights; li++) {
+        const DLight& L0 = S.lights[li];
+        V3 contrib;
+        if (!L0.disk) {
+          contrib = F.sh.vis[s] ? mk(F.sh.cr[s], F.sh.cg[s], F.sh.cb[s]) : mk(0.0, 0.0, 0.0);
+          s++;
+        } else {
+          V3 total = mk(0.0, 0.0, 0.0);
+          unsigned visible = 0;
+          for (int smp = 0; smp < 16; smp++, s++) {
+            if (F.sh.vis[s]) {
+              visible++;
+              total = total + mk(F.sh.cr[s], F.sh.cg[s], F.sh.cb[s]);
+            }
+          }
+          contrib = (total / 16.0) * ((double)visible / 16.0);
+        }
+        color = color + contrib;
+      }
+      if (S.has_fog) {
+        double dist = norm(hr.p - campos);
+        double f;
+        if (dist <= S.fog_start) f = 0.0;
+        else if (dist >= S.fog_end) f = 1.0;
+        else f = (dist - S.fog_start) / (S.fog_end - S.fog_start);
+        f = 1.0 - exp(-S.fog_density * f);
+        f = rclamp(f, 0.0, 1.0);
+        color = color * (1.0 - f) + ld3(S.fog_color) * f;
+      }
+      if (mat.has_refl && mat.refl > 0.0 && can_reflect) {
+        emit = true;
+        refl = mat.refl;
+        V3 vd = normalize(campos - hr.p);
+        ro = hr.p + 0.001 * hr.n;
+        rd = normalize(reflect(-vd, hr.n));
+      }
+      if (level == 0 && F.outline) {
+        F.phit[i] = 1;
+        F.pdepth[i] = norm(hr.p - campos);
+        F.pnx[i] = hr.n.x;
+        F.pny[i] = hr.n.y;
+        F.pnz[i] = hr.n.z;
+      }
+    }
+    int slot = warp_alloc(&F.counts[level + 1], emit);
+    if (active) {
+      L.r[i] = color.x;
+      L.g[i] = color.y;
+      L.b[i] = color.z;
+      L.refl[i] = refl;
+      L.child[i] = slot;
+      if (emit) {
+        qn.ox[slot] = ro.x;
+        qn.oy[slot] = ro.y;
+        qn.oz[slot] = ro.z;
+        qn.dx[slot] = rd.x;
+        qn.dy[slot] = rd.y;
+        qn.dz[slot] = rd.z;
+        qn.seed[slot] = seed;
+      }
+    }
+  }
+}
+
+// color * (1 - r) + reflected * r, deepest level first
+__global__ void k_fold(DFrame F, int level) {
+  int n = F.counts[level];
+  LevelBuf L = F.levels[level];
+  LevelBuf C = F.levels[level + 1];
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    int c = L.child[i];
+    if (c < 0) continue;
+    double r = L.refl[i];
+    double k = 1.0 - r;
+    L.r[i] = L.r[i] * k + C.r[c] * r;
+    L.g[i] = L.g[i] * k + C.g[c] * r;
+    L.b[i] = L.b[i] * k + C.b[c] * r;
+  }
+}
+
+// --------------------------------------------------------------------------
+// Per-pixel resolve, outline, quantise
+// --------------------------------------------------------------------------
+__device__ __forceinline__ void store_rgb(const DFrame& F, long long p, V3 c) {
+  F.rgb[3 * p + 0] = sat_u8(rclamp(c.x, 0.0, 1.0) * 255.0);
+  F.rgb[3 * p + 1] = sat_u8(rclamp(c.y, 0.0, 1.0) * 255.0);
+  F.rgb[3 * p + 2] = sat_u8(rclamp(c.z, 0.0, 1.0) * 255.0);
+  if (F.linear) {
+    F.linear[3 * p + 0] = c.x;
+    F.linear[3 * p + 1] = c.y;
+    F.linear[3 * p + 2] = c.z;
+  }
+}
+
+__global__ void k_pixels(DFrame F) {
+  long long np = (long long)F.W * F.H;
+  LevelBuf L = F.levels[0];
+  for (long long p = blockIdx.x * (long long)blockDim.x + threadIdx.x; p < np; p += (long long)gridDim.x * blockDim.x) {
+    V3 c;
+    if (F.max_depth <= 0) {
+      // ray_color returns black before any World::hit (src/lighting.rs:450-452)
+      c = mk(0.0, 0.0, 0.0);
+      if (F.aa == RT_AA_QUINCUNX) {
+        c = (c + c + c + c + c) / 5.0;
+      } else {
+        V3 t = mk(0.0, 0.0, 0.0);
+        for (int s = 0; s < F.S_per_px; s++) t = t + c;
+        c = t / (double)F.S_per_px;
+      }
+      if (F.outline) F.valid[p] = 0;
+    } else if (F.aa == RT_AA_QUINCUNX) {
+      // (center + tl + tr + bl + br) / 5 (src/renderer.rs:873-886)
+      long long x = p % F.W, y = p / F.W;
+      long long W1 = F.W + 1;
+      long long ci = F.n_corner + p;
+      long long k0 = y * W1 + x, k1 = y * W1 + x + 1, k2 = (y + 1) * W1 + x, k3 = (y + 1) * W1 + x + 1;
+      V3 cc = mk(L.r[ci], L.g[ci], L.b[ci]);
+      V3 c0 = mk(L.r[k0], L.g[k0], L.b[k0]);
+      V3 c1 = mk(L.r[k1], L.g[k1], L.b[k1]);
+      V3 c2 = mk(L.r[k2], L.g[k2], L.b[k2]);
+      V3 c3 = mk(L.r[k3], L.g[k3], L.b[k3]);
+      c = (cc + c0 + c1 + c2 + c3) / 5.0;
+    } else {
+      // sum / samples; outline keeps the nearest sample's depth and normal
+      // (src/renderer.rs:548-552, 690-702)
+      V3 t = mk(0.0, 0.0, 0.0);
+      bool have = false;
+      double pd = 0.0;
+      V3 pn = mk(0.0, 0.0, 0.0);
+      for (int s = 0; s < F.S_per_px; s++) {
+        long long i = p * F.S_per_px + s;
+        t = t + mk(L.r[i], L.g[i], L.b[i]);
+        if (F.outline && F.phit[i]) {
+          double d = F.pdepth[i];
+          if (!have || d < pd) {
+            have = true;
+            pd = d;
+            pn = mk(F.pnx[i], F.pny[i], F.pnz[i]);
+          }
+        }
+      }
+      c = t / (double)F.S_per_px;
+      if (F.outline) {
+        F.valid[p] = have ? 1 : 0;
+        F.dep[p] = pd;
+        F.nx[p] = pn.x;
+        F.ny[p] = pn.y;
+        F.nz[p] = pn.z;
+      }
+    }
+    if (F.outline) {
+      F.cr[p] = c.x;
+      F.cg[p] = c.y;
+      F.cb[p] = c.z;
+    } else {
+      store_rgb(F, p, c);
+    }
+  }
+}
+
+// detect_edges / compute_edge_strength (src/outline.rs:113-182): one tile of
+// OT_X x OT_Y pixels with a one-pixel halo staged in shared memory.
+#define OT_X 32
+#define OT_Y 8
+__global__ void __launch_bounds__(OT_X* OT_Y) k_outline_mask(DFrame F) {
+  __shared__ double sd[OT_Y + 2][OT_X + 2];
+  __shared__ double snx[OT_Y + 2][OT_X + 2], sny[OT_Y + 2][OT_X + 2], snz[OT_Y + 2][OT_X + 2];
+  __shared__ unsigned char sv[OT_Y + 2][OT_X + 2];
+  int x0 = blockIdx.x * OT_X - 1, y0 = blockIdx.y * OT_Y - 1;
+  for (int k = threadIdx.y * OT_X + threadIdx.x; k < (OT_X + 2) * (OT_Y + 2); k += OT_X * OT_Y) {
+    int lx = k % (OT_X + 2), ly = k / (OT_X + 2);
+    int gx = x0 + lx, gy = y0 + ly;
+    unsigned char v = 0;
+    double d = 0, a = 0, b = 0, c = 0;
+    if (gx >= 0 && gy >= 0 && gx < F.W && gy < F.H) {
+      long long p = (long long)gy * F.W + gx;
+      v = F.valid[p];
+      d = F.dep[p];
+      a = F.nx[p];
+      b = F.ny[p];
+      c = F.nz[p];
+    }
+    sv[ly][lx] = v;
+    sd[ly][lx] = d;
+    snx[ly][lx] = a;
+    sny[ly][lx] = b;
+    snz[ly][lx] = c;
+  }
+  __syncthreads();
+  int gx = blockIdx.x * OT_X + threadIdx.x, gy = blockIdx.y * OT_Y + threadIdx.y;
+  if (gx >= F.W || gy >= F.H) return;
+  int lx = threadIdx.x + 1, ly = threadIdx.y + 1;
+  bool cf = sv[ly][lx] != 0;
+  double cd = sd[ly][lx];
+  V3 cn = mk(snx[ly][lx], sny[ly][lx], snz[ly][lx]);
+  // neighbour lists of get_4_neighbors / get_8_neighbors (src/outline.rs:185-224)
+  int ndx[8], ndy[8], nn = 0;
+  if (F.o_use8) {
+    for (int dy = -1; dy <= 1; dy++)
+      for (int dx = -1; dx <= 1; dx++) {
+        if (dx == 0 && dy == 0) continue;
+        if (gx + dx >= 0 && gy + dy >= 0) {
+          ndx[nn] = dx;
+          ndy[nn] = dy;
+          nn++;
+        }
+      }
+  } else {
+    if (gx > 0) { ndx[nn] = -1; ndy[nn] = 0; nn++; }
+    ndx[nn] = 1; ndy[nn] = 0; nn++;
+    if (gy > 0) { ndx[nn] = 0; ndy[nn] = -1; nn++; }
+    ndx[nn] = 0; ndy[nn] = 1; nn++;
+  }
+  double maxe = 0.0;
+  for (int k = 0; k < nn; k++) {
+    int qx = gx + ndx[k], qy = gy + ndy[k];
+    bool nf = false;
+    double nd = 0.0;
+    V3 nnv = mk(0, 0, 0);
+    if (qx < F.W && qy < F.H) {  // get_depth / get_normal bounds (src/outline.rs:68-82)
+      nf = sv[ly + ndy[k]][lx + ndx[k]] != 0;
+      nd = sd[ly + ndy[k]][lx + ndx[k]];
+      nnv = mk(snx[ly + ndy[k]][lx + ndx[k]], sny[ly + ndy[k]][lx + ndx[k]], snz[ly + ndy[k]][lx + ndx[k]]);
+    }
+    double e;
+    if (cf && nf) {
+      double dd = fabs(cd - nd);
+      double ndd = dd / rmax(cd * 0.1, 0.1);
+      double dp = rclamp(dot(cn, nnv), -1.0, 1.0);
+      e = F.o_wd * ndd + F.o_wn * (1.0 - dp);
+    } else if (cf != nf) {
+      e = F.o_wd * 2.0 + F.o_wn * 2.0;
+    } else {
+      e = 0.0;
+    }
+    maxe = rmax(maxe, e);
+  }
+  double m = 0.0;
+  if (maxe > F.o_thr) m = (maxe - F.o_thr) / rmax(1.0 - F.o_thr, 0.001);
+  F.mask[(long long)gy * F.W + gx] = m;
+}
+
+// dilate_edges + blend_colors + quantise (src/outline.rs:227-278,
+// src/renderer.rs:899-912); the mask tile with a halo of `radius` pixels is
+// staged in dynamic shared memory.
+__global__ void __launch_bounds__(OT_X* OT_Y) k_outline_apply(DFrame F) {
+  extern __shared__ double sm[];
+  int R = F.o_radius;
+  int TW = OT_X + 2 * R, TH = OT_Y + 2 * R;
+  int x0 = blockIdx.x * OT_X - R, y0 = blockIdx.y * OT_Y - R;
+  for (int k = threadIdx.y * OT_X + threadIdx.x; k < TW * TH; k += OT_X * OT_Y) {
+    int lx = k % TW, ly = k / TW;
+    int gx = x0 + lx, gy = y0 + ly;
+    double v = 0.0;
+    if (gx >= 0 && gy >= 0 && gx < F.W && gy < F.H) v = F.mask[(long long)gy * F.W + gx];
+    sm[k] = v;
+  }
+  __syncthreads();
+  int gx = blockIdx.x * OT_X + threadIdx.x, gy = blockIdx.y * OT_Y + threadIdx.y;
+  if (gx >= F.W || gy >= F.H) return;
+  int lx = threadIdx.x + R, ly = threadIdx.y + R;
+  double ms = sm[ly * TW + lx];
+  if (R > 0) {
+    double th = F.o_thick;
+    for (int dy = -R; dy <= R; dy++)
+      for (int dx = -R; dx <= R; dx++) {
+        int nx = gx + dx, ny = gy + dy;
+        if (nx >= 0 && ny >= 0 && nx < F.W && ny < F.H) {
+          double dist = sqrt((double)(dx * dx + dy * dy));
+          if (dist <= th) {
+            double fo = 1.0 - (dist / th);
+            ms = rmax(ms, sm[(ly + dy) * TW + (lx + dx)] * fo);
+          }
+        }
+      }
+  }
+  long long p = (long long)gy * F.W + gx;
+  V3 c = mk(F.cr[p], F.cg[p], F.cb[p]);
+  if (ms > 0.0) {
+    double w = rclamp(rmin(ms, 1.0), 0.0, 1.0);
+    c = mk(c.x * (1.0 - w) + F.o_color[0] * w, c.y * (1.0 - w) + F.o_color[1] * w,
+           c.z * (1.0 - w) + F.o_color[2] * w);
+  }
+  store_rgb(F, p, c);
+}
+
+// --------------------------------------------------------------------------
+// Unit kernels for the parity tests and the FP64 rate probe
+// --------------------------------------------------------------------------
+// Eight independent add/multiply chains per thread; each iteration issues
+// 16 FP64 add and 16 FP64 multiply instructions.
+__global__ void k_fp64_rate(double* out, int iters, double a, double b) {
+  double x[8], y[8];
+  for (int k = 0; k < 8; k++) {
+    x[k] = threadIdx.x * 1e-3 + k;
+    y[k] = blockIdx.x * 1e-3 + k;
+  }
+  for (int i = 0; i < iters; i++) {
+#pragma unroll
+    for (int k = 0; k < 8; k++) {
+      x[k] = x[k] * a + b;
+      y[k] = y[k] * b + a;
+    }
+  }
+  double s = 0;
+  for (int k = 0; k < 8; k++) s += x[k] + y[k];
+  if (s == 12345.678) out[0] = s;  // keeps the chains live
+}
+__global__ void k_debug_rng(const uint64_t* seeds, long long n, int nw, uint32_t* out) {
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
+    StdRng r;
+    r.init(seeds[i]);
+    for (int k = 0; k < nw; k++) out[i * nw + k] = r.u32();
+  }
+}
+__global__ void k_debug_disk(const uint64_t* seeds, long long n, double radius, double* out, int* err) {
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
+    StdRng r;
+    r.init(seeds[i]);
+    for (int s = 0; s < 16; s++) {
+      double dx = 0, dy = 0;
+      for (int it = 0;; it++) {
+        if (it >= 4096 || !r.range(-radius, radius, &dx) || !r.range(-radius, radius, &dy)) {
+          atomicOr(err, ERR_WATCHDOG);
+          break;
+        }
+        if (dx * dx + dy * dy <= radius * radius) break;
+      }
+      out[i * 32 + 2 * s] = dx;
+      out[i * 32 + 2 * s + 1] = dy;
+    }
+  }
+}
+// mode 0: mesh_closest (BVH + verification), 1: exact k-d walk, 2: mesh_any
+__global__ void k_debug_mesh(DMesh M, int use_kd, int mode, const double* rays, long long n, double tmin,
+                             double tmax, double* out, int* err) {
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
+    const double* rr = rays + 6 * i;
+    V3 o = mk(rr[0], rr[1], rr[2]);
+    V3 d = normalize(mk(rr[3], rr[4], rr[5]));
+    RayC r = make_rayc(o, d);
+    double closest = tmax;
+    int best = -1;
+    double* oo = out + 8 * i;
+    for (int k = 0; k < 8; k++) oo[k] = 0.0;
+    if (mode == 2) {
+      oo[0] = mesh_any(M, r, tmin, tmax, use_kd != 0, err, nullptr) ? 1.0 : 0.0;
+      continue;
+    }
+    bool hit = mode == 0 ? mesh_closest(M, r, tmin, closest, best, use_kd != 0, err, nullptr)
+                         : (mesh_bounds(M, r, tmin, closest) &&
+                            mesh_kd_walk<false>(M, r, tmin, closest, best, err, nullptr));
+    if (hit) {
+      const double2* E = M.brute + 5 * (size_t)best;
+      double2 q1 = E[1], q2 = E[2], q3 = E[3], q4 = E[4];
+      V3 e1 = mk(q1.y, q2.x, q2.y), e2 = mk(q3.x, q3.y, q4.x);
+      double a = dot(e1, cross(r.d, e2));
+      double4 nn = M.normals[best];
+      V3 nv = mk(nn.x, nn.y, nn.z);
+      if (a < 0.0) nv = -nv;
+      V3 p = r.o + closest * r.d;
+      V3 fn = face_normal(r.d, nv);
+      oo[0] = 1.0;
+      oo[1] = closest;
+      oo[2] = p.x;
+      oo[3] = p.y;
+      oo[4] = p.z;
+      oo[5] = fn.x;
+      oo[6] = fn.y;
+      oo[7] = fn.z;
+    }
+  }
+}
+
+}  // namespace rtb

@@ -1,21 +1,10 @@
-// Wavefront render pipeline for SeaRyanC/rtrace scenes on B200 (sm_100a)
-// and the C ABI of include/rtrace_gpu.h.
+// Render orchestration and the C ABI of include/rtrace_gpu.h.
 //
-// One render = one pass per reflection depth over a compacted ray queue:
-//   k_raygen      camera rays for the three anti-aliasing modes
-//                 (src/renderer.rs:445-584, 752-897)
-//   k_trace       closest hit per queued ray (World::hit, src/ray.rs:699)
-//   k_shade       Phong + textures + point/area-light shadow rays + fog
-//                 (src/lighting.rs:9-319); reflective hits append their
-//                 reflection ray to the next queue (warp ballot + one
-//                 atomic per warp)
-//   k_fold        the reflection recursion's blend, deepest level first
-//                 (src/lighting.rs:469-493)
-//   k_resolve     quincunx / sample average per pixel, outline buffers,
-//                 quantisation (src/renderer.rs:552, 702, 881-886, 899-912)
-//   k_outline_*   edge mask, dilation and blend (src/outline.rs:86-278)
-// All arithmetic is IEEE double in the reference's operation order
-// (compile with -fmad=false).
+// A render is the wavefront pipeline of kernels.cuh: camera rays, then per
+// reflection depth trace -> emit -> shadow -> resolve over compacted
+// queues, then the reflection fold (deepest level first), the per-pixel
+// resolve and the outline post-process.  All arithmetic is IEEE double in
+// the reference's operation order (compile with -fmad=false).
 
 #include <cuda_runtime.h>
 
@@ -30,682 +19,24 @@
 #include <vector>
 
 #include "../../include/rtrace_gpu.h"
-#include "dscene.cuh"
+#include "bvh_build.hpp"
+#include "kernels.cuh"
 #include "scene_loader.hpp"
 
-namespace rtb {
-
-// --------------------------------------------------------------------------
-// Frame state passed by value to every kernel
-// --------------------------------------------------------------------------
-struct RayBuf {
-  double *ox, *oy, *oz, *dx, *dy, *dz;
-  uint64_t* seed;
-};
-struct LevelBuf {
-  double *r, *g, *b, *refl;
-  int* child;
-};
-
-#define RTB_MAX_LEVELS 64
-
-struct DFrame {
-  DScene S;
-  DCam C;
-  int W, H, S_per_px, aa, max_depth, use_kd, outline, camera_mode;
-  uint64_t seed;
-  long long n_primary;
-  long long n_corner;  // quincunx corner rays, (W+1)(H+1)
-  RayBuf q[2];
-  int* hobj;
-  int* haux;
-  double* ht;
-  LevelBuf* levels;  // device array [max_depth]
-  int* counts;       // device [max_depth + 1]
-  // per primary ray outline data
-  double *pdepth, *pnx, *pny, *pnz;
-  unsigned char* phit;
-  // per pixel
-  double *cr, *cg, *cb;
-  double *dep, *nx, *ny, *nz;
-  unsigned char* valid;
-  double* mask;
-  unsigned char* rgb;
-  double* linear;  // optional pixel colours (3 per pixel) before quantisation
-  unsigned long long* stats;  // [0] shadow rays
-  int* err;
-  // outline parameters
-  double o_wd, o_wn, o_thr, o_color[3], o_thick;
-  int o_use8, o_radius;
-};
-
-// --------------------------------------------------------------------------
-// Camera rays
-// --------------------------------------------------------------------------
-// Camera::get_ray (src/camera.rs:155-167) followed by Ray::new's normalise
-__device__ __forceinline__ void camera_ray(const DCam& c, double u, double v, V3* o, V3* d) {
-  V3 vp = ld3(c.llc) + u * ld3(c.hor) + v * ld3(c.ver);
-  if (c.persp) {
-    V3 dir = normalize(vp - ld3(c.origin));
-    *o = ld3(c.origin);
-    *d = normalize(dir);
-  } else {
-    *o = vp;
-    *d = normalize(ld3(c.vdir));
-  }
-}
-
-__global__ void k_raygen(DFrame F) {
-  const uint64_t GOLD = 0x9E3779B97F4A7C15ULL;
-  long long n = F.n_primary;
-  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
-    double u, v;
-    uint64_t seed;
-    if (F.aa == RT_AA_QUINCUNX) {
-      // render_quincunx (src/renderer.rs:752-897)
-      double pw = 1.0 / (double)F.W, ph = 1.0 / (double)F.H;
-      if (i < F.n_corner) {
-        unsigned cx = (unsigned)(i % (F.W + 1)), cy = (unsigned)(i / (F.W + 1));
-        u = rclamp((double)cx * pw, 0.0, 1.0);
-        v = rclamp(1.0 - (double)cy * ph, 0.0, 1.0);
-        seed = F.seed * GOLD + (uint64_t)cx + (uint64_t)cy * 0x85EBCA6BULL;
-      } else {
-        long long j = i - F.n_corner;
-        unsigned x = (unsigned)(j % F.W), y = (unsigned)(j / F.W);
-        u = ((double)x + 0.5) * pw;
-        v = 1.0 - ((double)y + 0.5) * ph;
-        seed = F.seed * GOLD + (uint64_t)x * 0x85EBCA6BULL + (uint64_t)y * 0xC2B2AE35ULL + 0x12345678ULL;
-      }
-    } else {
-      // render_standard (src/renderer.rs:445-584)
-      long long pix = i / F.S_per_px;
-      unsigned s = (unsigned)(i % F.S_per_px);
-      unsigned x = (unsigned)(pix % F.W), y = (unsigned)(pix / F.W);
-      double wm1 = (double)(unsigned)(F.W - 1), hm1 = (double)(unsigned)(F.H - 1);
-      double pu = (double)x / wm1;
-      double pv = (double)(unsigned)(F.H - 1 - y) / hm1;
-      double pwid = 1.0 / wm1, phei = 1.0 / hm1;
-      uint64_t pseed = F.seed * GOLD + (uint64_t)x * 0x85EBCA6BULL + (uint64_t)y * 0xC2B2AE35ULL;
-      seed = pseed + (uint64_t)s * 0x1F845FEDULL;
-      if (F.aa == RT_AA_NO_JITTER) {
-        u = pu;
-        v = pv;
-      } else {
-        // The pixel's StdRng stream: sample s draws u64 number 2s and 2s+1
-        // (samples == 1: numbers 0 and 1), i.e. words 4s..4s+3, which sit in
-        // ChaCha block s / 4.
-        uint32_t key[8], blk[16];
-        pcg32_key(pseed, key);
-        chacha_block(key, (uint64_t)(s >> 2), 6, blk);
-        int w0 = 4 * (s & 3);
-        uint64_t r0 = ((uint64_t)blk[w0 + 1] << 32) | blk[w0];
-        uint64_t r1 = ((uint64_t)blk[w0 + 3] << 32) | blk[w0 + 2];
-        const double scale = 1.0 / 9007199254740992.0;
-        double f0 = scale * (double)(r0 >> 11), f1 = scale * (double)(r1 >> 11);
-        if (F.S_per_px == 1) {
-          double ju = f0 - 0.5, jv = f1 - 0.5;
-          u = pu + ju * pwid;
-          v = pv + jv * phei;
-        } else {
-          const double PI = 3.141592653589793;
-          double ang = 2.0 * PI * (double)s / (double)F.S_per_px;
-          double phase = f0 * 2.0 * PI;
-          double ra = ang + phase;
-          double rad = 0.5 * f1;
-          double ju = rad * cos(ra), jv = rad * sin(ra);
-          u = pu + ju * pwid;
-          v = pv + jv * phei;
-        }
-      }
-    }
-    V3 o, d;
-    camera_ray(F.C, u, v, &o, &d);
-    RayBuf q = F.q[0];
-    q.ox[i] = o.x;
-    q.oy[i] = o.y;
-    q.oz[i] = o.z;
-    q.dx[i] = d.x;
-    q.dy[i] = d.y;
-    q.dz[i] = d.z;
-    q.seed[i] = seed;
-  }
-}
-
-// --------------------------------------------------------------------------
-// Closest hit
-// --------------------------------------------------------------------------
-__global__ void __launch_bounds__(128) k_trace(DFrame F, int level) {
-  int n = F.counts[level];
-  RayBuf q = F.q[level & 1];
-  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
-    V3 o = mk(q.ox[i], q.oy[i], q.oz[i]);
-    V3 d = mk(q.dx[i], q.dy[i], q.dz[i]);
-    RayC r = make_rayc(o, d);
-    WHit h = world_closest(F.S, r, 0.001, F.use_kd != 0, F.err);
-    F.hobj[i] = h.obj;
-    F.haux[i] = h.aux;
-    F.ht[i] = h.t;
-  }
-}
-
-// --------------------------------------------------------------------------
-// Shading
-// --------------------------------------------------------------------------
-struct SMat {
-  V3 c;
-  double ka, kd, ks, shin;
-};
-
-// apply_texture (src/lighting.rs:9-54) + the colour parse of phong_lighting
-__device__ __forceinline__ SMat effective_material(const DMat& m, const HitRec& h) {
-  SMat s;
-  s.c = ld3(m.color);
-  s.ka = m.ambient;
-  s.kd = m.diffuse;
-  s.ks = m.specular;
-  s.shin = m.shininess;
-  if (h.has_uv) {
-    if (m.texture == 1) {
-      double um = fabs(rfract(h.u / m.cell_size));
-      double vm = fabs(rfract(h.v / m.cell_size));
-      double hw = m.half_width;
-      bool onu = um <= hw || um >= (1.0 - hw);
-      bool onv = vm <= hw || vm >= (1.0 - hw);
-      if (onu || onv) s.c = ld3(m.grid_color);
-    } else if (m.texture == 2) {
-      int32_t cu = sat_i32(floor(h.u)), cv = sat_i32(floor(h.v));
-      int32_t sum = (int32_t)((uint32_t)cu + (uint32_t)cv);
-      if (sum % 2 != 0) {
-        s.c = ld3(m.cb_color);
-        s.ka = m.cb_ambient;
-        s.kd = m.cb_diffuse;
-        s.ks = m.cb_specular;
-        s.shin = m.cb_shininess;
-      }
-    }
-  }
-  return s;
-}
-
-// diffuse + specular of one light sample (src/lighting.rs:124-141, 191-208)
-__device__ __forceinline__ V3 light_term(const SMat& m, const HitRec& h, V3 ldir, V3 lc, double li, V3 view) {
-  double ds = rmax(dot(h.n, ldir), 0.0);
-  V3 diffuse = m.kd * ds * li * cmul(lc, m.c);
-  V3 spec = mk(0.0, 0.0, 0.0);
-  if (ds > 0.0) {
-    V3 rd = reflect(-ldir, h.n);
-    double ss = pow(rmax(dot(view, rd), 0.0), m.shin);
-    spec = m.ks * ss * li * lc;
-  }
-  return diffuse + spec;
-}
-
-__device__ __forceinline__ int warp_alloc(int* counter, bool want) {
-  unsigned m = __ballot_sync(0xffffffffu, want);
-  int lane = threadIdx.x & 31;
-  int base = 0;
-  if (m) {
-    int leader = __ffs(m) - 1;
-    if (lane == leader) base = atomicAdd(counter, __popc(m));
-    base = __shfl_sync(0xffffffffu, base, leader);
-  }
-  return want ? base + __popc(m & ((1u << lane) - 1u)) : -1;
-}
-
-__global__ void __launch_bounds__(128) k_shade(DFrame F, int level) {
-  const DScene& S = F.S;
-  int n = F.counts[level];
-  RayBuf q = F.q[level & 1];
-  RayBuf qn = F.q[(level + 1) & 1];
-  LevelBuf L = F.levels[level];
-  bool can_reflect = (F.max_depth - level) > 1;
-  V3 campos = ld3(F.C.campos);
-  int stride = gridDim.x * blockDim.x;
-  // uniform trip count per warp so the ballot below sees every lane
-  for (int base = blockIdx.x * blockDim.x; base < n; base += stride) {
-    int i = base + threadIdx.x;
-    bool active = i < n;
-    bool emit = false;
-    V3 ro, rd;
-    V3 color = mk(0.0, 0.0, 0.0);
-    double refl = 0.0;
-    int hitp = 0;
-    uint64_t seed = 0;
-    if (active) {
-      V3 o = mk(q.ox[i], q.oy[i], q.oz[i]);
-      V3 d = mk(q.dx[i], q.dy[i], q.dz[i]);
-      seed = q.seed[i];
-      WHit w{F.hobj[i], F.haux[i], F.ht[i]};
-      if (w.obj < 0) {
-        // miss: grid background (camera = Some) or the background colour
-        V3 g;
-        if (F.camera_mode && grid_color(F.C, o, d, &g)) color = g;
-        else color = ld3(S.bg);
-        if (level == 0 && F.outline) F.phit[i] = 0;
-      } else {
-        hitp = 1;
-        RayC r = make_rayc(o, d);
-        HitRec h = finalize_hit(S, r, w, F.use_kd != 0);
-        const DMat& mat = S.mat[h.mat];
-        SMat m = effective_material(mat, h);
-        // phong_lighting (src/lighting.rs:220-288)
-        color = m.ka * S.amb_int * cmul(ld3(S.amb_color), m.c);
-        V3 view = normalize(campos - h.p);
-        V3 so = h.p + 0.001 * h.n;
-        for (int li = 0; li < S.n_lights; li++) {
-          const DLight& L0 = S.lights[li];
-          V3 lp = ld3(L0.pos), lc = ld3(L0.color);
-          V3 contrib;
-          if (!L0.disk) {
-            // calculate_point_light_contribution (src/lighting.rs:100-142)
-            V3 ldir = normalize(lp - h.p);
-            double dist = norm(lp - h.p);
-            RayC sr = make_rayc(so, normalize(ldir));
-            if (world_any(S, sr, 0.001, dist, F.use_kd != 0, F.err)) contrib = mk(0.0, 0.0, 0.0);
-            else contrib = light_term(m, h, ldir, lc, L0.intensity, view);
-          } else {
-            // calculate_diffuse_light_contribution (src/lighting.rs:145-217)
-            uint64_t ls = seed * 0x9E3779B97F4A7C15ULL + sat_u64(h.p.x * 1000.0) * 0x85EBCA6BULL +
-                          sat_u64(h.p.y * 1000.0) * 0xC2B2AE35ULL + sat_u64(h.p.z * 1000.0) * 0x6C8E9CF5ULL;
-            StdRng rng;
-            rng.init(ls);
-            double radius = L0.diameter / 2.0;
-            V3 total = mk(0.0, 0.0, 0.0);
-            unsigned visible = 0;
-            // gen_range(-radius..radius) panics on an empty or infinite range
-            bool ok = -radius < radius;
-            if (!ok) atomicOr(F.err, ERR_EMPTY_RANGE);
-            if (ok && !isfinite(radius - -radius)) {
-              atomicOr(F.err, ERR_RANGE_OVERFLOW);
-              ok = false;
-            }
-            // sample_disk_light_point's basis (src/lighting.rs:75-90)
-            V3 cdir = normalize(lp - h.p);
-            V3 up = fabs(cdir.x) < 0.9 ? mk(1.0, 0.0, 0.0) : mk(0.0, 1.0, 0.0);
-            V3 bu = normalize(cross(up, cdir));
-            V3 bv = normalize(cross(cdir, bu));
-            for (int smp = 0; smp < 16 && ok; smp++) {
-              double dx = 0.0, dy = 0.0;
-              int it = 0;
-              for (;; it++) {
-                if (it >= 4096 || !rng.range(-radius, radius, &dx) || !rng.range(-radius, radius, &dy)) {
-                  atomicOr(F.err, ERR_WATCHDOG);
-                  ok = false;
-                  break;
-                }
-                if (dx * dx + dy * dy <= radius * radius) break;
-              }
-              if (!ok) break;
-              V3 sp = lp + dx * bu + dy * bv;
-              V3 sdir = normalize(sp - h.p);
-              double dist = norm(sp - h.p);
-              RayC sr = make_rayc(so, normalize(sdir));
-              if (world_any(S, sr, 0.001, dist, F.use_kd != 0, F.err)) continue;
-              visible++;
-              total = total + light_term(m, h, sdir, lc, L0.intensity, view);
-            }
-            contrib = (total / 16.0) * ((double)visible / 16.0);
-          }
-          color = color + contrib;
-        }
-        // apply_fog (src/lighting.rs:297-319)
-        if (S.has_fog) {
-          double dist = norm(h.p - campos);
-          double f;
-          if (dist <= S.fog_start) f = 0.0;
-          else if (dist >= S.fog_end) f = 1.0;
-          else f = (dist - S.fog_start) / (S.fog_end - S.fog_start);
-          f = 1.0 - exp(-S.fog_density * f);
-          f = rclamp(f, 0.0, 1.0);
-          color = color * (1.0 - f) + ld3(S.fog_color) * f;
-        }
-        if (mat.has_refl && mat.refl > 0.0 && can_reflect) {
-          emit = true;
-          refl = mat.refl;
-          V3 vd = normalize(campos - h.p);
-          ro = h.p + 0.001 * h.n;
-          rd = normalize(reflect(-vd, h.n));
-        }
-        if (level == 0 && F.outline) {
-          F.phit[i] = 1;
-          F.pdepth[i] = norm(h.p - campos);
-          F.pnx[i] = h.n.x;
-          F.pny[i] = h.n.y;
-          F.pnz[i] = h.n.z;
-        }
-      }
-    }
-    unsigned long long hits = (unsigned long long)__popc(__ballot_sync(0xffffffffu, hitp != 0));
-    if ((threadIdx.x & 31) == 0 && hits) atomicAdd(&F.stats[0], hits * (unsigned long long)S.shadow_per_hit);
-    int slot = warp_alloc(&F.counts[level + 1], emit);
-    if (active) {
-      L.r[i] = color.x;
-      L.g[i] = color.y;
-      L.b[i] = color.z;
-      L.refl[i] = refl;
-      L.child[i] = slot;
-      if (emit) {
-        qn.ox[slot] = ro.x;
-        qn.oy[slot] = ro.y;
-        qn.oz[slot] = ro.z;
-        qn.dx[slot] = rd.x;
-        qn.dy[slot] = rd.y;
-        qn.dz[slot] = rd.z;
-        qn.seed[slot] = seed;
-      }
-    }
-  }
-}
-
-// color * (1 - r) + reflected * r, deepest level first
-__global__ void k_fold(DFrame F, int level) {
-  int n = F.counts[level];
-  LevelBuf L = F.levels[level];
-  LevelBuf C = F.levels[level + 1];
-  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
-    int c = L.child[i];
-    if (c < 0) continue;
-    double r = L.refl[i];
-    double k = 1.0 - r;
-    L.r[i] = L.r[i] * k + C.r[c] * r;
-    L.g[i] = L.g[i] * k + C.g[c] * r;
-    L.b[i] = L.b[i] * k + C.b[c] * r;
-  }
-}
-
-// --------------------------------------------------------------------------
-// Per-pixel resolve, outline, quantise
-// --------------------------------------------------------------------------
-__device__ __forceinline__ void store_rgb(const DFrame& F, long long p, V3 c) {
-  F.rgb[3 * p + 0] = sat_u8(rclamp(c.x, 0.0, 1.0) * 255.0);
-  F.rgb[3 * p + 1] = sat_u8(rclamp(c.y, 0.0, 1.0) * 255.0);
-  F.rgb[3 * p + 2] = sat_u8(rclamp(c.z, 0.0, 1.0) * 255.0);
-  if (F.linear) {
-    F.linear[3 * p + 0] = c.x;
-    F.linear[3 * p + 1] = c.y;
-    F.linear[3 * p + 2] = c.z;
-  }
-}
-
-__global__ void k_resolve(DFrame F) {
-  long long np = (long long)F.W * F.H;
-  LevelBuf L = F.levels[0];
-  for (long long p = blockIdx.x * (long long)blockDim.x + threadIdx.x; p < np; p += (long long)gridDim.x * blockDim.x) {
-    V3 c;
-    if (F.max_depth <= 0) {
-      c = mk(0.0, 0.0, 0.0);
-      if (F.aa == RT_AA_QUINCUNX) {
-        c = (c + c + c + c + c) / 5.0;
-      } else {
-        V3 t = mk(0.0, 0.0, 0.0);
-        for (int s = 0; s < F.S_per_px; s++) t = t + c;
-        c = t / (double)F.S_per_px;
-      }
-      if (F.outline) F.valid[p] = 0;
-    } else if (F.aa == RT_AA_QUINCUNX) {
-      long long x = p % F.W, y = p / F.W;
-      long long W1 = F.W + 1;
-      long long ci = F.n_corner + p;
-      long long k0 = y * W1 + x, k1 = y * W1 + x + 1, k2 = (y + 1) * W1 + x, k3 = (y + 1) * W1 + x + 1;
-      V3 cc = mk(L.r[ci], L.g[ci], L.b[ci]);
-      V3 c0 = mk(L.r[k0], L.g[k0], L.b[k0]);
-      V3 c1 = mk(L.r[k1], L.g[k1], L.b[k1]);
-      V3 c2 = mk(L.r[k2], L.g[k2], L.b[k2]);
-      V3 c3 = mk(L.r[k3], L.g[k3], L.b[k3]);
-      c = (cc + c0 + c1 + c2 + c3) / 5.0;
-    } else {
-      V3 t = mk(0.0, 0.0, 0.0);
-      bool have = false;
-      double pd = 0.0;
-      V3 pn = mk(0.0, 0.0, 0.0);
-      for (int s = 0; s < F.S_per_px; s++) {
-        long long i = p * F.S_per_px + s;
-        t = t + mk(L.r[i], L.g[i], L.b[i]);
-        if (F.outline && F.phit[i]) {
-          double d = F.pdepth[i];
-          if (!have || d < pd) {
-            have = true;
-            pd = d;
-            pn = mk(F.pnx[i], F.pny[i], F.pnz[i]);
-          }
-        }
-      }
-      c = t / (double)F.S_per_px;
-      if (F.outline) {
-        F.valid[p] = have ? 1 : 0;
-        F.dep[p] = pd;
-        F.nx[p] = pn.x;
-        F.ny[p] = pn.y;
-        F.nz[p] = pn.z;
-      }
-    }
-    if (F.outline) {
-      F.cr[p] = c.x;
-      F.cg[p] = c.y;
-      F.cb[p] = c.z;
-    } else {
-      store_rgb(F, p, c);
-    }
-  }
-}
-
-// detect_edges / compute_edge_strength (src/outline.rs:113-182): one tile of
-// TX x TY pixels with a one-pixel halo staged in shared memory.
-#define OT_X 32
-#define OT_Y 8
-__global__ void __launch_bounds__(OT_X* OT_Y) k_outline_mask(DFrame F) {
-  __shared__ double sd[OT_Y + 2][OT_X + 2];
-  __shared__ double snx[OT_Y + 2][OT_X + 2], sny[OT_Y + 2][OT_X + 2], snz[OT_Y + 2][OT_X + 2];
-  __shared__ unsigned char sv[OT_Y + 2][OT_X + 2];
-  int x0 = blockIdx.x * OT_X - 1, y0 = blockIdx.y * OT_Y - 1;
-  for (int k = threadIdx.y * OT_X + threadIdx.x; k < (OT_X + 2) * (OT_Y + 2); k += OT_X * OT_Y) {
-    int lx = k % (OT_X + 2), ly = k / (OT_X + 2);
-    int gx = x0 + lx, gy = y0 + ly;
-    unsigned char v = 0;
-    double d = 0, a = 0, b = 0, c = 0;
-    if (gx >= 0 && gy >= 0 && gx < F.W && gy < F.H) {
-      long long p = (long long)gy * F.W + gx;
-      v = F.valid[p];
-      d = F.dep[p];
-      a = F.nx[p];
-      b = F.ny[p];
-      c = F.nz[p];
-    }
-    sv[ly][lx] = v;
-    sd[ly][lx] = d;
-    snx[ly][lx] = a;
-    sny[ly][lx] = b;
-    snz[ly][lx] = c;
-  }
-  __syncthreads();
-  int gx = blockIdx.x * OT_X + threadIdx.x, gy = blockIdx.y * OT_Y + threadIdx.y;
-  if (gx >= F.W || gy >= F.H) return;
-  int lx = threadIdx.x + 1, ly = threadIdx.y + 1;
-  bool cf = sv[ly][lx] != 0;
-  double cd = sd[ly][lx];
-  V3 cn = mk(snx[ly][lx], sny[ly][lx], snz[ly][lx]);
-  // neighbour lists of get_4_neighbors / get_8_neighbors (src/outline.rs:185-224)
-  int ndx[8], ndy[8], nn = 0;
-  if (F.o_use8) {
-    for (int dy = -1; dy <= 1; dy++)
-      for (int dx = -1; dx <= 1; dx++) {
-        if (dx == 0 && dy == 0) continue;
-        if (gx + dx >= 0 && gy + dy >= 0) {
-          ndx[nn] = dx;
-          ndy[nn] = dy;
-          nn++;
-        }
-      }
-  } else {
-    if (gx > 0) { ndx[nn] = -1; ndy[nn] = 0; nn++; }
-    ndx[nn] = 1; ndy[nn] = 0; nn++;
-    if (gy > 0) { ndx[nn] = 0; ndy[nn] = -1; nn++; }
-    ndx[nn] = 0; ndy[nn] = 1; nn++;
-  }
-  double maxe = 0.0;
-  for (int k = 0; k < nn; k++) {
-    int qx = gx + ndx[k], qy = gy + ndy[k];
-    bool nf = false;
-    double nd = 0.0;
-    V3 nnv = mk(0, 0, 0);
-    if (qx < F.W && qy < F.H) {  // get_depth / get_normal bounds (src/outline.rs:68-82)
-      nf = sv[ly + ndy[k]][lx + ndx[k]] != 0;
-      nd = sd[ly + ndy[k]][lx + ndx[k]];
-      nnv = mk(snx[ly + ndy[k]][lx + ndx[k]], sny[ly + ndy[k]][lx + ndx[k]], snz[ly + ndy[k]][lx + ndx[k]]);
-    }
-    double e;
-    if (cf && nf) {
-      double dd = fabs(cd - nd);
-      double ndd = dd / rmax(cd * 0.1, 0.1);
-      double dp = rclamp(dot(cn, nnv), -1.0, 1.0);
-      e = F.o_wd * ndd + F.o_wn * (1.0 - dp);
-    } else if (cf != nf) {
-      e = F.o_wd * 2.0 + F.o_wn * 2.0;
-    } else {
-      e = 0.0;
-    }
-    maxe = rmax(maxe, e);
-  }
-  double m = 0.0;
-  if (maxe > F.o_thr) m = (maxe - F.o_thr) / rmax(1.0 - F.o_thr, 0.001);
-  F.mask[(long long)gy * F.W + gx] = m;
-}
-
-// dilate_edges + blend_colors + quantise (src/outline.rs:227-278,
-// src/renderer.rs:899-912); the mask tile with a halo of `radius` pixels is
-// staged in dynamic shared memory.
-__global__ void __launch_bounds__(OT_X* OT_Y) k_outline_apply(DFrame F) {
-  extern __shared__ double sm[];
-  int R = F.o_radius;
-  int TW = OT_X + 2 * R, TH = OT_Y + 2 * R;
-  int x0 = blockIdx.x * OT_X - R, y0 = blockIdx.y * OT_Y - R;
-  for (int k = threadIdx.y * OT_X + threadIdx.x; k < TW * TH; k += OT_X * OT_Y) {
-    int lx = k % TW, ly = k / TW;
-    int gx = x0 + lx, gy = y0 + ly;
-    double v = 0.0;
-    if (gx >= 0 && gy >= 0 && gx < F.W && gy < F.H) v = F.mask[(long long)gy * F.W + gx];
-    sm[k] = v;
-  }
-  __syncthreads();
-  int gx = blockIdx.x * OT_X + threadIdx.x, gy = blockIdx.y * OT_Y + threadIdx.y;
-  if (gx >= F.W || gy >= F.H) return;
-  int lx = threadIdx.x + R, ly = threadIdx.y + R;
-  double ms = sm[ly * TW + lx];
-  if (R > 0) {
-    double th = F.o_thick;
-    for (int dy = -R; dy <= R; dy++)
-      for (int dx = -R; dx <= R; dx++) {
-        int nx = gx + dx, ny = gy + dy;
-        if (nx >= 0 && ny >= 0 && nx < F.W && ny < F.H) {
-          double dist = sqrt((double)(dx * dx + dy * dy));
-          if (dist <= th) {
-            double fo = 1.0 - (dist / th);
-            ms = rmax(ms, sm[(ly + dy) * TW + (lx + dx)] * fo);
-          }
-        }
-      }
-  }
-  long long p = (long long)gy * F.W + gx;
-  V3 c = mk(F.cr[p], F.cg[p], F.cb[p]);
-  if (ms > 0.0) {
-    double w = rclamp(rmin(ms, 1.0), 0.0, 1.0);
-    c = mk(c.x * (1.0 - w) + F.o_color[0] * w, c.y * (1.0 - w) + F.o_color[1] * w, c.z * (1.0 - w) + F.o_color[2] * w);
-  }
-  store_rgb(F, p, c);
-}
-
-// --------------------------------------------------------------------------
-// Debug / unit kernels for the parity tests
-// --------------------------------------------------------------------------
-__global__ void k_debug_rng(const uint64_t* seeds, long long n, int nw, uint32_t* out) {
-  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
-    StdRng r;
-    r.init(seeds[i]);
-    for (int k = 0; k < nw; k++) out[i * nw + k] = r.u32();
-  }
-}
-__global__ void k_debug_disk(const uint64_t* seeds, long long n, double radius, double* out, int* err) {
-  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
-    StdRng r;
-    r.init(seeds[i]);
-    for (int s = 0; s < 16; s++) {
-      double dx = 0, dy = 0;
-      int it = 0;
-      for (;; it++) {
-        if (it >= 4096 || !r.range(-radius, radius, &dx) || !r.range(-radius, radius, &dy)) {
-          atomicOr(err, ERR_WATCHDOG);
-          break;
-        }
-        if (dx * dx + dy * dy <= radius * radius) break;
-      }
-      out[i * 32 + 2 * s] = dx;
-      out[i * 32 + 2 * s + 1] = dy;
-    }
-  }
-}
-__global__ void k_debug_mesh(DMesh M, int use_kd, const double* rays, long long n, double tmin, double tmax,
-                             double* out, int* err) {
-  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
-    const double* rr = rays + 6 * i;
-    V3 o = mk(rr[0], rr[1], rr[2]);
-    V3 d = normalize(mk(rr[3], rr[4], rr[5]));
-    RayC r = make_rayc(o, d);
-    double closest = tmax;
-    int best = -1;
-    double* oo = out + 8 * i;
-    if (mesh_trace<false>(M, r, tmin, closest, best, use_kd != 0, err)) {
-      const double2* E = (use_kd ? M.entries : M.brute) + 5 * (size_t)best;
-      double2 q0 = E[0], q1 = E[1], q2 = E[2], q3 = E[3], q4 = E[4];
-      V3 e1 = mk(q1.y, q2.x, q2.y), e2 = mk(q3.x, q3.y, q4.x);
-      (void)q0;
-      double a = dot(e1, cross(r.d, e2));
-      double4 nn = M.normals[lo32(q4.y)];
-      V3 nv = mk(nn.x, nn.y, nn.z);
-      if (a < 0.0) nv = -nv;
-      V3 p = r.o + closest * r.d;
-      V3 fn = face_normal(r.d, nv);
-      oo[0] = 1.0;
-      oo[1] = closest;
-      oo[2] = p.x; oo[3] = p.y; oo[4] = p.z;
-      oo[5] = fn.x; oo[6] = fn.y; oo[7] = fn.z;
-    } else {
-      for (int k = 0; k < 8; k++) oo[k] = 0.0;
-    }
-  }
-}
-
-}  // namespace rtb
-
-// ==========================================================================
-// Host side: context, scene upload, render orchestration, C ABI
-// ==========================================================================
 using namespace rtb;
-
-namespace {
-
-std::mutex g_err_mu;
-std::string g_global_err;
-
-template <class T>
-struct DevArray {
-  T* p = nullptr;
-  size_t n = 0;
-};
-
-}  // namespace
 
 struct rt_scene {
   rt_ctx* ctx = nullptr;
   int device = 0;
   std::vector<void*> allocs;
+  size_t uploaded_bytes = 0;
   DScene S{};
   rt_camera_config camera{};
   rt_outline_config outline{};
   int has_outline = 0;
   std::string render_error;
-  std::vector<DMesh> host_meshes;  // device pointers, for the debug entry point
-  std::vector<int> obj_kind, obj_index;
-  bool disk_light_bad = false;
+  std::vector<DMesh> host_meshes;       // device pointers, for the debug entry point
+  std::vector<int> obj_kind, obj_mesh;  // per World object
 };
 
 struct rt_ctx {
@@ -713,25 +44,32 @@ struct rt_ctx {
   int num_sms = 148;
   cudaStream_t stream = nullptr;
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+  std::vector<cudaEvent_t> stage_ev;
   std::string err;
-  // scratch
   long long cap_rays = 0;
   int cap_levels = 0;
   long long cap_pixels = 0;
+  long long cap_shadow = 0;   // shadow-ray entries
+  long long cap_hits_sh = 0;  // per-hit shadow origins
   std::vector<void*> scratch;
   DFrame F{};
-  LevelBuf* d_levels = nullptr;
   std::vector<LevelBuf> h_levels;
+  LevelBuf* d_levels = nullptr;
   int* d_counts = nullptr;
+  int* d_nhits = nullptr;
   unsigned long long* d_stats = nullptr;
   int* d_err = nullptr;
 };
 
 namespace {
 
+std::mutex g_err_mu;
+std::string g_global_err;
+
 rt_status fail(rt_ctx* ctx, rt_status s, const std::string& m) {
-  if (ctx) ctx->err = m;
-  else {
+  if (ctx) {
+    ctx->err = m;
+  } else {
     std::lock_guard<std::mutex> g(g_err_mu);
     g_global_err = m;
   }
@@ -743,9 +81,9 @@ rt_status cuda_fail(rt_ctx* ctx, cudaError_t e, const char* what) {
   return fail(ctx, s, std::string(what) + ": " + cudaGetErrorString(e));
 }
 
-#define CK(call)                                        \
-  do {                                                  \
-    cudaError_t e_ = (call);                            \
+#define CK(call)                                             \
+  do {                                                       \
+    cudaError_t e_ = (call);                                 \
     if (e_ != cudaSuccess) return cuda_fail(ctx, e_, #call); \
   } while (0)
 
@@ -763,14 +101,22 @@ void free_all(std::vector<void*>& v) {
   v.clear();
 }
 
-// Scratch sized for n_rays queue entries per level, `levels` levels and
-// n_pix pixels; kept across renders and grown on demand.
-rt_status ensure_scratch(rt_ctx* ctx, long long n_rays, int levels, long long n_pix) {
-  if (n_rays <= ctx->cap_rays && levels <= ctx->cap_levels && n_pix <= ctx->cap_pixels) return RT_OK;
-  free_all(ctx->scratch);
+// Shadow-ray entries kept on the device at once (57 B each).
+const long long kShadowCap = 1LL << 26;
+
+rt_status ensure_scratch(rt_ctx* ctx, long long n_rays, int levels, long long n_pix, long long n_shadow,
+                         long long n_hits_sh) {
+  if (n_rays <= ctx->cap_rays && levels <= ctx->cap_levels && n_pix <= ctx->cap_pixels &&
+      n_shadow <= ctx->cap_shadow && n_hits_sh <= ctx->cap_hits_sh)
+    return RT_OK;
+  CK(cudaStreamSynchronize(ctx->stream));
   long long R = std::max(n_rays, ctx->cap_rays);
   int Lv = std::max(levels, ctx->cap_levels);
   long long P = std::max(n_pix, ctx->cap_pixels);
+  long long SH = std::max(n_shadow, ctx->cap_shadow), HS = std::max(n_hits_sh, ctx->cap_hits_sh);
+  free_all(ctx->scratch);
+  ctx->cap_rays = ctx->cap_levels = 0;
+  ctx->cap_pixels = ctx->cap_shadow = ctx->cap_hits_sh = 0;
   DFrame& F = ctx->F;
   auto& o = ctx->scratch;
   for (int k = 0; k < 2; k++) {
@@ -778,9 +124,8 @@ rt_status ensure_scratch(rt_ctx* ctx, long long n_rays, int levels, long long n_
     CK(dalloc(o, &F.q[k].dx, R)); CK(dalloc(o, &F.q[k].dy, R)); CK(dalloc(o, &F.q[k].dz, R));
     CK(dalloc(o, &F.q[k].seed, R));
   }
-  CK(dalloc(o, &F.hobj, R));
-  CK(dalloc(o, &F.haux, R));
-  CK(dalloc(o, &F.ht, R));
+  CK(dalloc(o, &F.hobj, R)); CK(dalloc(o, &F.haux, R)); CK(dalloc(o, &F.hent, R)); CK(dalloc(o, &F.ht, R));
+  CK(dalloc(o, &F.hit_ray, R));
   ctx->h_levels.assign(Lv + 1, LevelBuf{});
   for (int l = 0; l < Lv; l++) {
     LevelBuf& L = ctx->h_levels[l];
@@ -790,6 +135,12 @@ rt_status ensure_scratch(rt_ctx* ctx, long long n_rays, int levels, long long n_
   CK(dalloc(o, &ctx->d_levels, Lv + 1));
   CK(cudaMemcpy(ctx->d_levels, ctx->h_levels.data(), (Lv + 1) * sizeof(LevelBuf), cudaMemcpyHostToDevice));
   CK(dalloc(o, &ctx->d_counts, Lv + 2));
+  CK(dalloc(o, &ctx->d_nhits, Lv + 1));
+  CK(dalloc(o, &F.sh.dx, SH)); CK(dalloc(o, &F.sh.dy, SH)); CK(dalloc(o, &F.sh.dz, SH));
+  CK(dalloc(o, &F.sh.dist, SH));
+  CK(dalloc(o, &F.sh.cr, SH)); CK(dalloc(o, &F.sh.cg, SH)); CK(dalloc(o, &F.sh.cb, SH));
+  CK(dalloc(o, &F.sh.vis, SH));
+  CK(dalloc(o, &F.sh.ox, HS)); CK(dalloc(o, &F.sh.oy, HS)); CK(dalloc(o, &F.sh.oz, HS));
   CK(dalloc(o, &F.pdepth, R)); CK(dalloc(o, &F.pnx, R)); CK(dalloc(o, &F.pny, R)); CK(dalloc(o, &F.pnz, R));
   CK(dalloc(o, &F.phit, R));
   CK(dalloc(o, &F.cr, P)); CK(dalloc(o, &F.cg, P)); CK(dalloc(o, &F.cb, P));
@@ -797,11 +148,13 @@ rt_status ensure_scratch(rt_ctx* ctx, long long n_rays, int levels, long long n_
   CK(dalloc(o, &F.valid, P));
   CK(dalloc(o, &F.mask, P));
   CK(dalloc(o, &F.rgb, 3 * P));
-  CK(dalloc(o, &ctx->d_stats, 8));
+  CK(dalloc(o, &ctx->d_stats, 16));
   CK(dalloc(o, &ctx->d_err, 1));
   ctx->cap_rays = R;
   ctx->cap_levels = Lv;
   ctx->cap_pixels = P;
+  ctx->cap_shadow = SH;
+  ctx->cap_hits_sh = HS;
   return RT_OK;
 }
 
@@ -810,12 +163,241 @@ rt_status upload(rt_ctx* ctx, rt_scene* sc, const std::vector<T>& h, const T** o
   T* p = nullptr;
   CK(dalloc(sc->allocs, &p, h.size()));
   if (!h.empty()) CK(cudaMemcpy(p, h.data(), h.size() * sizeof(T), cudaMemcpyHostToDevice));
+  sc->uploaded_bytes += h.size() * sizeof(T);
   *out = p;
   return RT_OK;
 }
 
+// nalgebra 4x4 try_inverse: cofactors over the column-major slice, det from
+// the first column, every entry scaled by 1/det.  Cube::new_with_transform
+// (src/ray.rs:208-225) stores it as the world-to-local matrix.
+bool inverse4(const double* tm, double* inv) {
+  double m[16], iv[16];
+  for (int k = 0; k < 16; k++) m[k] = tm[(k % 4) * 4 + k / 4];
+  iv[0] = m[5] * m[10] * m[15] - m[5] * m[11] * m[14] - m[9] * m[6] * m[15] + m[9] * m[7] * m[14] +
+          m[13] * m[6] * m[11] - m[13] * m[7] * m[10];
+  iv[4] = -m[4] * m[10] * m[15] + m[4] * m[11] * m[14] + m[8] * m[6] * m[15] - m[8] * m[7] * m[14] -
+          m[12] * m[6] * m[11] + m[12] * m[7] * m[10];
+  iv[8] = m[4] * m[9] * m[15] - m[4] * m[11] * m[13] - m[8] * m[5] * m[15] + m[8] * m[7] * m[13] +
+          m[12] * m[5] * m[11] - m[12] * m[7] * m[9];
+  iv[12] = -m[4] * m[9] * m[14] + m[4] * m[10] * m[13] + m[8] * m[5] * m[14] - m[8] * m[6] * m[13] -
+           m[12] * m[5] * m[10] + m[12] * m[6] * m[9];
+  double det = m[0] * iv[0] + m[1] * iv[4] + m[2] * iv[8] + m[3] * iv[12];
+  if (det == 0.0) return false;
+  iv[1] = -m[1] * m[10] * m[15] + m[1] * m[11] * m[14] + m[9] * m[2] * m[15] - m[9] * m[3] * m[14] -
+          m[13] * m[2] * m[11] + m[13] * m[3] * m[10];
+  iv[5] = m[0] * m[10] * m[15] - m[0] * m[11] * m[14] - m[8] * m[2] * m[15] + m[8] * m[3] * m[14] +
+          m[12] * m[2] * m[11] - m[12] * m[3] * m[10];
+  iv[9] = -m[0] * m[9] * m[15] + m[0] * m[11] * m[13] + m[8] * m[1] * m[15] - m[8] * m[3] * m[13] -
+          m[12] * m[1] * m[11] + m[12] * m[3] * m[9];
+  iv[13] = m[0] * m[9] * m[14] - m[0] * m[10] * m[13] - m[8] * m[1] * m[14] + m[8] * m[2] * m[13] +
+           m[12] * m[1] * m[10] - m[12] * m[2] * m[9];
+  iv[2] = m[1] * m[6] * m[15] - m[1] * m[7] * m[14] - m[5] * m[2] * m[15] + m[5] * m[3] * m[14] +
+          m[13] * m[2] * m[7] - m[13] * m[3] * m[6];
+  iv[6] = -m[0] * m[6] * m[15] + m[0] * m[7] * m[14] + m[4] * m[2] * m[15] - m[4] * m[3] * m[14] -
+          m[12] * m[2] * m[7] + m[12] * m[3] * m[6];
+  iv[10] = m[0] * m[5] * m[15] - m[0] * m[7] * m[13] - m[4] * m[1] * m[15] + m[4] * m[3] * m[13] +
+           m[12] * m[1] * m[7] - m[12] * m[3] * m[5];
+  iv[14] = -m[0] * m[5] * m[14] + m[0] * m[6] * m[13] + m[4] * m[1] * m[14] - m[4] * m[2] * m[13] -
+           m[12] * m[1] * m[6] + m[12] * m[2] * m[5];
+  iv[3] = -m[1] * m[6] * m[11] + m[1] * m[7] * m[10] + m[5] * m[2] * m[11] - m[5] * m[3] * m[10] -
+          m[9] * m[2] * m[7] + m[9] * m[3] * m[6];
+  iv[7] = m[0] * m[6] * m[11] - m[0] * m[7] * m[10] - m[4] * m[2] * m[11] + m[4] * m[3] * m[10] +
+          m[8] * m[2] * m[7] - m[8] * m[3] * m[6];
+  iv[11] = -m[0] * m[5] * m[11] + m[0] * m[7] * m[9] + m[4] * m[1] * m[11] - m[4] * m[3] * m[9] -
+           m[8] * m[1] * m[7] + m[8] * m[3] * m[5];
+  iv[15] = m[0] * m[5] * m[10] - m[0] * m[6] * m[9] - m[4] * m[1] * m[10] + m[4] * m[2] * m[9] +
+           m[8] * m[1] * m[6] - m[8] * m[2] * m[5];
+  double id = 1.0 / det;
+  for (int k = 0; k < 16; k++) inv[(k % 4) * 4 + k / 4] = iv[k] * id;
+  return true;
+}
+
+// nalgebra 3x3 try_inverse (adjugate / determinant)
+bool inverse3(const double a[3][3], double ri[3][3]) {
+  double m11 = a[1][1] * a[2][2] - a[2][1] * a[1][2];
+  double m12 = a[1][0] * a[2][2] - a[2][0] * a[1][2];
+  double m13 = a[1][0] * a[2][1] - a[2][0] * a[1][1];
+  double det = a[0][0] * m11 - a[0][1] * m12 + a[0][2] * m13;
+  if (det == 0.0) return false;
+  double m21 = a[0][1] * a[2][2] - a[2][1] * a[0][2];
+  double m22 = a[0][0] * a[2][2] - a[2][0] * a[0][2];
+  double m23 = a[0][0] * a[2][1] - a[2][0] * a[0][1];
+  double m31 = a[0][1] * a[1][2] - a[1][1] * a[0][2];
+  double m32 = a[0][0] * a[1][2] - a[1][0] * a[0][2];
+  double m33 = a[0][0] * a[1][1] - a[1][0] * a[0][1];
+  ri[0][0] = m11 / det;
+  ri[1][0] = -m12 / det;
+  ri[2][0] = m13 / det;
+  ri[0][1] = -m21 / det;
+  ri[1][1] = m22 / det;
+  ri[2][1] = -m23 / det;
+  ri[0][2] = m31 / det;
+  ri[1][2] = -m32 / det;
+  ri[2][2] = m33 / det;
+  return true;
+}
+
+void put_bvh(const std::vector<BvhNode>& nodes, std::vector<double2>* out) {
+  out->resize(nodes.size() * 7);
+  for (size_t k = 0; k < nodes.size(); k++) {
+    const BvhNode& n = nodes[k];
+    double2* N = &(*out)[7 * k];
+    N[0] = double2{n.lmin[0], n.lmin[1]};
+    N[1] = double2{n.lmin[2], n.lmax[0]};
+    N[2] = double2{n.lmax[1], n.lmax[2]};
+    N[3] = double2{n.rmin[0], n.rmin[1]};
+    N[4] = double2{n.rmin[2], n.rmax[0]};
+    N[5] = double2{n.rmax[1], n.rmax[2]};
+    N[6] = double2{pack2(n.lidx, n.lcnt), pack2(n.ridx, n.rcnt)};
+  }
+}
+
+rt_status upload_mesh(rt_ctx* ctx, rt_scene* sc, const rt_mesh_desc& md, DMesh* out) {
+  DMesh M{};
+  for (int k = 0; k < 3; k++) {
+    M.bmin[k] = md.bounds_min[k];
+    M.bmax[k] = md.bounds_max[k];
+  }
+  long long nt = md.n_triangles;
+  if (nt < 0 || md.n_nodes < 0 || md.n_tri_index < 0) return fail(ctx, RT_ERR_INVALID_ARGUMENT, "negative count");
+  if (nt > 0x3fffffffLL || md.n_nodes > 0x3fffffffLL || md.n_tri_index > 0x3fffffffLL)
+    return fail(ctx, RT_ERR_INVALID_ARGUMENT, "mesh too large");
+  if ((nt > 0 && !md.vertices) || (md.n_nodes > 0 && !md.nodes) || (md.n_tri_index > 0 && !md.tri_index))
+    return fail(ctx, RT_ERR_INVALID_ARGUMENT, "null mesh array");
+  // triangle records and normals in original order
+  std::vector<double2> brute((size_t)nt * 5);
+  std::vector<double4> normals((size_t)nt);
+  std::vector<double> tmin((size_t)nt * 3), tmax((size_t)nt * 3);
+  double scale = 0.0;
+  for (long long t = 0; t < nt; t++) {
+    const double* v = md.vertices + 9 * t;
+    V3 v0 = mk(v[0], v[1], v[2]), v1 = mk(v[3], v[4], v[5]), v2 = mk(v[6], v[7], v[8]);
+    V3 e1 = v1 - v0, e2 = v2 - v0;
+    V3 n = cross(e1, e2);
+    int degenerate = norm(n) < 1e-8 ? 1 : 0;  // src/ray.rs:565-567
+    V3 nn = normalize(n);
+    normals[t] = double4{nn.x, nn.y, nn.z, 0.0};
+    double2* E = &brute[5 * t];
+    E[0] = double2{v0.x, v0.y};
+    E[1] = double2{v0.z, e1.x};
+    E[2] = double2{e1.y, e1.z};
+    E[3] = double2{e2.x, e2.y};
+    E[4] = double2{e2.z, pack2((int)t, degenerate)};
+    for (int k = 0; k < 3; k++) {
+      double a = v[k], b = v[3 + k], c = v[6 + k];
+      tmin[3 * t + k] = std::min(a, std::min(b, c));
+      tmax[3 * t + k] = std::max(a, std::max(b, c));
+      scale = std::max(scale, std::max(std::fabs(tmin[3 * t + k]), std::fabs(tmax[3 * t + k])));
+    }
+  }
+  // reference k-d tree: nodes, per-node root paths, leaf entries and the
+  // per-triangle occurrences (leaf node, position in the leaf)
+  std::vector<double2> nodes((size_t)md.n_nodes * 4);
+  std::vector<int2> leaf_path((size_t)md.n_nodes, int2{0, 0});
+  for (long long k = 0; k < md.n_nodes; k++) {
+    const rt_kd_node_desc& nd = md.nodes[k];
+    double2* N = &nodes[4 * k];
+    N[0] = double2{nd.bounds_min[0], nd.bounds_min[1]};
+    N[1] = double2{nd.bounds_min[2], nd.bounds_max[0]};
+    N[2] = double2{nd.bounds_max[1], nd.bounds_max[2]};
+    if (nd.axis < 0) {
+      if (nd.first < 0 || nd.count < 0 || (long long)nd.first + nd.count > md.n_tri_index)
+        return fail(ctx, RT_ERR_INVALID_ARGUMENT, "k-d leaf range out of bounds");
+      N[3] = double2{0.0, pack2(nd.first, -1 - nd.count)};
+    } else {
+      if (nd.axis > 2 || nd.right <= k + 1 || nd.right >= md.n_nodes)
+        return fail(ctx, RT_ERR_INVALID_ARGUMENT, "k-d node layout is not preorder");
+      N[3] = double2{nd.split, pack2(nd.right, nd.axis)};
+    }
+  }
+  if (md.n_nodes > 0) {
+    std::vector<std::pair<int, int2>> st;  // node, {path bits, depth}
+    st.push_back({0, int2{0, 0}});
+    std::vector<char> seen((size_t)md.n_nodes, 0);
+    while (!st.empty()) {
+      int k = st.back().first;
+      int2 pd = st.back().second;
+      st.pop_back();
+      if (seen[k]) return fail(ctx, RT_ERR_INVALID_ARGUMENT, "k-d nodes do not form a tree");
+      seen[k] = 1;
+      leaf_path[k] = pd;
+      const rt_kd_node_desc& nd = md.nodes[k];
+      if (nd.axis >= 0) {
+        if (pd.y >= 31) return fail(ctx, RT_ERR_INVALID_ARGUMENT, "k-d tree deeper than 31 levels");
+        st.push_back({k + 1, int2{pd.x, pd.y + 1}});
+        st.push_back({nd.right, int2{pd.x | (1 << pd.y), pd.y + 1}});
+      }
+    }
+  }
+  std::vector<double2> entries((size_t)md.n_tri_index * 5);
+  std::vector<int> occ_off((size_t)nt + 1, 0);
+  for (long long k = 0; k < md.n_tri_index; k++) {
+    int t = md.tri_index[k];
+    if (t < 0 || t >= nt) return fail(ctx, RT_ERR_INVALID_ARGUMENT, "k-d leaf index out of range");
+    for (int j = 0; j < 5; j++) entries[5 * k + j] = brute[5 * (size_t)t + j];
+    occ_off[t + 1]++;
+  }
+  for (long long t = 0; t < nt; t++) occ_off[t + 1] += occ_off[t];
+  std::vector<int2> occ((size_t)md.n_tri_index);
+  {
+    std::vector<int> fill(occ_off.begin(), occ_off.end() - 1);
+    for (long long k = 0; k < md.n_nodes; k++) {
+      const rt_kd_node_desc& nd = md.nodes[k];
+      if (nd.axis >= 0) continue;
+      for (int p = 0; p < nd.count; p++) {
+        int t = md.tri_index[nd.first + p];
+        occ[fill[t]++] = int2{(int)k, p};
+      }
+    }
+  }
+  // triangle BVH, the candidate search structure
+  std::vector<BvhNode> bnodes;
+  std::vector<int32_t> order;
+  build_bvh(tmin, tmax, 4, 1e-7 * (1.0 + scale), &bnodes, &order);
+  std::vector<double2> bvh, btris((size_t)nt * 5);
+  put_bvh(bnodes, &bvh);
+  for (long long k = 0; k < nt; k++)
+    for (int j = 0; j < 5; j++) btris[5 * k + j] = brute[5 * (size_t)order[k] + j];
+  rt_status st;
+  const double2* p2;
+  if ((st = upload(ctx, sc, bvh, &p2)) != RT_OK) return st;
+  M.bvh = p2;
+  if ((st = upload(ctx, sc, btris, &p2)) != RT_OK) return st;
+  M.btris = p2;
+  if ((st = upload(ctx, sc, brute, &p2)) != RT_OK) return st;
+  M.brute = p2;
+  const double4* p4;
+  if ((st = upload(ctx, sc, normals, &p4)) != RT_OK) return st;
+  M.normals = p4;
+  if ((st = upload(ctx, sc, nodes, &p2)) != RT_OK) return st;
+  M.nodes = p2;
+  if ((st = upload(ctx, sc, entries, &p2)) != RT_OK) return st;
+  M.entries = p2;
+  const int2* pi2;
+  if ((st = upload(ctx, sc, leaf_path, &pi2)) != RT_OK) return st;
+  M.leaf_path = pi2;
+  if ((st = upload(ctx, sc, occ, &pi2)) != RT_OK) return st;
+  M.occ = pi2;
+  const int* pi;
+  if ((st = upload(ctx, sc, occ_off, &pi)) != RT_OK) return st;
+  M.occ_off = pi;
+  M.n_nodes = (int)md.n_nodes;
+  M.n_tris = (int)nt;
+  *out = M;
+  return RT_OK;
+}
+
+// Runs of at least this many consecutive spheres are searched through a BVH.
+const int kMinSphereRun = 8;
+
 rt_status do_upload(rt_ctx* ctx, const rt_scene_desc* d, rt_scene** out) {
   if (!d) return fail(ctx, RT_ERR_INVALID_ARGUMENT, "null scene description");
+  if (d->n_objects < 0 || d->n_materials < 0 || d->n_lights < 0 || d->n_meshes < 0)
+    return fail(ctx, RT_ERR_INVALID_ARGUMENT, "negative count");
+  if ((d->n_objects && !d->objects) || (d->n_materials && !d->materials) || (d->n_lights && !d->lights) ||
+      (d->n_meshes && !d->meshes))
+    return fail(ctx, RT_ERR_INVALID_ARGUMENT, "null scene array");
   auto sc = std::make_unique<rt_scene>();
   sc->ctx = ctx;
   sc->device = ctx->device;
@@ -824,161 +406,119 @@ rt_status do_upload(rt_ctx* ctx, const rt_scene_desc* d, rt_scene** out) {
   sc->has_outline = d->has_outline;
   sc->render_error = d->render_error ? d->render_error : "";
   DScene& S = sc->S;
+  std::vector<DMesh> meshes(d->n_meshes);
+  for (int m = 0; m < d->n_meshes; m++) {
+    rt_status st = upload_mesh(ctx, sc.get(), d->meshes[m], &meshes[m]);
+    if (st != RT_OK) return st;
+  }
   std::vector<int4> obj;
   std::vector<double> sph, pln;
+  std::vector<int> sph_mat;
   std::vector<DCube> cub;
-  std::vector<DMesh> meshes;
-  for (int m = 0; m < d->n_meshes; m++) {
-    const rt_mesh_desc& md = d->meshes[m];
-    DMesh M{};
-    for (int k = 0; k < 3; k++) { M.bmin[k] = md.bounds_min[k]; M.bmax[k] = md.bounds_max[k]; }
-    long long nt = md.n_triangles;
-    // per-triangle entries in original order + normals
-    std::vector<double2> brute((size_t)nt * 5);
-    std::vector<double4> normals((size_t)nt);
-    for (long long t = 0; t < nt; t++) {
-      const double* v = md.vertices + 9 * t;
-      V3 v0 = mk(v[0], v[1], v[2]), v1 = mk(v[3], v[4], v[5]), v2 = mk(v[6], v[7], v[8]);
-      V3 e1 = v1 - v0, e2 = v2 - v0;
-      V3 n = cross(e1, e2);
-      int degenerate = norm(n) < 1e-8 ? 1 : 0;
-      V3 nn = normalize(n);
-      normals[t] = double4{nn.x, nn.y, nn.z, 0.0};
-      double2* E = &brute[5 * t];
-      E[0] = double2{v0.x, v0.y};
-      E[1] = double2{v0.z, e1.x};
-      E[2] = double2{e1.y, e1.z};
-      E[3] = double2{e2.x, e2.y};
-      E[4] = double2{e2.z, pack2((int)t, degenerate)};
-    }
-    std::vector<double2> entries((size_t)md.n_tri_index * 5);
-    for (long long k = 0; k < md.n_tri_index; k++) {
-      int t = md.tri_index[k];
-      if (t < 0 || t >= nt) return fail(ctx, RT_ERR_INVALID_ARGUMENT, "k-d leaf index out of range");
-      for (int j = 0; j < 5; j++) entries[5 * k + j] = brute[5 * (size_t)t + j];
-    }
-    std::vector<double2> nodes((size_t)md.n_nodes * 4);
-    for (long long k = 0; k < md.n_nodes; k++) {
-      const rt_kd_node_desc& nd = md.nodes[k];
-      double2* N = &nodes[4 * k];
-      N[0] = double2{nd.bounds_min[0], nd.bounds_min[1]};
-      N[1] = double2{nd.bounds_min[2], nd.bounds_max[0]};
-      N[2] = double2{nd.bounds_max[1], nd.bounds_max[2]};
-      if (nd.axis < 0) {
-        if (nd.first < 0 || nd.count < 0 || (long long)nd.first + nd.count > md.n_tri_index)
-          return fail(ctx, RT_ERR_INVALID_ARGUMENT, "k-d leaf range out of bounds");
-        N[3] = double2{0.0, pack2(nd.first, -1 - nd.count)};
-      } else {
-        if (nd.axis > 2 || nd.right <= k || nd.right >= md.n_nodes)
-          return fail(ctx, RT_ERR_INVALID_ARGUMENT, "k-d node layout is not preorder");
-        N[3] = double2{nd.split, pack2(nd.right, nd.axis)};
-      }
-    }
-    rt_status st;
-    const double2* p;
-    if ((st = upload(ctx, sc.get(), nodes, &p)) != RT_OK) return st;
-    M.nodes = p;
-    if ((st = upload(ctx, sc.get(), entries, &p)) != RT_OK) return st;
-    M.entries = p;
-    if ((st = upload(ctx, sc.get(), brute, &p)) != RT_OK) return st;
-    M.brute = p;
-    const double4* pn;
-    if ((st = upload(ctx, sc.get(), normals, &pn)) != RT_OK) return st;
-    M.normals = pn;
-    M.n_nodes = (int)md.n_nodes;
-    M.n_tris = (int)nt;
-    meshes.push_back(M);
-  }
   for (int i = 0; i < d->n_objects; i++) {
     const rt_object_desc& o = d->objects[i];
-    if (o.material < 0 || o.material >= d->n_materials) return fail(ctx, RT_ERR_INVALID_ARGUMENT, "material index out of range");
-    int4 e{o.kind, 0, o.material, 0};
+    if (o.material < 0 || o.material >= d->n_materials)
+      return fail(ctx, RT_ERR_INVALID_ARGUMENT, "material index out of range");
+    sc->obj_kind.push_back(o.kind);
+    sc->obj_mesh.push_back(o.kind == RT_OBJ_MESH ? o.mesh : -1);
     if (o.kind == RT_OBJ_SPHERE) {
-      e.y = (int)(sph.size() / 5);
+      int si = (int)(sph.size() / 5);
       sph.insert(sph.end(), {o.a[0], o.a[1], o.a[2], o.radius, o.radius * o.radius});
+      sph_mat.push_back(o.material);
+      obj.push_back(int4{OBJ_SPHERE, si, o.material, i});
     } else if (o.kind == RT_OBJ_PLANE) {
-      e.y = (int)(pln.size() / 12);
+      int pi = (int)(pln.size() / 12);
       V3 n = mk(o.b[0], o.b[1], o.b[2]);
+      // Plane::hit's texture axes (src/ray.rs:161-167)
       V3 ua = fabs(n.x) > 0.9 ? mk(0, 1, 0) : mk(1, 0, 0);
       V3 uax = normalize(cross(ua, n));
       V3 vax = normalize(cross(n, uax));
       pln.insert(pln.end(), {o.a[0], o.a[1], o.a[2], n.x, n.y, n.z, uax.x, uax.y, uax.z, vax.x, vax.y, vax.z});
+      obj.push_back(int4{OBJ_PLANE, pi, o.material, i});
     } else if (o.kind == RT_OBJ_CUBE) {
-      e.y = (int)cub.size();
       DCube C{};
-      for (int k = 0; k < 3; k++) { C.c[k] = o.a[k]; C.half[k] = o.b[k] / 2.0; }
+      for (int k = 0; k < 3; k++) {
+        C.c[k] = o.a[k];
+        C.half[k] = o.b[k] / 2.0;
+      }
       double tm[16], inv[16];
       for (int k = 0; k < 16; k++) tm[k] = o.has_transform ? o.transform[k] : ((k % 5) == 0 ? 1.0 : 0.0);
-      // Cube::new_with_transform (src/ray.rs:208-225): w2l = inverse (or identity)
-      {
-        // nalgebra 4x4 cofactor inverse on the column-major slice
-        double m[16], iv[16];
-        for (int k = 0; k < 16; k++) m[k] = tm[(k % 4) * 4 + k / 4];
-        iv[0] = m[5] * m[10] * m[15] - m[5] * m[11] * m[14] - m[9] * m[6] * m[15] + m[9] * m[7] * m[14] + m[13] * m[6] * m[11] - m[13] * m[7] * m[10];
-        iv[4] = -m[4] * m[10] * m[15] + m[4] * m[11] * m[14] + m[8] * m[6] * m[15] - m[8] * m[7] * m[14] - m[12] * m[6] * m[11] + m[12] * m[7] * m[10];
-        iv[8] = m[4] * m[9] * m[15] - m[4] * m[11] * m[13] - m[8] * m[5] * m[15] + m[8] * m[7] * m[13] + m[12] * m[5] * m[11] - m[12] * m[7] * m[9];
-        iv[12] = -m[4] * m[9] * m[14] + m[4] * m[10] * m[13] + m[8] * m[5] * m[14] - m[8] * m[6] * m[13] - m[12] * m[5] * m[10] + m[12] * m[6] * m[9];
-        double det = m[0] * iv[0] + m[1] * iv[4] + m[2] * iv[8] + m[3] * iv[12];
-        bool ok = o.has_transform && det != 0.0;
-        if (ok) {
-          iv[1] = -m[1] * m[10] * m[15] + m[1] * m[11] * m[14] + m[9] * m[2] * m[15] - m[9] * m[3] * m[14] - m[13] * m[2] * m[11] + m[13] * m[3] * m[10];
-          iv[5] = m[0] * m[10] * m[15] - m[0] * m[11] * m[14] - m[8] * m[2] * m[15] + m[8] * m[3] * m[14] + m[12] * m[2] * m[11] - m[12] * m[3] * m[10];
-          iv[9] = -m[0] * m[9] * m[15] + m[0] * m[11] * m[13] + m[8] * m[1] * m[15] - m[8] * m[3] * m[13] - m[12] * m[1] * m[11] + m[12] * m[3] * m[9];
-          iv[13] = m[0] * m[9] * m[14] - m[0] * m[10] * m[13] - m[8] * m[1] * m[14] + m[8] * m[2] * m[13] + m[12] * m[1] * m[10] - m[12] * m[2] * m[9];
-          iv[2] = m[1] * m[6] * m[15] - m[1] * m[7] * m[14] - m[5] * m[2] * m[15] + m[5] * m[3] * m[14] + m[13] * m[2] * m[7] - m[13] * m[3] * m[6];
-          iv[6] = -m[0] * m[6] * m[15] + m[0] * m[7] * m[14] + m[4] * m[2] * m[15] - m[4] * m[3] * m[14] - m[12] * m[2] * m[7] + m[12] * m[3] * m[6];
-          iv[10] = m[0] * m[5] * m[15] - m[0] * m[7] * m[13] - m[4] * m[1] * m[15] + m[4] * m[3] * m[13] + m[12] * m[1] * m[7] - m[12] * m[3] * m[5];
-          iv[14] = -m[0] * m[5] * m[14] + m[0] * m[6] * m[13] + m[4] * m[1] * m[14] - m[4] * m[2] * m[13] - m[12] * m[1] * m[6] + m[12] * m[2] * m[5];
-          iv[3] = -m[1] * m[6] * m[11] + m[1] * m[7] * m[10] + m[5] * m[2] * m[11] - m[5] * m[3] * m[10] - m[9] * m[2] * m[7] + m[9] * m[3] * m[6];
-          iv[7] = m[0] * m[6] * m[11] - m[0] * m[7] * m[10] - m[4] * m[2] * m[11] + m[4] * m[3] * m[10] + m[8] * m[2] * m[7] - m[8] * m[3] * m[6];
-          iv[11] = -m[0] * m[5] * m[11] + m[0] * m[7] * m[9] + m[4] * m[1] * m[11] - m[4] * m[3] * m[9] - m[8] * m[1] * m[7] + m[8] * m[3] * m[5];
-          iv[15] = m[0] * m[5] * m[10] - m[0] * m[6] * m[9] - m[4] * m[1] * m[10] + m[4] * m[2] * m[9] + m[8] * m[1] * m[6] - m[8] * m[2] * m[5];
-          double id = 1.0 / det;
-          for (int k = 0; k < 16; k++) inv[(k % 4) * 4 + k / 4] = iv[k] * id;
-        } else {
-          for (int k = 0; k < 16; k++) inv[k] = (k % 5) == 0 ? 1.0 : 0.0;
-        }
+      if (!o.has_transform || !inverse4(tm, inv))
+        for (int k = 0; k < 16; k++) inv[k] = (k % 5) == 0 ? 1.0 : 0.0;
+      for (int k = 0; k < 12; k++) {
+        C.w2l[k] = inv[k];
+        C.l2w[k] = tm[k];
       }
-      for (int k = 0; k < 12; k++) { C.w2l[k] = inv[k]; C.l2w[k] = tm[k]; }
       bool ident = true;
       for (int k = 0; k < 16; k++)
         if (inv[k] != ((k % 5) == 0 ? 1.0 : 0.0)) ident = false;
       C.identity = ident ? 1 : 0;
-      // normal transform: nalgebra 3x3 inverse of w2l's rotation part, transposed
-      double a[3][3];
+      // normal transform: inverse of w2l's rotation part, transposed (src/ray.rs:474-481)
+      double a[3][3], ri[3][3];
       for (int r = 0; r < 3; r++)
         for (int c = 0; c < 3; c++) a[r][c] = inv[4 * r + c];
-      double m11 = a[1][1] * a[2][2] - a[2][1] * a[1][2];
-      double m12 = a[1][0] * a[2][2] - a[2][0] * a[1][2];
-      double m13 = a[1][0] * a[2][1] - a[2][0] * a[1][1];
-      double det = a[0][0] * m11 - a[0][1] * m12 + a[0][2] * m13;
-      double ri[3][3];
-      if (det != 0.0) {
-        double m21 = a[0][1] * a[2][2] - a[2][1] * a[0][2];
-        double m22 = a[0][0] * a[2][2] - a[2][0] * a[0][2];
-        double m23 = a[0][0] * a[2][1] - a[2][0] * a[0][1];
-        double m31 = a[0][1] * a[1][2] - a[1][1] * a[0][2];
-        double m32 = a[0][0] * a[1][2] - a[1][0] * a[0][2];
-        double m33 = a[0][0] * a[1][1] - a[1][0] * a[0][1];
-        ri[0][0] = m11 / det; ri[1][0] = -m12 / det; ri[2][0] = m13 / det;
-        ri[0][1] = -m21 / det; ri[1][1] = m22 / det; ri[2][1] = -m23 / det;
-        ri[0][2] = m31 / det; ri[1][2] = -m32 / det; ri[2][2] = m33 / det;
-      } else {
+      if (!inverse3(a, ri))
         for (int r = 0; r < 3; r++)
           for (int c = 0; c < 3; c++) ri[r][c] = r == c ? 1.0 : 0.0;
-      }
       for (int r = 0; r < 3; r++)
         for (int c = 0; c < 3; c++) C.ntr[3 * r + c] = ri[c][r];
+      obj.push_back(int4{OBJ_CUBE, (int)cub.size(), o.material, i});
       cub.push_back(C);
     } else if (o.kind == RT_OBJ_MESH) {
       if (o.mesh < 0 || o.mesh >= d->n_meshes) return fail(ctx, RT_ERR_INVALID_ARGUMENT, "mesh index out of range");
-      e.y = o.mesh;
+      obj.push_back(int4{OBJ_MESH, o.mesh, o.material, i});
     } else {
       return fail(ctx, RT_ERR_INVALID_ARGUMENT, "unknown object kind");
     }
-    obj.push_back(e);
-    sc->obj_kind.push_back(o.kind);
-    sc->obj_index.push_back(e.y);
+  }
+  // Long runs of consecutive spheres become one BVH group entry.
+  std::vector<DSphGroup> groups;
+  std::vector<int4> entries;
+  for (size_t k = 0; k < obj.size();) {
+    size_t e = k;
+    while (e < obj.size() && obj[e].x == OBJ_SPHERE) e++;
+    int run = (int)(e - k);
+    if (run >= kMinSphereRun) {
+      int first_sph = obj[k].y;
+      std::vector<double> bmin(3 * (size_t)run), bmax(3 * (size_t)run);
+      double scale = 0.0;
+      for (int s = 0; s < run; s++) {
+        const double* sp = &sph[5 * (size_t)(first_sph + s)];
+        double r = std::fabs(sp[3]);
+        for (int c = 0; c < 3; c++) {
+          bmin[3 * s + c] = sp[c] - r;
+          bmax[3 * s + c] = sp[c] + r;
+          scale = std::max(scale, std::fabs(sp[c]) + r);
+        }
+      }
+      std::vector<BvhNode> bn;
+      std::vector<int32_t> order;
+      build_bvh(bmin, bmax, 2, 1e-6 * (1.0 + scale), &bn, &order);
+      std::vector<double2> bvh;
+      put_bvh(bn, &bvh);
+      DSphGroup G{};
+      const double2* pb;
+      rt_status st = upload(ctx, sc.get(), bvh, &pb);
+      if (st != RT_OK) return st;
+      std::vector<int> ord(order.begin(), order.end());
+      const int* po;
+      st = upload(ctx, sc.get(), ord, &po);
+      if (st != RT_OK) return st;
+      G.bvh = pb;
+      G.order = po;
+      G.first_sphere = first_sph;
+      G.first_obj = obj[k].w;
+      G.count = run;
+      entries.push_back(int4{OBJ_SPHERE_GROUP, (int)groups.size(), -1, obj[k].w});
+      groups.push_back(G);
+      k = e;
+    } else if (run > 0) {
+      for (size_t j = k; j < e; j++) entries.push_back(obj[j]);
+      k = e;
+    } else {
+      entries.push_back(obj[k]);
+      k++;
+    }
   }
   std::vector<DMat> mats(d->n_materials);
   for (int i = 0; i < d->n_materials; i++) {
@@ -986,16 +526,23 @@ rt_status do_upload(rt_ctx* ctx, const rt_scene_desc* d, rt_scene** out) {
     DMat& M = mats[i];
     M = DMat{};
     for (int k = 0; k < 3; k++) M.color[k] = m.color[k];
-    M.ambient = m.ambient; M.diffuse = m.diffuse; M.specular = m.specular; M.shininess = m.shininess;
-    M.refl = m.reflectivity; M.has_refl = m.has_reflectivity; M.texture = m.texture;
+    M.ambient = m.ambient;
+    M.diffuse = m.diffuse;
+    M.specular = m.specular;
+    M.shininess = m.shininess;
+    M.refl = m.reflectivity;
+    M.has_refl = m.has_reflectivity;
+    M.texture = m.texture;
     // the grid colour is formatted as #RRGGBB from (c * 255) as u8 and parsed
     // back (src/lighting.rs:28-36)
     for (int k = 0; k < 3; k++) M.grid_color[k] = (double)sat_u8(m.grid_line_color[k] * 255.0) / 255.0;
     M.half_width = m.grid_line_width / 2.0;
     M.cell_size = m.grid_cell_size;
     for (int k = 0; k < 3; k++) M.cb_color[k] = m.checker_color[k];
-    M.cb_ambient = m.checker_ambient; M.cb_diffuse = m.checker_diffuse;
-    M.cb_specular = m.checker_specular; M.cb_shininess = m.checker_shininess;
+    M.cb_ambient = m.checker_ambient;
+    M.cb_diffuse = m.checker_diffuse;
+    M.cb_specular = m.checker_specular;
+    M.cb_shininess = m.checker_shininess;
   }
   std::vector<DLight> lights(d->n_lights);
   int K = 0;
@@ -1003,19 +550,25 @@ rt_status do_upload(rt_ctx* ctx, const rt_scene_desc* d, rt_scene** out) {
     const rt_light_desc& l = d->lights[i];
     DLight& L = lights[i];
     L = DLight{};
-    for (int k = 0; k < 3; k++) { L.pos[k] = l.position[k]; L.color[k] = l.color[k]; }
+    for (int k = 0; k < 3; k++) {
+      L.pos[k] = l.position[k];
+      L.color[k] = l.color[k];
+    }
     L.intensity = l.intensity;
     L.disk = l.has_diameter ? 1 : 0;
     L.diameter = l.diameter;
     K += L.disk ? 16 : 1;
   }
   rt_status st;
-  const int4* po;
-  if ((st = upload(ctx, sc.get(), obj, &po)) != RT_OK) return st;
-  S.obj = po;
+  const int4* po4;
+  if ((st = upload(ctx, sc.get(), entries, &po4)) != RT_OK) return st;
+  S.obj = po4;
   const double* pd;
   if ((st = upload(ctx, sc.get(), sph, &pd)) != RT_OK) return st;
   S.sph = pd;
+  const int* pmi;
+  if ((st = upload(ctx, sc.get(), sph_mat, &pmi)) != RT_OK) return st;
+  S.sph_mat = pmi;
   if ((st = upload(ctx, sc.get(), pln, &pd)) != RT_OK) return st;
   S.pln = pd;
   const DCube* pc;
@@ -1024,13 +577,16 @@ rt_status do_upload(rt_ctx* ctx, const rt_scene_desc* d, rt_scene** out) {
   const DMesh* pm;
   if ((st = upload(ctx, sc.get(), meshes, &pm)) != RT_OK) return st;
   S.mesh = pm;
+  const DSphGroup* pg;
+  if ((st = upload(ctx, sc.get(), groups, &pg)) != RT_OK) return st;
+  S.grp = pg;
   const DMat* pmt;
   if ((st = upload(ctx, sc.get(), mats, &pmt)) != RT_OK) return st;
   S.mat = pmt;
   const DLight* pl;
   if ((st = upload(ctx, sc.get(), lights, &pl)) != RT_OK) return st;
   S.lights = pl;
-  S.n_obj = (int)obj.size();
+  S.n_obj = (int)entries.size();
   S.n_lights = d->n_lights;
   for (int k = 0; k < 3; k++) {
     S.amb_color[k] = d->ambient_color[k];
@@ -1047,6 +603,44 @@ rt_status do_upload(rt_ctx* ctx, const rt_scene_desc* d, rt_scene** out) {
   *out = sc.release();
   return RT_OK;
 }
+
+// Counts launches and, for profiling renders, records an event after each
+// one so that stage times can be attributed.
+struct Launcher {
+  rt_ctx* ctx;
+  bool timed;
+  unsigned launches = 0;
+  std::vector<std::pair<int, cudaEvent_t>> marks;
+  int ev_used = 0;
+  cudaEvent_t next_event() {
+    if (ev_used >= (int)ctx->stage_ev.size()) {
+      cudaEvent_t e;
+      cudaEventCreate(&e);
+      ctx->stage_ev.push_back(e);
+    }
+    return ctx->stage_ev[ev_used++];
+  }
+  void begin() {
+    if (!timed) return;
+    cudaEvent_t e = next_event();
+    cudaEventRecord(e, ctx->stream);
+    marks.push_back({-1, e});
+  }
+  void after(int stage) {
+    launches++;
+    if (!timed) return;
+    cudaEvent_t e = next_event();
+    cudaEventRecord(e, ctx->stream);
+    marks.push_back({stage, e});
+  }
+  void collect(double* stage_ms) {
+    for (size_t k = 1; k < marks.size(); k++) {
+      float ms = 0.f;
+      cudaEventElapsedTime(&ms, marks[k - 1].second, marks[k].second);
+      if (marks[k].first >= 0) stage_ms[marks[k].first] += ms;
+    }
+  }
+};
 
 rt_status render_impl(rt_ctx* ctx, const rt_scene* sc, const rt_render_params* P, uint8_t* rgb_out, int on_device,
                       double* linear_out, rt_stats* stats) {
@@ -1073,9 +667,12 @@ rt_status render_impl(rt_ctx* ctx, const rt_scene* sc, const rt_render_params* P
   long long nprim = aa == RT_AA_QUINCUNX ? ncorner + npix : npix * spp;
   if (nprim > 0x7fffffffLL) return fail(ctx, RT_ERR_INVALID_ARGUMENT, "too many rays for one render");
   int max_depth = P->max_depth;
-  int levels = std::max(1, std::min(max_depth, RTB_MAX_LEVELS));
   if (max_depth > RTB_MAX_LEVELS) return fail(ctx, RT_ERR_INVALID_ARGUMENT, "max_depth above 64 is not supported");
-  rt_status st = ensure_scratch(ctx, nprim, levels, npix);
+  int levels = std::max(1, std::min(max_depth, RTB_MAX_LEVELS));
+  const int K = sc->S.shadow_per_hit;
+  long long chunk = K > 0 ? std::max(1LL, std::min(nprim, kShadowCap / K)) : nprim;
+  long long n_shadow = std::max(1LL, chunk * std::max(K, 1));
+  rt_status st = ensure_scratch(ctx, nprim, levels, npix, n_shadow, chunk);
   if (st != RT_OK) return st;
 
   DFrame F = ctx->F;
@@ -1106,6 +703,8 @@ rt_status render_impl(rt_ctx* ctx, const rt_scene* sc, const rt_render_params* P
   F.n_corner = ncorner;
   F.levels = ctx->d_levels;
   F.counts = ctx->d_counts;
+  F.nhits = ctx->d_nhits;
+  F.chunk_hits = chunk;
   F.stats = ctx->d_stats;
   F.err = ctx->d_err;
   F.linear = nullptr;
@@ -1118,8 +717,8 @@ rt_status render_impl(rt_ctx* ctx, const rt_scene* sc, const rt_render_params* P
   F.o_radius = 0;
   if (F.outline && P->outline.line_thickness > 1.0) {
     double rr = std::ceil(P->outline.line_thickness - 1.0);
-    F.o_radius = rr > 64.0 ? 64 : (int)rr;
     if (rr > 64.0) return fail(ctx, RT_ERR_INVALID_ARGUMENT, "outline thickness above 65 is not supported");
+    F.o_radius = (int)rr;
   }
   double* d_linear = nullptr;
   std::vector<void*> tmp;
@@ -1131,6 +730,8 @@ rt_status render_impl(rt_ctx* ctx, const rt_scene* sc, const rt_render_params* P
   uint8_t* d_rgb = F.rgb;
   if (rgb_out && on_device) F.rgb = rgb_out;
 
+  const bool count = (P->flags & RT_FLAG_COUNT_WORK) != 0;
+  Launcher Lc{ctx, (P->flags & RT_FLAG_STAGE_TIMES) != 0};
   cudaStream_t s = ctx->stream;
   int nsm = ctx->num_sms;
   auto blocks = [&](long long n, int bs, int per_sm) {
@@ -1139,35 +740,60 @@ rt_status render_impl(rt_ctx* ctx, const rt_scene* sc, const rt_render_params* P
     return (int)std::max<long long>(1, std::min(b, cap));
   };
   CK(cudaMemsetAsync(ctx->d_counts, 0, (levels + 2) * sizeof(int), s));
+  CK(cudaMemsetAsync(ctx->d_nhits, 0, (levels + 1) * sizeof(int), s));
   int n0 = (int)nprim;
   CK(cudaMemcpyAsync(ctx->d_counts, &n0, sizeof(int), cudaMemcpyHostToDevice, s));
-  CK(cudaMemsetAsync(ctx->d_stats, 0, 8 * sizeof(unsigned long long), s));
+  CK(cudaMemsetAsync(ctx->d_stats, 0, 16 * sizeof(unsigned long long), s));
   CK(cudaMemsetAsync(ctx->d_err, 0, sizeof(int), s));
   CK(cudaEventRecord(ctx->ev0, s));
+  Lc.begin();
   if (max_depth > 0) {
     k_raygen<<<blocks(nprim, 256, 16), 256, 0, s>>>(F);
+    Lc.after(RT_STAGE_RAYGEN);
+    long long nchunks = (nprim + chunk - 1) / chunk;
     for (int l = 0; l < levels; l++) {
-      k_trace<<<blocks(nprim, 128, 16), 128, 0, s>>>(F, l);
-      k_shade<<<blocks(nprim, 128, 16), 128, 0, s>>>(F, l);
+      if (count) k_trace<true><<<blocks(nprim, 128, 16), 128, 0, s>>>(F, l);
+      else k_trace<false><<<blocks(nprim, 128, 16), 128, 0, s>>>(F, l);
+      Lc.after(RT_STAGE_TRACE);
+      for (long long c = 0; c < nchunks; c++) {
+        long long c0 = c * chunk;
+        k_emit<<<blocks(chunk, 128, 16), 128, 0, s>>>(F, l, c0);
+        Lc.after(RT_STAGE_EMIT);
+        if (K > 0) {
+          if (count) k_shadow<true><<<blocks(chunk * K, 128, 32), 128, 0, s>>>(F, l, c0);
+          else k_shadow<false><<<blocks(chunk * K, 128, 32), 128, 0, s>>>(F, l, c0);
+          Lc.after(RT_STAGE_SHADOW);
+        }
+        k_resolve<<<blocks(chunk, 128, 16), 128, 0, s>>>(F, l, c0);
+        Lc.after(RT_STAGE_RESOLVE);
+      }
     }
-    for (int l = levels - 2; l >= 0; l--) k_fold<<<blocks(nprim, 256, 16), 256, 0, s>>>(F, l);
+    for (int l = levels - 2; l >= 0; l--) {
+      k_fold<<<blocks(nprim, 256, 16), 256, 0, s>>>(F, l);
+      Lc.after(RT_STAGE_FOLD);
+    }
   }
-  k_resolve<<<blocks(npix, 256, 16), 256, 0, s>>>(F);
+  k_pixels<<<blocks(npix, 256, 16), 256, 0, s>>>(F);
+  Lc.after(RT_STAGE_POST);
   if (F.outline) {
     dim3 ob(OT_X, OT_Y), og((W + OT_X - 1) / OT_X, (H + OT_Y - 1) / OT_Y);
     k_outline_mask<<<og, ob, 0, s>>>(F);
+    Lc.after(RT_STAGE_POST);
     size_t shm = (size_t)(OT_X + 2 * F.o_radius) * (OT_Y + 2 * F.o_radius) * sizeof(double);
-    if (shm > 48 * 1024) CK(cudaFuncSetAttribute(k_outline_apply, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)shm));
+    if (shm > 48 * 1024)
+      CK(cudaFuncSetAttribute(k_outline_apply, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)shm));
     k_outline_apply<<<og, ob, shm, s>>>(F);
+    Lc.after(RT_STAGE_POST);
   }
   CK(cudaGetLastError());
   CK(cudaEventRecord(ctx->ev1, s));
   if (rgb_out && !on_device) CK(cudaMemcpyAsync(rgb_out, d_rgb, 3 * npix, cudaMemcpyDeviceToHost, s));
   if (linear_out) CK(cudaMemcpyAsync(linear_out, d_linear, 3 * npix * sizeof(double), cudaMemcpyDeviceToHost, s));
-  std::vector<int> counts(levels + 2, 0);
-  unsigned long long hstats[8];
+  std::vector<int> counts(levels + 2, 0), nh(levels + 1, 0);
+  unsigned long long hstats[16];
   int herr = 0;
   CK(cudaMemcpyAsync(counts.data(), ctx->d_counts, (levels + 2) * sizeof(int), cudaMemcpyDeviceToHost, s));
+  CK(cudaMemcpyAsync(nh.data(), ctx->d_nhits, (levels + 1) * sizeof(int), cudaMemcpyDeviceToHost, s));
   CK(cudaMemcpyAsync(hstats, ctx->d_stats, sizeof hstats, cudaMemcpyDeviceToHost, s));
   CK(cudaMemcpyAsync(&herr, ctx->d_err, sizeof(int), cudaMemcpyDeviceToHost, s));
   cudaError_t se = cudaStreamSynchronize(s);
@@ -1176,19 +802,32 @@ rt_status render_impl(rt_ctx* ctx, const rt_scene* sc, const rt_render_params* P
   if (herr & ERR_EMPTY_RANGE) return fail(ctx, RT_ERR_RENDER, "cannot sample empty range");
   if (herr & ERR_RANGE_OVERFLOW) return fail(ctx, RT_ERR_RENDER, "UniformSampler::sample_single: range overflow");
   if (herr & (ERR_WATCHDOG | ERR_STACK))
-    return fail(ctx, RT_ERR_DEVICE_WATCHDOG, herr & ERR_STACK ? "k-d traversal stack exhausted" : "rejection sampling did not terminate");
+    return fail(ctx, RT_ERR_DEVICE_WATCHDOG,
+                herr & ERR_STACK ? "traversal stack exhausted" : "rejection sampling did not terminate");
   if (stats) {
     float ms = 0.f;
     cudaEventElapsedTime(&ms, ctx->ev0, ctx->ev1);
     memset(stats, 0, sizeof *stats);
     if (max_depth > 0) {
       stats->primary_rays = (uint64_t)counts[0];
-      uint64_t refl = 0;
+      uint64_t refl = 0, hits = 0;
       for (int l = 1; l < levels; l++) refl += (uint64_t)counts[l];
+      for (int l = 0; l < levels; l++) hits += (uint64_t)nh[l];
       stats->reflection_rays = refl;
-      stats->shadow_rays = hstats[0];
+      stats->hits = hits;
+      stats->shadow_rays = hits * (uint64_t)K;
+      stats->trace_nodes = hstats[2];
+      stats->trace_triangles = hstats[3];
+      stats->trace_spheres = hstats[4];
+      stats->trace_verifications = hstats[5];
+      stats->shadow_nodes = hstats[6];
+      stats->shadow_triangles = hstats[7];
+      stats->shadow_spheres = hstats[8];
+      stats->shadow_verifications = hstats[9];
     }
+    stats->kernel_launches = Lc.launches;
     stats->device_ms = ms;
+    Lc.collect(stats->stage_ms);
     stats->total_ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
   }
   ctx->err.clear();
@@ -1208,7 +847,8 @@ rt_status rt_ctx_create(int device, rt_ctx** out) {
   int n = 0;
   cudaError_t e = cudaGetDeviceCount(&n);
   if (e != cudaSuccess || n == 0)
-    return fail(nullptr, RT_ERR_CUDA, std::string("no CUDA device: ") + (e != cudaSuccess ? cudaGetErrorString(e) : "count is 0"));
+    return fail(nullptr, RT_ERR_CUDA,
+                std::string("no CUDA device: ") + (e != cudaSuccess ? cudaGetErrorString(e) : "count is 0"));
   if (device < 0 || device >= n) return fail(nullptr, RT_ERR_INVALID_ARGUMENT, "device index out of range");
   auto c = std::make_unique<rt_ctx>();
   c->device = device;
@@ -1230,6 +870,7 @@ void rt_ctx_destroy(rt_ctx* ctx) {
   cudaSetDevice(ctx->device);
   if (ctx->stream) cudaStreamSynchronize(ctx->stream);
   free_all(ctx->scratch);
+  for (cudaEvent_t e : ctx->stage_ev) cudaEventDestroy(e);
   if (ctx->ev0) cudaEventDestroy(ctx->ev0);
   if (ctx->ev1) cudaEventDestroy(ctx->ev1);
   if (ctx->stream) cudaStreamDestroy(ctx->stream);
@@ -1291,6 +932,64 @@ void rt_scene_free(rt_scene* scene) {
   delete scene;
 }
 
+struct rt_host_scene {
+  HostScene hs;
+};
+
+rt_status rt_host_scene_load_json_file(const char* path, rt_host_scene** out) {
+  rt_ctx* ctx = nullptr;
+  if (!path || !out) return fail(ctx, RT_ERR_INVALID_ARGUMENT, "null argument");
+  *out = nullptr;
+  std::string text, err;
+  if (!read_text_file(path, &text, &err)) return fail(ctx, RT_ERR_IO, err);
+  auto h = std::make_unique<rt_host_scene>();
+  if (!load_scene_json(text, parent_dir(path), &h->hs, &err)) return fail(ctx, RT_ERR_SCENE, err);
+  *out = h.release();
+  return RT_OK;
+}
+
+rt_status rt_host_scene_load_json_str(const char* json, rt_host_scene** out) {
+  rt_ctx* ctx = nullptr;
+  if (!json || !out) return fail(ctx, RT_ERR_INVALID_ARGUMENT, "null argument");
+  *out = nullptr;
+  std::string err;
+  auto h = std::make_unique<rt_host_scene>();
+  if (!load_scene_json(json, ".", &h->hs, &err)) return fail(ctx, RT_ERR_SCENE, err);
+  *out = h.release();
+  return RT_OK;
+}
+
+const rt_scene_desc* rt_host_scene_desc(const rt_host_scene* hs) { return hs ? &hs->hs.desc : nullptr; }
+
+void rt_host_scene_free(rt_host_scene* hs) { delete hs; }
+
+rt_status rt_scene_device_bytes(rt_ctx* ctx, const rt_scene* scene, uint64_t* out) {
+  if (!scene || !out) return fail(ctx, RT_ERR_INVALID_ARGUMENT, "null argument");
+  *out = scene->uploaded_bytes;
+  return RT_OK;
+}
+
+rt_status rt_debug_fp64_rate(rt_ctx* ctx, double* gops) {
+  if (!ctx || !gops) return fail(ctx, RT_ERR_INVALID_ARGUMENT, "null argument");
+  CK(cudaSetDevice(ctx->device));
+  std::vector<void*> tmp;
+  double* d;
+  CK(dalloc(tmp, &d, 1));
+  const int blocks = ctx->num_sms * 8, threads = 256, iters = 4096;
+  k_fp64_rate<<<blocks, threads, 0, ctx->stream>>>(d, 64, 1.0000001, 1e-9);  // warm-up
+  CK(cudaEventRecord(ctx->ev0, ctx->stream));
+  k_fp64_rate<<<blocks, threads, 0, ctx->stream>>>(d, iters, 1.0000001, 1e-9);
+  CK(cudaEventRecord(ctx->ev1, ctx->stream));
+  CK(cudaGetLastError());
+  CK(cudaStreamSynchronize(ctx->stream));
+  float ms = 0.f;
+  CK(cudaEventElapsedTime(&ms, ctx->ev0, ctx->ev1));
+  free_all(tmp);
+  double ops = (double)blocks * threads * iters * 32.0;
+  *gops = ops / (ms * 1e-3) / 1e9;
+  return RT_OK;
+}
+
 rt_status rt_render(rt_ctx* ctx, const rt_scene* scene, const rt_render_params* params, uint8_t* rgb_out,
                     int out_on_device, rt_stats* stats) {
   return render_impl(ctx, scene, params, rgb_out, out_on_device, nullptr, stats);
@@ -1322,6 +1021,8 @@ rt_status rt_debug_stdrng_u32(rt_ctx* ctx, const uint64_t* seeds, int64_t n, int
 rt_status rt_debug_disk_offsets(rt_ctx* ctx, const uint64_t* light_seeds, int64_t n, double radius, double* out) {
   if (!ctx || !light_seeds || !out || n < 0) return fail(ctx, RT_ERR_INVALID_ARGUMENT, "bad argument");
   if (!(-radius < radius)) return fail(ctx, RT_ERR_RENDER, "cannot sample empty range");
+  if (!std::isfinite(radius - -radius))
+    return fail(ctx, RT_ERR_RENDER, "UniformSampler::sample_single: range overflow");
   if (n == 0) return RT_OK;
   CK(cudaSetDevice(ctx->device));
   std::vector<void*> tmp;
@@ -1347,11 +1048,16 @@ rt_status rt_debug_disk_offsets(rt_ctx* ctx, const uint64_t* light_seeds, int64_
 rt_status rt_debug_mesh_hit(rt_ctx* ctx, const rt_scene* scene, int32_t object_index, int32_t use_kdtree,
                             const double* rays, int64_t n, double t_min, double t_max, double* out) {
   if (!ctx || !scene || !rays || !out || n < 0) return fail(ctx, RT_ERR_INVALID_ARGUMENT, "bad argument");
-  if (object_index < 0 || object_index >= (int)scene->obj_kind.size() || scene->obj_kind[object_index] != RT_OBJ_MESH)
+  if (object_index < 0 || object_index >= (int)scene->obj_kind.size() ||
+      scene->obj_kind[object_index] != RT_OBJ_MESH)
     return fail(ctx, RT_ERR_INVALID_ARGUMENT, "object is not a mesh");
+  // bit 0: use_kdtree as the Renderer field; bits 1-2: the query
+  // (0 closest hit, 1 the plain k-d walk, 2 any hit)
+  int mode = (use_kdtree >> 1) & 3;
+  if (mode > 2) return fail(ctx, RT_ERR_INVALID_ARGUMENT, "bad query mode");
   if (n == 0) return RT_OK;
   CK(cudaSetDevice(ctx->device));
-  DMesh M = scene->host_meshes[scene->obj_index[object_index]];
+  DMesh M = scene->host_meshes[scene->obj_mesh[object_index]];
   std::vector<void*> tmp;
   double *dr, *dout;
   int* derr;
@@ -1360,15 +1066,15 @@ rt_status rt_debug_mesh_hit(rt_ctx* ctx, const rt_scene* scene, int32_t object_i
   CK(dalloc(tmp, &derr, 1));
   CK(cudaMemset(derr, 0, sizeof(int)));
   CK(cudaMemcpy(dr, rays, (size_t)n * 6 * sizeof(double), cudaMemcpyHostToDevice));
-  k_debug_mesh<<<(int)std::min<int64_t>((n + 127) / 128, 4096), 128, 0, ctx->stream>>>(M, use_kdtree, dr, n, t_min, t_max,
-                                                                                      dout, derr);
+  k_debug_mesh<<<(int)std::min<int64_t>((n + 127) / 128, 4096), 128, 0, ctx->stream>>>(
+      M, use_kdtree & 1, mode, dr, n, t_min, t_max, dout, derr);
   CK(cudaGetLastError());
   CK(cudaStreamSynchronize(ctx->stream));
   CK(cudaMemcpy(out, dout, (size_t)n * 8 * sizeof(double), cudaMemcpyDeviceToHost));
   int herr = 0;
   CK(cudaMemcpy(&herr, derr, sizeof(int), cudaMemcpyDeviceToHost));
   free_all(tmp);
-  if (herr) return fail(ctx, RT_ERR_DEVICE_WATCHDOG, "k-d traversal stack exhausted");
+  if (herr) return fail(ctx, RT_ERR_DEVICE_WATCHDOG, "traversal stack exhausted");
   return RT_OK;
 }
 

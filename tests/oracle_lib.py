@@ -37,6 +37,11 @@ def load():
                                 ctypes.c_uint32, ctypes.c_int, ctypes.c_uint64, ctypes.c_int, ctypes.c_int,
                                 ctypes.c_int, vp, vp, vp, ctypes.c_char_p, ctypes.c_int]
     L.oracle_render.restype = ctypes.c_int
+    L.oracle_render_rows.argtypes = [ctypes.c_char_p, ctypes.c_char_p, ctypes.c_uint32, ctypes.c_uint32,
+                                     ctypes.c_int, ctypes.c_uint32, ctypes.c_int, ctypes.c_uint64, ctypes.c_int,
+                                     ctypes.c_int, ctypes.c_int, ctypes.c_uint32, ctypes.c_uint32, vp, vp, vp,
+                                     ctypes.c_char_p, ctypes.c_int]
+    L.oracle_render_rows.restype = ctypes.c_int
     L.oracle_stdrng_u32.argtypes = [ctypes.c_uint64, ctypes.c_int, vp]
     L.oracle_stdrng_f64.argtypes = [ctypes.c_uint64, ctypes.c_int, vp]
     L.oracle_stdrng_range.argtypes = [ctypes.c_uint64, ctypes.c_double, ctypes.c_double, ctypes.c_int, vp]
@@ -72,7 +77,7 @@ def render(path=None, json_text=None, width=100, height=100, aa="quincunx", samp
     threads = threads or os.cpu_count() or 1
     rc = L.oracle_render(path.encode() if path else None, json_text.encode() if json_text else None, width, height,
                          AA[aa] if isinstance(aa, str) else int(aa), samples, max_depth, seed, 1 if use_kdtree else 0,
-                         1 if outline else 0, threads if not counts else 1, out.ctypes.data,
+                         1 if outline else 0, 1 if (counts and aa in ("quincunx", 1)) else threads, out.ctypes.data,
                          lin.ctypes.data if linear else None, cnt.ctypes.data if counts else None, err, 1024)
     if rc != 0:
         raise OracleError(err.value.decode())

@@ -76,24 +76,68 @@ def test_device_disk_samples(gpu_ctx, radius):
         assert np.array_equal(out[i], oracle_lib.disk_offsets(int(s), radius))
 
 
-@pytest.mark.parametrize("use_kd", [True, False])
-def test_kd_traversal_matches_oracle(gpu_ctx, tmp_path, use_kd):
-    from tests.kd_rays import plus_rays
-    stl = os.path.join(oracle_lib.SCENES, "plus.stl")
-    scene = {"camera": {"kind": "ortho", "position": [0, -5, 0], "target": [0, 0, 0], "up": [0, 0, 1],
-                        "width": 1, "height": 1},
-             "objects": [{"kind": "mesh", "filename": stl, "material": {"color": "#FFFFFF", "ambient": 0.1,
-                                                                       "diffuse": 0.7, "specular": 0.3,
-                                                                       "shininess": 32}}],
-             "lights": [], "scene_settings": {"ambient_illumination": {"color": "#FFFFFF", "intensity": 0.1}}}
-    sc = rt.Scene.from_json_str(json.dumps(scene))
-    rays = plus_rays(stl, extra_random=3000)
+def _mesh_scene(stl):
+    return json.dumps({
+        "camera": {"kind": "ortho", "position": [0, -5, 0], "target": [0, 0, 0], "up": [0, 0, 1], "width": 1,
+                   "height": 1},
+        "objects": [{"kind": "mesh", "filename": stl, "material": {"color": "#FFFFFF", "ambient": 0.1,
+                                                                  "diffuse": 0.7, "specular": 0.3,
+                                                                  "shininess": 32}}],
+        "lights": [], "scene_settings": {"ambient_illumination": {"color": "#FFFFFF", "intensity": 0.1}}})
+
+
+def _surface_rays(stl, n, seed):
+    """Rays starting on (or 0.001 above) triangles, in random directions:
+    the shape of shadow and reflection rays."""
+    from tests.kd_rays import stl_bounds
+    import struct
+    data = open(stl, "rb").read()
+    nt = struct.unpack("<I", data[80:84])[0]
+    rec = np.frombuffer(data[84:84 + 50 * nt], dtype=np.dtype([("n", "<f4", 3), ("v", "<f4", (3, 3)),
+                                                               ("a", "<u2")]))
+    v = rec["v"].astype(np.float64)
+    rng = np.random.default_rng(seed)
+    t = rng.integers(0, nt, n)
+    a, b = rng.random(n), rng.random(n)
+    flip = a + b > 1
+    a[flip], b[flip] = 1 - a[flip], 1 - b[flip]
+    p = v[t, 0] + a[:, None] * (v[t, 1] - v[t, 0]) + b[:, None] * (v[t, 2] - v[t, 0])
+    d = rng.normal(size=(n, 3))
+    return np.concatenate([p, d], 1)
+
+
+def _gpu_mesh(ctx, sc, rays, use_kd, mode, tmax=float("inf")):
     out = np.zeros((len(rays), 8))
-    st = rt._capi.lib().rt_debug_mesh_hit(gpu_ctx.handle, sc._handle, 0, 1 if use_kd else 0, rays.ctypes.data,
-                                          len(rays), 0.001, float("inf"), out.ctypes.data)
-    assert st == 0
+    st = rt._capi.lib().rt_debug_mesh_hit(ctx.handle, sc._handle, 0, (1 if use_kd else 0) | (mode << 1),
+                                          np.ascontiguousarray(rays).ctypes.data, len(rays), 0.001, tmax,
+                                          out.ctypes.data)
+    assert st == 0, rt._capi.lib().rt_last_error(ctx.handle)
+    return out
+
+
+@pytest.mark.parametrize("stl_name", ["plus.stl", "icosphere"])
+@pytest.mark.parametrize("use_kd", [True, False])
+def test_mesh_queries_match_oracle(gpu_ctx, tmp_path, use_kd, stl_name):
+    from tests.kd_rays import plus_rays
+    if stl_name == "plus.stl":
+        stl = os.path.join(oracle_lib.SCENES, "plus.stl")
+    else:
+        stl = os.path.join(str(tmp_path), "ico.stl")
+        v, f = workloads.noisy_icosphere(4, 3)
+        workloads.write_binary_stl(stl, v, f)
+    sc = rt.Scene.from_json_str(_mesh_scene(stl))
+    rays = np.concatenate([plus_rays(stl, extra_random=3000), _surface_rays(stl, 3000, 9)])
     ref = oracle_lib.mesh_hit(stl, rays, use_kdtree=use_kd)
-    assert np.array_equal(out, ref)
+    # closest hit: BVH candidates + reference-leaf verification, and the plain k-d walk
+    for mode in ((0, 1) if use_kd else (0,)):
+        out = _gpu_mesh(gpu_ctx, sc, rays, use_kd, mode)
+        bad = np.nonzero((out != ref).any(1))[0]
+        assert len(bad) == 0, (mode, len(bad), rays[bad[:3]].tolist(), out[bad[:3]].tolist(), ref[bad[:3]].tolist())
+    # any hit below a finite t_max == the reference's closest hit below it exists
+    tmax = 0.7
+    refa = oracle_lib.mesh_hit(stl, rays, use_kdtree=use_kd, tmax=tmax)
+    outa = _gpu_mesh(gpu_ctx, sc, rays, use_kd, 2, tmax)
+    assert np.array_equal(outa[:, 0], refa[:, 0])
 
 
 def _synthetic_scenes(tmp):
