@@ -67,7 +67,7 @@ struct DMesh {
   const double2* brute;    // triangle records in original order
   const double4* normals;  // normalize(e1 x e2) per triangle
   const double2* nodes;    // reference k-d tree, preorder
-  const double2* entries;  // k-d leaf entries (triangle records), leaf order
+  const int* leaf_tris;    // k-d leaf triangle lists, leaf order (KdNode::Leaf.triangles)
   const int2* leaf_path;   // per k-d node: {path bits (bit k: right at depth k), depth}
   const int* occ_off;      // per triangle: occurrences [occ_off[t], occ_off[t+1])
   const int2* occ;         // {k-d leaf node, position in the leaf}
@@ -315,6 +315,16 @@ __device__ __forceinline__ bool box_hit(const double* mn, const double* mx, cons
   return tl <= th && th >= 0.0 && !(tl > tmax * RTB_PRUNE_REL + RTB_PRUNE_ABS);
 }
 
+// `(split - origin) / dir >= 0.0` without the division (src/mesh.rs:441,
+// :448).  Here |dir| >= 1e-9 and |dir| <= 1 (a unit direction), so a
+// non-zero numerator gives a quotient of magnitude at least the smallest
+// subnormal: the quotient is non-negative exactly when the numerator is
+// zero or both signs agree (and neither operand is NaN).
+__device__ __forceinline__ bool split_ahead(double split, double origin, double dir) {
+  double diff = split - origin;
+  return (diff == 0.0 && dir == dir) || (diff > 0.0 && dir > 0.0) || (diff < 0.0 && dir < 0.0);
+}
+
 // Whether the reference's traversal tests k-d leaf `leaf` for this ray
 // (src/mesh.rs:399-465, leaf test :411); *key orders visited leaves in the
 // reference's depth-first visiting order (bit 31-k: far child at depth k).
@@ -334,8 +344,7 @@ __device__ __forceinline__ bool kd_leaf_visited(const DMesh& M, const RayC& r, i
     if (r.par & (1 << axis)) {
       if (go_right == left_side) return false;  // only the origin's side
     } else if (go_right == left_side) {         // far child: needs t_split >= 0
-      double ts = (split - op) / r.d[axis];
-      if (!(ts >= 0.0)) return false;
+      if (!split_ahead(split, op, r.d[axis])) return false;
       k_out |= 1u << (31 - k);
     }
     node = go_right ? right : node + 1;
@@ -344,6 +353,51 @@ __device__ __forceinline__ bool kd_leaf_visited(const DMesh& M, const RayC& r, i
   if (!kd_slab(M.nodes + 4 * (size_t)node, r, &te)) return false;
   *key = k_out;
   return true;
+}
+
+// Descends the reference's k-d tree towards the leaf whose cell holds point
+// p (a candidate's hit point), checking the reference's visiting rules on
+// the way.  Returns that leaf if the reference tests it, else -1.
+__device__ __forceinline__ int kd_locate_visited(const DMesh& M, const RayC& r, V3 p, unsigned* key, Work* w) {
+  int node = 0;
+  unsigned k_out = 0;
+  for (int depth = 0; depth < 32; depth++) {
+    double2 n3 = __ldg(M.nodes + 4 * (size_t)node + 3);
+    if (w) w->verify++;
+    int right = lo32(n3.y), axis = hi32(n3.y);
+    if (axis < 0) {
+      if (w) w->verify += 3;
+      double te;
+      if (!kd_slab(M.nodes + 4 * (size_t)node, r, &te)) return -1;
+      *key = k_out;
+      return node;
+    }
+    double split = n3.x;
+    bool go_right = !(p[axis] <= split);
+    double op = r.o[axis];
+    bool left_side = op <= split;
+    if (r.par & (1 << axis)) {
+      if (go_right == left_side) return -1;
+    } else if (go_right == left_side) {
+      if (!split_ahead(split, op, r.d[axis])) return -1;
+      k_out |= 1u << (31 - depth);
+    }
+    node = go_right ? right : node + 1;
+  }
+  return -1;
+}
+
+// Whether the reference tests triangle `tri` (hit at t) for this ray.  The
+// leaf whose cell holds the hit point is tried first; when it holds the
+// triangle and is visited, that settles it (need_order == false).
+__device__ __forceinline__ bool tri_visited_fast(const DMesh& M, const RayC& r, int tri, double t, Work* w) {
+  unsigned key;
+  int leaf = kd_locate_visited(M, r, r.o + t * r.d, &key, w);
+  if (leaf < 0) return false;
+  int b = __ldg(M.occ_off + tri), e = __ldg(M.occ_off + tri + 1);
+  for (int k = b; k < e; k++)
+    if (__ldg(M.occ + k).x == leaf) return true;
+  return false;
 }
 
 // The reference's first test of triangle `tri` for this ray: the smallest
@@ -392,11 +446,12 @@ __device__ bool mesh_kd_walk(const DMesh& M, const RayC& r, double tmin, double&
         int first = ma, cnt = -1 - mb;
         for (int k = 0; k < cnt; k++) {
           double t;
-          const double2* E = M.entries + 5 * (size_t)(first + k);
+          int tri = __ldg(M.leaf_tris + first + k);
+          const double2* E = M.brute + 5 * (size_t)tri;
           if (w) w->tris++;
           if (tri_t(E, r, tmin, closest, &t) && t < closest) {
             closest = t;
-            best_tri = lo32(__ldg(E + 4).y);
+            best_tri = tri;
             found = true;
             if (ANY) return true;
           }
@@ -411,8 +466,7 @@ __device__ bool mesh_kd_walk(const DMesh& M, const RayC& r, double tmin, double&
           node = near_c;
           continue;
         }
-        double ts = (split - op) / r.d[axis];
-        if (ts >= 0.0) {
+        if (split_ahead(split, op, r.d[axis])) {
           if (sp >= RTB_STACK) {
             atomicOr(err, ERR_STACK);
             return found;
@@ -555,6 +609,11 @@ __device__ bool mesh_closest(const DMesh& M, const RayC& r, double tmin, double&
     best_tri = bi;
     return true;
   }
+  if (nt == 1 && tri_visited_fast(M, r, ties[0], bt, w)) {
+    closest = bt;
+    best_tri = ties[0];
+    return true;
+  }
   if (!overflow) {
     unsigned long long bo = ~0ULL;
     int bi = -1;
@@ -589,8 +648,9 @@ __device__ bool mesh_any(const DMesh& M, const RayC& r, double tmin, double tmax
           if (w) w->tris++;
           if (tri_t(E, r, tmin, tmax, &t)) {
             if (!use_kd) return true;
+            int tri = lo32(__ldg(E + 4).y);
             unsigned long long o;
-            if (tri_first_visit(M, r, lo32(__ldg(E + 4).y), &o, w)) return true;
+            if (tri_visited_fast(M, r, tri, t, w) || tri_first_visit(M, r, tri, &o, w)) return true;
           }
         }
         return false;

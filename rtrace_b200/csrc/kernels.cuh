@@ -26,9 +26,11 @@ struct LevelBuf {
   double *r, *g, *b, *refl;
   int* child;
 };
+// Shadow rays of a chunk, sample-major: ray k of hit h (h relative to the
+// chunk) lives at k * chunk_hits + h, so that k_emit and k_resolve (one
+// thread per hit) read and write coalesced.
 struct ShadowBuf {
-  double *dx, *dy, *dz, *dist;  // per shadow ray
-  double *cr, *cg, *cb;         // contribution if visible
+  double *dx, *dy, *dz, *dist;  // per shadow ray: unit direction to the light sample, distance
   unsigned char* vis;
   double *ox, *oy, *oz;         // per hit: shadow-ray origin p + 0.001 n
 };
@@ -300,38 +302,31 @@ __global__ void __launch_bounds__(128) k_emit(DFrame F, int level, long long c0)
   const DScene& S = F.S;
   long long nh = F.nhits[level];
   long long c1 = c0 + F.chunk_hits < nh ? c0 + F.chunk_hits : nh;
-  const int K = S.shadow_per_hit;
   V3 campos = ld3(F.C.campos);
   for (long long h = c0 + blockIdx.x * (long long)blockDim.x + threadIdx.x; h < c1;
        h += (long long)gridDim.x * blockDim.x) {
     RayC rc;
     uint64_t seed;
     HitRec hr = load_hit(F, level, (int)h, &rc, &seed);
-    SMat m = effective_material(S.mat[hr.mat], hr);
-    V3 view = normalize(campos - hr.p);
     V3 so = hr.p + 0.001 * hr.n;
     long long hl = h - c0;
     F.sh.ox[hl] = so.x;
     F.sh.oy[hl] = so.y;
     F.sh.oz[hl] = so.z;
-    long long s = hl * K;
+    const long long CH = F.chunk_hits;
+    long long s = hl;  // advances by CH per shadow ray
     for (int li = 0; li < S.n_lights; li++) {
       const DLight& L0 = S.lights[li];
-      V3 lp = ld3(L0.pos), lc = ld3(L0.color);
+      V3 lp = ld3(L0.pos);
       if (!L0.disk) {
         // calculate_point_light_contribution (src/lighting.rs:100-142)
         V3 ldir = normalize(lp - hr.p);
         double dist = norm(lp - hr.p);
-        V3 sd = normalize(ldir);  // Ray::new
-        V3 c = light_term(m, hr, ldir, lc, L0.intensity, view);
-        F.sh.dx[s] = sd.x;
-        F.sh.dy[s] = sd.y;
-        F.sh.dz[s] = sd.z;
+        F.sh.dx[s] = ldir.x;
+        F.sh.dy[s] = ldir.y;
+        F.sh.dz[s] = ldir.z;
         F.sh.dist[s] = dist;
-        F.sh.cr[s] = c.x;
-        F.sh.cg[s] = c.y;
-        F.sh.cb[s] = c.z;
-        s++;
+        s += CH;
       } else {
         // calculate_diffuse_light_contribution (src/lighting.rs:145-217),
         // sample_disk_light_point (:69-97), sample_disk_point (:57-66)
@@ -351,7 +346,7 @@ __global__ void __launch_bounds__(128) k_emit(DFrame F, int level, long long c0)
         V3 up = fabs(cdir.x) < 0.9 ? mk(1.0, 0.0, 0.0) : mk(0.0, 1.0, 0.0);
         V3 bu = normalize(cross(up, cdir));
         V3 bv = normalize(cross(cdir, bu));
-        for (int smp = 0; smp < 16; smp++, s++) {
+        for (int smp = 0; smp < 16; smp++, s += CH) {
           double dx = 0.0, dy = 0.0;
           if (ok) {
             for (int it = 0;; it++) {
@@ -366,15 +361,10 @@ __global__ void __launch_bounds__(128) k_emit(DFrame F, int level, long long c0)
           V3 sp = lp + dx * bu + dy * bv;
           V3 sdir = normalize(sp - hr.p);
           double dist = norm(sp - hr.p);
-          V3 sd = normalize(sdir);
-          V3 c = light_term(m, hr, sdir, lc, L0.intensity, view);
-          F.sh.dx[s] = sd.x;
-          F.sh.dy[s] = sd.y;
-          F.sh.dz[s] = sd.z;
+          F.sh.dx[s] = sdir.x;
+          F.sh.dy[s] = sdir.y;
+          F.sh.dz[s] = sdir.z;
           F.sh.dist[s] = ok ? dist : -1.0;  // -1: never traced
-          F.sh.cr[s] = c.x;
-          F.sh.cg[s] = c.y;
-          F.sh.cb[s] = c.z;
         }
       }
     }
@@ -387,14 +377,20 @@ __global__ void __launch_bounds__(128) k_shadow(DFrame F, int level, long long c
   long long nh = F.nhits[level];
   long long c1 = c0 + F.chunk_hits < nh ? c0 + F.chunk_hits : nh;
   const int K = F.S.shadow_per_hit;
-  long long ns = c1 > c0 ? (c1 - c0) * K : 0;
+  long long nhc = c1 > c0 ? c1 - c0 : 0;
+  long long ns = nhc * K;
   Work w{0, 0, 0, 0};
-  for (long long s = blockIdx.x * (long long)blockDim.x + threadIdx.x; s < ns; s += (long long)gridDim.x * blockDim.x) {
-    long long hl = s / K;
+  for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < ns; t += (long long)gridDim.x * blockDim.x) {
+    // hit-major thread order: the K rays of one hit point run in adjacent
+    // lanes, which keeps a warp's traversals coherent
+    long long hl = t / K, k = t - hl * K;
+    long long s = k * F.chunk_hits + hl;
     double dist = F.sh.dist[s];
     unsigned char vis = 0;
     if (dist >= 0.0 || dist != dist) {
-      RayC r = make_rayc(mk(F.sh.ox[hl], F.sh.oy[hl], F.sh.oz[hl]), mk(F.sh.dx[s], F.sh.dy[s], F.sh.dz[s]));
+      // Ray::new normalises the (already unit) light direction once more
+      RayC r = make_rayc(mk(F.sh.ox[hl], F.sh.oy[hl], F.sh.oz[hl]),
+                         normalize(mk(F.sh.dx[s], F.sh.dy[s], F.sh.dz[s])));
       vis = world_any(F.S, r, 0.001, dist, F.use_kd != 0, F.err, COUNT ? &w : nullptr) ? 0 : 1;
     }
     F.sh.vis[s] = vis;
@@ -408,7 +404,6 @@ __global__ void __launch_bounds__(128) k_resolve(DFrame F, int level, long long 
   const DScene& S = F.S;
   long long nh = F.nhits[level];
   long long c1 = c0 + F.chunk_hits < nh ? c0 + F.chunk_hits : nh;
-  const int K = S.shadow_per_hit;
   RayBuf qn = F.q[(level + 1) & 1];
   LevelBuf L = F.levels[level];
   bool can_reflect = (F.max_depth - level) > 1;
@@ -430,20 +425,24 @@ __global__ void __launch_bounds__(128) k_resolve(DFrame F, int level, long long 
       const DMat& mat = S.mat[hr.mat];
       SMat m = effective_material(mat, hr);
       color = m.ka * S.amb_int * cmul(ld3(S.amb_color), m.c);
-      long long s = (h - c0) * K;
+      V3 view = normalize(campos - hr.p);
+      const long long CH = F.chunk_hits;
+      long long s = h - c0;  // advances by CH per shadow ray
       for (int li = 0; li < S.n_lights; li++) {
         const DLight& L0 = S.lights[li];
+        V3 lc = ld3(L0.color);
         V3 contrib;
         if (!L0.disk) {
-          contrib = F.sh.vis[s] ? mk(F.sh.cr[s], F.sh.cg[s], F.sh.cb[s]) : mk(0.0, 0.0, 0.0);
-          s++;
+          contrib = F.sh.vis[s] ? light_term(m, hr, mk(F.sh.dx[s], F.sh.dy[s], F.sh.dz[s]), lc, L0.intensity, view)
+                                : mk(0.0, 0.0, 0.0);
+          s += CH;
         } else {
           V3 total = mk(0.0, 0.0, 0.0);
           unsigned visible = 0;
-          for (int smp = 0; smp < 16; smp++, s++) {
+          for (int smp = 0; smp < 16; smp++, s += CH) {
             if (F.sh.vis[s]) {
               visible++;
-              total = total + mk(F.sh.cr[s], F.sh.cg[s], F.sh.cb[s]);
+              total = total + light_term(m, hr, mk(F.sh.dx[s], F.sh.dy[s], F.sh.dz[s]), lc, L0.intensity, view);
             }
           }
           contrib = (total / 16.0) * ((double)visible / 16.0);

@@ -101,7 +101,7 @@ void free_all(std::vector<void*>& v) {
   v.clear();
 }
 
-// Shadow-ray entries kept on the device at once (57 B each).
+// Shadow-ray entries kept on the device at once (33 B each).
 const long long kShadowCap = 1LL << 26;
 
 rt_status ensure_scratch(rt_ctx* ctx, long long n_rays, int levels, long long n_pix, long long n_shadow,
@@ -138,7 +138,6 @@ rt_status ensure_scratch(rt_ctx* ctx, long long n_rays, int levels, long long n_
   CK(dalloc(o, &ctx->d_nhits, Lv + 1));
   CK(dalloc(o, &F.sh.dx, SH)); CK(dalloc(o, &F.sh.dy, SH)); CK(dalloc(o, &F.sh.dz, SH));
   CK(dalloc(o, &F.sh.dist, SH));
-  CK(dalloc(o, &F.sh.cr, SH)); CK(dalloc(o, &F.sh.cg, SH)); CK(dalloc(o, &F.sh.cb, SH));
   CK(dalloc(o, &F.sh.vis, SH));
   CK(dalloc(o, &F.sh.ox, HS)); CK(dalloc(o, &F.sh.oy, HS)); CK(dalloc(o, &F.sh.oz, HS));
   CK(dalloc(o, &F.pdepth, R)); CK(dalloc(o, &F.pnx, R)); CK(dalloc(o, &F.pny, R)); CK(dalloc(o, &F.pnz, R));
@@ -330,12 +329,12 @@ rt_status upload_mesh(rt_ctx* ctx, rt_scene* sc, const rt_mesh_desc& md, DMesh* 
       }
     }
   }
-  std::vector<double2> entries((size_t)md.n_tri_index * 5);
+  std::vector<int> leaf_tris((size_t)md.n_tri_index);
   std::vector<int> occ_off((size_t)nt + 1, 0);
   for (long long k = 0; k < md.n_tri_index; k++) {
     int t = md.tri_index[k];
     if (t < 0 || t >= nt) return fail(ctx, RT_ERR_INVALID_ARGUMENT, "k-d leaf index out of range");
-    for (int j = 0; j < 5; j++) entries[5 * k + j] = brute[5 * (size_t)t + j];
+    leaf_tris[k] = t;
     occ_off[t + 1]++;
   }
   for (long long t = 0; t < nt; t++) occ_off[t + 1] += occ_off[t];
@@ -372,14 +371,14 @@ rt_status upload_mesh(rt_ctx* ctx, rt_scene* sc, const rt_mesh_desc& md, DMesh* 
   M.normals = p4;
   if ((st = upload(ctx, sc, nodes, &p2)) != RT_OK) return st;
   M.nodes = p2;
-  if ((st = upload(ctx, sc, entries, &p2)) != RT_OK) return st;
-  M.entries = p2;
+  const int* pi;
+  if ((st = upload(ctx, sc, leaf_tris, &pi)) != RT_OK) return st;
+  M.leaf_tris = pi;
   const int2* pi2;
   if ((st = upload(ctx, sc, leaf_path, &pi2)) != RT_OK) return st;
   M.leaf_path = pi2;
   if ((st = upload(ctx, sc, occ, &pi2)) != RT_OK) return st;
   M.occ = pi2;
-  const int* pi;
   if ((st = upload(ctx, sc, occ_off, &pi)) != RT_OK) return st;
   M.occ_off = pi;
   M.n_nodes = (int)md.n_nodes;
