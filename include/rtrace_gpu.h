@@ -286,6 +286,17 @@ rt_status rt_render(rt_ctx* ctx, const rt_scene* scene, const rt_render_params* 
 rt_status rt_render_linear(rt_ctx* ctx, const rt_scene* scene, const rt_render_params* params, uint8_t* rgb_out,
                            double* linear_out, rt_stats* stats);
 
+/* The outline post-process on its own (apply_outline_detection,
+ * src/outline.rs:86-278, then create_image_from_data, src/renderer.rs:
+ * 899-912), for hosts that produce their own colour and G-buffers.  All
+ * pointers are device memory on the context's device, one value per pixel,
+ * row-major: colours r/g/b before quantisation, valid = 1 where the pixel
+ * has a depth and normal, depth = camera distance, nx/ny/nz = world normal.
+ * rgb_out receives width*height*3 bytes.  config->enabled is ignored. */
+rt_status rt_outline_apply(rt_ctx* ctx, uint32_t width, uint32_t height, const double* r, const double* g,
+                           const double* b, const uint8_t* valid, const double* depth, const double* nx,
+                           const double* ny, const double* nz, const rt_outline_config* config, uint8_t* rgb_out);
+
 /* ------------------------------------------------------------------ */
 /* Device unit entry points used by the parity tests                   */
 /* ------------------------------------------------------------------ */

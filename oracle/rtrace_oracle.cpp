@@ -2222,6 +2222,29 @@ void oracle_chacha_block(const uint32_t* key, uint64_t counter, const uint32_t* 
   for (int i = 0; i < 16; i++) out[i] = x[i] + s[i];
 }
 
+// apply_outline_detection + create_image_from_data (src/outline.rs:86-110,
+// src/renderer.rs:899-912) on caller buffers: colours, depths and normals
+// planar (one double per pixel per plane), valid = 1 where the pixel has a
+// depth and normal.
+void oracle_outline(uint32_t W, uint32_t H, const double* r, const double* g, const double* b,
+                    const uint8_t* valid, const double* depth, const double* nx, const double* ny, const double* nz,
+                    double depth_weight, double normal_weight, double threshold, const double* edge_color,
+                    int use_8_neighbors, double thickness, uint8_t* rgb) {
+  using namespace orc;
+  size_t n = (size_t)W * H;
+  std::vector<V3> img(n), nrm(n);
+  std::vector<uint8_t> val(valid, valid + n);
+  std::vector<double> dep(depth, depth + n);
+  for (size_t i = 0; i < n; i++) {
+    img[i] = v3(r[i], g[i], b[i]);
+    nrm[i] = v3(nx[i], ny[i], nz[i]);
+  }
+  OutlineCfg cfg{depth_weight, normal_weight, threshold, v3(edge_color[0], edge_color[1], edge_color[2]),
+                 use_8_neighbors != 0, thickness};
+  apply_outline(img, val, dep, nrm, W, H, cfg);
+  quantize(img, rgb);
+}
+
 // The first n u32 words of StdRng::seed_from_u64(seed).
 void oracle_stdrng_u32(uint64_t seed, int n, uint32_t* out) {
   orc::StdRng r(seed);

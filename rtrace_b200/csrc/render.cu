@@ -989,6 +989,73 @@ rt_status rt_debug_fp64_rate(rt_ctx* ctx, double* gops) {
   return RT_OK;
 }
 
+namespace {
+// Checks the arguments of the outline entry points and fills the frame
+// fields the outline kernels read.
+rt_status outline_frame(rt_ctx* ctx, uint32_t width, uint32_t height, const double* r, const double* g,
+                        const double* b, const uint8_t* valid, const double* depth, const double* nx,
+                        const double* ny, const double* nz, const rt_outline_config* cfg, uint8_t* rgb_out,
+                        DFrame* F) {
+  if (!ctx || !r || !g || !b || !valid || !depth || !nx || !ny || !nz || !cfg || !rgb_out)
+    return fail(ctx, RT_ERR_INVALID_ARGUMENT, "null argument");
+  if (width == 0 || height == 0 || (uint64_t)width * height > 0x7fffffffULL)
+    return fail(ctx, RT_ERR_INVALID_ARGUMENT, "bad image size");
+  *F = DFrame{};
+  F->W = (int)width;
+  F->H = (int)height;
+  F->cr = const_cast<double*>(r);
+  F->cg = const_cast<double*>(g);
+  F->cb = const_cast<double*>(b);
+  F->valid = const_cast<unsigned char*>(valid);
+  F->dep = const_cast<double*>(depth);
+  F->nx = const_cast<double*>(nx);
+  F->ny = const_cast<double*>(ny);
+  F->nz = const_cast<double*>(nz);
+  F->rgb = rgb_out;
+  F->linear = nullptr;
+  F->o_wd = cfg->depth_weight;
+  F->o_wn = cfg->normal_weight;
+  F->o_thr = cfg->threshold;
+  for (int k = 0; k < 3; k++) F->o_color[k] = cfg->edge_color[k];
+  F->o_thick = cfg->line_thickness;
+  F->o_use8 = cfg->use_8_neighbors ? 1 : 0;
+  F->o_radius = 0;
+  if (cfg->line_thickness > 1.0) {
+    double rr = std::ceil(cfg->line_thickness - 1.0);
+    if (rr > 64.0) return fail(ctx, RT_ERR_INVALID_ARGUMENT, "outline thickness above 65 is not supported");
+    F->o_radius = (int)rr;
+  }
+  return RT_OK;
+}
+
+rt_status launch_outline(rt_ctx* ctx, const DFrame& F) {
+  dim3 ob(OT_X, OT_Y), og((F.W + OT_X - 1) / OT_X, (F.H + OT_Y - 1) / OT_Y);
+  k_outline_mask<<<og, ob, 0, ctx->stream>>>(F);
+  size_t shm = (size_t)(OT_X + 2 * F.o_radius) * (OT_Y + 2 * F.o_radius) * sizeof(double);
+  if (shm > 48 * 1024)
+    CK(cudaFuncSetAttribute(k_outline_apply, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)shm));
+  k_outline_apply<<<og, ob, shm, ctx->stream>>>(F);
+  CK(cudaGetLastError());
+  CK(cudaStreamSynchronize(ctx->stream));
+  return RT_OK;
+}
+}  // namespace
+
+rt_status rt_outline_apply(rt_ctx* ctx, uint32_t width, uint32_t height, const double* r, const double* g,
+                           const double* b, const uint8_t* valid, const double* depth, const double* nx,
+                           const double* ny, const double* nz, const rt_outline_config* config, uint8_t* rgb_out) {
+  DFrame F;
+  rt_status st = outline_frame(ctx, width, height, r, g, b, valid, depth, nx, ny, nz, config, rgb_out, &F);
+  if (st != RT_OK) return st;
+  CK(cudaSetDevice(ctx->device));
+  std::vector<void*> tmp;
+  CK(dalloc(tmp, &F.mask, (size_t)width * height));  // edge-strength scratch
+  st = launch_outline(ctx, F);
+  free_all(tmp);
+  if (st == RT_OK) ctx->err.clear();
+  return st;
+}
+
 rt_status rt_render(rt_ctx* ctx, const rt_scene* scene, const rt_render_params* params, uint8_t* rgb_out,
                     int out_on_device, rt_stats* stats) {
   return render_impl(ctx, scene, params, rgb_out, out_on_device, nullptr, stats);

@@ -58,6 +58,8 @@ def load():
     L.oracle_json_f64.argtypes = [ctypes.c_char_p, vp]
     L.oracle_json_f64.restype = ctypes.c_int
     L.oracle_chacha_block.argtypes = [vp, ctypes.c_uint64, vp, ctypes.c_int, vp]
+    L.oracle_outline.argtypes = [ctypes.c_uint32, ctypes.c_uint32] + [vp] * 8 + [ctypes.c_double] * 3 + \
+        [vp, ctypes.c_int, ctypes.c_double, vp]
     _lib = L
     return L
 
@@ -125,4 +127,21 @@ def mesh_hit(stl_path, rays, use_kdtree=True, tmin=0.001, tmax=float("inf")):
                                out.ctypes.data, err, 512)
     if r < 0:
         raise OracleError(err.value.decode())
+    return out
+
+
+def outline(color, valid, depth, normal, depth_weight=1.0, normal_weight=1.0, threshold=0.1,
+            edge_color=(0.0, 0.0, 0.0), use_8_neighbors=False, thickness=1.0):
+    """apply_outline_detection + quantisation on (H, W, 3) colours,
+    (H, W) valid/depth and (H, W, 3) normals; returns (H, W, 3) uint8."""
+    H, W = valid.shape
+    c = [np.ascontiguousarray(color[..., k], np.float64) for k in range(3)]
+    n = [np.ascontiguousarray(normal[..., k], np.float64) for k in range(3)]
+    v = np.ascontiguousarray(valid, np.uint8)
+    d = np.ascontiguousarray(depth, np.float64)
+    ec = np.asarray(edge_color, np.float64)
+    out = np.zeros((H, W, 3), np.uint8)
+    load().oracle_outline(W, H, c[0].ctypes.data, c[1].ctypes.data, c[2].ctypes.data, v.ctypes.data, d.ctypes.data,
+                          n[0].ctypes.data, n[1].ctypes.data, n[2].ctypes.data, depth_weight, normal_weight,
+                          threshold, ec.ctypes.data, 1 if use_8_neighbors else 0, thickness, out.ctypes.data)
     return out

@@ -203,3 +203,25 @@ def test_render_errors(gpu_ctx):
             rt.Renderer(10, 10).render(rt.Scene.from_json_str(json.dumps(s2)))
     with pytest.raises(rt.SceneError):
         rt.Scene.from_json_str("{\"camera\": 3}")
+
+
+OUTLINE_CFGS = [
+    {},
+    {"use_8_neighbors": True, "thickness": 2.0, "depth_weight": 0.8, "normal_weight": 2.0, "threshold": 0.06,
+     "edge_color": (0.2, 0.3, 0.4)},
+    {"thickness": 3.5, "threshold": 0.9, "edge_color": (1.0, 0.0, 0.5)},
+]
+
+
+@pytest.mark.parametrize("cfg", OUTLINE_CFGS)
+def test_outline_entry_point_matches_oracle(gpu_ctx, cfg):
+    from tests.gpu_outline import device_outline, gbuffers
+    for (w, h, seed) in [(97, 61, 1), (320, 200, 2)]:
+        color, valid, depth, normal = gbuffers(w, h, seed)
+        st, img = device_outline(gpu_ctx, rt._capi.lib().rt_outline_apply, color, valid, depth, normal, cfg)
+        assert st == 0
+        ref = oracle_lib.outline(color, valid, depth, normal, cfg.get("depth_weight", 1.0),
+                                 cfg.get("normal_weight", 1.0), cfg.get("threshold", 0.1),
+                                 cfg.get("edge_color", (0.0, 0.0, 0.0)), cfg.get("use_8_neighbors", False),
+                                 cfg.get("thickness", 1.0))
+        assert np.array_equal(img, ref), (w, h, int((img != ref).any(2).sum()))
