@@ -1,0 +1,48 @@
+"""Renders one of the benchmark workloads a few times, for profiler captures.
+
+    python -m rtrace_b200.profile_render --workload noisy_icosphere --width 960 --height 540 --reps 1
+
+Workloads (see rtrace_b200.workloads): sphere_grid (quincunx), noisy_icosphere
+(no-jitter + outline, the bench.py scene), ring_spheres (stochastic, 4 spp).
+Scene files are written to --dir (default: a temporary directory).
+"""
+import argparse
+import json
+import os
+import sys
+import tempfile
+
+
+def main(argv=None):
+    import rtrace_b200 as rt
+    from rtrace_b200 import workloads
+    ap = argparse.ArgumentParser(description="render a benchmark workload for profiling")
+    ap.add_argument("--workload", default="noisy_icosphere", choices=["sphere_grid", "noisy_icosphere", "ring_spheres"])
+    ap.add_argument("--width", type=int, default=960)
+    ap.add_argument("--height", type=int, default=540)
+    ap.add_argument("--reps", type=int, default=1)
+    ap.add_argument("--dir", default=None)
+    a = ap.parse_args(argv)
+    d = a.dir or tempfile.mkdtemp(prefix="rtb_prof_")
+    if a.workload == "sphere_grid":
+        path, aa, spp = workloads.write_scene(d, "sphere_grid.json", workloads.sphere_grid_scene()), 1, 1
+    elif a.workload == "noisy_icosphere":
+        path, aa, spp = workloads.make_noisy_icosphere(d, level=6, seed=7), 0, 1
+    else:
+        path, aa, spp = workloads.write_scene(d, "ring_spheres.json", workloads.ring_spheres_scene(seed=0)), 2, 4
+    scene = rt.Scene.from_json_file(path)
+    r = rt.Renderer(a.width, a.height)
+    r.anti_aliasing_mode = rt.AntiAliasingMode(aa)
+    r.samples = spp
+    if aa != 1:
+        r.outline_config = scene.get_outline_config()
+    for _ in range(a.reps):
+        r.render(scene)
+    st = r.last_stats
+    print(json.dumps({"workload": a.workload, "width": a.width, "height": a.height, "rays": st.rays,
+                      "device_ms": st.device_ms}))
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

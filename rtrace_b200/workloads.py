@@ -264,6 +264,5 @@ def make_terrain(directory, n=1024, seed=11):
 
 def cli_size(aspect, diagonal):
     """Image size from a diagonal (cli/src/main.rs:339-350)."""
-    h = diagonal / math.sqrt(aspect * aspect + 1.0)
-    w = aspect * h
-    return int(math.floor(w + 0.5)), int(math.floor(h + 0.5))
+    from rtrace_b200.cli import image_size
+    return image_size(aspect, diagonal)
