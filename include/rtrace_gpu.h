@@ -297,6 +297,31 @@ rt_status rt_outline_apply(rt_ctx* ctx, uint32_t width, uint32_t height, const d
                            const double* b, const uint8_t* valid, const double* depth, const double* nx,
                            const double* ny, const double* nz, const rt_outline_config* config, uint8_t* rgb_out);
 
+/* rt_outline_apply without any device allocation.  No counterpart in the
+ * reference (which never touches a GPU); it exists for callers that may
+ * not allocate device memory while they run this step: hosts whose device
+ * memory is owned by another allocator or arena (an engine or compositor
+ * that budgets every byte itself), frame loops where cudaMalloc's implicit
+ * device-wide synchronisation would stall their other streams, and
+ * long-running services that must not fail with out-of-memory mid-frame.
+ *
+ * The per-pixel edge-strength scratch lives in one static device array of
+ * RT_OUTLINE_NOALLOC_MAX_PIXELS doubles (32 MiB), which every device that
+ * loads this library keeps until the process exits; width * height above
+ * that limit is rejected with RT_ERR_INVALID_ARGUMENT.  The first call on
+ * a device looks up the array's device address (cudaGetSymbolAddress) and
+ * remembers it, so make that first call before any stream capture.  All
+ * calls share the array: calls whose work overlaps on the GPU (other
+ * threads, other contexts on the same device) race on it and must be
+ * serialised by the caller.  Nothing in it needs clearing between calls:
+ * the mask pass writes every pixel the blend pass reads.  Arguments and
+ * results are those of rt_outline_apply. */
+#define RT_OUTLINE_NOALLOC_MAX_PIXELS (2048u * 2048u)
+rt_status rt_outline_apply_noalloc(rt_ctx* ctx, uint32_t width, uint32_t height, const double* r,
+                                   const double* g, const double* b, const uint8_t* valid, const double* depth,
+                                   const double* nx, const double* ny, const double* nz,
+                                   const rt_outline_config* config, uint8_t* rgb_out);
+
 /* ------------------------------------------------------------------ */
 /* Device unit entry points used by the parity tests                   */
 /* ------------------------------------------------------------------ */

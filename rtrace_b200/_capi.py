@@ -57,6 +57,7 @@ class rt_render_params(ctypes.Structure):
     ]
 
 
+RT_OUTLINE_NOALLOC_MAX_PIXELS = 2048 * 2048
 RT_FLAG_STAGE_TIMES = 1
 RT_FLAG_COUNT_WORK = 2
 STAGES = ["raygen", "trace", "emit", "shadow", "resolve", "fold", "post", "other"]
@@ -120,6 +121,8 @@ def lib():
         "rt_debug_fp64_rate": (ctypes.c_int, [_vp, ctypes.POINTER(ctypes.c_double)]),
         "rt_outline_apply": (ctypes.c_int, [_vp, ctypes.c_uint32, ctypes.c_uint32, _vp, _vp, _vp, _vp, _vp, _vp,
                                             _vp, _vp, ctypes.POINTER(rt_outline_config), _vp]),
+        "rt_outline_apply_noalloc": (ctypes.c_int, [_vp, ctypes.c_uint32, ctypes.c_uint32, _vp, _vp, _vp, _vp,
+                                                    _vp, _vp, _vp, _vp, ctypes.POINTER(rt_outline_config), _vp]),
         "rt_debug_stdrng_u32": (ctypes.c_int, [_vp, _vp, ctypes.c_int64, ctypes.c_int32, _vp]),
         "rt_debug_disk_offsets": (ctypes.c_int, [_vp, _vp, ctypes.c_int64, ctypes.c_double, _vp]),
         "rt_debug_mesh_hit": (ctypes.c_int, [_vp, _vp, ctypes.c_int32, ctypes.c_int32, _vp, ctypes.c_int64,

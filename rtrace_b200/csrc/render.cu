@@ -1056,6 +1056,50 @@ rt_status rt_outline_apply(rt_ctx* ctx, uint32_t width, uint32_t height, const d
   return st;
 }
 
+// Scratch of rt_outline_apply_noalloc: the per-pixel edge strengths.  One
+// copy per device, alive for the life of the process; host code must not
+// use the symbol as an address (it is a host-side shadow), only the device
+// address that cudaGetSymbolAddress returns.
+static __device__ __align__(256) double g_outline_mask[RT_OUTLINE_NOALLOC_MAX_PIXELS];
+
+namespace {
+const int kMaxDevices = 64;
+std::mutex g_mask_mu;
+double* g_mask_addr[kMaxDevices] = {};  // device address of g_outline_mask, per device ordinal
+
+// Set-up, once per device, with that device current.
+rt_status noalloc_mask(rt_ctx* ctx, double** out) {
+  if (ctx->device < 0 || ctx->device >= kMaxDevices) return fail(ctx, RT_ERR_INVALID_ARGUMENT, "device ordinal too large");
+  std::lock_guard<std::mutex> g(g_mask_mu);
+  if (!g_mask_addr[ctx->device]) {
+    double* p = nullptr;
+    CK(cudaGetSymbolAddress((void**)&p, g_outline_mask));
+    if (!p) return fail(ctx, RT_ERR_CUDA, "cudaGetSymbolAddress returned a null address");
+    g_mask_addr[ctx->device] = p;
+  }
+  *out = g_mask_addr[ctx->device];
+  return RT_OK;
+}
+}  // namespace
+
+rt_status rt_outline_apply_noalloc(rt_ctx* ctx, uint32_t width, uint32_t height, const double* r,
+                                   const double* g, const double* b, const uint8_t* valid, const double* depth,
+                                   const double* nx, const double* ny, const double* nz,
+                                   const rt_outline_config* config, uint8_t* rgb_out) {
+  DFrame F;
+  rt_status st = outline_frame(ctx, width, height, r, g, b, valid, depth, nx, ny, nz, config, rgb_out, &F);
+  if (st != RT_OK) return st;
+  if ((uint64_t)width * height > RT_OUTLINE_NOALLOC_MAX_PIXELS)
+    return fail(ctx, RT_ERR_INVALID_ARGUMENT,
+                "image larger than the static outline scratch (RT_OUTLINE_NOALLOC_MAX_PIXELS = 4194304 pixels)");
+  CK(cudaSetDevice(ctx->device));
+  st = noalloc_mask(ctx, &F.mask);
+  if (st != RT_OK) return st;
+  st = launch_outline(ctx, F);
+  if (st == RT_OK) ctx->err.clear();
+  return st;
+}
+
 rt_status rt_render(rt_ctx* ctx, const rt_scene* scene, const rt_render_params* params, uint8_t* rgb_out,
                     int out_on_device, rt_stats* stats) {
   return render_impl(ctx, scene, params, rgb_out, out_on_device, nullptr, stats);
