@@ -204,6 +204,7 @@ def main():
 
     import rtrace_b200 as rt
     from rtrace_b200 import _capi
+    from rtrace_b200.distributed import reduce_timings
 
     if world > 1:
         torch.cuda.set_device(local)
@@ -270,13 +271,8 @@ def main():
         e2e_rays += r.last_stats.rays
 
     # max over ranks of the device time, sum of the work
-    t = torch.tensor([dev_ms, e2e_s], dtype=torch.float64, device=dev)
-    n = torch.tensor([float(rays), float(e2e_rays)], dtype=torch.float64, device=dev)
-    if world > 1:
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        dist.all_reduce(n, op=dist.ReduceOp.SUM)
-    dev_ms_max, e2e_s_max = float(t[0]), float(t[1])
-    rays_all, e2e_rays_all = float(n[0]), float(n[1])
+    (dev_ms_max, e2e_s_max), (rays_all, e2e_rays_all) = reduce_timings([dev_ms, e2e_s], [rays, e2e_rays],
+                                                                        device=dev)
     value = rays_all / (dev_ms_max * 1e-3) / 1e6
     e2e_value = e2e_rays_all / e2e_s_max / 1e6
 

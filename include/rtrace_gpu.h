@@ -281,6 +281,17 @@ rt_status rt_scene_device_bytes(rt_ctx* ctx, const rt_scene* scene, uint64_t* ou
 rt_status rt_render(rt_ctx* ctx, const rt_scene* scene, const rt_render_params* params, uint8_t* rgb_out,
                     int out_on_device, rt_stats* stats);
 
+/* Rows [row_begin, row_end) of the image rt_render produces, byte for byte
+ * (the unit of work of a frame split into row bands across GPUs; the
+ * reference renders whole frames only, so there is no single reference
+ * function, and the rows are those of Renderer::render, src/renderer.rs:
+ * 120-382).  rgb_out receives (row_end - row_begin) * width * 3 bytes.
+ * With the outline on, 1 + ceil(thickness - 1) rows beyond each inner band
+ * edge are traced as well (the outline stencil reads them); the stats count
+ * those rays too. */
+rt_status rt_render_rows(rt_ctx* ctx, const rt_scene* scene, const rt_render_params* params, uint32_t row_begin,
+                         uint32_t row_end, uint8_t* rgb_out, int out_on_device, rt_stats* stats);
+
 /* Same as rt_render but also returns the pre-quantisation colours
  * (width*height*3 doubles, host memory).  Used by parity tests. */
 rt_status rt_render_linear(rt_ctx* ctx, const rt_scene* scene, const rt_render_params* params, uint8_t* rgb_out,

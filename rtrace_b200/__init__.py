@@ -344,7 +344,7 @@ class Renderer:
                 _raise(code, ctxh)
             self.last_stats = RenderStats.from_c(st)
             return None
-        img = out if out is not None else np.empty((self.height, self.width, 3), np.uint8)
+        img = _check_out(out, (self.height, self.width, 3))
         if linear:
             lin = np.empty((self.height, self.width, 3), np.float64)
             code = L.rt_render_linear(ctxh, scene._handle, ctypes.byref(p), img.ctypes.data, lin.ctypes.data,
@@ -356,9 +356,37 @@ class Renderer:
         self.last_stats = RenderStats.from_c(st)
         return (img, lin) if linear else img
 
+    def render_rows(self, scene, row_begin, row_end, out=None, device_ptr=None):
+        """Rows [row_begin, row_end) of the image render() returns, as a
+        (row_end - row_begin, width, 3) uint8 array (or written to device_ptr,
+        returning None).  The unit of work of a frame split across GPUs."""
+        p = self._params()
+        st = _capi.rt_stats()
+        L = _capi.lib()
+        ctxh = scene._ctx.handle
+        if device_ptr is not None:
+            img, ptr, on_dev = None, int(device_ptr), 1
+        else:
+            img = _check_out(out, (max(0, int(row_end) - int(row_begin)), self.width, 3))
+            ptr, on_dev = img.ctypes.data, 0
+        code = L.rt_render_rows(ctxh, scene._handle, ctypes.byref(p), int(row_begin), int(row_end), ptr, on_dev,
+                                ctypes.byref(st))
+        if code != _capi.RT_OK:
+            _raise(code, ctxh)
+        self.last_stats = RenderStats.from_c(st)
+        return img
+
     def render_to_file(self, scene, output_path):
         """Renderer::render_to_file: renders and writes a PNG."""
         write_png(output_path, self.render(scene))
+
+
+def _check_out(out, shape):
+    if out is None:
+        return np.empty(shape, np.uint8)
+    if out.dtype != np.uint8 or tuple(out.shape) != tuple(shape) or not out.flags.c_contiguous:
+        raise ValueError(f"out must be a C-contiguous uint8 array of shape {tuple(shape)}")
+    return out
 
 
 def write_png(path, img):

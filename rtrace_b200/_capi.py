@@ -111,6 +111,8 @@ def lib():
         "rt_scene_free": (None, [_vp]),
         "rt_render": (ctypes.c_int, [_vp, _vp, ctypes.POINTER(rt_render_params), _vp, ctypes.c_int,
                                      ctypes.POINTER(rt_stats)]),
+        "rt_render_rows": (ctypes.c_int, [_vp, _vp, ctypes.POINTER(rt_render_params), ctypes.c_uint32,
+                                          ctypes.c_uint32, _vp, ctypes.c_int, ctypes.POINTER(rt_stats)]),
         "rt_render_linear": (ctypes.c_int, [_vp, _vp, ctypes.POINTER(rt_render_params), _vp, _vp,
                                             ctypes.POINTER(rt_stats)]),
         "rt_host_scene_load_json_file": (ctypes.c_int, [ctypes.c_char_p, ctypes.POINTER(_vp)]),

@@ -41,6 +41,10 @@ struct DFrame {
   DScene S;
   DCam C;
   int W, H, S_per_px, aa, max_depth, use_kd, outline, camera_mode;
+  // The frame buffers hold image rows [y0, y0 + H) of an image of height
+  // Himg (a row band; y0 = 0 and H = Himg for a whole image).  Camera
+  // coordinates and seeds use absolute rows.
+  int y0, Himg;
   uint64_t seed;
   long long n_primary;
   long long n_corner;  // quincunx corner rays, (W+1)(H+1)
@@ -121,15 +125,15 @@ __global__ void k_raygen(DFrame F) {
     uint64_t seed;
     if (F.aa == RT_AA_QUINCUNX) {
       // render_quincunx (src/renderer.rs:752-897)
-      double pw = 1.0 / (double)F.W, ph = 1.0 / (double)F.H;
+      double pw = 1.0 / (double)F.W, ph = 1.0 / (double)F.Himg;
       if (i < F.n_corner) {
-        unsigned cx = (unsigned)(i % (F.W + 1)), cy = (unsigned)(i / (F.W + 1));
+        unsigned cx = (unsigned)(i % (F.W + 1)), cy = (unsigned)(F.y0 + i / (F.W + 1));
         u = rclamp((double)cx * pw, 0.0, 1.0);
         v = rclamp(1.0 - (double)cy * ph, 0.0, 1.0);
         seed = F.seed * GOLD + (uint64_t)cx + (uint64_t)cy * 0x85EBCA6BULL;
       } else {
         long long j = i - F.n_corner;
-        unsigned x = (unsigned)(j % F.W), y = (unsigned)(j / F.W);
+        unsigned x = (unsigned)(j % F.W), y = (unsigned)(F.y0 + j / F.W);
         u = ((double)x + 0.5) * pw;
         v = 1.0 - ((double)y + 0.5) * ph;
         seed = F.seed * GOLD + (uint64_t)x * 0x85EBCA6BULL + (uint64_t)y * 0xC2B2AE35ULL + 0x12345678ULL;
@@ -138,10 +142,10 @@ __global__ void k_raygen(DFrame F) {
       // render_standard (src/renderer.rs:445-584)
       long long pix = i / F.S_per_px;
       unsigned s = (unsigned)(i % F.S_per_px);
-      unsigned x = (unsigned)(pix % F.W), y = (unsigned)(pix / F.W);
-      double wm1 = (double)(unsigned)(F.W - 1), hm1 = (double)(unsigned)(F.H - 1);
+      unsigned x = (unsigned)(pix % F.W), y = (unsigned)(F.y0 + pix / F.W);
+      double wm1 = (double)(unsigned)(F.W - 1), hm1 = (double)(unsigned)(F.Himg - 1);
       double pu = (double)x / wm1;
-      double pv = (double)(unsigned)(F.H - 1 - y) / hm1;
+      double pv = (double)(unsigned)(F.Himg - 1 - y) / hm1;
       double pwid = 1.0 / wm1, phei = 1.0 / hm1;
       uint64_t pseed = F.seed * GOLD + (uint64_t)x * 0x85EBCA6BULL + (uint64_t)y * 0xC2B2AE35ULL;
       seed = pseed + (uint64_t)s * 0x1F845FEDULL;

@@ -641,8 +641,14 @@ struct Launcher {
   }
 };
 
-rt_status render_impl(rt_ctx* ctx, const rt_scene* sc, const rt_render_params* P, uint8_t* rgb_out, int on_device,
-                      double* linear_out, rt_stats* stats) {
+// Renders image rows [row_begin, row_end) (the whole image when they are 0
+// and height) into rgb_out / linear_out, which hold those rows only.  A band
+// with the outline on traces 1 + radius extra rows on each inner side: the
+// edge mask of a kept row reads its neighbours' G-buffers and the dilation
+// reads masks up to radius rows away, so the extra rows make every kept
+// pixel's inputs those of the whole-image render.
+rt_status render_impl(rt_ctx* ctx, const rt_scene* sc, const rt_render_params* P, uint32_t row_begin,
+                      uint32_t row_end, uint8_t* rgb_out, int on_device, double* linear_out, rt_stats* stats) {
   auto t0 = std::chrono::steady_clock::now();
   if (!ctx || !sc || !P) return fail(ctx, RT_ERR_INVALID_ARGUMENT, "null argument");
   if (!rgb_out && !linear_out) return fail(ctx, RT_ERR_INVALID_ARGUMENT, "no output buffer");
@@ -658,8 +664,22 @@ rt_status render_impl(rt_ctx* ctx, const rt_scene* sc, const rt_render_params* P
   if (!sc->render_error.empty()) return fail(ctx, RT_ERR_RENDER, sc->render_error);
   CK(cudaSetDevice(ctx->device));
 
-  const int W = (int)P->width, H = (int)P->height;
+  const int W = (int)P->width, Himg = (int)P->height;
+  if (row_begin >= row_end || row_end > P->height)
+    return fail(ctx, RT_ERR_INVALID_ARGUMENT, "row range must satisfy row_begin < row_end <= height");
   const int aa = P->anti_aliasing_mode;
+  const bool outline = aa != RT_AA_QUINCUNX && P->outline.enabled;
+  int o_radius = 0;
+  if (outline && P->outline.line_thickness > 1.0) {
+    double rr = std::ceil(P->outline.line_thickness - 1.0);
+    if (rr > 64.0) return fail(ctx, RT_ERR_INVALID_ARGUMENT, "outline thickness above 65 is not supported");
+    o_radius = (int)rr;
+  }
+  const int halo = outline ? 1 + o_radius : 0;
+  const int y0 = std::max(0, (int)row_begin - halo);
+  const int H = std::min(Himg, (int)row_end + halo) - y0;  // rows traced
+  const long long keep_off = (long long)((int)row_begin - y0) * W;
+  const long long keep_pix = (long long)(row_end - row_begin) * W;
   const int spp = aa == RT_AA_QUINCUNX ? 1 : (int)P->samples;
   long long npix = (long long)W * H;
   long long ncorner = aa == RT_AA_QUINCUNX ? (long long)(W + 1) * (H + 1) : 0;
@@ -691,12 +711,14 @@ rt_status render_impl(rt_ctx* ctx, const rt_scene* sc, const rt_render_params* P
   F.C.half_th = cam.grid_half_thickness;
   F.W = W;
   F.H = H;
+  F.y0 = y0;
+  F.Himg = Himg;
   F.S_per_px = spp;
   F.aa = aa;
   F.max_depth = max_depth;
   F.use_kd = P->use_kdtree ? 1 : 0;
   F.camera_mode = aa == RT_AA_QUINCUNX ? 0 : 1;  // quincunx passes camera = None
-  F.outline = (aa != RT_AA_QUINCUNX && P->outline.enabled) ? 1 : 0;
+  F.outline = outline ? 1 : 0;
   F.seed = P->seed;
   F.n_primary = nprim;
   F.n_corner = ncorner;
@@ -713,12 +735,7 @@ rt_status render_impl(rt_ctx* ctx, const rt_scene* sc, const rt_render_params* P
   for (int k = 0; k < 3; k++) F.o_color[k] = P->outline.edge_color[k];
   F.o_thick = P->outline.line_thickness;
   F.o_use8 = P->outline.use_8_neighbors ? 1 : 0;
-  F.o_radius = 0;
-  if (F.outline && P->outline.line_thickness > 1.0) {
-    double rr = std::ceil(P->outline.line_thickness - 1.0);
-    if (rr > 64.0) return fail(ctx, RT_ERR_INVALID_ARGUMENT, "outline thickness above 65 is not supported");
-    F.o_radius = (int)rr;
-  }
+  F.o_radius = o_radius;
   double* d_linear = nullptr;
   std::vector<void*> tmp;
   if (linear_out) {
@@ -727,7 +744,8 @@ rt_status render_impl(rt_ctx* ctx, const rt_scene* sc, const rt_render_params* P
     F.linear = d_linear;
   }
   uint8_t* d_rgb = F.rgb;
-  if (rgb_out && on_device) F.rgb = rgb_out;
+  const bool direct = rgb_out && on_device && keep_off == 0 && keep_pix == npix;
+  if (direct) F.rgb = rgb_out;
 
   const bool count = (P->flags & RT_FLAG_COUNT_WORK) != 0;
   Launcher Lc{ctx, (P->flags & RT_FLAG_STAGE_TIMES) != 0};
@@ -786,8 +804,12 @@ rt_status render_impl(rt_ctx* ctx, const rt_scene* sc, const rt_render_params* P
   }
   CK(cudaGetLastError());
   CK(cudaEventRecord(ctx->ev1, s));
-  if (rgb_out && !on_device) CK(cudaMemcpyAsync(rgb_out, d_rgb, 3 * npix, cudaMemcpyDeviceToHost, s));
-  if (linear_out) CK(cudaMemcpyAsync(linear_out, d_linear, 3 * npix * sizeof(double), cudaMemcpyDeviceToHost, s));
+  if (rgb_out && !direct)
+    CK(cudaMemcpyAsync(rgb_out, d_rgb + 3 * keep_off, 3 * keep_pix,
+                       on_device ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost, s));
+  if (linear_out)
+    CK(cudaMemcpyAsync(linear_out, d_linear + 3 * keep_off, 3 * keep_pix * sizeof(double), cudaMemcpyDeviceToHost,
+                       s));
   std::vector<int> counts(levels + 2, 0), nh(levels + 1, 0);
   unsigned long long hstats[16];
   int herr = 0;
@@ -1102,12 +1124,20 @@ rt_status rt_outline_apply_noalloc(rt_ctx* ctx, uint32_t width, uint32_t height,
 
 rt_status rt_render(rt_ctx* ctx, const rt_scene* scene, const rt_render_params* params, uint8_t* rgb_out,
                     int out_on_device, rt_stats* stats) {
-  return render_impl(ctx, scene, params, rgb_out, out_on_device, nullptr, stats);
+  if (!params) return fail(ctx, RT_ERR_INVALID_ARGUMENT, "null argument");
+  return render_impl(ctx, scene, params, 0, params->height, rgb_out, out_on_device, nullptr, stats);
+}
+
+rt_status rt_render_rows(rt_ctx* ctx, const rt_scene* scene, const rt_render_params* params, uint32_t row_begin,
+                         uint32_t row_end, uint8_t* rgb_out, int out_on_device, rt_stats* stats) {
+  if (!rgb_out) return fail(ctx, RT_ERR_INVALID_ARGUMENT, "no output buffer");
+  return render_impl(ctx, scene, params, row_begin, row_end, rgb_out, out_on_device, nullptr, stats);
 }
 
 rt_status rt_render_linear(rt_ctx* ctx, const rt_scene* scene, const rt_render_params* params, uint8_t* rgb_out,
                            double* linear_out, rt_stats* stats) {
-  return render_impl(ctx, scene, params, rgb_out, 0, linear_out, stats);
+  if (!params) return fail(ctx, RT_ERR_INVALID_ARGUMENT, "null argument");
+  return render_impl(ctx, scene, params, 0, params->height, rgb_out, 0, linear_out, stats);
 }
 
 rt_status rt_debug_stdrng_u32(rt_ctx* ctx, const uint64_t* seeds, int64_t n, int32_t n_words, uint32_t* out) {
