@@ -112,6 +112,62 @@ class ClockSampler:
                 "samples": len(sm)}
 
 
+def learned_vs_plain(rt, torch, ctx, directory, steps):
+    """The metric's second half: the 1,000-sphere ring scene (two disk
+    lights) at 1920x1080, stochastic, 4 samples per pixel, rendered with the
+    reference's 16 shadow rays per disk light ("plain") and with one ray per
+    disk light at the primary hits plus the learned denoiser ("learned").
+    Both are timed (device events, L2 flushed per frame) and their primary
+    hits' visibility is compared, as PSNR over hit pixels of each present
+    light, with a 64-ray-per-light render of the same frame."""
+    from rtrace_b200 import denoiser, workloads
+    if not os.path.exists(denoiser.DEFAULT_WEIGHTS):
+        return {"unavailable": "no trained denoiser weights in the package"}
+    path = workloads.write_scene(directory, "ring_spheres.json", workloads.ring_spheres_scene(seed=0))
+    scene = rt.Scene.from_json_file(path, ctx)
+    dev = torch.device("cuda", ctx.device)
+    spp = 4
+    r = rt.Renderer(W, H)
+    r.anti_aliasing_mode = rt.AntiAliasingMode.Stochastic
+    r.samples = spp
+    vis = {k: torch.empty((spp, 2, H, W), dtype=torch.float32, device=dev) for k in ("target", "plain", "learned")}
+    feat = torch.empty((spp, H, W, 16), dtype=torch.float16, device=dev)
+    r.disk_samples = 64
+    r.render_shadow_aov(scene, vis["target"].data_ptr(), feat.data_ptr())
+    r.disk_samples = 16
+    r.render_shadow_aov(scene, vis["plain"].data_ptr(), None)
+    ctx.load_denoiser()
+    r.learned_shadows = True
+    r.render_shadow_aov(scene, vis["learned"].data_ptr(), None)
+    present = torch.stack([feat[..., 8], feat[..., 12]], 1) > 0
+    mask = (feat[..., 0] > 0).unsqueeze(1) & present
+    out = {"workload": "ring_spheres_1000_1080p_4spp", "target": "64 rays per disk light, same frame",
+           "psnr_over": "primary-hit samples x present disk lights"}
+    img = torch.empty(W * H * 3, dtype=torch.uint8, device=dev)
+    flush = torch.empty(512 * 1024 * 1024, dtype=torch.uint8, device=dev)
+    for mode in ("plain", "learned"):
+        r.learned_shadows = mode == "learned"
+        for _ in range(3):
+            r.render(scene, device_ptr=img.data_ptr())
+        ms, rays = 0.0, 0
+        for _ in range(steps):
+            flush.zero_()
+            torch.cuda.synchronize(dev)
+            r.render(scene, device_ptr=img.data_ptr())
+            ms += r.last_stats.device_ms
+            rays += r.last_stats.rays
+        out[mode] = {"ms_per_frame": ms / steps, "mrays_per_s": rays / (ms * 1e-3) / 1e6,
+                     "rays_per_frame": rays // steps,
+                     "vis_psnr_db": denoiser.psnr(vis[mode], vis["target"], mask)}
+    r.learned_shadows = True
+    r.flags = 1  # stage times
+    r.render(scene, device_ptr=img.data_ptr())
+    out["learned"]["denoise_ms"] = r.last_stats.stage_ms.get("denoise")
+    out["speedup"] = out["plain"]["ms_per_frame"] / out["learned"]["ms_per_frame"]
+    scene.close()
+    return out
+
+
 def read_traffic():
     """Per-launch DRAM bytes of the shadow kernel from the committed ncu summary."""
     try:
@@ -191,6 +247,7 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--cpu-seconds", type=float, default=15.0)
+    ap.add_argument("--no-learned", action="store_true", help="skip the learned-vs-plain shadow comparison")
     args = ap.parse_args()
     args.warmup = max(3, args.warmup)
     rank, world, local = env_int("RANK", 0), env_int("WORLD_SIZE", 1), env_int("LOCAL_RANK", 0)
@@ -310,6 +367,12 @@ def main():
             except Exception as e:  # the oracle is test infrastructure; report, do not fail
                 cpu = {"value": None, "unit": "Mrays/s", "cores": os.cpu_count(), "kind": "port",
                        "sample": "failed: %s" % e}
+        learned = None
+        if world == 1 and not args.no_learned:
+            try:
+                learned = learned_vs_plain(rt, torch, ctx, d, min(args.steps, 10))
+            except Exception as e:  # report, do not lose the headline line
+                learned = {"unavailable": "failed: %s" % e}
         line = {
             "metric": METRIC, "value": value, "unit": "Mrays/s", "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": dev_ms_max / args.steps, "higher_is_better": True,
@@ -327,6 +390,7 @@ def main():
             "stage_ms": {k: round(v, 4) for k, v in stages.items()},
             "work_per_frame": w,
             "cpu_baseline": cpu,
+            "learned_vs_plain": learned,
             "clocks": clk,
         }
         print(json.dumps(line), flush=True)

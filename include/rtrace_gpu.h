@@ -87,6 +87,15 @@ typedef struct rt_render_params {
   rt_outline_config outline;
   uint32_t flags;
   uint32_t reserved;
+  /* Extensions with no counterpart in the reference; zero keeps its
+   * behaviour.  disk_samples: shadow rays per disk light and shading point
+   * (0 means 16, the reference's constant; more samples continue the same
+   * StdRng stream).  learned_shadows: primary hits cast one ray per disk
+   * light and the learned denoiser (rt_denoiser_load) estimates each disk
+   * light's visibility from those rays and the hit's G-buffer; the light
+   * then contributes its light-centre term times the squared estimate. */
+  uint32_t disk_samples;
+  int32_t learned_shadows;
 } rt_render_params;
 
 /* Profiling flags: per-stage CUDA-event times, and device work counters
@@ -96,7 +105,7 @@ typedef struct rt_render_params {
 
 /* Stages reported in rt_stats.stage_ms */
 enum { RT_STAGE_RAYGEN = 0, RT_STAGE_TRACE = 1, RT_STAGE_EMIT = 2, RT_STAGE_SHADOW = 3, RT_STAGE_RESOLVE = 4,
-       RT_STAGE_FOLD = 5, RT_STAGE_POST = 6, RT_STAGE_COUNT = 8 };
+       RT_STAGE_FOLD = 5, RT_STAGE_POST = 6, RT_STAGE_DENOISE = 7, RT_STAGE_COUNT = 8 };
 
 /* Counters of one render.  Rays are counted the way the reference casts
  * them: primary (one per camera sample; quincunx casts W*H centre rays and
@@ -332,6 +341,35 @@ rt_status rt_outline_apply_noalloc(rt_ctx* ctx, uint32_t width, uint32_t height,
                                    const double* g, const double* b, const uint8_t* valid, const double* depth,
                                    const double* nx, const double* ny, const double* nz,
                                    const rt_outline_config* config, uint8_t* rgb_out);
+
+/* ------------------------------------------------------------------ */
+/* Learned soft shadows (extension; no counterpart in the reference)  */
+/* ------------------------------------------------------------------ */
+
+/* Loads the denoiser's weights into the context (replacing earlier ones).
+ * Blob layout, little endian: "RTDN", u32 version = 1, u32 n_layers, then
+ * per layer u32 cin, cout, dilation, activation (0 ReLU; 2 sigmoid, last
+ * layer only); then per layer FP16 weights [cout][3][3][cin] and FP32 bias
+ * [cout].  Channel counts are 16 or 32; the first layer reads the 16
+ * feature channels, the last writes 16 of which the first two are the
+ * visibility of disk-light slots 0 and 1. */
+rt_status rt_denoiser_load(rt_ctx* ctx, const void* blob, size_t bytes);
+
+/* Runs the loaded denoiser on a feature image ([planes][height][width][16]
+ * FP16, device) and writes the visibility estimates ([planes][2][height]
+ * [width] float, device). */
+rt_status rt_denoiser_run(rt_ctx* ctx, const uint16_t* features, uint32_t planes, uint32_t height, uint32_t width,
+                          float* visibility);
+
+/* rt_render plus, for the primary samples (plane = sample index within
+ * the pixel, so planes = samples), the shadow visibility each of the first
+ * two disk lights got (visible / disk_samples, or the denoised estimate
+ * with learned_shadows; meaningful where the feature image says the ray
+ * hit) and the denoiser's feature image.  vis and features are device
+ * pointers or NULL; rgb_out is host memory or NULL.  No-jitter or
+ * stochastic sampling only. */
+rt_status rt_render_shadow_aov(rt_ctx* ctx, const rt_scene* scene, const rt_render_params* params, uint8_t* rgb_out,
+                               float* vis, uint16_t* features, rt_stats* stats);
 
 /* ------------------------------------------------------------------ */
 /* Device unit entry points used by the parity tests                   */

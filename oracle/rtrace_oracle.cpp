@@ -1610,6 +1610,7 @@ struct Ctx {
   V3 background;
   std::vector<const Material*> materials;  // by object index
   Counters* ct;
+  uint32_t disk_samples = 16;  // shadow rays per disk light; the reference's constant is 16
 };
 
 // apply_texture (src/lighting.rs:9-54) then hex_to_color of the effective colour
@@ -1676,7 +1677,7 @@ static V3 point_light(const Ctx& c, const Hit& h, const ShadeMat& m, V3 lp, V3 l
 // sample_disk_light_point (:69-97) and sample_disk_point (:57-66)
 static V3 disk_light(const Ctx& c, const Hit& h, const ShadeMat& m, V3 lp, V3 lc, double li, double diameter,
                      uint64_t seed) {
-  const uint32_t SAMPLES = 16;
+  const uint32_t SAMPLES = c.disk_samples;
   uint64_t ls = seed * 0x9E3779B97F4A7C15ULL + sat_u64(h.point.x * 1000.0) * 0x85EBCA6BULL +
                 sat_u64(h.point.y * 1000.0) * 0xC2B2AE35ULL + sat_u64(h.point.z * 1000.0) * 0x6C8E9CF5ULL;
   StdRng rng(ls);
@@ -1877,6 +1878,7 @@ struct RenderOpts {
   bool outline = false;  // apply the scene's outline settings
   int threads = 1;
   uint32_t y0 = 0, y1 = UINT32_MAX;  // render only rows [y0, y1) (CPU baseline samples)
+  uint32_t disk_samples = 16;        // extension: shadow rays per disk light (16 in the reference)
 };
 
 static void build_world(const Scene& s, bool use_kd, World* w, std::vector<const Material*>* mats) {
@@ -2005,7 +2007,7 @@ static void render(const Scene& s, const RenderOpts& o, std::vector<V3>* out, Co
   }
   const uint32_t W = o.width, H = o.height;
   out->assign((size_t)W * H, v3(0, 0, 0));
-  Ctx c{&world, &s, nullptr, s.camera.position, bg, mats, ct};
+  Ctx c{&world, &s, nullptr, s.camera.position, bg, mats, ct, o.disk_samples};
   const uint64_t GOLD = 0x9E3779B97F4A7C15ULL;
 
   if (o.aa == 1) {  // render_quincunx (src/renderer.rs:752-897)
@@ -2155,11 +2157,31 @@ int oracle_render(const char* scene_path, const char* scene_json, uint32_t width
 // rows stay black and the outline pass (which needs whole-image buffers) is
 // skipped unless the band is the whole image.  Used to time bounded samples
 // of a frame for the CPU baseline.
+int oracle_render_ex(const char* scene_path, const char* scene_json, uint32_t width, uint32_t height, int aa,
+                     uint32_t samples, int max_depth, uint64_t seed, int use_kdtree, int outline, int threads,
+                     uint32_t y0, uint32_t y1, uint32_t disk_samples, uint8_t* out_rgb, double* out_linear,
+                     uint64_t* counts, char* err, int err_len);
+
 int oracle_render_rows(const char* scene_path, const char* scene_json, uint32_t width, uint32_t height, int aa,
                        uint32_t samples, int max_depth, uint64_t seed, int use_kdtree, int outline, int threads,
                        uint32_t y0, uint32_t y1, uint8_t* out_rgb, double* out_linear, uint64_t* counts, char* err,
                        int err_len) {
+  return oracle_render_ex(scene_path, scene_json, width, height, aa, samples, max_depth, seed, use_kdtree, outline,
+                          threads, y0, y1, 16, out_rgb, out_linear, counts, err, err_len);
+}
+
+// As oracle_render_rows with disk_samples shadow rays per disk light and
+// shading point (an extension: the reference always casts 16; the samples
+// continue the same StdRng stream, so the first 16 are the reference's).
+int oracle_render_ex(const char* scene_path, const char* scene_json, uint32_t width, uint32_t height, int aa,
+                     uint32_t samples, int max_depth, uint64_t seed, int use_kdtree, int outline, int threads,
+                     uint32_t y0, uint32_t y1, uint32_t disk_samples, uint8_t* out_rgb, double* out_linear,
+                     uint64_t* counts, char* err, int err_len) {
   using namespace orc;
+  if (disk_samples == 0) {
+    set_err(err, err_len, "disk_samples must be positive");
+    return 1;
+  }
   try {
     Scene s = scene_path ? parse_scene(read_file(scene_path), dir_of(scene_path))
                          : parse_scene(std::string(scene_json), ".");
@@ -2175,6 +2197,7 @@ int oracle_render_rows(const char* scene_path, const char* scene_json, uint32_t 
     o.threads = threads;
     o.y0 = y0;
     o.y1 = y1;
+    o.disk_samples = disk_samples;
     std::vector<V3> img;
     Counters ct;
     render(s, o, &img, counts ? &ct : nullptr);

@@ -114,6 +114,16 @@ class Context:
         self.handle = h
         self.device = device
 
+    def load_denoiser(self, weights=None):
+        """Loads the learned soft-shadow denoiser: a weight blob (bytes) or a
+        path; None loads the weights shipped with the package."""
+        from . import denoiser
+        blob = denoiser.read_blob(weights)
+        buf = ctypes.create_string_buffer(blob, len(blob))
+        st = _capi.lib().rt_denoiser_load(self.handle, buf, len(blob))
+        if st != _capi.RT_OK:
+            _raise(st, self.handle)
+
     def close(self):
         if self.handle:
             _capi.lib().rt_ctx_destroy(self.handle)
@@ -276,6 +286,9 @@ class Renderer:
         self.seed = 0
         self.outline_config = None
         self.flags = 0  # rtrace_b200._capi.RT_FLAG_* (profiling)
+        # extensions (the reference always casts 16 rays per disk light)
+        self.disk_samples = 16
+        self.learned_shadows = False  # needs Context.load_denoiser first
         self.last_stats = RenderStats()
 
     @classmethod
@@ -315,6 +328,8 @@ class Renderer:
         p.anti_aliasing_mode = int(self.anti_aliasing_mode)
         p.seed = int(self.seed or 0) & 0xFFFFFFFFFFFFFFFF
         p.flags = int(self.flags)
+        p.disk_samples = int(self.disk_samples)
+        p.learned_shadows = 1 if self.learned_shadows else 0
         oc = self.outline_config
         if oc is not None:
             p.outline.enabled = 1
@@ -371,6 +386,23 @@ class Renderer:
             ptr, on_dev = img.ctypes.data, 0
         code = L.rt_render_rows(ctxh, scene._handle, ctypes.byref(p), int(row_begin), int(row_end), ptr, on_dev,
                                 ctypes.byref(st))
+        if code != _capi.RT_OK:
+            _raise(code, ctxh)
+        self.last_stats = RenderStats.from_c(st)
+        return img
+
+    def render_shadow_aov(self, scene, vis_ptr=None, feat_ptr=None, out=None):
+        """Renders and also writes the primary samples' disk-light visibility
+        ([samples][2][H][W] float) and the denoiser feature image
+        ([samples][H][W][16] half) to the given device pointers (either may
+        be None).  Returns the (H, W, 3) uint8 image."""
+        p = self._params()
+        st = _capi.rt_stats()
+        ctxh = scene._ctx.handle
+        img = _check_out(out, (self.height, self.width, 3))
+        code = _capi.lib().rt_render_shadow_aov(ctxh, scene._handle, ctypes.byref(p), img.ctypes.data,
+                                                 None if vis_ptr is None else int(vis_ptr),
+                                                 None if feat_ptr is None else int(feat_ptr), ctypes.byref(st))
         if code != _capi.RT_OK:
             _raise(code, ctxh)
         self.last_stats = RenderStats.from_c(st)

@@ -54,13 +54,15 @@ class rt_render_params(ctypes.Structure):
         ("outline", rt_outline_config),
         ("flags", ctypes.c_uint32),
         ("reserved", ctypes.c_uint32),
+        ("disk_samples", ctypes.c_uint32),
+        ("learned_shadows", ctypes.c_int32),
     ]
 
 
 RT_OUTLINE_NOALLOC_MAX_PIXELS = 2048 * 2048
 RT_FLAG_STAGE_TIMES = 1
 RT_FLAG_COUNT_WORK = 2
-STAGES = ["raygen", "trace", "emit", "shadow", "resolve", "fold", "post", "other"]
+STAGES = ["raygen", "trace", "emit", "shadow", "resolve", "fold", "post", "denoise"]
 
 
 class rt_stats(ctypes.Structure):
@@ -113,6 +115,10 @@ def lib():
                                      ctypes.POINTER(rt_stats)]),
         "rt_render_rows": (ctypes.c_int, [_vp, _vp, ctypes.POINTER(rt_render_params), ctypes.c_uint32,
                                           ctypes.c_uint32, _vp, ctypes.c_int, ctypes.POINTER(rt_stats)]),
+        "rt_denoiser_load": (ctypes.c_int, [_vp, _vp, ctypes.c_size_t]),
+        "rt_denoiser_run": (ctypes.c_int, [_vp, _vp, ctypes.c_uint32, ctypes.c_uint32, ctypes.c_uint32, _vp]),
+        "rt_render_shadow_aov": (ctypes.c_int, [_vp, _vp, ctypes.POINTER(rt_render_params), _vp, _vp, _vp,
+                                                ctypes.POINTER(rt_stats)]),
         "rt_render_linear": (ctypes.c_int, [_vp, _vp, ctypes.POINTER(rt_render_params), _vp, _vp,
                                             ctypes.POINTER(rt_stats)]),
         "rt_host_scene_load_json_file": (ctypes.c_int, [ctypes.c_char_p, ctypes.POINTER(_vp)]),

@@ -3,9 +3,9 @@
 //              misses get their background/grid colour here, hits are
 //              compacted into the level's hit list (warp ballot + one atomic
 //              per warp)
-//   k_emit     per hit: effective material, light sampling (point lights:
-//              one ray; disk lights: 16 ChaCha12-driven disk samples) and
-//              each shadow ray's would-be contribution
+//   k_emit     per hit: light sampling (point lights: one ray; disk
+//              lights: 16 ChaCha12-driven disk samples in the reference,
+//              dsamp in general)
 //   k_shadow   one any-hit query per shadow ray
 //   k_resolve  per hit: ambient + visible contributions in the reference's
 //              summation order, fog, and the reflection ray, appended to
@@ -14,6 +14,9 @@
 // (src/lighting.rs:469-493), and k_pixels/k_outline_* produce the image.
 #pragma once
 
+#include <cuda_fp16.h>
+
+#include "denoise.hpp"
 #include "dscene.cuh"
 
 namespace rtb {
@@ -45,6 +48,19 @@ struct DFrame {
   // Himg (a row band; y0 = 0 and H = Himg for a whole image).  Camera
   // coordinates and seeds use absolute rows.
   int y0, Himg;
+  // Shadow rays per hit at the current level (point lights 1 each, disk
+  // lights dsamp each) and the disk-light sample count; both are set per
+  // level by the host.  The reference casts 16 per disk light.
+  int K, dsamp;
+  // Learned soft shadows (extension): at level 0 each disk light gets one
+  // ray, and its visibility comes from the denoiser's vhat
+  // ([plane][slot][H][W], plane = sample index within the pixel).
+  int learned;
+  int feat_on;          // write the feature image (and vis_aov) at level 0
+  __half* feat;         // [plane][H][W][FEAT_CHANNELS]
+  float* vhat;          // denoised visibility, read by k_resolve at level 0
+  float* vis_aov;       // optional: per slot visible/dsamp of level-0 hits
+  int n_slots;          // disk lights that are denoiser slots (<= DN_MAX_SLOTS)
   uint64_t seed;
   long long n_primary;
   long long n_corner;  // quincunx corner rays, (W+1)(H+1)
@@ -350,7 +366,7 @@ __global__ void __launch_bounds__(128) k_emit(DFrame F, int level, long long c0)
         V3 up = fabs(cdir.x) < 0.9 ? mk(1.0, 0.0, 0.0) : mk(0.0, 1.0, 0.0);
         V3 bu = normalize(cross(up, cdir));
         V3 bv = normalize(cross(cdir, bu));
-        for (int smp = 0; smp < 16; smp++, s += CH) {
+        for (int smp = 0; smp < F.dsamp; smp++, s += CH) {
           double dx = 0.0, dy = 0.0;
           if (ok) {
             for (int it = 0;; it++) {
@@ -380,7 +396,7 @@ template <bool COUNT>
 __global__ void __launch_bounds__(128) k_shadow(DFrame F, int level, long long c0) {
   long long nh = F.nhits[level];
   long long c1 = c0 + F.chunk_hits < nh ? c0 + F.chunk_hits : nh;
-  const int K = F.S.shadow_per_hit;
+  const int K = F.K;
   long long nhc = c1 > c0 ? c1 - c0 : 0;
   long long ns = nhc * K;
   Work w{0, 0, 0, 0};
@@ -432,6 +448,13 @@ __global__ void __launch_bounds__(128) k_resolve(DFrame F, int level, long long 
       V3 view = normalize(campos - hr.p);
       const long long CH = F.chunk_hits;
       long long s = h - c0;  // advances by CH per shadow ray
+      const bool learned = level == 0 && F.learned;
+      long long vix = 0;
+      if (learned) {
+        long long pix = i / F.S_per_px;
+        vix = ((long long)(i % F.S_per_px) * DN_MAX_SLOTS * F.H) * F.W + pix;  // slot 0 of this sample
+      }
+      int slot = 0;
       for (int li = 0; li < S.n_lights; li++) {
         const DLight& L0 = S.lights[li];
         V3 lc = ld3(L0.color);
@@ -440,16 +463,27 @@ __global__ void __launch_bounds__(128) k_resolve(DFrame F, int level, long long 
           contrib = F.sh.vis[s] ? light_term(m, hr, mk(F.sh.dx[s], F.sh.dy[s], F.sh.dz[s]), lc, L0.intensity, view)
                                 : mk(0.0, 0.0, 0.0);
           s += CH;
+        } else if (learned) {
+          // extension: the light-centre term times the squared visibility
+          // estimate, the expectation of the reference's
+          // (sum of visible terms / n) * (visible / n)
+          double v = (double)F.vhat[vix + (long long)slot * F.H * F.W];
+          v = rclamp(v, 0.0, 1.0);
+          V3 cdir = normalize(ld3(L0.pos) - hr.p);
+          contrib = light_term(m, hr, cdir, lc, L0.intensity, view) * (v * v);
+          slot++;
+          s += (long long)F.dsamp * CH;
         } else {
           V3 total = mk(0.0, 0.0, 0.0);
           unsigned visible = 0;
-          for (int smp = 0; smp < 16; smp++, s += CH) {
+          for (int smp = 0; smp < F.dsamp; smp++, s += CH) {
             if (F.sh.vis[s]) {
               visible++;
               total = total + light_term(m, hr, mk(F.sh.dx[s], F.sh.dy[s], F.sh.dz[s]), lc, L0.intensity, view);
             }
           }
-          contrib = (total / 16.0) * ((double)visible / 16.0);
+          const double n = (double)F.dsamp;  // 16.0 in the reference
+          contrib = (total / n) * ((double)visible / n);
         }
         color = color + contrib;
       }
@@ -495,6 +529,69 @@ __global__ void __launch_bounds__(128) k_resolve(DFrame F, int level, long long 
         qn.seed[slot] = seed;
       }
     }
+  }
+}
+
+// Denoiser input of the level-0 hits [c0, c1): one FEAT_CHANNELS FP16
+// pixel per (sample plane, pixel); misses stay zero (FEAT_VALID = 0).  Also
+// the plain visibility (visible / dsamp) of each slot into vis_aov.
+__global__ void __launch_bounds__(128) k_features(DFrame F, long long c0) {
+  const DScene& S = F.S;
+  long long nh = F.nhits[0];
+  long long c1 = c0 + F.chunk_hits < nh ? c0 + F.chunk_hits : nh;
+  V3 campos = ld3(F.C.campos);
+  const long long CH = F.chunk_hits;
+  const long long plane_px = (long long)F.H * F.W;
+  for (long long h = c0 + blockIdx.x * (long long)blockDim.x + threadIdx.x; h < c1;
+       h += (long long)gridDim.x * blockDim.x) {
+    RayC rc;
+    uint64_t seed;
+    HitRec hr = load_hit(F, 0, (int)h, &rc, &seed);
+    int i = F.hit_ray[h];
+    long long pix = i / F.S_per_px;
+    long long plane = i % F.S_per_px;
+    float f[FEAT_CHANNELS];
+#pragma unroll
+    for (int c = 0; c < FEAT_CHANNELS; c++) f[c] = 0.f;
+    f[FEAT_VALID] = 1.f;
+    double d = norm(hr.p - campos);
+    f[FEAT_DEPTH] = (float)(d / (d + 4.0));
+    f[FEAT_NX] = (float)hr.n.x;
+    f[FEAT_NX + 1] = (float)hr.n.y;
+    f[FEAT_NX + 2] = (float)hr.n.z;
+    long long s = h - c0;
+    int slot = 0;
+    for (int li = 0; li < S.n_lights; li++) {
+      const DLight& L0 = S.lights[li];
+      if (!L0.disk) {
+        s += CH;
+        continue;
+      }
+      unsigned visible = 0;
+      for (int smp = 0; smp < F.dsamp; smp++, s += CH) visible += F.sh.vis[s];
+      if (slot < DN_MAX_SLOTS) {
+        float v = (float)visible / (float)F.dsamp;
+        V3 lp = ld3(L0.pos);
+        double dist = norm(lp - hr.p);
+        V3 cdir = normalize(lp - hr.p);
+        double cosc = rmax(dot(hr.n, cdir), 0.0);
+        double ang = rclamp(0.5 * L0.diameter / dist, 0.0, 1.0);
+        int b = FEAT_SLOT0 + FEAT_SLOT_STRIDE * slot;
+        f[b] = v;
+        f[b + 1] = (float)cosc;
+        f[b + 2] = (float)ang;
+        f[b + 3] = 1.f;
+        if (F.vis_aov) F.vis_aov[(plane * DN_MAX_SLOTS + slot) * plane_px + pix] = v;
+      }
+      slot++;
+    }
+    __align__(16) __half hv[FEAT_CHANNELS];
+#pragma unroll
+    for (int c = 0; c < FEAT_CHANNELS; c++) hv[c] = __float2half_rn(f[c]);
+    uint4* dst = reinterpret_cast<uint4*>(F.feat + (plane * plane_px + pix) * FEAT_CHANNELS);
+    const uint4* src = reinterpret_cast<const uint4*>(hv);
+    dst[0] = src[0];
+    dst[1] = src[1];
   }
 }
 

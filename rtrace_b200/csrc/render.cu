@@ -37,6 +37,7 @@ struct rt_scene {
   std::string render_error;
   std::vector<DMesh> host_meshes;       // device pointers, for the debug entry point
   std::vector<int> obj_kind, obj_mesh;  // per World object
+  int n_point_lights = 0, n_disk_lights = 0;
 };
 
 struct rt_ctx {
@@ -59,6 +60,12 @@ struct rt_ctx {
   int* d_nhits = nullptr;
   unsigned long long* d_stats = nullptr;
   int* d_err = nullptr;
+  // learned soft shadows: network and its buffers (grown on demand)
+  DenoiseNet net;
+  std::vector<void*> dn_scratch;
+  long long dn_cap = 0;  // primary samples the buffers hold
+  __half *d_feat = nullptr, *d_act0 = nullptr, *d_act1 = nullptr;
+  float* d_vhat = nullptr;
 };
 
 namespace {
@@ -154,6 +161,22 @@ rt_status ensure_scratch(rt_ctx* ctx, long long n_rays, int levels, long long n_
   ctx->cap_pixels = P;
   ctx->cap_shadow = SH;
   ctx->cap_hits_sh = HS;
+  return RT_OK;
+}
+
+// Feature image, two activation buffers and the visibility estimate for n
+// primary samples (32 + 2 * 64 + 8 bytes each).
+rt_status ensure_dn_scratch(rt_ctx* ctx, long long n) {
+  if (n <= ctx->dn_cap) return RT_OK;
+  CK(cudaStreamSynchronize(ctx->stream));
+  free_all(ctx->dn_scratch);
+  ctx->dn_cap = 0;
+  auto& o = ctx->dn_scratch;
+  CK(dalloc(o, &ctx->d_feat, n * FEAT_CHANNELS));
+  CK(dalloc(o, &ctx->d_act0, n * 32));
+  CK(dalloc(o, &ctx->d_act1, n * 32));
+  CK(dalloc(o, &ctx->d_vhat, n * DN_MAX_SLOTS));
+  ctx->dn_cap = n;
   return RT_OK;
 }
 
@@ -557,6 +580,7 @@ rt_status do_upload(rt_ctx* ctx, const rt_scene_desc* d, rt_scene** out) {
     L.disk = l.has_diameter ? 1 : 0;
     L.diameter = l.diameter;
     K += L.disk ? 16 : 1;
+    (L.disk ? sc->n_disk_lights : sc->n_point_lights)++;
   }
   rt_status st;
   const int4* po4;
@@ -647,8 +671,15 @@ struct Launcher {
 // edge mask of a kept row reads its neighbours' G-buffers and the dilation
 // reads masks up to radius rows away, so the extra rows make every kept
 // pixel's inputs those of the whole-image render.
+// Optional per-sample outputs of the primary hits (device pointers).
+struct AovOut {
+  float* vis = nullptr;   // [plane][DN_MAX_SLOTS][H][W]
+  __half* feat = nullptr; // [plane][H][W][FEAT_CHANNELS]
+};
+
 rt_status render_impl(rt_ctx* ctx, const rt_scene* sc, const rt_render_params* P, uint32_t row_begin,
-                      uint32_t row_end, uint8_t* rgb_out, int on_device, double* linear_out, rt_stats* stats) {
+                      uint32_t row_end, uint8_t* rgb_out, int on_device, double* linear_out, rt_stats* stats,
+                      const AovOut* aov = nullptr) {
   auto t0 = std::chrono::steady_clock::now();
   if (!ctx || !sc || !P) return fail(ctx, RT_ERR_INVALID_ARGUMENT, "null argument");
   if (!rgb_out && !linear_out) return fail(ctx, RT_ERR_INVALID_ARGUMENT, "no output buffer");
@@ -688,11 +719,36 @@ rt_status render_impl(rt_ctx* ctx, const rt_scene* sc, const rt_render_params* P
   int max_depth = P->max_depth;
   if (max_depth > RTB_MAX_LEVELS) return fail(ctx, RT_ERR_INVALID_ARGUMENT, "max_depth above 64 is not supported");
   int levels = std::max(1, std::min(max_depth, RTB_MAX_LEVELS));
-  const int K = sc->S.shadow_per_hit;
-  long long chunk = K > 0 ? std::max(1LL, std::min(nprim, kShadowCap / K)) : nprim;
-  long long n_shadow = std::max(1LL, chunk * std::max(K, 1));
-  rt_status st = ensure_scratch(ctx, nprim, levels, npix, n_shadow, chunk);
+  // Shadow rays per hit: 1 per point light, dsamp per disk light (16 in the
+  // reference).  Learned shadows cast 1 per disk light at level 0.
+  if (P->disk_samples > 4096) return fail(ctx, RT_ERR_INVALID_ARGUMENT, "disk_samples above 4096 is not supported");
+  const int dsamp = P->disk_samples ? (int)P->disk_samples : 16;
+  const bool learned = P->learned_shadows != 0 && sc->n_disk_lights > 0;
+  const bool want_aov = aov && (aov->vis || aov->feat);
+  const bool full_frame = row_begin == 0 && row_end == P->height;
+  if (learned || want_aov) {
+    if (aa == RT_AA_QUINCUNX)
+      return fail(ctx, RT_ERR_INVALID_ARGUMENT, "learned shadows and shadow AOVs need no-jitter or stochastic sampling");
+    if (!full_frame) return fail(ctx, RT_ERR_INVALID_ARGUMENT, "learned shadows and shadow AOVs render whole frames");
+  }
+  if (learned) {
+    if (sc->n_disk_lights > DN_MAX_SLOTS)
+      return fail(ctx, RT_ERR_INVALID_ARGUMENT, "learned shadows support at most two disk lights");
+    if (!ctx->net.loaded()) return fail(ctx, RT_ERR_INVALID_ARGUMENT, "learned shadows need rt_denoiser_load first");
+  }
+  const int K_full = sc->n_point_lights + sc->n_disk_lights * dsamp;
+  const int K_0 = learned ? sc->n_point_lights + sc->n_disk_lights : K_full;
+  auto chunk_for = [&](int K) { return K > 0 ? std::max(1LL, std::min(nprim, kShadowCap / K)) : nprim; };
+  const long long chunk_0 = chunk_for(K_0), chunk_n = chunk_for(K_full);
+  if (learned && chunk_0 < nprim)
+    return fail(ctx, RT_ERR_INVALID_ARGUMENT, "too many primary samples for learned shadows in one pass");
+  long long n_shadow = std::max(1LL, std::max(chunk_0 * std::max(K_0, 1), chunk_n * std::max(K_full, 1)));
+  rt_status st = ensure_scratch(ctx, nprim, levels, npix, n_shadow, std::max(chunk_0, chunk_n));
   if (st != RT_OK) return st;
+  if (learned || want_aov) {
+    st = ensure_dn_scratch(ctx, nprim);
+    if (st != RT_OK) return st;
+  }
 
   DFrame F = ctx->F;
   F.S = sc->S;
@@ -725,7 +781,15 @@ rt_status render_impl(rt_ctx* ctx, const rt_scene* sc, const rt_render_params* P
   F.levels = ctx->d_levels;
   F.counts = ctx->d_counts;
   F.nhits = ctx->d_nhits;
-  F.chunk_hits = chunk;
+  F.chunk_hits = chunk_0;
+  F.K = K_0;
+  F.dsamp = dsamp;
+  F.learned = learned ? 1 : 0;
+  F.feat_on = (learned || want_aov) ? 1 : 0;
+  F.feat = (aov && aov->feat) ? aov->feat : ctx->d_feat;
+  F.vhat = (aov && aov->vis) ? aov->vis : ctx->d_vhat;
+  F.vis_aov = (aov && aov->vis && !learned) ? aov->vis : nullptr;
+  F.n_slots = std::min(sc->n_disk_lights, (int)DN_MAX_SLOTS);
   F.stats = ctx->d_stats;
   F.err = ctx->d_err;
   F.linear = nullptr;
@@ -767,11 +831,22 @@ rt_status render_impl(rt_ctx* ctx, const rt_scene* sc, const rt_render_params* P
   if (max_depth > 0) {
     k_raygen<<<blocks(nprim, 256, 16), 256, 0, s>>>(F);
     Lc.after(RT_STAGE_RAYGEN);
-    long long nchunks = (nprim + chunk - 1) / chunk;
     for (int l = 0; l < levels; l++) {
+      // per-level shadow layout (k_emit/k_shadow/k_resolve read it from F)
+      const int K = l == 0 ? K_0 : K_full;
+      const long long chunk = l == 0 ? chunk_0 : chunk_n;
+      F.K = K;
+      F.chunk_hits = chunk;
+      F.dsamp = (l == 0 && learned) ? 1 : dsamp;
+      const bool feat = l == 0 && F.feat_on;
+      const long long nchunks = (nprim + chunk - 1) / chunk;
       if (count) k_trace<true><<<blocks(nprim, 128, 16), 128, 0, s>>>(F, l);
       else k_trace<false><<<blocks(nprim, 128, 16), 128, 0, s>>>(F, l);
       Lc.after(RT_STAGE_TRACE);
+      if (feat) {
+        CK(cudaMemsetAsync(F.feat, 0, (size_t)nprim * FEAT_CHANNELS * sizeof(__half), s));
+        if (F.vis_aov) CK(cudaMemsetAsync(F.vis_aov, 0, (size_t)nprim * DN_MAX_SLOTS * sizeof(float), s));
+      }
       for (long long c = 0; c < nchunks; c++) {
         long long c0 = c * chunk;
         k_emit<<<blocks(chunk, 128, 16), 128, 0, s>>>(F, l, c0);
@@ -781,7 +856,20 @@ rt_status render_impl(rt_ctx* ctx, const rt_scene* sc, const rt_render_params* P
           else k_shadow<false><<<blocks(chunk * K, 128, 32), 128, 0, s>>>(F, l, c0);
           Lc.after(RT_STAGE_SHADOW);
         }
+        if (feat) {
+          k_features<<<blocks(chunk, 128, 16), 128, 0, s>>>(F, c0);
+          Lc.after(RT_STAGE_DENOISE);
+        }
+        if (l == 0 && learned) continue;  // resolved after the denoiser (one chunk)
         k_resolve<<<blocks(chunk, 128, 16), 128, 0, s>>>(F, l, c0);
+        Lc.after(RT_STAGE_RESOLVE);
+      }
+      if (l == 0 && learned) {
+        cudaError_t le = cudaSuccess;
+        int nl = denoise_run(ctx->net, F.feat, spp, H, W, ctx->d_act0, ctx->d_act1, F.vhat, F.err, s, nsm, &le);
+        for (int k = 0; k < nl; k++) Lc.after(RT_STAGE_DENOISE);
+        if (le != cudaSuccess) return cuda_fail(ctx, le, "denoiser launch");
+        k_resolve<<<blocks(chunk, 128, 16), 128, 0, s>>>(F, l, 0);
         Lc.after(RT_STAGE_RESOLVE);
       }
     }
@@ -822,6 +910,7 @@ rt_status render_impl(rt_ctx* ctx, const rt_scene* sc, const rt_render_params* P
   if (se != cudaSuccess) return cuda_fail(ctx, se, "render");
   if (herr & ERR_EMPTY_RANGE) return fail(ctx, RT_ERR_RENDER, "cannot sample empty range");
   if (herr & ERR_RANGE_OVERFLOW) return fail(ctx, RT_ERR_RENDER, "UniformSampler::sample_single: range overflow");
+  if (herr & DN_ERR_WAIT) return fail(ctx, RT_ERR_DEVICE_WATCHDOG, "denoiser: a tensor-core wait timed out");
   if (herr & (ERR_WATCHDOG | ERR_STACK))
     return fail(ctx, RT_ERR_DEVICE_WATCHDOG,
                 herr & ERR_STACK ? "traversal stack exhausted" : "rejection sampling did not terminate");
@@ -836,7 +925,7 @@ rt_status render_impl(rt_ctx* ctx, const rt_scene* sc, const rt_render_params* P
       for (int l = 0; l < levels; l++) hits += (uint64_t)nh[l];
       stats->reflection_rays = refl;
       stats->hits = hits;
-      stats->shadow_rays = hits * (uint64_t)K;
+      stats->shadow_rays = (uint64_t)nh[0] * (uint64_t)K_0 + (hits - (uint64_t)nh[0]) * (uint64_t)K_full;
       stats->trace_nodes = hstats[2];
       stats->trace_triangles = hstats[3];
       stats->trace_spheres = hstats[4];
@@ -891,6 +980,8 @@ void rt_ctx_destroy(rt_ctx* ctx) {
   cudaSetDevice(ctx->device);
   if (ctx->stream) cudaStreamSynchronize(ctx->stream);
   free_all(ctx->scratch);
+  free_all(ctx->dn_scratch);
+  denoise_free(&ctx->net);
   for (cudaEvent_t e : ctx->stage_ev) cudaEventDestroy(e);
   if (ctx->ev0) cudaEventDestroy(ctx->ev0);
   if (ctx->ev1) cudaEventDestroy(ctx->ev1);
@@ -1132,6 +1223,62 @@ rt_status rt_render_rows(rt_ctx* ctx, const rt_scene* scene, const rt_render_par
                          uint32_t row_end, uint8_t* rgb_out, int out_on_device, rt_stats* stats) {
   if (!rgb_out) return fail(ctx, RT_ERR_INVALID_ARGUMENT, "no output buffer");
   return render_impl(ctx, scene, params, row_begin, row_end, rgb_out, out_on_device, nullptr, stats);
+}
+
+rt_status rt_denoiser_load(rt_ctx* ctx, const void* blob, size_t bytes) {
+  if (!ctx) return fail(nullptr, RT_ERR_INVALID_ARGUMENT, "null context");
+  CK(cudaSetDevice(ctx->device));
+  CK(cudaStreamSynchronize(ctx->stream));
+  std::string e = denoise_load(blob, bytes, &ctx->net);
+  if (!e.empty()) return fail(ctx, RT_ERR_INVALID_ARGUMENT, e);
+  ctx->err.clear();
+  return RT_OK;
+}
+
+rt_status rt_denoiser_run(rt_ctx* ctx, const uint16_t* features, uint32_t planes, uint32_t height, uint32_t width,
+                          float* visibility) {
+  if (!ctx) return fail(nullptr, RT_ERR_INVALID_ARGUMENT, "null context");
+  if (!features || !visibility) return fail(ctx, RT_ERR_INVALID_ARGUMENT, "null argument");
+  if (!ctx->net.loaded()) return fail(ctx, RT_ERR_INVALID_ARGUMENT, "no denoiser weights loaded");
+  if (planes == 0 || height == 0 || width == 0 || (uint64_t)planes * height * width > 0x7fffffffULL)
+    return fail(ctx, RT_ERR_INVALID_ARGUMENT, "bad feature image size");
+  if (((uintptr_t)features & 15) != 0) return fail(ctx, RT_ERR_INVALID_ARGUMENT, "features must be 16-byte aligned");
+  CK(cudaSetDevice(ctx->device));
+  long long n = (long long)planes * height * width;
+  rt_status st = ensure_dn_scratch(ctx, n);
+  if (st != RT_OK) return st;
+  // the scratch error word is shared with renders on this context
+  if (!ctx->d_err) {
+    st = ensure_scratch(ctx, 1, 1, 1, 1, 1);
+    if (st != RT_OK) return st;
+  }
+  CK(cudaMemsetAsync(ctx->d_err, 0, sizeof(int), ctx->stream));
+  cudaError_t le = cudaSuccess;
+  denoise_run(ctx->net, reinterpret_cast<const __half*>(features), (int)planes, (int)height, (int)width,
+              ctx->d_act0, ctx->d_act1, visibility, ctx->d_err, ctx->stream, ctx->num_sms, &le);
+  if (le != cudaSuccess) return cuda_fail(ctx, le, "denoiser launch");
+  int herr = 0;
+  CK(cudaMemcpyAsync(&herr, ctx->d_err, sizeof(int), cudaMemcpyDeviceToHost, ctx->stream));
+  CK(cudaStreamSynchronize(ctx->stream));
+  if (herr & DN_ERR_WAIT) return fail(ctx, RT_ERR_DEVICE_WATCHDOG, "denoiser: a tensor-core wait timed out");
+  ctx->err.clear();
+  return RT_OK;
+}
+
+rt_status rt_render_shadow_aov(rt_ctx* ctx, const rt_scene* scene, const rt_render_params* params, uint8_t* rgb_out,
+                               float* vis, uint16_t* features, rt_stats* stats) {
+  if (!params) return fail(ctx, RT_ERR_INVALID_ARGUMENT, "null argument");
+  if (features && ((uintptr_t)features & 15) != 0)
+    return fail(ctx, RT_ERR_INVALID_ARGUMENT, "features must be 16-byte aligned");
+  AovOut aov;
+  aov.vis = vis;
+  aov.feat = reinterpret_cast<__half*>(features);
+  std::vector<uint8_t> sink;
+  if (!rgb_out) {
+    sink.resize((size_t)params->width * params->height * 3);
+    rgb_out = sink.data();
+  }
+  return render_impl(ctx, scene, params, 0, params->height, rgb_out, 0, nullptr, stats, &aov);
 }
 
 rt_status rt_render_linear(rt_ctx* ctx, const rt_scene* scene, const rt_render_params* params, uint8_t* rgb_out,

@@ -42,6 +42,11 @@ def load():
                                      ctypes.c_int, ctypes.c_int, ctypes.c_uint32, ctypes.c_uint32, vp, vp, vp,
                                      ctypes.c_char_p, ctypes.c_int]
     L.oracle_render_rows.restype = ctypes.c_int
+    L.oracle_render_ex.argtypes = [ctypes.c_char_p, ctypes.c_char_p, ctypes.c_uint32, ctypes.c_uint32, ctypes.c_int,
+                                   ctypes.c_uint32, ctypes.c_int, ctypes.c_uint64, ctypes.c_int, ctypes.c_int,
+                                   ctypes.c_int, ctypes.c_uint32, ctypes.c_uint32, ctypes.c_uint32, vp, vp, vp,
+                                   ctypes.c_char_p, ctypes.c_int]
+    L.oracle_render_ex.restype = ctypes.c_int
     L.oracle_stdrng_u32.argtypes = [ctypes.c_uint64, ctypes.c_int, vp]
     L.oracle_stdrng_f64.argtypes = [ctypes.c_uint64, ctypes.c_int, vp]
     L.oracle_stdrng_range.argtypes = [ctypes.c_uint64, ctypes.c_double, ctypes.c_double, ctypes.c_int, vp]
@@ -69,18 +74,21 @@ class OracleError(Exception):
 
 
 def render(path=None, json_text=None, width=100, height=100, aa="quincunx", samples=1, max_depth=10, seed=0,
-           use_kdtree=True, outline=False, threads=None, linear=False, counts=False):
-    """Renders like Renderer::render; returns uint8 (H, W, 3) [, linear] [, counts]."""
+           use_kdtree=True, outline=False, threads=None, linear=False, counts=False, disk_samples=16):
+    """Renders like Renderer::render; returns uint8 (H, W, 3) [, linear] [, counts].
+    disk_samples: shadow rays per disk light (16 is the reference)."""
     L = load()
     out = np.zeros((height, width, 3), np.uint8)
     lin = np.zeros((height, width, 3), np.float64) if linear else None
     cnt = np.zeros(6, np.uint64) if counts else None
     err = ctypes.create_string_buffer(1024)
     threads = threads or os.cpu_count() or 1
-    rc = L.oracle_render(path.encode() if path else None, json_text.encode() if json_text else None, width, height,
-                         AA[aa] if isinstance(aa, str) else int(aa), samples, max_depth, seed, 1 if use_kdtree else 0,
-                         1 if outline else 0, 1 if (counts and aa in ("quincunx", 1)) else threads, out.ctypes.data,
-                         lin.ctypes.data if linear else None, cnt.ctypes.data if counts else None, err, 1024)
+    rc = L.oracle_render_ex(path.encode() if path else None, json_text.encode() if json_text else None, width, height,
+                            AA[aa] if isinstance(aa, str) else int(aa), samples, max_depth, seed,
+                            1 if use_kdtree else 0, 1 if outline else 0,
+                            1 if (counts and aa in ("quincunx", 1)) else threads, 0, 0xFFFFFFFF, disk_samples,
+                            out.ctypes.data, lin.ctypes.data if linear else None,
+                            cnt.ctypes.data if counts else None, err, 1024)
     if rc != 0:
         raise OracleError(err.value.decode())
     res = [out]
