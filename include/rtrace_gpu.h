@@ -96,6 +96,10 @@ typedef struct rt_render_params {
    * then contributes its light-centre term times the squared estimate. */
   uint32_t disk_samples;
   int32_t learned_shadows;
+  /* learned_shadows: rays per disk light at the primary hits (1..16); 0
+   * uses the count the loaded network was trained on. */
+  uint32_t learned_rays;
+  uint32_t reserved2;
 } rt_render_params;
 
 /* Profiling flags: per-stage CUDA-event times, and device work counters
@@ -278,6 +282,14 @@ void rt_scene_free(rt_scene* scene);
  * reported through rt_last_error(NULL). */
 typedef struct rt_host_scene rt_host_scene;
 rt_status rt_host_scene_load_json_file(const char* path, rt_host_scene** out);
+
+/* AutoCamera::generate_cameras (src/auto_camera.rs:9-130) over
+ * Scene::compute_finite_bounds (src/scene.rs:538-690): writes the left,
+ * front, top and perspective cameras, in that order, to out[0..3].  Fails
+ * with the scene's parse error or "Scene has no finite objects to compute
+ * bounds" (reported by rt_last_error(NULL)). */
+rt_status rt_auto_cameras_json_file(const char* path, rt_camera_config* out);
+rt_status rt_auto_cameras_json_str(const char* json, rt_camera_config* out);
 rt_status rt_host_scene_load_json_str(const char* json, rt_host_scene** out);
 const rt_scene_desc* rt_host_scene_desc(const rt_host_scene* hs);
 void rt_host_scene_free(rt_host_scene* hs);
@@ -343,14 +355,59 @@ rt_status rt_outline_apply_noalloc(rt_ctx* ctx, uint32_t width, uint32_t height,
                                    const rt_outline_config* config, uint8_t* rgb_out);
 
 /* ------------------------------------------------------------------ */
+/* Batched rendering (extension: the reference renders one frame per    */
+/* Renderer::render call; its CLI's auto-camera mode renders four)      */
+/* ------------------------------------------------------------------ */
+
+typedef struct rt_job {
+  const rt_scene* scene;          /* uploaded on the batch context's device */
+  const rt_camera_config* camera; /* NULL: the scene's camera; else this one (e.g. an auto-camera view) */
+  rt_render_params params;
+  uint8_t* rgb_out;               /* width * height * 3 bytes, host or device memory */
+  int32_t out_on_device;
+  int32_t status;                 /* out: this job's rt_status */
+  rt_stats stats;                 /* out */
+} rt_job;
+
+typedef struct rt_batch_stats {
+  uint32_t jobs;
+  uint32_t lanes;
+  uint64_t rays;          /* primary + reflection + shadow rays of all jobs */
+  double wall_ms;         /* host time of the whole batch */
+  double device_ms;       /* sum of the jobs' device times */
+  double busiest_lane_ms; /* largest per-lane sum of device times */
+} rt_batch_stats;
+
+/* Renders n jobs on `lanes` concurrent streams of the context's device
+ * (0: the count rt_batch_autotune chose for this context, else 4).  Jobs
+ * are assigned to lanes longest first by their estimated rays (width *
+ * height * samples * (1 + shadow rays per hit)) and each lane renders its
+ * jobs in that order, so small jobs run beside large ones.  Every job's
+ * image is byte for byte the one rt_render gives for the same scene,
+ * camera and params.  Returns RT_OK when every job rendered, else the
+ * first failing job's status (each job's own status is in jobs[i].status;
+ * rt_last_error names the job). */
+rt_status rt_render_batch(rt_ctx* ctx, rt_job* jobs, uint32_t n, uint32_t lanes, rt_batch_stats* stats);
+
+/* Renders the batch with 1, 2, 4 and 8 lanes, keeps the fastest for later
+ * rt_render_batch calls with lanes = 0, and returns it in *best_lanes. */
+rt_status rt_batch_autotune(rt_ctx* ctx, rt_job* jobs, uint32_t n, uint32_t* best_lanes);
+
+/* The assignment rt_render_batch makes: job i (estimated cost costs[i])
+ * goes to lane lane_of_job[i]; longest job first onto the least-loaded
+ * lane, ties to the lower lane. */
+rt_status rt_batch_assign(const double* costs, uint32_t n, uint32_t lanes, uint32_t* lane_of_job);
+
+/* ------------------------------------------------------------------ */
 /* Learned soft shadows (extension; no counterpart in the reference)  */
 /* ------------------------------------------------------------------ */
 
 /* Loads the denoiser's weights into the context (replacing earlier ones).
- * Blob layout, little endian: "RTDN", u32 version = 1, u32 n_layers, then
- * per layer u32 cin, cout, dilation, activation (0 ReLU; 2 sigmoid, last
- * layer only); then per layer FP16 weights [cout][3][3][cin] and FP32 bias
- * [cout].  Channel counts are 16 or 32; the first layer reads the 16
+ * Blob layout, little endian: "RTDN", u32 version (1 or 2), u32 n_layers,
+ * (version 2) u32 rays per disk light the network was trained on, then per
+ * layer u32 cin, cout, dilation (1..64), activation (0 ReLU; 2 sigmoid,
+ * last layer only); then per layer FP16 weights [cout][3][3][cin] and FP32
+ * bias [cout].  Channel counts are 16 or 32; the first layer reads the 16
  * feature channels, the last writes 16 of which the first two are the
  * visibility of disk-light slots 0 and 1. */
 rt_status rt_denoiser_load(rt_ctx* ctx, const void* blob, size_t bytes);

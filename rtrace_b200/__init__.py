@@ -22,7 +22,8 @@ from . import _capi
 __all__ = [
     "AntiAliasingMode", "OutlineConfig", "Scene", "Renderer", "RtraceError", "SceneError",
     "RenderError", "DeviceError", "Context", "RenderStats", "default_context", "write_png", "HostScene",
-    "fp64_rate",
+    "fp64_rate", "auto_cameras", "Job", "BatchStats", "render_batch", "batch_autotune", "batch_assign",
+    "camera_config",
 ]
 
 
@@ -289,6 +290,7 @@ class Renderer:
         # extensions (the reference always casts 16 rays per disk light)
         self.disk_samples = 16
         self.learned_shadows = False  # needs Context.load_denoiser first
+        self.learned_rays = 0  # rays per disk light at primary hits; 0: what the network was trained on
         self.last_stats = RenderStats()
 
     @classmethod
@@ -330,6 +332,7 @@ class Renderer:
         p.flags = int(self.flags)
         p.disk_samples = int(self.disk_samples)
         p.learned_shadows = 1 if self.learned_shadows else 0
+        p.learned_rays = int(self.learned_rays)
         oc = self.outline_config
         if oc is not None:
             p.outline.enabled = 1
@@ -419,6 +422,122 @@ def _check_out(out, shape):
     if out.dtype != np.uint8 or tuple(out.shape) != tuple(shape) or not out.flags.c_contiguous:
         raise ValueError(f"out must be a C-contiguous uint8 array of shape {tuple(shape)}")
     return out
+
+
+def camera_config(cam):
+    """A scene-JSON camera dict as an rt_camera_config."""
+    c = _capi.rt_camera_config()
+    c.kind = cam["kind"].encode()[:31]
+    for k in range(3):
+        c.position[k] = cam["position"][k]
+        c.target[k] = cam["target"][k]
+        c.up[k] = cam["up"][k]
+    c.width = cam.get("width", 1.0)
+    c.height = cam.get("height", 1.0)
+    if cam.get("fov") is not None:
+        c.has_fov = 1
+        c.fov = cam["fov"]
+    return c
+
+
+@dataclass
+class Job:
+    """One render of a batch: a scene, the Renderer settings, optionally a
+    camera dict that replaces the scene's (an auto-camera view)."""
+    scene: "Scene"
+    renderer: "Renderer"
+    camera: dict = None
+
+
+@dataclass
+class BatchStats:
+    jobs: int
+    lanes: int
+    rays: int
+    wall_ms: float
+    device_ms: float
+    busiest_lane_ms: float
+
+
+def _jobs_array(jobs, outs):
+    arr = (_capi.rt_job * len(jobs))()
+    keep = []
+    for i, j in enumerate(jobs):
+        a = arr[i]
+        a.scene = j.scene._handle.value if isinstance(j.scene._handle, ctypes.c_void_p) else j.scene._handle
+        if j.camera is not None:
+            c = camera_config(j.camera)
+            keep.append(c)
+            a.camera = ctypes.pointer(c)
+        a.params = j.renderer._params()
+        a.rgb_out = outs[i].ctypes.data
+        a.out_on_device = 0
+    return arr, keep
+
+
+def render_batch(jobs, lanes=0, ctx=None):
+    """rt_render_batch: renders every job (longest first over `lanes`
+    concurrent streams; 0 = the autotuned count) and returns their (H, W, 3)
+    uint8 images and the BatchStats.  Each image equals
+    job.renderer.render(job.scene) with the job's camera."""
+    if not jobs:
+        return [], BatchStats(0, 0, 0, 0.0, 0.0, 0.0)
+    ctx = ctx or jobs[0].scene._ctx
+    outs = [np.empty((j.renderer.height, j.renderer.width, 3), np.uint8) for j in jobs]
+    arr, keep = _jobs_array(jobs, outs)
+    bs = _capi.rt_batch_stats()
+    st = _capi.lib().rt_render_batch(ctx.handle, arr, len(jobs), int(lanes), ctypes.byref(bs))
+    if st != _capi.RT_OK:
+        _raise(st, ctx.handle)
+    for j, a in zip(jobs, arr):
+        j.renderer.last_stats = RenderStats.from_c(a.stats)
+    return outs, BatchStats(bs.jobs, bs.lanes, bs.rays, bs.wall_ms, bs.device_ms, bs.busiest_lane_ms)
+
+
+def batch_autotune(jobs, ctx=None):
+    """rt_batch_autotune: the fastest lane count for this batch (kept by the
+    context for render_batch(lanes=0))."""
+    ctx = ctx or jobs[0].scene._ctx
+    outs = [np.empty((j.renderer.height, j.renderer.width, 3), np.uint8) for j in jobs]
+    arr, keep = _jobs_array(jobs, outs)
+    best = ctypes.c_uint32()
+    st = _capi.lib().rt_batch_autotune(ctx.handle, arr, len(jobs), ctypes.byref(best))
+    if st != _capi.RT_OK:
+        _raise(st, ctx.handle)
+    return int(best.value)
+
+
+def batch_assign(costs, lanes):
+    """rt_batch_assign: the lane of each job for the given cost estimates."""
+    c = np.ascontiguousarray(costs, dtype=np.float64)
+    out = np.zeros(len(c), np.uint32)
+    st = _capi.lib().rt_batch_assign(c.ctypes.data if len(c) else None, len(c), int(lanes),
+                                     out.ctypes.data if len(c) else None)
+    if st != _capi.RT_OK:
+        _raise(st, None)
+    return out
+
+
+def auto_cameras(path=None, json_text=None):
+    """AutoCamera::generate_cameras (src/auto_camera.rs:9-130): the left,
+    front, top and perspective cameras framing the scene's finite objects,
+    as scene-JSON camera dicts keyed like AutoCameraResult::to_cameras_json."""
+    L = _capi.lib()
+    out = (_capi.rt_camera_config * 4)()
+    if path is not None:
+        st = L.rt_auto_cameras_json_file(str(path).encode(), out)
+    else:
+        st = L.rt_auto_cameras_json_str(json_text.encode(), out)
+    if st != _capi.RT_OK:
+        _raise(st, None)
+    res = {}
+    for name, c in zip(("left", "front", "top", "perspective"), out):
+        cam = {"kind": c.kind.decode(), "position": list(c.position), "target": list(c.target), "up": list(c.up),
+               "width": c.width, "height": c.height}
+        if c.has_fov:
+            cam["fov"] = c.fov
+        res[name] = cam
+    return res
 
 
 def write_png(path, img):

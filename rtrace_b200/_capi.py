@@ -42,6 +42,25 @@ class rt_outline_config(ctypes.Structure):
     ]
 
 
+class rt_camera_config(ctypes.Structure):
+    _fields_ = [
+        ("kind", ctypes.c_char * 32),
+        ("position", ctypes.c_double * 3),
+        ("target", ctypes.c_double * 3),
+        ("up", ctypes.c_double * 3),
+        ("width", ctypes.c_double),
+        ("height", ctypes.c_double),
+        ("has_fov", ctypes.c_int32),
+        ("has_grid_pitch", ctypes.c_int32),
+        ("has_grid_thickness", ctypes.c_int32),
+        ("grid_color_state", ctypes.c_int32),
+        ("fov", ctypes.c_double),
+        ("grid_pitch", ctypes.c_double),
+        ("grid_thickness", ctypes.c_double),
+        ("grid_color", ctypes.c_double * 3),
+    ]
+
+
 class rt_render_params(ctypes.Structure):
     _fields_ = [
         ("width", ctypes.c_uint32),
@@ -56,6 +75,8 @@ class rt_render_params(ctypes.Structure):
         ("reserved", ctypes.c_uint32),
         ("disk_samples", ctypes.c_uint32),
         ("learned_shadows", ctypes.c_int32),
+        ("learned_rays", ctypes.c_uint32),
+        ("reserved2", ctypes.c_uint32),
     ]
 
 
@@ -87,6 +108,29 @@ class rt_stats(ctypes.Structure):
     ]
 
 
+class rt_job(ctypes.Structure):
+    _fields_ = [
+        ("scene", ctypes.c_void_p),
+        ("camera", ctypes.POINTER(rt_camera_config)),
+        ("params", rt_render_params),
+        ("rgb_out", ctypes.c_void_p),
+        ("out_on_device", ctypes.c_int32),
+        ("status", ctypes.c_int32),
+        ("stats", rt_stats),
+    ]
+
+
+class rt_batch_stats(ctypes.Structure):
+    _fields_ = [
+        ("jobs", ctypes.c_uint32),
+        ("lanes", ctypes.c_uint32),
+        ("rays", ctypes.c_uint64),
+        ("wall_ms", ctypes.c_double),
+        ("device_ms", ctypes.c_double),
+        ("busiest_lane_ms", ctypes.c_double),
+    ]
+
+
 _vp = ctypes.c_void_p
 _lib = None
 
@@ -115,6 +159,13 @@ def lib():
                                      ctypes.POINTER(rt_stats)]),
         "rt_render_rows": (ctypes.c_int, [_vp, _vp, ctypes.POINTER(rt_render_params), ctypes.c_uint32,
                                           ctypes.c_uint32, _vp, ctypes.c_int, ctypes.POINTER(rt_stats)]),
+        "rt_auto_cameras_json_file": (ctypes.c_int, [ctypes.c_char_p, ctypes.POINTER(rt_camera_config)]),
+        "rt_auto_cameras_json_str": (ctypes.c_int, [ctypes.c_char_p, ctypes.POINTER(rt_camera_config)]),
+        "rt_render_batch": (ctypes.c_int, [_vp, ctypes.POINTER(rt_job), ctypes.c_uint32, ctypes.c_uint32,
+                                           ctypes.POINTER(rt_batch_stats)]),
+        "rt_batch_autotune": (ctypes.c_int, [_vp, ctypes.POINTER(rt_job), ctypes.c_uint32,
+                                             ctypes.POINTER(ctypes.c_uint32)]),
+        "rt_batch_assign": (ctypes.c_int, [_vp, ctypes.c_uint32, ctypes.c_uint32, _vp]),
         "rt_denoiser_load": (ctypes.c_int, [_vp, _vp, ctypes.c_size_t]),
         "rt_denoiser_run": (ctypes.c_int, [_vp, _vp, ctypes.c_uint32, ctypes.c_uint32, ctypes.c_uint32, _vp]),
         "rt_render_shadow_aov": (ctypes.c_int, [_vp, _vp, ctypes.POINTER(rt_render_params), _vp, _vp, _vp,

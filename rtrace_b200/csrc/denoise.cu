@@ -18,11 +18,15 @@
 // whole persistent loop.  Every wait is bounded; a wait that runs out sets
 // the error word and the CTA leaves after releasing its tensor memory.
 
+#include <cuda.h>
 #include <cuda_fp16.h>
 #include <cuda_runtime.h>
+#include <cudaTypedefs.h>
 
+#include <algorithm>
 #include <cstdint>
 #include <cstring>
+#include <mutex>
 
 #include "denoise.hpp"
 
@@ -77,10 +81,6 @@ __device__ __forceinline__ bool mbar_wait(uint32_t mbar, uint32_t parity) {
   return false;
 }
 
-__device__ __forceinline__ void cp_async16(uint32_t dst, const void* src, int bytes) {
-  asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;\n" ::"r"(dst), "l"(src), "r"(bytes) : "memory");
-}
-
 template <int N>
 __device__ __forceinline__ void tmem_ld(uint32_t taddr, uint32_t (&r)[N]);
 
@@ -107,52 +107,110 @@ __device__ __forceinline__ void tmem_ld<32>(uint32_t taddr, uint32_t (&r)[32]) {
 
 constexpr int TILE_M = 128;
 constexpr int TMEM_COLS = 32;  // >= COUT, power of two >= 32
+constexpr int MAX_DIL = 64;    // 128 + 2 * dilation pixels must fit one TMA box (<= 256)
 
+// Shared memory of one CTA: NSTAGE input halos of a tile (3 rows of
+// TILE_M + 2 * dil pixels, one block of 16-byte rows per 8 channels), the
+// weights, the pipeline's mbarriers, the TMEM address and an abort flag.
+constexpr int NSTAGE = 2;  // halo stages (TMA -> MMA)
+constexpr int NACC = 2;    // TMEM accumulators (MMA -> epilogue)
+constexpr int CONV_THREADS = 192;  // warps 0-3 epilogue, warp 4 TMA, warp 5 MMA
+__host__ __device__ constexpr int halo_px(int dil) { return TILE_M + 2 * dil; }
+__host__ __device__ constexpr int halo_block(int dil) { return ((halo_px(dil) * 16 + 127) / 128) * 128; }
 template <int CIN, int COUT>
 struct ConvSmem {
-  static constexpr int KCH = 9 * CIN / 8;                 // 16-byte K chunks
-  static constexpr int A_BYTES = KCH * TILE_M * 16;       // im2col tile
-  static constexpr int B_BYTES = KCH * COUT * 16;         // weights
-  // 32 KB of slack past the operands: a descriptor whose strides were
-  // misread would still read inside the CTA's own shared memory
-  static constexpr int SLACK = 32 * 1024;
-  static constexpr int TOTAL = 1024 + A_BYTES + B_BYTES + 64 + SLACK;
+  static constexpr int CPT = CIN / 8;                     // 16-byte channel chunks per pixel
+  static constexpr int B_BYTES = 9 * CPT * COUT * 16;     // weights
+  static constexpr int TAIL = 128;                        // barriers, TMEM slot, abort flag
+  static int a_bytes(int dil) { return 3 * CPT * halo_block(dil); }
+  static int total(int dil) { return 1024 + NSTAGE * a_bytes(dil) + B_BYTES + TAIL; }
 };
+
+__device__ __forceinline__ void tma_load_4d(uint32_t dst, const CUtensorMap* map, int c0, int c1, int c2, int c3,
+                                            uint32_t mbar) {
+  asm volatile(
+      "cp.async.bulk.tensor.4d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, %4, %5}], "
+      "[%6];" ::"r"(dst),
+      "l"(reinterpret_cast<uint64_t>(map)), "r"(c0), "r"(c1), "r"(c2), "r"(c3), "r"(mbar)
+      : "memory");
+}
+
+__device__ __forceinline__ void mbar_expect_tx(uint32_t mbar, uint32_t bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(mbar), "r"(bytes) : "memory");
+}
+
+__device__ __forceinline__ void mbar_arrive(uint32_t mbar) {
+  asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(mbar) : "memory");
+}
 
 // MODE 0: ReLU, FP16 output [plane][H][W][COUT].  MODE 2: sigmoid of the
 // first DN_MAX_SLOTS channels, float output [plane][slot][H][W].
+//
+// Tiles are 128-pixel runs of one row; the CTA walks tiles blockIdx.x,
+// blockIdx.x + gridDim.x, ... with three roles working on different tiles:
+//   warp 4 (TMA): loads tile i's halo into stage i % NSTAGE with 3 * CIN / 8
+//     boxes (8 channels x halo_px pixels of one row; the hardware zero-fills
+//     outside the image and the plane), once the MMAs of tile i - NSTAGE
+//     have released the stage;
+//   warp 5 (MMA): once the halo has landed and the epilogue has drained
+//     accumulator i % NACC, issues the 9 * CIN / 16 MMAs; tap (ky, kx) reads
+//     row ky's block from pixel kx * dil on (same staged data, descriptor
+//     start kx * dil * 16 bytes further); commits to the stage's "empty" and
+//     the accumulator's "full" barriers;
+//   warps 0-3 (epilogue): thread t reads accumulator row t (tcgen05.ld
+//     32x32b), releases the accumulator, adds the bias, applies the
+//     activation and stores.
+// Every wait is bounded; one that runs out raises the abort flag, all roles
+// leave their loops, and the TMA and MMA threads wait (bounded) for their
+// operations still in flight before the tensor memory is released.
 template <int CIN, int COUT, int MODE>
-__global__ void __launch_bounds__(128) k_conv3x3_tc(const __half* __restrict__ in, int planes, int H, int W, int dil,
-                                                     const uint4* __restrict__ wl, const float* __restrict__ bias,
-                                                     __half* __restrict__ out, float* __restrict__ vis, int* err) {
+__global__ void __launch_bounds__(CONV_THREADS) k_conv3x3_tc(const __grid_constant__ CUtensorMap in_map, int planes,
+                                                              int H, int W, int dil, const uint4* __restrict__ wl,
+                                                              const float* __restrict__ bias,
+                                                              __half* __restrict__ out, float* __restrict__ vis,
+                                                              int* err) {
   static_assert(CIN % 16 == 0 && COUT % 16 == 0 && COUT <= TMEM_COLS, "unsupported channel counts");
   using SM = ConvSmem<CIN, COUT>;
+  constexpr int CPT = SM::CPT;
   extern __shared__ unsigned char smem_raw[];
-  // 1024-byte aligned operand region
   uint32_t raw = smem_u32(smem_raw);
   uint32_t pad = (1024u - (raw & 1023u)) & 1023u;
   unsigned char* base = smem_raw + pad;
-  const uint32_t sA = raw + pad;
-  const uint32_t sB = sA + SM::A_BYTES;
-  unsigned char* tail = base + SM::A_BYTES + SM::B_BYTES;
-  uint64_t* mbar_p = reinterpret_cast<uint64_t*>(tail);
-  uint32_t* tslot = reinterpret_cast<uint32_t*>(tail + 8);
-  volatile int* s_fail = reinterpret_cast<volatile int*>(tail + 16);
-  const uint32_t mbar = smem_u32(mbar_p);
-  const int tid = threadIdx.x, warp = tid >> 5;
+  const int BLK = halo_block(dil);
+  const int A_BYTES = 3 * CPT * BLK;
+  const uint32_t sA = raw + pad;  // stage k at sA + k * A_BYTES
+  const uint32_t sB = sA + NSTAGE * A_BYTES;
+  unsigned char* tail = base + NSTAGE * A_BYTES + SM::B_BYTES;
+  const uint32_t bar0 = smem_u32(tail);  // full[NSTAGE], empty[NSTAGE], accf[NACC], acce[NACC]
+  auto full_bar = [&](int k) { return bar0 + 8u * k; };
+  auto empty_bar = [&](int k) { return bar0 + 8u * (NSTAGE + k); };
+  auto accf_bar = [&](int k) { return bar0 + 8u * (2 * NSTAGE + k); };
+  auto acce_bar = [&](int k) { return bar0 + 8u * (2 * NSTAGE + NACC + k); };
+  uint32_t* tslot = reinterpret_cast<uint32_t*>(tail + 8 * (2 * NSTAGE + 2 * NACC));
+  volatile int* abort_flag = reinterpret_cast<volatile int*>(tail + 8 * (2 * NSTAGE + 2 * NACC) + 4);
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
 
-  // weights -> shared memory (already in operand layout)
   {
-    uint4* dst = reinterpret_cast<uint4*>(base + SM::A_BYTES);
-    for (int i = tid; i < SM::B_BYTES / 16; i += 128) dst[i] = wl[i];
+    uint4* dst = reinterpret_cast<uint4*>(base + NSTAGE * A_BYTES);
+    for (int i = tid; i < SM::B_BYTES / 16; i += CONV_THREADS) dst[i] = wl[i];
   }
   if (tid == 0) {
-    asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(mbar) : "memory");
+    for (int k = 0; k < NSTAGE; k++) {
+      asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(full_bar(k)) : "memory");
+      asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(empty_bar(k)) : "memory");
+    }
+    for (int k = 0; k < NACC; k++) {
+      asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(accf_bar(k)) : "memory");
+      asm volatile("mbarrier.init.shared::cta.b64 [%0], 4;" ::"r"(acce_bar(k)) : "memory");
+    }
+    *abort_flag = 0;
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    asm volatile("prefetch.tensormap [%0];" ::"l"(reinterpret_cast<uint64_t>(&in_map)) : "memory");
   }
-  if (warp == 0) {
+  if (warp == 5) {
+    __syncwarp();
     asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(tslot)),
-                 "r"(TMEM_COLS)
+                 "r"(NACC * TMEM_COLS)
                  : "memory");
     asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
   }
@@ -162,120 +220,199 @@ __global__ void __launch_bounds__(128) k_conv3x3_tc(const __half* __restrict__ i
   asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
   const uint32_t tmem = *tslot;
   constexpr uint32_t IDESC = umma_idesc(TILE_M, COUT);
-  constexpr int KSTEPS = 9 * CIN / 16;
-  constexpr int CPT = CIN / 8;  // chunks per tap
-
+  const uint32_t tx_bytes = (uint32_t)(3 * CPT * halo_px(dil) * 16);
   const int tiles_x = (W + TILE_M - 1) / TILE_M;
   const long long ntiles = (long long)planes * H * tiles_x;
-  uint32_t phase = 0;
-  bool failed = false;
-  for (long long tile = blockIdx.x; tile < ntiles && !failed; tile += gridDim.x) {
-    const int tx = (int)(tile % tiles_x);
-    const long long py = tile / tiles_x;
-    const int y = (int)(py % H);
-    const long long p = py / H;
-    const int x0 = tx * TILE_M;
-    // 1. im2col: q -> (tap, pixel, chunk), chunk fastest so that a warp reads
-    // consecutive 16-byte pieces of consecutive pixels
-    for (int q = tid; q < 9 * TILE_M * CPT; q += 128) {
-      const int j = q % CPT;
-      const int rest = q / CPT;
-      const int r = rest % TILE_M;
-      const int t = rest / TILE_M;
-      const int xs = x0 + r + (t % 3 - 1) * dil;
-      const int ys = y + (t / 3 - 1) * dil;
-      const bool ok = xs >= 0 && xs < W && ys >= 0 && ys < H;
-      const __half* src = ok ? in + ((p * H + ys) * (long long)W + xs) * CIN + 8 * j : in;
-      cp_async16(sA + (uint32_t)((t * CPT + j) * (TILE_M * 16) + r * 16), src, ok ? 16 : 0);
-    }
-    asm volatile("cp.async.commit_group;\n" ::: "memory");
-    asm volatile("cp.async.wait_all;\n" ::: "memory");
-    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-    __syncthreads();
-    // 2. the MMA chain, issued by one thread
-    if (tid == 0) {
-      asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-#pragma unroll
-      for (int s = 0; s < KSTEPS; s++) {
-        uint64_t da = umma_desc(sA + (uint32_t)(s * 2 * TILE_M * 16), TILE_M * 16, 128);
-        uint64_t db = umma_desc(sB + (uint32_t)(s * 2 * COUT * 16), COUT * 16, 128);
-        mma_f16(tmem, da, db, IDESC, s > 0 ? 1u : 0u);
+  auto fail = [&]() {
+    if (!*abort_flag) atomicOr(err, DN_ERR_WAIT);
+    *abort_flag = 1;
+  };
+
+  if (warp == 4) {
+    // ---- TMA producer
+    if (lane == 0) {
+      long long issued = 0;
+      for (long long tile = blockIdx.x; tile < ntiles && !*abort_flag; tile += gridDim.x, issued++) {
+        const int s = (int)(issued % NSTAGE);
+        const uint32_t ph = (uint32_t)((issued / NSTAGE) & 1);
+        if (!mbar_wait(empty_bar(s), ph ^ 1u)) {
+          fail();
+          break;
+        }
+        const int tx = (int)(tile % tiles_x);
+        const long long py = tile / tiles_x;
+        const int y = (int)(py % H), p = (int)(py / H), x0 = tx * TILE_M;
+        mbar_expect_tx(full_bar(s), tx_bytes);
+        const uint32_t st = sA + (uint32_t)(s * A_BYTES);
+        for (int ky = 0; ky < 3; ky++)
+          for (int j = 0; j < CPT; j++)
+            tma_load_4d(st + (uint32_t)((ky * CPT + j) * BLK), &in_map, 8 * j, x0 - dil, y + (ky - 1) * dil, p,
+                        full_bar(s));
       }
-      mma_commit(mbar);
-    }
-    // thread 0 waits for the chain (bounded) and publishes the outcome, so
-    // that every thread takes the same path below
-    if (tid == 0) {
-      int f = 0;
-      if (!mbar_wait(mbar, phase)) {
-        atomicOr(err, DN_ERR_WAIT);
-        f = 1;
-        mbar_wait(mbar, phase);  // give the chain a second bound before TMEM is released
+      if (*abort_flag) {
+        // let the last NSTAGE loads land before the CTA's shared memory goes away
+        for (long long k = issued - NSTAGE; k < issued; k++)
+          if (k >= 0) mbar_wait(full_bar((int)(k % NSTAGE)), (uint32_t)((k / NSTAGE) & 1));
       }
-      *s_fail = f;
     }
-    __syncthreads();
-    if (*s_fail) {
-      failed = true;
-      break;
-    }
-    phase ^= 1u;
-    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-    // 3. epilogue: thread tid owns accumulator row (pixel) tid
-    uint32_t acc[COUT];
-    tmem_ld<COUT>(tmem + ((uint32_t)(warp * 32) << 16), acc);
-    asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
-    const int x = x0 + tid;
-    if (x < W) {
-      if (MODE == 0) {
-        __half* o = out + ((p * H + y) * (long long)W + x) * COUT;
+  } else if (warp == 5) {
+    // ---- MMA issuer
+    if (lane == 0) {
+      long long i = 0;
+      for (long long tile = blockIdx.x; tile < ntiles && !*abort_flag; tile += gridDim.x, i++) {
+        const int s = (int)(i % NSTAGE), a = (int)(i % NACC);
+        if (!mbar_wait(full_bar(s), (uint32_t)((i / NSTAGE) & 1)) ||
+            !mbar_wait(acce_bar(a), (uint32_t)((i / NACC) & 1) ^ 1u)) {
+          fail();
+          break;
+        }
+        asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+        const uint32_t st = sA + (uint32_t)(s * A_BYTES);
+        const uint32_t acc = tmem + (uint32_t)(a * TMEM_COLS);
 #pragma unroll
-        for (int c = 0; c < COUT; c += 8) {
-          __align__(16) __half h[8];
+        for (int t = 0; t < 9; t++) {
+          const int ky = t / 3, kx = t % 3;
 #pragma unroll
-          for (int e = 0; e < 8; e++) {
-            float v = __uint_as_float(acc[c + e]) + __ldg(bias + c + e);
-            h[e] = __float2half_rn(v > 0.f ? v : 0.f);
+          for (int s2 = 0; s2 < CIN / 16; s2++) {
+            uint64_t da = umma_desc(st + (uint32_t)((ky * CPT + 2 * s2) * BLK + kx * dil * 16), (uint32_t)BLK, 128);
+            uint64_t db = umma_desc(sB + (uint32_t)((t * CPT + 2 * s2) * COUT * 16), COUT * 16, 128);
+            mma_f16(acc, da, db, IDESC, (t > 0 || s2 > 0) ? 1u : 0u);
           }
-          *reinterpret_cast<uint4*>(o + c) = *reinterpret_cast<const uint4*>(h);
         }
-      } else {
+        mma_commit(empty_bar(s));
+        mma_commit(accf_bar(a));
+      }
+      if (*abort_flag && i > 0) mbar_wait(accf_bar((int)((i - 1) % NACC)), (uint32_t)(((i - 1) / NACC) & 1));
+    }
+  } else {
+    // ---- epilogue (warps 0-3: thread tid <-> TMEM lane tid <-> pixel x0 + tid)
+    long long i = 0;
+    for (long long tile = blockIdx.x; tile < ntiles; tile += gridDim.x, i++) {
+      const int a = (int)(i % NACC);
+      bool ok = true;
+      for (long long k = 0; k < kWaitLimit; k++) {
+        uint32_t done;
+        asm volatile(
+            "{\n\t.reg .pred p;\n\t"
+            "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+            "selp.u32 %0, 1, 0, p;\n\t"
+            "}\n"
+            : "=r"(done)
+            : "r"(accf_bar(a)), "r"((uint32_t)((i / NACC) & 1))
+            : "memory");
+        if (done) break;
+        if (*abort_flag || k + 1 == kWaitLimit) {
+          ok = false;
+          break;
+        }
+      }
+      // the four warps agree before the warp-collective TMEM load
+      if (__any_sync(0xffffffffu, !ok)) ok = false;
+      if (!ok) {
+        if (lane == 0) fail();
+        break;
+      }
+      asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+      uint32_t accv[COUT];
+      tmem_ld<COUT>(tmem + (uint32_t)(a * TMEM_COLS) + ((uint32_t)(warp * 32) << 16), accv);
+      asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+      asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+      if (lane == 0) mbar_arrive(acce_bar(a));
+      const int tx = (int)(tile % tiles_x);
+      const long long py = tile / tiles_x;
+      const int y = (int)(py % H), p = (int)(py / H);
+      const int x = tx * TILE_M + tid;
+      if (x < W) {
+        if (MODE == 0) {
+          __half* o = out + (((long long)p * H + y) * (long long)W + x) * COUT;
 #pragma unroll
-        for (int j = 0; j < DN_MAX_SLOTS; j++) {
-          float v = __uint_as_float(acc[j]) + __ldg(bias + j);
-          vis[((p * DN_MAX_SLOTS + j) * H + y) * (long long)W + x] = 1.f / (1.f + __expf(-v));
+          for (int c = 0; c < COUT; c += 8) {
+            __align__(16) __half h[8];
+#pragma unroll
+            for (int e = 0; e < 8; e++) {
+              float v = __uint_as_float(accv[c + e]) + __ldg(bias + c + e);
+              h[e] = __float2half_rn(v > 0.f ? v : 0.f);
+            }
+            *reinterpret_cast<uint4*>(o + c) = *reinterpret_cast<const uint4*>(h);
+          }
+        } else {
+#pragma unroll
+          for (int j = 0; j < DN_MAX_SLOTS; j++) {
+            float v = __uint_as_float(accv[j]) + __ldg(bias + j);
+            vis[(((long long)p * DN_MAX_SLOTS + j) * H + y) * (long long)W + x] = 1.f / (1.f + __expf(-v));
+          }
         }
       }
     }
-    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
-    __syncthreads();
   }
+  asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
   __syncthreads();
-  if (warp == 0) {
+  if (warp == 5) {
+    __syncwarp();
     asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(TMEM_COLS) : "memory");
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(NACC * TMEM_COLS)
+                 : "memory");
   }
+}
+
+PFN_cuTensorMapEncodeTiled_v12000 encode_fn() {
+  static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
+  static std::once_flag once;
+  std::call_once(once, [] {
+    void* p = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) == cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+      fn = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(p);
+  });
+  return fn;
+}
+
+// 4-D map over an NHWC activation [planes][H][W][cin] (FP16): box of 8
+// channels x halo_px(dil) pixels x 1 row x 1 plane.
+cudaError_t make_in_map(CUtensorMap* map, const __half* in, int planes, int H, int W, int cin, int dil) {
+  PFN_cuTensorMapEncodeTiled_v12000 enc = encode_fn();
+  if (!enc) return cudaErrorNotSupported;
+  cuuint64_t dims[4] = {(cuuint64_t)cin, (cuuint64_t)W, (cuuint64_t)H, (cuuint64_t)planes};
+  cuuint64_t strides[3] = {(cuuint64_t)cin * 2, (cuuint64_t)W * cin * 2, (cuuint64_t)H * W * cin * 2};
+  cuuint32_t box[4] = {8, (cuuint32_t)halo_px(dil), 1, 1};
+  cuuint32_t estr[4] = {1, 1, 1, 1};
+  CUresult r = enc(map, CU_TENSOR_MAP_DATA_TYPE_FLOAT16, 4, const_cast<__half*>(in), dims, strides, box, estr,
+                   CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
+                   CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+  return r == CUDA_SUCCESS ? cudaSuccess : cudaErrorInvalidValue;
 }
 
 template <int CIN, int COUT, int MODE>
 cudaError_t launch_conv(const __half* in, int planes, int H, int W, int dil, const void* w, const float* b, __half* out,
                         float* vis, int* err, cudaStream_t s, int num_sms) {
   using SM = ConvSmem<CIN, COUT>;
-  static unsigned long long attr_set = 0;  // one bit per device ordinal (< 64)
+  if (dil < 1 || dil > MAX_DIL) return cudaErrorInvalidValue;
+  const int smem = SM::total(dil);
+  static int attr_bytes[64] = {};  // per device ordinal: the largest size set so far
+  static std::mutex attr_mu;       // batch lanes launch from several host threads
   int dev = 0;
   cudaError_t e = cudaGetDevice(&dev);
   if (e != cudaSuccess) return e;
-  unsigned long long bit = dev < 64 ? 1ull << dev : 0;
-  if (!(attr_set & bit)) {
-    e = cudaFuncSetAttribute(k_conv3x3_tc<CIN, COUT, MODE>, cudaFuncAttributeMaxDynamicSharedMemorySize, SM::TOTAL);
-    if (e != cudaSuccess) return e;
-    attr_set |= bit;
+  {
+    std::lock_guard<std::mutex> g(attr_mu);
+    if (dev >= 64 || attr_bytes[dev] < smem) {
+      e = cudaFuncSetAttribute(k_conv3x3_tc<CIN, COUT, MODE>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+      if (e != cudaSuccess) return e;
+      if (dev < 64) attr_bytes[dev] = smem;
+    }
   }
+  CUtensorMap map;
+  e = make_in_map(&map, in, planes, H, W, CIN, dil);
+  if (e != cudaSuccess) return e;
+  // persistent grid: 4 CTAs per SM (each holds 64 of the SM's 512 TMEM
+  // columns; shared memory allows 2-6 resident); CTAs beyond the resident
+  // ones start as others finish
   long long ntiles = (long long)planes * H * ((W + TILE_M - 1) / TILE_M);
-  long long grid = std::min<long long>(ntiles, (long long)num_sms * 2);
+  long long grid = std::min<long long>(ntiles, (long long)num_sms * 4);
   if (grid < 1) grid = 1;
-  k_conv3x3_tc<CIN, COUT, MODE><<<(int)grid, 128, SM::TOTAL, s>>>(in, planes, H, W, dil, (const uint4*)w, b, out, vis,
-                                                                  err);
+  k_conv3x3_tc<CIN, COUT, MODE><<<(int)grid, CONV_THREADS, smem, s>>>(map, planes, H, W, dil, (const uint4*)w, b,
+                                                                      out, vis, err);
   return cudaGetLastError();
 }
 
@@ -296,21 +433,29 @@ std::string denoise_load(const void* blob, size_t bytes, DenoiseNet* net) {
     return v;
   };
   if (!blob || bytes < 12 || memcmp(p, "RTDN", 4) != 0) return "not a denoiser weight blob (magic RTDN)";
-  if (u32(4) != 1) return "unsupported denoiser blob version";
+  const uint32_t ver = u32(4);
+  if (ver != 1 && ver != 2) return "unsupported denoiser blob version";
   uint32_t n = u32(8);
   if (n < 1 || n > 32) return "denoiser layer count must be 1..32";
-  size_t off = 12 + 16 * (size_t)n;
+  size_t head = ver == 1 ? 12 : 16;  // version 2 adds the rays per disk light the network was trained on
+  int rays = 1;
+  if (ver == 2) {
+    if (bytes < 16) return "truncated denoiser blob";
+    rays = (int)u32(12);
+    if (rays < 1 || rays > 16) return "denoiser rays per light must be 1..16";
+  }
+  size_t off = head + 16 * (size_t)n;
   if (bytes < off) return "truncated denoiser blob";
   std::vector<DnLayer> L(n);
   for (uint32_t i = 0; i < n; i++) {
-    L[i].cin = (int)u32(12 + 16 * i);
-    L[i].cout = (int)u32(16 + 16 * i);
-    L[i].dil = (int)u32(20 + 16 * i);
-    L[i].act = (int)u32(24 + 16 * i);
+    L[i].cin = (int)u32(head + 16 * i);
+    L[i].cout = (int)u32(head + 4 + 16 * i);
+    L[i].dil = (int)u32(head + 8 + 16 * i);
+    L[i].act = (int)u32(head + 12 + 16 * i);
     bool last = i + 1 == n;
     if ((L[i].cin != 16 && L[i].cin != 32) || (L[i].cout != 16 && L[i].cout != 32))
       return "denoiser layers must have 16 or 32 input and output channels";
-    if (L[i].dil < 1 || L[i].dil > 256) return "denoiser dilation must be 1..256";
+    if (L[i].dil < 1 || L[i].dil > MAX_DIL) return "denoiser dilation must be 1..64";
     if (L[i].act != (last ? 2 : 0)) return "denoiser layers must be ReLU, the last one sigmoid";
     if (last && L[i].cout != 16) return "the last denoiser layer must have 16 output channels";
     if (i == 0 && L[i].cin != FEAT_CHANNELS) return "the first denoiser layer must read 16 feature channels";
@@ -356,6 +501,7 @@ std::string denoise_load(const void* blob, size_t bytes, DenoiseNet* net) {
   net->layers = L;
   net->allocs = allocs;
   net->param_count = params;
+  net->rays_per_light = rays;
   return std::string();
 }
 
@@ -364,6 +510,7 @@ void denoise_free(DenoiseNet* net) {
   net->allocs.clear();
   net->layers.clear();
   net->param_count = 0;
+  net->rays_per_light = 1;
 }
 
 int denoise_run(const DenoiseNet& net, const __half* feat, int planes, int H, int W, __half* act0, __half* act1,

@@ -42,6 +42,7 @@ struct DenoiseNet {
   std::vector<DnLayer> layers;
   std::vector<void*> allocs;
   size_t param_count = 0;
+  int rays_per_light = 1;  // disk-light rays per primary hit the network was trained on
   bool loaded() const { return !layers.empty(); }
 };
 

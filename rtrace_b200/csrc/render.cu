@@ -16,6 +16,7 @@
 #include <memory>
 #include <mutex>
 #include <string>
+#include <thread>
 #include <vector>
 
 #include "../../include/rtrace_gpu.h"
@@ -66,6 +67,10 @@ struct rt_ctx {
   long long dn_cap = 0;  // primary samples the buffers hold
   __half *d_feat = nullptr, *d_act0 = nullptr, *d_act1 = nullptr;
   float* d_vhat = nullptr;
+  // batched rendering: lanes are child contexts (own stream and scratch)
+  std::vector<rt_ctx*> lanes;
+  uint32_t tuned_lanes = 0;
+  bool borrowed_net = false;  // a lane's net points at its parent's weights
 };
 
 namespace {
@@ -162,6 +167,21 @@ rt_status ensure_scratch(rt_ctx* ctx, long long n_rays, int levels, long long n_
   ctx->cap_shadow = SH;
   ctx->cap_hits_sh = HS;
   return RT_OK;
+}
+
+// Raises k_outline_apply's dynamic shared-memory limit to at least `bytes`
+// (never lowers it: batch lanes render from several host threads).
+cudaError_t outline_smem_attr(int bytes) {
+  static std::mutex mu;
+  static int set[64] = {};
+  int dev = 0;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e != cudaSuccess) return e;
+  std::lock_guard<std::mutex> g(mu);
+  if (dev < 64 && set[dev] >= bytes) return cudaSuccess;
+  e = cudaFuncSetAttribute(k_outline_apply, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+  if (e == cudaSuccess && dev < 64) set[dev] = bytes;
+  return e;
 }
 
 // Feature image, two activation buffers and the visibility estimate for n
@@ -679,7 +699,7 @@ struct AovOut {
 
 rt_status render_impl(rt_ctx* ctx, const rt_scene* sc, const rt_render_params* P, uint32_t row_begin,
                       uint32_t row_end, uint8_t* rgb_out, int on_device, double* linear_out, rt_stats* stats,
-                      const AovOut* aov = nullptr) {
+                      const AovOut* aov = nullptr, const rt_camera_config* camera = nullptr) {
   auto t0 = std::chrono::steady_clock::now();
   if (!ctx || !sc || !P) return fail(ctx, RT_ERR_INVALID_ARGUMENT, "null argument");
   if (!rgb_out && !linear_out) return fail(ctx, RT_ERR_INVALID_ARGUMENT, "no output buffer");
@@ -691,7 +711,8 @@ rt_status render_impl(rt_ctx* ctx, const rt_scene* sc, const rt_render_params* P
   CameraBasis cam;
   std::string cerr;
   double aspect = (double)P->width / (double)P->height;
-  if (!make_camera(sc->camera, aspect, &cam, &cerr)) return fail(ctx, RT_ERR_RENDER, cerr);
+  const rt_camera_config& camcfg = camera ? *camera : sc->camera;
+  if (!make_camera(camcfg, aspect, &cam, &cerr)) return fail(ctx, RT_ERR_RENDER, cerr);
   if (!sc->render_error.empty()) return fail(ctx, RT_ERR_RENDER, sc->render_error);
   CK(cudaSetDevice(ctx->device));
 
@@ -736,8 +757,10 @@ rt_status render_impl(rt_ctx* ctx, const rt_scene* sc, const rt_render_params* P
       return fail(ctx, RT_ERR_INVALID_ARGUMENT, "learned shadows support at most two disk lights");
     if (!ctx->net.loaded()) return fail(ctx, RT_ERR_INVALID_ARGUMENT, "learned shadows need rt_denoiser_load first");
   }
+  if (P->learned_rays > 16) return fail(ctx, RT_ERR_INVALID_ARGUMENT, "learned_rays above 16 is not supported");
+  const int lrays = learned ? (P->learned_rays ? (int)P->learned_rays : ctx->net.rays_per_light) : 0;
   const int K_full = sc->n_point_lights + sc->n_disk_lights * dsamp;
-  const int K_0 = learned ? sc->n_point_lights + sc->n_disk_lights : K_full;
+  const int K_0 = learned ? sc->n_point_lights + sc->n_disk_lights * lrays : K_full;
   auto chunk_for = [&](int K) { return K > 0 ? std::max(1LL, std::min(nprim, kShadowCap / K)) : nprim; };
   const long long chunk_0 = chunk_for(K_0), chunk_n = chunk_for(K_full);
   if (learned && chunk_0 < nprim)
@@ -758,7 +781,7 @@ rt_status render_impl(rt_ctx* ctx, const rt_scene* sc, const rt_render_params* P
     F.C.ver[k] = cam.vertical[k];
     F.C.llc[k] = cam.llc[k];
     F.C.vdir[k] = cam.view_dir[k];
-    F.C.campos[k] = sc->camera.position[k];
+    F.C.campos[k] = camcfg.position[k];
     F.C.gcolor[k] = cam.grid_color[k];
   }
   F.C.persp = cam.persp;
@@ -837,7 +860,7 @@ rt_status render_impl(rt_ctx* ctx, const rt_scene* sc, const rt_render_params* P
       const long long chunk = l == 0 ? chunk_0 : chunk_n;
       F.K = K;
       F.chunk_hits = chunk;
-      F.dsamp = (l == 0 && learned) ? 1 : dsamp;
+      F.dsamp = (l == 0 && learned) ? lrays : dsamp;
       const bool feat = l == 0 && F.feat_on;
       const long long nchunks = (nprim + chunk - 1) / chunk;
       if (count) k_trace<true><<<blocks(nprim, 128, 16), 128, 0, s>>>(F, l);
@@ -886,7 +909,7 @@ rt_status render_impl(rt_ctx* ctx, const rt_scene* sc, const rt_render_params* P
     Lc.after(RT_STAGE_POST);
     size_t shm = (size_t)(OT_X + 2 * F.o_radius) * (OT_Y + 2 * F.o_radius) * sizeof(double);
     if (shm > 48 * 1024)
-      CK(cudaFuncSetAttribute(k_outline_apply, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)shm));
+      CK(outline_smem_attr((int)shm));
     k_outline_apply<<<og, ob, shm, s>>>(F);
     Lc.after(RT_STAGE_POST);
   }
@@ -979,9 +1002,11 @@ void rt_ctx_destroy(rt_ctx* ctx) {
   if (!ctx) return;
   cudaSetDevice(ctx->device);
   if (ctx->stream) cudaStreamSynchronize(ctx->stream);
+  for (rt_ctx* l : ctx->lanes) rt_ctx_destroy(l);
+  ctx->lanes.clear();
   free_all(ctx->scratch);
   free_all(ctx->dn_scratch);
-  denoise_free(&ctx->net);
+  if (!ctx->borrowed_net) denoise_free(&ctx->net);
   for (cudaEvent_t e : ctx->stage_ev) cudaEventDestroy(e);
   if (ctx->ev0) cudaEventDestroy(ctx->ev0);
   if (ctx->ev1) cudaEventDestroy(ctx->ev1);
@@ -1057,6 +1082,21 @@ rt_status rt_host_scene_load_json_file(const char* path, rt_host_scene** out) {
   auto h = std::make_unique<rt_host_scene>();
   if (!load_scene_json(text, parent_dir(path), &h->hs, &err)) return fail(ctx, RT_ERR_SCENE, err);
   *out = h.release();
+  return RT_OK;
+}
+
+rt_status rt_auto_cameras_json_file(const char* path, rt_camera_config* out) {
+  if (!path || !out) return fail(nullptr, RT_ERR_INVALID_ARGUMENT, "null argument");
+  std::string text, err;
+  if (!read_text_file(path, &text, &err)) return fail(nullptr, RT_ERR_IO, err);
+  if (!auto_cameras(text, parent_dir(path), out, &err)) return fail(nullptr, RT_ERR_SCENE, err);
+  return RT_OK;
+}
+
+rt_status rt_auto_cameras_json_str(const char* json, rt_camera_config* out) {
+  if (!json || !out) return fail(nullptr, RT_ERR_INVALID_ARGUMENT, "null argument");
+  std::string err;
+  if (!auto_cameras(json, ".", out, &err)) return fail(nullptr, RT_ERR_SCENE, err);
   return RT_OK;
 }
 
@@ -1146,7 +1186,7 @@ rt_status launch_outline(rt_ctx* ctx, const DFrame& F) {
   k_outline_mask<<<og, ob, 0, ctx->stream>>>(F);
   size_t shm = (size_t)(OT_X + 2 * F.o_radius) * (OT_Y + 2 * F.o_radius) * sizeof(double);
   if (shm > 48 * 1024)
-    CK(cudaFuncSetAttribute(k_outline_apply, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)shm));
+    CK(outline_smem_attr((int)shm));
   k_outline_apply<<<og, ob, shm, ctx->stream>>>(F);
   CK(cudaGetLastError());
   CK(cudaStreamSynchronize(ctx->stream));
@@ -1223,6 +1263,132 @@ rt_status rt_render_rows(rt_ctx* ctx, const rt_scene* scene, const rt_render_par
                          uint32_t row_end, uint8_t* rgb_out, int out_on_device, rt_stats* stats) {
   if (!rgb_out) return fail(ctx, RT_ERR_INVALID_ARGUMENT, "no output buffer");
   return render_impl(ctx, scene, params, row_begin, row_end, rgb_out, out_on_device, nullptr, stats);
+}
+
+rt_status rt_batch_assign(const double* costs, uint32_t n, uint32_t lanes, uint32_t* lane_of_job) {
+  if ((n && (!costs || !lane_of_job)) || lanes == 0 || lanes > 64)
+    return fail(nullptr, RT_ERR_INVALID_ARGUMENT, "rt_batch_assign: bad arguments (lanes must be 1..64)");
+  std::vector<uint32_t> order(n);
+  for (uint32_t i = 0; i < n; i++) order[i] = i;
+  std::stable_sort(order.begin(), order.end(), [&](uint32_t a, uint32_t b) { return costs[a] > costs[b]; });
+  std::vector<double> load(lanes, 0.0);
+  for (uint32_t i : order) {
+    uint32_t best = 0;
+    for (uint32_t l = 1; l < lanes; l++)
+      if (load[l] < load[best]) best = l;
+    load[best] += costs[i];
+    lane_of_job[i] = best;
+  }
+  return RT_OK;
+}
+
+rt_status rt_render_batch(rt_ctx* ctx, rt_job* jobs, uint32_t n, uint32_t lanes, rt_batch_stats* stats) {
+  if (!ctx) return fail(nullptr, RT_ERR_INVALID_ARGUMENT, "null context");
+  if (n && !jobs) return fail(ctx, RT_ERR_INVALID_ARGUMENT, "null jobs");
+  if (lanes == 0) lanes = ctx->tuned_lanes ? ctx->tuned_lanes : 4;
+  if (lanes > 16) return fail(ctx, RT_ERR_INVALID_ARGUMENT, "at most 16 lanes");
+  lanes = std::max(1u, std::min(lanes, std::max(n, 1u)));
+  auto t0 = std::chrono::steady_clock::now();
+  // lanes: child contexts on the same device, sharing the parent's denoiser
+  while (ctx->lanes.size() < lanes) {
+    rt_ctx* l = nullptr;
+    rt_status st = rt_ctx_create(ctx->device, &l);
+    if (st != RT_OK) return fail(ctx, st, "creating a batch lane: " + std::string(rt_last_error(nullptr)));
+    l->borrowed_net = true;
+    ctx->lanes.push_back(l);
+  }
+  for (uint32_t k = 0; k < lanes; k++) {
+    rt_ctx* l = ctx->lanes[k];
+    l->net.layers = ctx->net.layers;
+    l->net.param_count = ctx->net.param_count;
+    l->net.rays_per_light = ctx->net.rays_per_light;
+    l->net.allocs.clear();
+  }
+  // estimated rays per job -> lanes, longest first
+  std::vector<double> cost(n, 0.0);
+  for (uint32_t i = 0; i < n; i++) {
+    const rt_render_params& P = jobs[i].params;
+    const rt_scene* sc = jobs[i].scene;
+    double spp = P.anti_aliasing_mode == RT_AA_QUINCUNX ? 2.0 : (double)std::max(1u, P.samples);
+    int ds = P.disk_samples ? (int)P.disk_samples : 16;
+    double K = sc ? (double)(sc->n_point_lights + sc->n_disk_lights * ds) : 0.0;
+    cost[i] = (double)P.width * P.height * spp * (1.0 + K);
+  }
+  std::vector<uint32_t> lane_of(n, 0);
+  rt_status st = rt_batch_assign(cost.data(), n, lanes, lane_of.data());
+  if (st != RT_OK) return fail(ctx, st, "rt_batch_assign failed");
+  std::vector<std::vector<uint32_t>> per_lane(lanes);
+  {
+    std::vector<uint32_t> order(n);
+    for (uint32_t i = 0; i < n; i++) order[i] = i;
+    std::stable_sort(order.begin(), order.end(), [&](uint32_t a, uint32_t b) { return cost[a] > cost[b]; });
+    for (uint32_t i : order) per_lane[lane_of[i]].push_back(i);
+  }
+  std::vector<std::string> errs(n);
+  std::vector<double> lane_ms(lanes, 0.0);
+  auto run_lane = [&](uint32_t k) {
+    rt_ctx* l = ctx->lanes[k];
+    for (uint32_t i : per_lane[k]) {
+      rt_job& J = jobs[i];
+      memset(&J.stats, 0, sizeof J.stats);
+      if (!J.scene || !J.rgb_out) {
+        J.status = RT_ERR_INVALID_ARGUMENT;
+        errs[i] = "null scene or output";
+        continue;
+      }
+      J.status = render_impl(l, J.scene, &J.params, 0, J.params.height, J.rgb_out, J.out_on_device, nullptr, &J.stats,
+                             nullptr, J.camera);
+      if (J.status != RT_OK) errs[i] = l->err;
+      lane_ms[k] += J.stats.device_ms;
+    }
+  };
+  std::vector<std::thread> threads;
+  for (uint32_t k = 1; k < lanes; k++) threads.emplace_back(run_lane, k);
+  run_lane(0);
+  for (auto& t : threads) t.join();
+  rt_status first = RT_OK;
+  std::string msg;
+  uint64_t rays = 0;
+  double dev = 0.0;
+  for (uint32_t i = 0; i < n; i++) {
+    if (jobs[i].status != RT_OK && first == RT_OK) {
+      first = (rt_status)jobs[i].status;
+      msg = "job " + std::to_string(i) + ": " + errs[i];
+    }
+    rays += jobs[i].stats.primary_rays + jobs[i].stats.reflection_rays + jobs[i].stats.shadow_rays;
+    dev += jobs[i].stats.device_ms;
+  }
+  if (stats) {
+    memset(stats, 0, sizeof *stats);
+    stats->jobs = n;
+    stats->lanes = lanes;
+    stats->rays = rays;
+    stats->device_ms = dev;
+    stats->busiest_lane_ms = *std::max_element(lane_ms.begin(), lane_ms.end());
+    stats->wall_ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
+  }
+  if (first != RT_OK) return fail(ctx, first, msg);
+  ctx->err.clear();
+  return RT_OK;
+}
+
+rt_status rt_batch_autotune(rt_ctx* ctx, rt_job* jobs, uint32_t n, uint32_t* best_lanes) {
+  if (!ctx) return fail(nullptr, RT_ERR_INVALID_ARGUMENT, "null context");
+  const uint32_t cand[4] = {1, 2, 4, 8};
+  double best_ms = 1e300;
+  uint32_t best = 4;
+  for (uint32_t c : cand) {
+    rt_batch_stats bs;
+    rt_status st = rt_render_batch(ctx, jobs, n, c, &bs);
+    if (st != RT_OK) return st;
+    if (bs.wall_ms < best_ms) {
+      best_ms = bs.wall_ms;
+      best = c;
+    }
+  }
+  ctx->tuned_lanes = best;
+  if (best_lanes) *best_lanes = best;
+  return RT_OK;
 }
 
 rt_status rt_denoiser_load(rt_ctx* ctx, const void* blob, size_t bytes) {

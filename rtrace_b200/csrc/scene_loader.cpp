@@ -805,6 +805,30 @@ struct ObjIn {
   std::string filename;
 };
 
+// The scene's "objects" array (src/scene.rs:55-96 deserialisation).
+std::vector<ObjIn> parse_objects(const J& j) {
+  std::vector<ObjIn> objs;
+  const J& oa = req(j, "objects");
+  if (oa.k != J::ARR) throw LoadError("invalid type: expected a sequence");
+  for (const J& o : oa.a) {
+    ObjIn ob;
+    std::string k = str(req(o, "kind"));
+    if (k == "sphere") { ob.kind = RT_OBJ_SPHERE; ob.a = vec3(req(o, "center")); ob.radius = f64(req(o, "radius")); }
+    else if (k == "plane") { ob.kind = RT_OBJ_PLANE; ob.a = vec3(req(o, "point")); ob.b = vec3(req(o, "normal")); }
+    else if (k == "cube") { ob.kind = RT_OBJ_CUBE; ob.a = vec3(req(o, "center")); ob.b = vec3(req(o, "size")); }
+    else if (k == "mesh") { ob.kind = RT_OBJ_MESH; ob.filename = str(req(o, "filename")); }
+    else throw LoadError("unknown variant `" + k + "`, expected one of `sphere`, `plane`, `cube`, `mesh`");
+    ob.mat = parse_material(req(o, "material"));
+    if (const J* tr = opt(o, "transform")) {
+      if (tr->k != J::ARR) throw LoadError("invalid type: expected a sequence");
+      ob.has_transform = true;
+      for (auto& e : tr->a) ob.transform.push_back(str(e));
+    }
+    objs.push_back(std::move(ob));
+  }
+  return objs;
+}
+
 }  // namespace
 
 // --------------------------------------------------------- public API -----
@@ -909,25 +933,7 @@ bool load_scene_json(const std::string& text, const std::string& base_dir, HostS
     if (const J* f = opt(cam, "grid_thickness")) { cc.has_grid_thickness = 1; cc.grid_thickness = f64(*f); }
     if (const J* f = opt(cam, "grid_color")) cc.grid_color_state = hex_to_color(str(*f), cc.grid_color, nullptr) ? 1 : 2;
 
-    std::vector<ObjIn> objs;
-    const J& oa = req(j, "objects");
-    if (oa.k != J::ARR) throw LoadError("invalid type: expected a sequence");
-    for (const J& o : oa.a) {
-      ObjIn ob;
-      std::string k = str(req(o, "kind"));
-      if (k == "sphere") { ob.kind = RT_OBJ_SPHERE; ob.a = vec3(req(o, "center")); ob.radius = f64(req(o, "radius")); }
-      else if (k == "plane") { ob.kind = RT_OBJ_PLANE; ob.a = vec3(req(o, "point")); ob.b = vec3(req(o, "normal")); }
-      else if (k == "cube") { ob.kind = RT_OBJ_CUBE; ob.a = vec3(req(o, "center")); ob.b = vec3(req(o, "size")); }
-      else if (k == "mesh") { ob.kind = RT_OBJ_MESH; ob.filename = str(req(o, "filename")); }
-      else throw LoadError("unknown variant `" + k + "`, expected one of `sphere`, `plane`, `cube`, `mesh`");
-      ob.mat = parse_material(req(o, "material"));
-      if (const J* tr = opt(o, "transform")) {
-        if (tr->k != J::ARR) throw LoadError("invalid type: expected a sequence");
-        ob.has_transform = true;
-        for (auto& e : tr->a) ob.transform.push_back(str(e));
-      }
-      objs.push_back(std::move(ob));
-    }
+    std::vector<ObjIn> objs = parse_objects(j);
     const J& la = req(j, "lights");
     if (la.k != J::ARR) throw LoadError("invalid type: expected a sequence");
     static const double WHITE[3] = {1, 1, 1}, BLACK[3] = {0, 0, 0}, GREY[3] = {0.5, 0.5, 0.5};
@@ -1145,6 +1151,144 @@ bool make_camera(const rt_camera_config& cfg, double aspect, CameraBasis* c, std
   c->grid_pitch = cfg.grid_pitch;
   c->grid_half_thickness = cfg.grid_thickness / 2.0;
   return true;
+}
+
+
+// Scene::compute_finite_bounds (src/scene.rs:538-690) and
+// AutoCamera::generate_cameras (src/auto_camera.rs:9-130).
+bool auto_cameras(const std::string& text, const std::string& base_dir, rt_camera_config out[4], std::string* err) {
+  try {
+    J j = parse_json(text);
+    if (j.k != J::OBJ) throw LoadError("invalid type: expected struct Scene");
+    std::vector<ObjIn> objs = parse_objects(j);
+    bool have = false;
+    V mn{}, mx{};
+    auto grow = [&](V a, V b) {
+      if (!have) {
+        mn = a;
+        mx = b;
+        have = true;
+        return;
+      }
+      mn = {rmin(mn.x, a.x), rmin(mn.y, a.y), rmin(mn.z, a.z)};
+      mx = {rmax(mx.x, b.x), rmax(mx.y, b.y), rmax(mx.z, b.z)};
+    };
+    for (const ObjIn& o : objs) {
+      M4 tm;
+      bool ht = o.has_transform && parse_transforms(o.transform, &tm);
+      if (o.kind == RT_OBJ_SPHERE) {
+        V c = o.a;
+        double r = o.radius;
+        if (ht) {
+          c = xform_point(tm, c);
+          double sx = norm({tm.m[0][0], tm.m[1][0], tm.m[2][0]});
+          double sy = norm({tm.m[0][1], tm.m[1][1], tm.m[2][1]});
+          double sz = norm({tm.m[0][2], tm.m[1][2], tm.m[2][2]});
+          r *= rmax(rmax(sx, sy), sz);
+        }
+        V rv{r, r, r};
+        grow(c - rv, c + rv);
+      } else if (o.kind == RT_OBJ_CUBE) {
+        // Cube::bounds (src/ray.rs:228-262)
+        V h = o.b / 2.0;
+        M4 inv;
+        bool oriented = ht;
+        if (ht && inverse4(tm, &inv)) {
+          bool ident = true;
+          for (int a = 0; a < 4; a++)
+            for (int b = 0; b < 4; b++) ident = ident && inv.m[a][b] == (a == b ? 1.0 : 0.0);
+          oriented = !ident;
+        } else if (ht) {
+          oriented = false;  // try_inverse failed: the cube keeps the identity
+        }
+        if (!oriented) {
+          grow(o.a - h, o.a + h);
+        } else {
+          const double INF = std::numeric_limits<double>::infinity();
+          V cmn{INF, INF, INF}, cmx{-INF, -INF, -INF};
+          for (int k = 0; k < 8; k++) {
+            V corner{(k & 4) ? h.x : -h.x, (k & 2) ? h.y : -h.y, (k & 1) ? h.z : -h.z};
+            V w = o.a + xform_point(tm, corner);
+            cmn = {rmin(cmn.x, w.x), rmin(cmn.y, w.y), rmin(cmn.z, w.z)};
+            cmx = {rmax(cmx.x, w.x), rmax(cmx.y, w.y), rmax(cmx.z, w.z)};
+          }
+          grow(cmn, cmx);
+        }
+      } else if (o.kind == RT_OBJ_MESH) {
+        const std::string& fn = o.filename;
+        std::string path = (base_dir.empty() || (!fn.empty() && fn[0] == '/')) ? fn : base_dir + "/" + fn;
+        std::string bytes, e2;
+        if (!read_text_file(path, &bytes, &e2)) throw LoadError(e2);
+        std::vector<Tri> tris = load_stl(bytes);
+        if (tris.empty()) continue;
+        // Mesh::bounds (src/mesh.rs:26-36)
+        V bmn = tris[0].v[0], bmx = tris[0].v[0];
+        for (const Tri& t : tris)
+          for (int k = 0; k < 3; k++) {
+            bmn = {rmin(bmn.x, t.v[k].x), rmin(bmn.y, t.v[k].y), rmin(bmn.z, t.v[k].z)};
+            bmx = {rmax(bmx.x, t.v[k].x), rmax(bmx.y, t.v[k].y), rmax(bmx.z, t.v[k].z)};
+          }
+        if (ht) {
+          V c0 = xform_point(tm, {bmn.x, bmn.y, bmn.z});
+          V tmn = c0, tmx = c0;
+          for (int k = 1; k < 8; k++) {
+            V corner{(k & 4) ? bmx.x : bmn.x, (k & 2) ? bmx.y : bmn.y, (k & 1) ? bmx.z : bmn.z};
+            V w = xform_point(tm, corner);
+            tmn = {rmin(tmn.x, w.x), rmin(tmn.y, w.y), rmin(tmn.z, w.z)};
+            tmx = {rmax(tmx.x, w.x), rmax(tmx.y, w.y), rmax(tmx.z, w.z)};
+          }
+          grow(tmn, tmx);
+        } else {
+          grow(bmn, bmx);
+        }
+      }
+    }
+    if (!have) throw LoadError("Scene has no finite objects to compute bounds");
+    V c{(mn.x + mx.x) / 2.0, (mn.y + mx.y) / 2.0, (mn.z + mx.z) / 2.0};
+    V size = mx - mn;
+    const double margin = 1.15;
+    double vw = rmax(rmax(size.x, size.y), size.z) * margin;
+    double dist = vw * 2.0;
+    auto ortho = [&](rt_camera_config* cc, V pos, V up) {
+      *cc = rt_camera_config{};
+      snprintf(cc->kind, sizeof cc->kind, "%s", "ortho");
+      double pp[3] = {pos.x, pos.y, pos.z}, tt[3] = {c.x, c.y, c.z}, uu[3] = {up.x, up.y, up.z};
+      for (int k = 0; k < 3; k++) {
+        cc->position[k] = pp[k];
+        cc->target[k] = tt[k];
+        cc->up[k] = uu[k];
+      }
+      cc->width = vw;
+      cc->height = vw;
+    };
+    ortho(&out[0], {c.x, c.y - dist, c.z}, {0, 0, 1});  // left
+    ortho(&out[1], {c.x - dist, c.y, c.z}, {0, 0, 1});  // front
+    ortho(&out[2], {c.x, c.y, c.z + dist}, {0, 1, 0});  // top
+    // perspective: 50 degree FOV, 35 degrees down, along the +x +y diagonal
+    double maxd = rmax(rmax(size.x, size.y), size.z) * margin;
+    double fov_rad = to_radians(50.0);
+    double dfov = maxd / std::tan(fov_rad / 2.0);
+    double xy = to_radians(45.0), down = to_radians(35.0);
+    double hd = dfov * std::cos(down);
+    rt_camera_config& pc = out[3];
+    pc = rt_camera_config{};
+    snprintf(pc.kind, sizeof pc.kind, "%s", "perspective");
+    double pp[3] = {c.x + hd * std::cos(xy), c.y + hd * std::sin(xy), c.z + dfov * std::sin(down)};
+    double tt[3] = {c.x, c.y, c.z};
+    for (int k = 0; k < 3; k++) {
+      pc.position[k] = pp[k];
+      pc.target[k] = tt[k];
+      pc.up[k] = k == 2 ? 1.0 : 0.0;
+    }
+    pc.width = 1.0;
+    pc.height = 1.0;
+    pc.has_fov = 1;
+    pc.fov = 50.0;
+    return true;
+  } catch (const std::exception& e) {
+    if (err) *err = e.what();
+    return false;
+  }
 }
 
 }  // namespace rtb

@@ -48,4 +48,8 @@ struct CameraBasis {
 };
 bool make_camera(const rt_camera_config& cfg, double aspect, CameraBasis* out, std::string* err);
 
+// AutoCamera::generate_cameras (src/auto_camera.rs:9-130): left, front, top
+// and perspective views framing the scene's finite objects.
+bool auto_cameras(const std::string& text, const std::string& base_dir, rt_camera_config out[4], std::string* err);
+
 }  // namespace rtb

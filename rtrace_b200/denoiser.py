@@ -40,11 +40,12 @@ ARCH = [(16, 32, 1), (32, 32, 2), (32, 32, 4), (32, 32, 8), (32, 32, 16), (32, 3
 # --------------------------------------------------------------------------
 # Blobs
 # --------------------------------------------------------------------------
-def pack(layers):
+def pack(layers, rays=1):
     """layers: [(weight [cout][3][3][cin] array, bias [cout] array, dilation)]
-    -> bytes in the rt_denoiser_load format (FP16 weights, FP32 bias)."""
+    -> bytes in the rt_denoiser_load format (version 2: FP16 weights, FP32
+    bias, and the rays per disk light the network expects)."""
     n = len(layers)
-    out = [MAGIC, struct.pack("<II", 1, n)]
+    out = [MAGIC, struct.pack("<III", 2, n, int(rays))]
     for i, (w, b, dil) in enumerate(layers):
         cout, kh, kw, cin = np.asarray(w).shape
         assert (kh, kw) == (3, 3) and np.asarray(b).shape == (cout,)
@@ -55,15 +56,18 @@ def pack(layers):
     return b"".join(out)
 
 
-def unpack(blob):
-    """bytes -> [(weight float16 [cout][3][3][cin], bias float32 [cout], dilation)]"""
+def unpack(blob, with_rays=False):
+    """bytes -> [(weight float16 [cout][3][3][cin], bias float32 [cout],
+    dilation)] (and the rays per disk light, with_rays=True)."""
     if blob[:4] != MAGIC:
         raise ValueError("not a denoiser weight blob")
     ver, n = struct.unpack_from("<II", blob, 4)
-    if ver != 1:
+    if ver not in (1, 2):
         raise ValueError("unsupported blob version")
-    heads = [struct.unpack_from("<IIII", blob, 12 + 16 * i) for i in range(n)]
-    off = 12 + 16 * n
+    head = 12 if ver == 1 else 16
+    rays = 1 if ver == 1 else struct.unpack_from("<I", blob, 12)[0]
+    heads = [struct.unpack_from("<IIII", blob, head + 16 * i) for i in range(n)]
+    off = head + 16 * n
     layers = []
     for cin, cout, dil, _act in heads:
         nw = cout * 9 * cin
@@ -74,7 +78,7 @@ def unpack(blob):
         layers.append((w, b, dil))
     if off != len(blob):
         raise ValueError("trailing bytes in denoiser blob")
-    return layers
+    return (layers, rays) if with_rays else layers
 
 
 def read_blob(weights=None):
@@ -170,9 +174,10 @@ def training_scene(seed):
     return sc
 
 
-def render_pair(ctx, scene_path, width, height, target_samples=64, seed=0):
+def render_pair(ctx, scene_path, width, height, rays=1, target_samples=128, seed=0):
     """(features [1,H,W,16] half, target visibility [1,2,H,W] float) on the
-    GPU: the 1-ray feature image and the target_samples-ray visibility."""
+    GPU: the feature image of `rays` rays per disk light (what learned mode
+    casts at primary hits) and the target_samples-ray visibility."""
     import torch
     import rtrace_b200 as rt
     scene = rt.Scene.from_json_file(scene_path, ctx)
@@ -182,7 +187,7 @@ def render_pair(ctx, scene_path, width, height, target_samples=64, seed=0):
     r.seed = seed
     r.max_depth = 1
     feat = torch.empty((1, height, width, FEAT_CHANNELS), dtype=torch.float16, device=dev)
-    r.disk_samples = 1
+    r.disk_samples = rays
     r.render_shadow_aov(scene, feat_ptr=feat.data_ptr())
     vis = torch.empty((1, SLOTS, height, width), dtype=torch.float32, device=dev)
     r.disk_samples = target_samples
@@ -201,7 +206,8 @@ def psnr(est, ref, mask):
     return float("inf") if mse == 0 else 10.0 * math.log10(1.0 / mse)
 
 
-def train(out_path, n_scenes=160, width=1920, height=1080, iters=6000, batch=12, crop=192, seed=0, log=print):
+def train(out_path, n_scenes=160, width=1920, height=1080, iters=6000, batch=12, crop=192, seed=0, rays=1,
+          target_samples=128, log=print):
     import tempfile
     import torch
     import rtrace_b200 as rt
@@ -214,7 +220,7 @@ def train(out_path, n_scenes=160, width=1920, height=1080, iters=6000, batch=12,
     t0 = time.time()
     for k in range(n_scenes):
         path = write_scene(d, "s%d.json" % k, training_scene(1 + k))
-        f, v = render_pair(ctx, path, width, height, seed=k)
+        f, v = render_pair(ctx, path, width, height, rays=rays, target_samples=target_samples, seed=k)
         feats.append(f)
         targs.append(v)
     log("rendered %d training scenes in %.1f s" % (n_scenes, time.time() - t0))
@@ -243,7 +249,7 @@ def train(out_path, n_scenes=160, width=1920, height=1080, iters=6000, batch=12,
         sched.step()
         if it % 500 == 0 or it == iters - 1:
             log("iter %d loss %.6f (%.1f s)" % (it, loss.item(), time.time() - t0))
-    blob = pack(net.export())
+    blob = pack(net.export(), rays=rays)
     with open(out_path, "wb") as f:
         f.write(blob)
     log("wrote %s (%d bytes, %d parameters)" % (out_path, len(blob),
@@ -259,6 +265,8 @@ def main(argv=None):
     ap.add_argument("--iters", type=int, default=6000)
     ap.add_argument("--width", type=int, default=1920)
     ap.add_argument("--height", type=int, default=1080)
+    ap.add_argument("--rays", type=int, default=1, help="rays per disk light at primary hits")
+    ap.add_argument("--target-samples", type=int, default=128)
     ap.add_argument("--log", default=None)
     a = ap.parse_args(argv)
     logf = open(a.log, "w") if a.log else None
@@ -269,7 +277,8 @@ def main(argv=None):
             logf.write(msg + "\n")
             logf.flush()
 
-    train(a.out, n_scenes=a.scenes, width=a.width, height=a.height, iters=a.iters, log=log)
+    train(a.out, n_scenes=a.scenes, width=a.width, height=a.height, iters=a.iters, rays=a.rays,
+          target_samples=a.target_samples, log=log)
     return 0
 
 

@@ -1,6 +1,7 @@
 """Renders one of the benchmark workloads a few times, for profiler captures.
 
     python -m rtrace_b200.profile_render --workload noisy_icosphere --width 960 --height 540 --reps 1
+    python -m rtrace_b200.profile_render --workload ring_spheres --width 1920 --height 1080 --learned
 
 Workloads (see rtrace_b200.workloads): sphere_grid (quincunx), noisy_icosphere
 (no-jitter + outline, the bench.py scene), ring_spheres (stochastic, 4 spp).
@@ -22,6 +23,8 @@ def main(argv=None):
     ap.add_argument("--height", type=int, default=540)
     ap.add_argument("--reps", type=int, default=1)
     ap.add_argument("--dir", default=None)
+    ap.add_argument("--disk-samples", type=int, default=16, help="shadow rays per disk light (16: the reference)")
+    ap.add_argument("--learned", action="store_true", help="learned soft shadows with the shipped denoiser weights")
     a = ap.parse_args(argv)
     d = a.dir or tempfile.mkdtemp(prefix="rtb_prof_")
     if a.workload == "sphere_grid":
@@ -36,6 +39,10 @@ def main(argv=None):
     r.samples = spp
     if aa != 1:
         r.outline_config = scene.get_outline_config()
+    r.disk_samples = a.disk_samples
+    if a.learned:
+        scene._ctx.load_denoiser()
+        r.learned_shadows = True
     for _ in range(a.reps):
         r.render(scene)
     st = r.last_stats

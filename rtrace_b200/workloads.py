@@ -266,3 +266,92 @@ def cli_size(aspect, diagonal):
     """Image size from a diagonal (cli/src/main.rs:339-350)."""
     from rtrace_b200.cli import image_size
     return image_size(aspect, diagonal)
+
+
+# ------------------------------------------------------------ batch (C4) --
+BATCH_RESOLUTIONS = [(128, 128), (256, 256), (640, 480), (1280, 720), (1920, 1080)]
+BATCH_MESH_LEVELS = [3, 4, 5, 6]  # noisy icospheres of 1,280 .. 81,920 triangles
+
+
+def batch_scene(seed, mesh_dir_rel="meshes"):
+    """One scene of the batch workload: 1-4 lights (point or disk), 0-3
+    noisy-icosphere meshes placed by transforms, 0-200 spheres and one grid
+    plane.  Mesh files are referenced as mesh_dir_rel/ico_l<level>_s<k>.stl
+    (batch_meshes writes them)."""
+    rng = np.random.default_rng(50_000 + seed)
+    objs = []
+    n_mesh = int(rng.integers(0, 4))
+    for _ in range(n_mesh):
+        level = int(rng.choice(BATCH_MESH_LEVELS))
+        k = int(rng.integers(0, 2))
+        s = float(rng.uniform(0.8, 2.5))
+        tx, ty = (float(v) for v in rng.uniform(-6, 6, 2))
+        col = colorsys.hsv_to_rgb(rng.uniform(0, 1), rng.uniform(0.3, 0.9), rng.uniform(0.6, 1.0))
+        objs.append({"kind": "mesh", "filename": "%s/ico_l%d_s%d.stl" % (mesh_dir_rel, level, k),
+                     "transform": ["scale(%.4f, %.4f, %.4f)" % (s, s, s), "translate(%.4f, %.4f, %.4f)" % (tx, ty, s)],
+                     "material": _mat(_hex(col), 0.1, 0.7, 0.4, 32,
+                                      reflectivity=round(float(rng.uniform(0, 0.5)), 3))})
+    n_sph = int(rng.integers(0, 201))
+    for _ in range(n_sph):
+        r = float(rng.uniform(0.1, 0.6))
+        c = [round(float(v), 4) for v in (rng.uniform(-9, 9), rng.uniform(-9, 9), r + rng.uniform(0, 2))]
+        col = colorsys.hsv_to_rgb(rng.uniform(0, 1), rng.uniform(0.4, 1.0), rng.uniform(0.6, 1.0))
+        m = _mat(_hex(col), 0.1, 0.7, 0.5, 64)
+        if rng.uniform() < 0.3:
+            m["reflectivity"] = round(float(rng.uniform(0.2, 0.8)), 3)
+        objs.append({"kind": "sphere", "center": c, "radius": round(r, 4), "material": m})
+    objs.append({"kind": "plane", "point": [0, 0, 0], "normal": [0, 0, 1],
+                 "material": _mat("#B4B4B4", 0.1, 0.8, 0.1, 8, reflectivity=0.2,
+                                  texture={"type": "grid", "line_color": "#404040", "line_width": 0.04,
+                                           "cell_size": 1.0})})
+    lights = []
+    for _ in range(int(rng.integers(1, 5))):
+        L = {"position": [round(float(v), 3) for v in (rng.uniform(-10, 10), rng.uniform(-10, 10),
+                                                        rng.uniform(6, 14))],
+             "color": _hex(colorsys.hsv_to_rgb(rng.uniform(0, 1), 0.15, 1.0)),
+             "intensity": round(float(rng.uniform(0.3, 0.8)), 3)}
+        if rng.uniform() < 0.5:
+            L["diameter"] = round(float(rng.uniform(0.5, 2.5)), 3)
+        lights.append(L)
+    if not n_mesh and not n_sph:  # keep a finite object for the auto cameras
+        objs.insert(0, {"kind": "sphere", "center": [0, 0, 1], "radius": 1.0, "material": _mat("#E0C080")})
+    return {
+        "camera": {"kind": "perspective", "position": [12, -12, 9], "target": [0, 0, 0], "up": [0, 0, 1],
+                   "fov": 50, "width": 16, "height": 9},
+        "objects": objs,
+        "lights": lights,
+        "scene_settings": {"ambient_illumination": {"color": "#FFFFFF", "intensity": 0.1},
+                           "background_color": "#1A2030"},
+    }
+
+
+def batch_meshes(directory):
+    """Writes the batch workload's mesh files (two noise seeds per level)."""
+    d = os.path.join(directory, "meshes")
+    os.makedirs(d, exist_ok=True)
+    for level in BATCH_MESH_LEVELS:
+        for k in range(2):
+            p = os.path.join(d, "ico_l%d_s%d.stl" % (level, k))
+            if not os.path.exists(p):
+                v, f = noisy_icosphere(level, 300 + 10 * level + k)
+                write_binary_stl(p, v, f)
+
+
+def batch_workload(directory, n_scenes=64, seed=0):
+    """The batch configuration: n_scenes seeded scenes, each rendered from
+    its four auto-camera views (left, front, top, perspective) at a
+    resolution drawn uniformly from BATCH_RESOLUTIONS.  Returns
+    [(scene_path, [(view, camera_dict, (width, height)), ...]), ...]."""
+    import rtrace_b200 as rt
+    batch_meshes(directory)
+    rng = np.random.default_rng(seed)
+    out = []
+    for k in range(n_scenes):
+        path = write_scene(directory, "batch_%03d.json" % k, batch_scene(seed * 1000 + k))
+        cams = rt.auto_cameras(path=path)
+        views = []
+        for name in ("left", "front", "top", "perspective"):
+            w, h = BATCH_RESOLUTIONS[int(rng.integers(0, len(BATCH_RESOLUTIONS)))]
+            views.append((name, cams[name], (w, h)))
+        out.append((path, views))
+    return out
