@@ -293,6 +293,12 @@ rt_status rt_auto_cameras_json_str(const char* json, rt_camera_config* out);
 rt_status rt_host_scene_load_json_str(const char* json, rt_host_scene** out);
 const rt_scene_desc* rt_host_scene_desc(const rt_host_scene* hs);
 void rt_host_scene_free(rt_host_scene* hs);
+
+/* rt_scene_upload of a host scene's own description.  The first upload
+ * prepares the meshes' device data on the host (BVH, triangle records,
+ * k-d root paths and occurrence lists) and keeps it in the host scene;
+ * later uploads of the same host scene, to any context, only copy it. */
+rt_status rt_host_scene_upload(rt_ctx* ctx, rt_host_scene* hs, rt_scene** out);
 /* Bytes rt_scene_upload copied to the device for this scene. */
 rt_status rt_scene_device_bytes(rt_ctx* ctx, const rt_scene* scene, uint64_t* out);
 

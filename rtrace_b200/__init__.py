@@ -190,11 +190,12 @@ class Scene:
 
     @classmethod
     def upload(cls, host_scene, ctx=None):
-        """Uploads a HostScene (rt_scene_upload)."""
+        """Uploads a HostScene (rt_host_scene_upload: its meshes' device data
+        is prepared on the first upload and copied on later ones)."""
         ctx = ctx or default_context()
         h = ctypes.c_void_p()
         L = _capi.lib()
-        st = L.rt_scene_upload(ctx.handle, L.rt_host_scene_desc(host_scene.handle), ctypes.byref(h))
+        st = L.rt_host_scene_upload(ctx.handle, host_scene.handle, ctypes.byref(h))
         if st != _capi.RT_OK:
             _raise(st, ctx.handle)
         return cls(h, ctx)

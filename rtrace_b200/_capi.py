@@ -159,6 +159,7 @@ def lib():
                                      ctypes.POINTER(rt_stats)]),
         "rt_render_rows": (ctypes.c_int, [_vp, _vp, ctypes.POINTER(rt_render_params), ctypes.c_uint32,
                                           ctypes.c_uint32, _vp, ctypes.c_int, ctypes.POINTER(rt_stats)]),
+        "rt_host_scene_upload": (ctypes.c_int, [_vp, _vp, ctypes.POINTER(_vp)]),
         "rt_auto_cameras_json_file": (ctypes.c_int, [ctypes.c_char_p, ctypes.POINTER(rt_camera_config)]),
         "rt_auto_cameras_json_str": (ctypes.c_int, [ctypes.c_char_p, ctypes.POINTER(rt_camera_config)]),
         "rt_render_batch": (ctypes.c_int, [_vp, ctypes.POINTER(rt_job), ctypes.c_uint32, ctypes.c_uint32,

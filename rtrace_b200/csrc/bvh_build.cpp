@@ -10,6 +10,11 @@
 namespace rtb {
 namespace {
 
+// Subtrees of at least kParallelMin primitives in the top kParallelDepth
+// levels are built on their own threads (up to 2^kParallelDepth at once).
+constexpr int kParallelMin = 8192;
+constexpr int kParallelDepth = 4;
+
 struct Builder {
   const std::vector<double>& bmin;
   const std::vector<double>& bmax;
@@ -52,8 +57,29 @@ struct Builder {
     BvhNode nd{};
     box(ids, mid, nd.lmin, nd.lmax);
     box(ids + mid, n - mid, nd.rmin, nd.rmax);
-    auto l = build(ids, mid, base, out, depth + 1);
-    auto r = build(ids + mid, n - mid, base + mid, out, depth + 1);
+    std::pair<int32_t, int32_t> l, r;
+    if (n >= kParallelMin && depth < kParallelDepth) {
+      // the two subtrees on two threads, into their own node lists, then
+      // appended left then right: the node order of the sequential build
+      std::vector<BvhNode> lo, ro;
+      auto fut = std::async(std::launch::async, [&] { return build(ids, mid, base, lo, depth + 1); });
+      r = build(ids + mid, n - mid, base + mid, ro, depth + 1);
+      l = fut.get();
+      auto append = [&](std::vector<BvhNode>& sub, std::pair<int32_t, int32_t>& ref) {
+        int32_t off = (int32_t)out.size();
+        for (BvhNode& c : sub) {
+          if (c.lcnt == 0) c.lidx += off;
+          if (c.rcnt == 0) c.ridx += off;
+          out.push_back(c);
+        }
+        if (ref.second == 0) ref.first += off;
+      };
+      append(lo, l);
+      append(ro, r);
+    } else {
+      l = build(ids, mid, base, out, depth + 1);
+      r = build(ids + mid, n - mid, base + mid, out, depth + 1);
+    }
     nd.lidx = l.first;
     nd.lcnt = l.second;
     nd.ridx = r.first;

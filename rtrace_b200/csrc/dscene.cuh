@@ -787,6 +787,149 @@ __device__ __forceinline__ bool world_any(const DScene& S, const RayC& r, double
   return false;
 }
 
+// ---------------------------------------------------------------------------
+// Warp-packet any-hit (shadow rays).  All 32 lanes of a warp call these
+// together, each with its own ray (or none: active = false).  The warp walks
+// one BVH with one stack: every lane loads the same node (a broadcast load),
+// tests its own ray against both child boxes, and the warp descends into a
+// child when any still-searching lane's ray hits its box.  A lane tests a
+// leaf's primitives only when its own ray hits the leaf's box, and stops
+// searching at its first accepted primitive.  Every leaf the lane's own
+// walk would test is tested (the packet visits a superset of its nodes and
+// the boxes are conservative), and extra box tests never accept anything, so
+// each lane's answer is that of world_any: the packet only changes how the
+// work is shared out.  The stack and the control flow are warp-uniform.
+// ---------------------------------------------------------------------------
+template <class Leaf>
+__device__ __forceinline__ bool bvh_any_warp(const double2* bvh, const RayC& r, double tmax, bool active,
+                                             Leaf visit_leaf, int* err, Work* w) {
+  const unsigned FULL = 0xffffffffu;
+  bool found = false;
+  if (!__any_sync(FULL, active)) return false;
+  int stack[RTB_STACK];
+  int sp = 0;
+  int node = 0;
+  for (;;) {
+    BNode n = load_bnode(bvh, node);
+    if (w && active) w->nodes++;
+    double tl = 0, tr = 0;
+    bool hl = active && n.lcnt >= 0 && box_hit(n.lmn, n.lmx, r, tmax, &tl);
+    bool hr = active && n.rcnt >= 0 && box_hit(n.rmn, n.rmx, r, tmax, &tr);
+    // leaf children first: they may retire lanes
+    if (n.lcnt > 0 && hl && visit_leaf(n.lidx, n.lcnt)) {
+      found = true;
+      active = false;
+    }
+    if (n.rcnt > 0 && hr && active && visit_leaf(n.ridx, n.rcnt)) {
+      found = true;
+      active = false;
+    }
+    const bool gl = __any_sync(FULL, n.lcnt == 0 && hl && active);
+    const bool gr = __any_sync(FULL, n.rcnt == 0 && hr && active);
+    int next = -1;
+    if (gl && gr) {
+      // nearer child first for most of the searching lanes
+      const unsigned both = __ballot_sync(FULL, hl && hr && active);
+      const unsigned rfirst = __ballot_sync(FULL, hl && hr && active && tr < tl);
+      const bool right_first = __popc(rfirst) * 2 > __popc(both);
+      if (sp >= RTB_STACK) {
+        if ((threadIdx.x & 31) == 0) atomicOr(err, ERR_STACK);
+        return found;
+      }
+      stack[sp++] = right_first ? n.lidx : n.ridx;
+      next = right_first ? n.ridx : n.lidx;
+    } else if (gl) {
+      next = n.lidx;
+    } else if (gr) {
+      next = n.ridx;
+    }
+    if (!__any_sync(FULL, active)) return found;
+    if (next >= 0) {
+      node = next;
+      continue;
+    }
+    if (sp == 0) return found;
+    node = stack[--sp];
+  }
+}
+
+// mesh_any for a warp of shadow rays.
+__device__ __forceinline__ bool mesh_any_warp(const DMesh& M, const RayC& r, double tmin, double tmax, bool active,
+                                              bool use_kd, int* err, Work* w) {
+  active = active && mesh_bounds(M, r, tmin, tmax);
+  return bvh_any_warp(
+      M.bvh, r, tmax, active,
+      [&](int first, int cnt) {
+        for (int k = 0; k < cnt; k++) {
+          const double2* E = M.btris + 5 * (size_t)(first + k);
+          double t;
+          if (w) w->tris++;
+          if (tri_t(E, r, tmin, tmax, &t)) {
+            if (!use_kd) return true;
+            int tri = lo32(__ldg(E + 4).y);
+            unsigned long long o;
+            if (tri_visited_fast(M, r, tri, t, w) || tri_first_visit(M, r, tri, &o, w)) return true;
+          }
+        }
+        return false;
+      },
+      err, w);
+}
+
+// group_hit<true> (any sphere of the run accepts within t_max) for a warp.
+__device__ __forceinline__ bool group_any_warp(const DScene& S, const DSphGroup& G, const RayC& r, double tmin,
+                                               double tmax, bool active, int* err, Work* w) {
+  return bvh_any_warp(
+      G.bvh, r, tmax, active,
+      [&](int first, int cnt) {
+        for (int k = 0; k < cnt; k++) {
+          int sidx = __ldg(G.order + first + k);
+          double t;
+          if (w) w->spheres++;
+          if (sphere_t(S.sph + 5 * (size_t)(G.first_sphere + sidx), r, tmin, tmax, &t)) return true;
+        }
+        return false;
+      },
+      err, w);
+}
+
+// world.hit(ray, t_min, t_max).is_some() for a warp of rays (all 32 lanes
+// call it; lanes with valid == false take part without a ray).  Objects are
+// visited in scene order; the answer does not depend on the order.
+__device__ __forceinline__ bool world_any_warp(const DScene& S, const RayC& r, double tmin, double tmax, bool valid,
+                                               bool use_kd, int* err, Work* w) {
+  bool blocked = false;
+  for (int i = 0; i < S.n_obj; i++) {
+    int4 ob = __ldg(S.obj + i);
+    const bool live = valid && !blocked;
+    double t;
+    switch (ob.x) {
+      case OBJ_SPHERE:
+        if (live) {
+          if (w) w->spheres++;
+          blocked = sphere_t(S.sph + 5 * (size_t)ob.y, r, tmin, tmax, &t);
+        }
+        break;
+      case OBJ_PLANE:
+        if (live) blocked = plane_t(S.pln + 12 * (size_t)ob.y, r, tmin, tmax, &t);
+        break;
+      case OBJ_CUBE:
+        if (live) {
+          int ax;
+          blocked = cube_t(S.cub[ob.y], r, tmin, tmax, &t, &ax);
+        }
+        break;
+      case OBJ_MESH:
+        if (mesh_any_warp(S.mesh[ob.y], r, tmin, tmax, live, use_kd, err, w)) blocked = true;
+        break;
+      default:
+        if (group_any_warp(S, S.grp[ob.y], r, tmin, tmax, live, err, w)) blocked = true;
+        break;
+    }
+  }
+  return blocked;
+}
+
 struct HitRec {
   V3 p, n;
   int mat;

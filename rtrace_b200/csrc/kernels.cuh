@@ -400,20 +400,33 @@ __global__ void __launch_bounds__(128) k_shadow(DFrame F, int level, long long c
   long long nhc = c1 > c0 ? c1 - c0 : 0;
   long long ns = nhc * K;
   Work w{0, 0, 0, 0};
-  for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < ns; t += (long long)gridDim.x * blockDim.x) {
-    // hit-major thread order: the K rays of one hit point run in adjacent
-    // lanes, which keeps a warp's traversals coherent
-    long long hl = t / K, k = t - hl * K;
-    long long s = k * F.chunk_hits + hl;
-    double dist = F.sh.dist[s];
-    unsigned char vis = 0;
-    if (dist >= 0.0 || dist != dist) {
-      // Ray::new normalises the (already unit) light direction once more
-      RayC r = make_rayc(mk(F.sh.ox[hl], F.sh.oy[hl], F.sh.oz[hl]),
-                         normalize(mk(F.sh.dx[s], F.sh.dy[s], F.sh.dz[s])));
-      vis = world_any(F.S, r, 0.001, dist, F.use_kd != 0, F.err, COUNT ? &w : nullptr) ? 0 : 1;
+  // The warp steps through the rays together (world_any_warp is a warp
+  // collective).  Hit-major order: the K rays of one hit point sit in
+  // adjacent lanes, so a warp holds a bundle of rays from one or two points
+  // towards one light, which the packet traversal shares out.
+  const long long stride = (long long)gridDim.x * blockDim.x;
+  for (long long base = blockIdx.x * (long long)blockDim.x + (threadIdx.x & ~31); base < ns; base += stride) {
+    const long long t = base + (threadIdx.x & 31);
+    const bool have = t < ns;
+    long long hl = 0, s = 0;
+    double dist = -1.0;
+    if (have) {
+      hl = t / K;
+      long long k = t - hl * K;
+      s = k * F.chunk_hits + hl;
+      dist = F.sh.dist[s];
     }
-    F.sh.vis[s] = vis;
+    const bool valid = have && (dist >= 0.0 || dist != dist);
+    RayC r;
+    if (valid) {
+      // Ray::new normalises the (already unit) light direction once more
+      r = make_rayc(mk(F.sh.ox[hl], F.sh.oy[hl], F.sh.oz[hl]), normalize(mk(F.sh.dx[s], F.sh.dy[s], F.sh.dz[s])));
+    } else {
+      r = make_rayc(mk(0.0, 0.0, 0.0), mk(0.0, 0.0, 1.0));
+    }
+    bool blocked = world_any_warp(F.S, r, 0.001, valid ? dist : 0.0, valid, F.use_kd != 0, F.err,
+                                  COUNT ? &w : nullptr);
+    if (have) F.sh.vis[s] = (valid && !blocked) ? 1 : 0;
   }
   if (COUNT) flush_work(F, w, 1);
 }

@@ -39,6 +39,10 @@ struct rt_scene {
   std::vector<DMesh> host_meshes;       // device pointers, for the debug entry point
   std::vector<int> obj_kind, obj_mesh;  // per World object
   int n_point_lights = 0, n_disk_lights = 0;
+  // upload arena: one device block, filled through the context's pinned
+  // staging buffer and copied once (see upload())
+  char* blk = nullptr;
+  size_t blk_cap = 0, blk_used = 0;
 };
 
 struct rt_ctx {
@@ -70,6 +74,8 @@ struct rt_ctx {
   // batched rendering: lanes are child contexts (own stream and scratch)
   std::vector<rt_ctx*> lanes;
   uint32_t tuned_lanes = 0;
+  char* pin = nullptr;  // pinned staging of scene uploads
+  size_t pin_cap = 0;
   bool borrowed_net = false;  // a lane's net points at its parent's weights
 };
 
@@ -200,14 +206,73 @@ rt_status ensure_dn_scratch(rt_ctx* ctx, long long n) {
   return RT_OK;
 }
 
+// Scene uploads go into one device block per scene (sized from the scene
+// description by arena_open), staged in the context's pinned buffer and
+// copied with one asynchronous transfer per block (arena_flush); arrays that
+// do not fit get their own allocation.  One cudaMalloc and one cudaFree per
+// scene instead of one per array.
+rt_status arena_flush(rt_ctx* ctx, rt_scene* sc) {
+  if (sc->blk && sc->blk_used) {
+    CK(cudaMemcpyAsync(sc->blk, ctx->pin, sc->blk_used, cudaMemcpyHostToDevice, ctx->stream));
+    CK(cudaStreamSynchronize(ctx->stream));
+  }
+  sc->blk = nullptr;
+  sc->blk_cap = sc->blk_used = 0;
+  return RT_OK;
+}
+
+rt_status arena_open(rt_ctx* ctx, rt_scene* sc, size_t bytes) {
+  rt_status st = arena_flush(ctx, sc);
+  if (st != RT_OK) return st;
+  bytes = (bytes + 255) & ~(size_t)255;
+  char* b = nullptr;
+  CK(dalloc(sc->allocs, &b, bytes));
+  if (ctx->pin_cap < bytes) {
+    if (ctx->pin) cudaFreeHost(ctx->pin);
+    ctx->pin = nullptr;
+    ctx->pin_cap = 0;
+    CK(cudaMallocHost((void**)&ctx->pin, bytes));
+    ctx->pin_cap = bytes;
+  }
+  sc->blk = b;
+  sc->blk_cap = bytes;
+  sc->blk_used = 0;
+  return RT_OK;
+}
+
 template <class T>
 rt_status upload(rt_ctx* ctx, rt_scene* sc, const std::vector<T>& h, const T** out) {
-  T* p = nullptr;
-  CK(dalloc(sc->allocs, &p, h.size()));
-  if (!h.empty()) CK(cudaMemcpy(p, h.data(), h.size() * sizeof(T), cudaMemcpyHostToDevice));
-  sc->uploaded_bytes += h.size() * sizeof(T);
-  *out = p;
+  const size_t bytes = h.size() * sizeof(T);
+  const size_t take = (std::max<size_t>(bytes, 16) + 255) & ~(size_t)255;
+  if (sc->blk && sc->blk_used + take <= sc->blk_cap) {
+    if (bytes) memcpy(ctx->pin + sc->blk_used, h.data(), bytes);
+    *out = reinterpret_cast<const T*>(sc->blk + sc->blk_used);
+    sc->blk_used += take;
+  } else {
+    T* p = nullptr;
+    CK(dalloc(sc->allocs, &p, h.size()));
+    if (bytes) CK(cudaMemcpy(p, h.data(), bytes, cudaMemcpyHostToDevice));
+    *out = p;
+  }
+  sc->uploaded_bytes += bytes;
   return RT_OK;
+}
+
+// Device bytes a scene description needs (an upper bound for the arena).
+size_t scene_bytes_bound(const rt_scene_desc* d) {
+  size_t b = 1 << 16;
+  for (int m = 0; m < d->n_meshes; m++) {
+    const rt_mesh_desc& md = d->meshes[m];
+    size_t nt = (size_t)std::max<int64_t>(md.n_triangles, 0);
+    // triangle records twice (80 B), normals (32), BVH nodes (<= nt/2, 112 B),
+    // k-d nodes (64 + 8), leaf entries and occurrences (4 + 8), padding
+    b += nt * (80 * 2 + 32 + 64) + (size_t)std::max<int64_t>(md.n_nodes, 0) * 72 +
+         (size_t)std::max<int64_t>(md.n_tri_index, 0) * 12 + 8 * 256;
+  }
+  // objects, spheres (+ run BVHs), planes, cubes, materials, lights
+  b += (size_t)std::max(d->n_objects, 0) * 512 + (size_t)std::max(d->n_materials, 0) * 256 +
+       (size_t)std::max(d->n_lights, 0) * 128 + 32 * 256;
+  return b;
 }
 
 // nalgebra 4x4 try_inverse: cofactors over the column-major slice, det from
@@ -295,18 +360,31 @@ void put_bvh(const std::vector<BvhNode>& nodes, std::vector<double2>* out) {
   }
 }
 
-rt_status upload_mesh(rt_ctx* ctx, rt_scene* sc, const rt_mesh_desc& md, DMesh* out) {
-  DMesh M{};
+// Everything the device needs for one mesh, computed on the host: triangle
+// records in original and BVH order, normals, the reference k-d tree with
+// root paths and occurrence lists, the BVH.  Pure function of the mesh
+// description, so a host scene can keep it across uploads.
+struct MeshPrep {
+  std::vector<double2> bvh, btris, brute, nodes;
+  std::vector<double4> normals;
+  std::vector<int> leaf_tris, occ_off;
+  std::vector<int2> leaf_path, occ;
+  double bmin[3], bmax[3];
+  int n_nodes = 0, n_tris = 0;
+};
+
+// Returns an empty string, or why the description is invalid.
+std::string prep_mesh(const rt_mesh_desc& md, MeshPrep* P) {
   for (int k = 0; k < 3; k++) {
-    M.bmin[k] = md.bounds_min[k];
-    M.bmax[k] = md.bounds_max[k];
+    P->bmin[k] = md.bounds_min[k];
+    P->bmax[k] = md.bounds_max[k];
   }
   long long nt = md.n_triangles;
-  if (nt < 0 || md.n_nodes < 0 || md.n_tri_index < 0) return fail(ctx, RT_ERR_INVALID_ARGUMENT, "negative count");
+  if (nt < 0 || md.n_nodes < 0 || md.n_tri_index < 0) return "negative count";
   if (nt > 0x3fffffffLL || md.n_nodes > 0x3fffffffLL || md.n_tri_index > 0x3fffffffLL)
-    return fail(ctx, RT_ERR_INVALID_ARGUMENT, "mesh too large");
+    return "mesh too large";
   if ((nt > 0 && !md.vertices) || (md.n_nodes > 0 && !md.nodes) || (md.n_tri_index > 0 && !md.tri_index))
-    return fail(ctx, RT_ERR_INVALID_ARGUMENT, "null mesh array");
+    return "null mesh array";
   // triangle records and normals in original order
   std::vector<double2> brute((size_t)nt * 5);
   std::vector<double4> normals((size_t)nt);
@@ -345,11 +423,11 @@ rt_status upload_mesh(rt_ctx* ctx, rt_scene* sc, const rt_mesh_desc& md, DMesh* 
     N[2] = double2{nd.bounds_max[1], nd.bounds_max[2]};
     if (nd.axis < 0) {
       if (nd.first < 0 || nd.count < 0 || (long long)nd.first + nd.count > md.n_tri_index)
-        return fail(ctx, RT_ERR_INVALID_ARGUMENT, "k-d leaf range out of bounds");
+        return "k-d leaf range out of bounds";
       N[3] = double2{0.0, pack2(nd.first, -1 - nd.count)};
     } else {
       if (nd.axis > 2 || nd.right <= k + 1 || nd.right >= md.n_nodes)
-        return fail(ctx, RT_ERR_INVALID_ARGUMENT, "k-d node layout is not preorder");
+        return "k-d node layout is not preorder";
       N[3] = double2{nd.split, pack2(nd.right, nd.axis)};
     }
   }
@@ -361,12 +439,12 @@ rt_status upload_mesh(rt_ctx* ctx, rt_scene* sc, const rt_mesh_desc& md, DMesh* 
       int k = st.back().first;
       int2 pd = st.back().second;
       st.pop_back();
-      if (seen[k]) return fail(ctx, RT_ERR_INVALID_ARGUMENT, "k-d nodes do not form a tree");
+      if (seen[k]) return "k-d nodes do not form a tree";
       seen[k] = 1;
       leaf_path[k] = pd;
       const rt_kd_node_desc& nd = md.nodes[k];
       if (nd.axis >= 0) {
-        if (pd.y >= 31) return fail(ctx, RT_ERR_INVALID_ARGUMENT, "k-d tree deeper than 31 levels");
+        if (pd.y >= 31) return "k-d tree deeper than 31 levels";
         st.push_back({k + 1, int2{pd.x, pd.y + 1}});
         st.push_back({nd.right, int2{pd.x | (1 << pd.y), pd.y + 1}});
       }
@@ -376,7 +454,7 @@ rt_status upload_mesh(rt_ctx* ctx, rt_scene* sc, const rt_mesh_desc& md, DMesh* 
   std::vector<int> occ_off((size_t)nt + 1, 0);
   for (long long k = 0; k < md.n_tri_index; k++) {
     int t = md.tri_index[k];
-    if (t < 0 || t >= nt) return fail(ctx, RT_ERR_INVALID_ARGUMENT, "k-d leaf index out of range");
+    if (t < 0 || t >= nt) return "k-d leaf index out of range";
     leaf_tris[k] = t;
     occ_off[t + 1]++;
   }
@@ -401,39 +479,64 @@ rt_status upload_mesh(rt_ctx* ctx, rt_scene* sc, const rt_mesh_desc& md, DMesh* 
   put_bvh(bnodes, &bvh);
   for (long long k = 0; k < nt; k++)
     for (int j = 0; j < 5; j++) btris[5 * k + j] = brute[5 * (size_t)order[k] + j];
+  P->bvh = std::move(bvh);
+  P->btris = std::move(btris);
+  P->brute = std::move(brute);
+  P->nodes = std::move(nodes);
+  P->normals = std::move(normals);
+  P->leaf_tris = std::move(leaf_tris);
+  P->occ_off = std::move(occ_off);
+  P->leaf_path = std::move(leaf_path);
+  P->occ = std::move(occ);
+  P->n_nodes = (int)md.n_nodes;
+  P->n_tris = (int)nt;
+  return std::string();
+}
+
+rt_status upload_prep(rt_ctx* ctx, rt_scene* sc, const MeshPrep& P, DMesh* out) {
+  DMesh M{};
+  for (int k = 0; k < 3; k++) {
+    M.bmin[k] = P.bmin[k];
+    M.bmax[k] = P.bmax[k];
+  }
   rt_status st;
   const double2* p2;
-  if ((st = upload(ctx, sc, bvh, &p2)) != RT_OK) return st;
+  if ((st = upload(ctx, sc, P.bvh, &p2)) != RT_OK) return st;
   M.bvh = p2;
-  if ((st = upload(ctx, sc, btris, &p2)) != RT_OK) return st;
+  if ((st = upload(ctx, sc, P.btris, &p2)) != RT_OK) return st;
   M.btris = p2;
-  if ((st = upload(ctx, sc, brute, &p2)) != RT_OK) return st;
+  if ((st = upload(ctx, sc, P.brute, &p2)) != RT_OK) return st;
   M.brute = p2;
   const double4* p4;
-  if ((st = upload(ctx, sc, normals, &p4)) != RT_OK) return st;
+  if ((st = upload(ctx, sc, P.normals, &p4)) != RT_OK) return st;
   M.normals = p4;
-  if ((st = upload(ctx, sc, nodes, &p2)) != RT_OK) return st;
+  if ((st = upload(ctx, sc, P.nodes, &p2)) != RT_OK) return st;
   M.nodes = p2;
   const int* pi;
-  if ((st = upload(ctx, sc, leaf_tris, &pi)) != RT_OK) return st;
+  if ((st = upload(ctx, sc, P.leaf_tris, &pi)) != RT_OK) return st;
   M.leaf_tris = pi;
   const int2* pi2;
-  if ((st = upload(ctx, sc, leaf_path, &pi2)) != RT_OK) return st;
+  if ((st = upload(ctx, sc, P.leaf_path, &pi2)) != RT_OK) return st;
   M.leaf_path = pi2;
-  if ((st = upload(ctx, sc, occ, &pi2)) != RT_OK) return st;
+  if ((st = upload(ctx, sc, P.occ, &pi2)) != RT_OK) return st;
   M.occ = pi2;
-  if ((st = upload(ctx, sc, occ_off, &pi)) != RT_OK) return st;
+  if ((st = upload(ctx, sc, P.occ_off, &pi)) != RT_OK) return st;
   M.occ_off = pi;
-  M.n_nodes = (int)md.n_nodes;
-  M.n_tris = (int)nt;
+  M.n_nodes = P.n_nodes;
+  M.n_tris = P.n_tris;
   *out = M;
   return RT_OK;
 }
 
+
 // Runs of at least this many consecutive spheres are searched through a BVH.
 const int kMinSphereRun = 8;
 
-rt_status do_upload(rt_ctx* ctx, const rt_scene_desc* d, rt_scene** out) {
+// Uploads a scene description.  preps, when given, holds one prepared mesh
+// per d->meshes entry (kept by a host scene); missing entries are prepared
+// here and stored into it.
+rt_status do_upload(rt_ctx* ctx, const rt_scene_desc* d, rt_scene** out,
+                    std::vector<std::shared_ptr<MeshPrep>>* preps = nullptr) {
   if (!d) return fail(ctx, RT_ERR_INVALID_ARGUMENT, "null scene description");
   if (d->n_objects < 0 || d->n_materials < 0 || d->n_lights < 0 || d->n_meshes < 0)
     return fail(ctx, RT_ERR_INVALID_ARGUMENT, "negative count");
@@ -448,9 +551,24 @@ rt_status do_upload(rt_ctx* ctx, const rt_scene_desc* d, rt_scene** out) {
   sc->has_outline = d->has_outline;
   sc->render_error = d->render_error ? d->render_error : "";
   DScene& S = sc->S;
+  for (int m = 0; m < d->n_meshes; m++)
+    if (d->meshes[m].n_triangles < 0 || d->meshes[m].n_nodes < 0 || d->meshes[m].n_tri_index < 0)
+      return fail(ctx, RT_ERR_INVALID_ARGUMENT, "negative count");
+  {
+    rt_status st = arena_open(ctx, sc.get(), scene_bytes_bound(d));
+    if (st != RT_OK) return st;
+  }
   std::vector<DMesh> meshes(d->n_meshes);
+  if (preps && preps->size() != (size_t)d->n_meshes) preps->assign(d->n_meshes, nullptr);
   for (int m = 0; m < d->n_meshes; m++) {
-    rt_status st = upload_mesh(ctx, sc.get(), d->meshes[m], &meshes[m]);
+    std::shared_ptr<MeshPrep> P = preps ? (*preps)[m] : nullptr;
+    if (!P) {
+      P = std::make_shared<MeshPrep>();
+      std::string e = prep_mesh(d->meshes[m], P.get());
+      if (!e.empty()) return fail(ctx, RT_ERR_INVALID_ARGUMENT, e);
+      if (preps) (*preps)[m] = P;
+    }
+    rt_status st = upload_prep(ctx, sc.get(), *P, &meshes[m]);
     if (st != RT_OK) return st;
   }
   std::vector<int4> obj;
@@ -643,6 +761,10 @@ rt_status do_upload(rt_ctx* ctx, const rt_scene_desc* d, rt_scene** out) {
   S.fog_end = d->fog_end;
   S.shadow_per_hit = K;
   sc->host_meshes = meshes;
+  {
+    rt_status st = arena_flush(ctx, sc.get());
+    if (st != RT_OK) return st;
+  }
   *out = sc.release();
   return RT_OK;
 }
@@ -1004,6 +1126,8 @@ void rt_ctx_destroy(rt_ctx* ctx) {
   if (ctx->stream) cudaStreamSynchronize(ctx->stream);
   for (rt_ctx* l : ctx->lanes) rt_ctx_destroy(l);
   ctx->lanes.clear();
+  if (ctx->pin) cudaFreeHost(ctx->pin);
+  ctx->pin = nullptr;
   free_all(ctx->scratch);
   free_all(ctx->dn_scratch);
   if (!ctx->borrowed_net) denoise_free(&ctx->net);
@@ -1071,6 +1195,10 @@ void rt_scene_free(rt_scene* scene) {
 
 struct rt_host_scene {
   HostScene hs;
+  // the meshes' device data prepared on the host, kept for later uploads
+  // (a host scene never changes after loading)
+  std::mutex mu;
+  std::vector<std::shared_ptr<MeshPrep>> prep;
 };
 
 rt_status rt_host_scene_load_json_file(const char* path, rt_host_scene** out) {
@@ -1083,6 +1211,16 @@ rt_status rt_host_scene_load_json_file(const char* path, rt_host_scene** out) {
   if (!load_scene_json(text, parent_dir(path), &h->hs, &err)) return fail(ctx, RT_ERR_SCENE, err);
   *out = h.release();
   return RT_OK;
+}
+
+rt_status rt_host_scene_upload(rt_ctx* ctx, rt_host_scene* hs, rt_scene** out) {
+  if (!ctx || !hs || !out) return fail(ctx, RT_ERR_INVALID_ARGUMENT, "null argument");
+  *out = nullptr;
+  CK(cudaSetDevice(ctx->device));
+  std::lock_guard<std::mutex> g(hs->mu);
+  rt_status s = do_upload(ctx, &hs->hs.desc, out, &hs->prep);
+  if (s == RT_OK) ctx->err.clear();
+  return s;
 }
 
 rt_status rt_auto_cameras_json_file(const char* path, rt_camera_config* out) {
@@ -1377,6 +1515,14 @@ rt_status rt_batch_autotune(rt_ctx* ctx, rt_job* jobs, uint32_t n, uint32_t* bes
   const uint32_t cand[4] = {1, 2, 4, 8};
   double best_ms = 1e300;
   uint32_t best = 4;
+  {
+    // warm-up with the most lanes: creates them and sizes their scratch for
+    // the largest jobs (the longest jobs go to the first lanes), so that the
+    // timed runs below allocate nothing
+    rt_batch_stats bs;
+    rt_status st = rt_render_batch(ctx, jobs, n, cand[3], &bs);
+    if (st != RT_OK) return st;
+  }
   for (uint32_t c : cand) {
     rt_batch_stats bs;
     rt_status st = rt_render_batch(ctx, jobs, n, c, &bs);
