@@ -800,13 +800,16 @@ __device__ __forceinline__ bool world_any(const DScene& S, const RayC& r, double
 // each lane's answer is that of world_any: the packet only changes how the
 // work is shared out.  The stack and the control flow are warp-uniform.
 // ---------------------------------------------------------------------------
+//
+// `stack` is the warp's RTB_STACK-entry traversal stack in shared memory:
+// every lane writes the same value to the same entry and reads back only
+// values it wrote itself, so it needs no synchronisation.
 template <class Leaf>
 __device__ __forceinline__ bool bvh_any_warp(const double2* bvh, const RayC& r, double tmax, bool active,
-                                             Leaf visit_leaf, int* err, Work* w) {
+                                             Leaf visit_leaf, volatile int* stack, int* err, Work* w) {
   const unsigned FULL = 0xffffffffu;
   bool found = false;
   if (!__any_sync(FULL, active)) return false;
-  int stack[RTB_STACK];
   int sp = 0;
   int node = 0;
   for (;;) {
@@ -855,7 +858,7 @@ __device__ __forceinline__ bool bvh_any_warp(const double2* bvh, const RayC& r, 
 
 // mesh_any for a warp of shadow rays.
 __device__ __forceinline__ bool mesh_any_warp(const DMesh& M, const RayC& r, double tmin, double tmax, bool active,
-                                              bool use_kd, int* err, Work* w) {
+                                              bool use_kd, volatile int* stack, int* err, Work* w) {
   active = active && mesh_bounds(M, r, tmin, tmax);
   return bvh_any_warp(
       M.bvh, r, tmax, active,
@@ -873,12 +876,12 @@ __device__ __forceinline__ bool mesh_any_warp(const DMesh& M, const RayC& r, dou
         }
         return false;
       },
-      err, w);
+      stack, err, w);
 }
 
 // group_hit<true> (any sphere of the run accepts within t_max) for a warp.
 __device__ __forceinline__ bool group_any_warp(const DScene& S, const DSphGroup& G, const RayC& r, double tmin,
-                                               double tmax, bool active, int* err, Work* w) {
+                                               double tmax, bool active, volatile int* stack, int* err, Work* w) {
   return bvh_any_warp(
       G.bvh, r, tmax, active,
       [&](int first, int cnt) {
@@ -890,14 +893,14 @@ __device__ __forceinline__ bool group_any_warp(const DScene& S, const DSphGroup&
         }
         return false;
       },
-      err, w);
+      stack, err, w);
 }
 
 // world.hit(ray, t_min, t_max).is_some() for a warp of rays (all 32 lanes
 // call it; lanes with valid == false take part without a ray).  Objects are
 // visited in scene order; the answer does not depend on the order.
 __device__ __forceinline__ bool world_any_warp(const DScene& S, const RayC& r, double tmin, double tmax, bool valid,
-                                               bool use_kd, int* err, Work* w) {
+                                               bool use_kd, volatile int* stack, int* err, Work* w) {
   bool blocked = false;
   for (int i = 0; i < S.n_obj; i++) {
     int4 ob = __ldg(S.obj + i);
@@ -920,10 +923,10 @@ __device__ __forceinline__ bool world_any_warp(const DScene& S, const RayC& r, d
         }
         break;
       case OBJ_MESH:
-        if (mesh_any_warp(S.mesh[ob.y], r, tmin, tmax, live, use_kd, err, w)) blocked = true;
+        if (mesh_any_warp(S.mesh[ob.y], r, tmin, tmax, live, use_kd, stack, err, w)) blocked = true;
         break;
       default:
-        if (group_any_warp(S, S.grp[ob.y], r, tmin, tmax, live, err, w)) blocked = true;
+        if (group_any_warp(S, S.grp[ob.y], r, tmin, tmax, live, stack, err, w)) blocked = true;
         break;
     }
   }

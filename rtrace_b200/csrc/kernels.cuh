@@ -393,13 +393,15 @@ __global__ void __launch_bounds__(128) k_emit(DFrame F, int level, long long c0)
 
 // world.hit(&shadow_ray, 0.001, distance).is_some() per shadow ray
 template <bool COUNT>
-__global__ void __launch_bounds__(128) k_shadow(DFrame F, int level, long long c0) {
+__global__ void __launch_bounds__(128, 8) k_shadow(DFrame F, int level, long long c0) {
   long long nh = F.nhits[level];
   long long c1 = c0 + F.chunk_hits < nh ? c0 + F.chunk_hits : nh;
   const int K = F.K;
   long long nhc = c1 > c0 ? c1 - c0 : 0;
   long long ns = nhc * K;
   Work w{0, 0, 0, 0};
+  __shared__ int s_stack[4][RTB_STACK];  // one traversal stack per warp (128 threads)
+  volatile int* stack = s_stack[threadIdx.x >> 5];
   // The warp steps through the rays together (world_any_warp is a warp
   // collective).  Hit-major order: the K rays of one hit point sit in
   // adjacent lanes, so a warp holds a bundle of rays from one or two points
@@ -424,7 +426,7 @@ __global__ void __launch_bounds__(128) k_shadow(DFrame F, int level, long long c
     } else {
       r = make_rayc(mk(0.0, 0.0, 0.0), mk(0.0, 0.0, 1.0));
     }
-    bool blocked = world_any_warp(F.S, r, 0.001, valid ? dist : 0.0, valid, F.use_kd != 0, F.err,
+    bool blocked = world_any_warp(F.S, r, 0.001, valid ? dist : 0.0, valid, F.use_kd != 0, stack, F.err,
                                   COUNT ? &w : nullptr);
     if (have) F.sh.vis[s] = (valid && !blocked) ? 1 : 0;
   }
