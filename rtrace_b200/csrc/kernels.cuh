@@ -340,8 +340,9 @@ __global__ void __launch_bounds__(128) k_emit(DFrame F, int level, long long c0)
       V3 lp = ld3(L0.pos);
       if (!L0.disk) {
         // calculate_point_light_contribution (src/lighting.rs:100-142)
-        V3 ldir = normalize(lp - hr.p);
-        double dist = norm(lp - hr.p);
+        V3 lv = lp - hr.p;
+        double dist = norm(lv);
+        V3 ldir = lv / dist;
         F.sh.dx[s] = ldir.x;
         F.sh.dy[s] = ldir.y;
         F.sh.dz[s] = ldir.z;
@@ -379,8 +380,10 @@ __global__ void __launch_bounds__(128) k_emit(DFrame F, int level, long long c0)
             }
           }
           V3 sp = lp + dx * bu + dy * bv;
-          V3 sdir = normalize(sp - hr.p);
-          double dist = norm(sp - hr.p);
+          // normalize(v) divides by norm(v): one square root for both
+          V3 sv = sp - hr.p;
+          double dist = norm(sv);
+          V3 sdir = sv / dist;
           F.sh.dx[s] = sdir.x;
           F.sh.dy[s] = sdir.y;
           F.sh.dz[s] = sdir.z;
