@@ -812,12 +812,21 @@ __device__ __forceinline__ bool bvh_any_warp(const double2* bvh, const RayC& r, 
   if (!__any_sync(FULL, active)) return false;
   int sp = 0;
   int node = 0;
+  // work counting only: whether this lane's own walk reaches the node (its
+  // ray hit the node's box), one bit per stack entry, so that the counters
+  // hold the single-ray work rather than the packet's shared visits
+  bool mine = true;
+  unsigned long long mine_bits = 0;
   for (;;) {
     BNode n = load_bnode(bvh, node);
-    if (w && active) w->nodes++;
+    if (w && active && mine) w->nodes++;
     double tl = 0, tr = 0;
     bool hl = active && n.lcnt >= 0 && box_hit(n.lmn, n.lmx, r, tmax, &tl);
     bool hr = active && n.rcnt >= 0 && box_hit(n.rmn, n.rmx, r, tmax, &tr);
+    if (w) {
+      hl = hl && mine;
+      hr = hr && mine;
+    }
     // leaf children first: they may retire lanes
     if (n.lcnt > 0 && hl && visit_leaf(n.lidx, n.lcnt)) {
       found = true;
@@ -839,12 +848,19 @@ __device__ __forceinline__ bool bvh_any_warp(const double2* bvh, const RayC& r, 
         if ((threadIdx.x & 31) == 0) atomicOr(err, ERR_STACK);
         return found;
       }
+      if (w) {
+        const bool pushed_mine = right_first ? hl : hr;
+        mine_bits = pushed_mine ? (mine_bits | (1ull << sp)) : (mine_bits & ~(1ull << sp));
+        mine = right_first ? hr : hl;
+      }
       stack[sp++] = right_first ? n.lidx : n.ridx;
       next = right_first ? n.ridx : n.lidx;
     } else if (gl) {
       next = n.lidx;
+      if (w) mine = hl;
     } else if (gr) {
       next = n.ridx;
+      if (w) mine = hr;
     }
     if (!__any_sync(FULL, active)) return found;
     if (next >= 0) {
@@ -853,6 +869,7 @@ __device__ __forceinline__ bool bvh_any_warp(const double2* bvh, const RayC& r, 
     }
     if (sp == 0) return found;
     node = stack[--sp];
+    if (w) mine = (mine_bits >> sp) & 1ull;
   }
 }
 
