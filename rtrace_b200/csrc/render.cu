@@ -26,6 +26,12 @@
 
 using namespace rtb;
 
+struct DirectCopy {
+  size_t off, take;
+  const char* src;
+  size_t bytes;
+};
+
 struct rt_scene {
   rt_ctx* ctx = nullptr;
   int device = 0;
@@ -43,6 +49,7 @@ struct rt_scene {
   // staging buffer and copied once (see upload())
   char* blk = nullptr;
   size_t blk_cap = 0, blk_used = 0;
+  std::vector<DirectCopy> direct;  // arena regions copied from pinned images
 };
 
 struct rt_ctx {
@@ -213,11 +220,40 @@ rt_status ensure_dn_scratch(rt_ctx* ctx, long long n) {
 // scene instead of one per array.
 rt_status arena_flush(rt_ctx* ctx, rt_scene* sc) {
   if (sc->blk && sc->blk_used) {
-    CK(cudaMemcpyAsync(sc->blk, ctx->pin, sc->blk_used, cudaMemcpyHostToDevice, ctx->stream));
+    // staged ranges from the pinned staging buffer, regions reserved by
+    // upload_image straight from their own pinned source
+    size_t pos = 0;
+    for (const DirectCopy& d : sc->direct) {
+      if (d.off > pos) CK(cudaMemcpyAsync(sc->blk + pos, ctx->pin + pos, d.off - pos, cudaMemcpyHostToDevice, ctx->stream));
+      if (d.bytes) CK(cudaMemcpyAsync(sc->blk + d.off, d.src, d.bytes, cudaMemcpyHostToDevice, ctx->stream));
+      pos = d.off + d.take;
+    }
+    if (sc->blk_used > pos)
+      CK(cudaMemcpyAsync(sc->blk + pos, ctx->pin + pos, sc->blk_used - pos, cudaMemcpyHostToDevice, ctx->stream));
     CK(cudaStreamSynchronize(ctx->stream));
   }
+  sc->direct.clear();
   sc->blk = nullptr;
   sc->blk_cap = sc->blk_used = 0;
+  return RT_OK;
+}
+
+// Reserves `bytes` of the arena for a pinned host image and copies it there
+// at the flush (no staging copy); a dedicated allocation and a direct copy
+// when the arena has no room.
+rt_status upload_image(rt_ctx* ctx, rt_scene* sc, const char* src, size_t bytes, char** dev) {
+  const size_t take = (std::max<size_t>(bytes, 16) + 255) & ~(size_t)255;
+  if (sc->blk && sc->blk_used + take <= sc->blk_cap) {
+    *dev = sc->blk + sc->blk_used;
+    sc->direct.push_back(DirectCopy{sc->blk_used, take, src, bytes});
+    sc->blk_used += take;
+  } else {
+    char* p = nullptr;
+    CK(dalloc(sc->allocs, &p, take));
+    if (bytes) CK(cudaMemcpy(p, src, bytes, cudaMemcpyHostToDevice));
+    *dev = p;
+  }
+  sc->uploaded_bytes += bytes;
   return RT_OK;
 }
 
@@ -371,7 +407,51 @@ struct MeshPrep {
   std::vector<int2> leaf_path, occ;
   double bmin[3], bmax[3];
   int n_nodes = 0, n_tris = 0;
+  // Kept by a host scene, the nine arrays above are packed into one pinned
+  // buffer (each at a 256-byte aligned offset) and the vectors released:
+  // uploads then copy the image straight from pinned memory.
+  char* image = nullptr;
+  size_t image_bytes = 0;
+  size_t off[9] = {}, len[9] = {};
+  ~MeshPrep() {
+    if (image) cudaFreeHost(image);
+  }
 };
+
+// Packs P's arrays into a pinned image (see MeshPrep); leaves P as it is if
+// pinned memory cannot be had.
+void pack_prep(MeshPrep* P) {
+  const void* src[9] = {P->bvh.data(), P->btris.data(), P->brute.data(), P->normals.data(), P->nodes.data(),
+                        P->leaf_tris.data(), P->leaf_path.data(), P->occ.data(), P->occ_off.data()};
+  size_t n[9] = {P->bvh.size() * sizeof(double2), P->btris.size() * sizeof(double2),
+                 P->brute.size() * sizeof(double2), P->normals.size() * sizeof(double4),
+                 P->nodes.size() * sizeof(double2), P->leaf_tris.size() * sizeof(int),
+                 P->leaf_path.size() * sizeof(int2), P->occ.size() * sizeof(int2), P->occ_off.size() * sizeof(int)};
+  size_t total = 0;
+  for (int k = 0; k < 9; k++) {
+    P->off[k] = total;
+    P->len[k] = n[k];
+    total += (std::max<size_t>(n[k], 16) + 255) & ~(size_t)255;
+  }
+  char* img = nullptr;
+  if (cudaHostAlloc((void**)&img, total, cudaHostAllocPortable) != cudaSuccess) {
+    cudaGetLastError();
+    return;
+  }
+  for (int k = 0; k < 9; k++)
+    if (n[k]) memcpy(img + P->off[k], src[k], n[k]);
+  P->image = img;
+  P->image_bytes = total;
+  P->bvh = {};
+  P->btris = {};
+  P->brute = {};
+  P->normals = {};
+  P->nodes = {};
+  P->leaf_tris = {};
+  P->leaf_path = {};
+  P->occ = {};
+  P->occ_off = {};
+}
 
 // Returns an empty string, or why the description is invalid.
 std::string prep_mesh(const rt_mesh_desc& md, MeshPrep* P) {
@@ -499,6 +579,24 @@ rt_status upload_prep(rt_ctx* ctx, rt_scene* sc, const MeshPrep& P, DMesh* out) 
     M.bmin[k] = P.bmin[k];
     M.bmax[k] = P.bmax[k];
   }
+  M.n_nodes = P.n_nodes;
+  M.n_tris = P.n_tris;
+  if (P.image) {
+    char* base = nullptr;
+    rt_status st = upload_image(ctx, sc, P.image, P.image_bytes, &base);
+    if (st != RT_OK) return st;
+    M.bvh = reinterpret_cast<const double2*>(base + P.off[0]);
+    M.btris = reinterpret_cast<const double2*>(base + P.off[1]);
+    M.brute = reinterpret_cast<const double2*>(base + P.off[2]);
+    M.normals = reinterpret_cast<const double4*>(base + P.off[3]);
+    M.nodes = reinterpret_cast<const double2*>(base + P.off[4]);
+    M.leaf_tris = reinterpret_cast<const int*>(base + P.off[5]);
+    M.leaf_path = reinterpret_cast<const int2*>(base + P.off[6]);
+    M.occ = reinterpret_cast<const int2*>(base + P.off[7]);
+    M.occ_off = reinterpret_cast<const int*>(base + P.off[8]);
+    *out = M;
+    return RT_OK;
+  }
   rt_status st;
   const double2* p2;
   if ((st = upload(ctx, sc, P.bvh, &p2)) != RT_OK) return st;
@@ -566,7 +664,10 @@ rt_status do_upload(rt_ctx* ctx, const rt_scene_desc* d, rt_scene** out,
       P = std::make_shared<MeshPrep>();
       std::string e = prep_mesh(d->meshes[m], P.get());
       if (!e.empty()) return fail(ctx, RT_ERR_INVALID_ARGUMENT, e);
-      if (preps) (*preps)[m] = P;
+      if (preps) {
+        pack_prep(P.get());
+        (*preps)[m] = P;
+      }
     }
     rt_status st = upload_prep(ctx, sc.get(), *P, &meshes[m]);
     if (st != RT_OK) return st;

@@ -225,3 +225,33 @@ def test_outline_entry_point_matches_oracle(gpu_ctx, cfg):
                                  cfg.get("edge_color", (0.0, 0.0, 0.0)), cfg.get("use_8_neighbors", False),
                                  cfg.get("thickness", 1.0))
         assert np.array_equal(img, ref), (w, h, int((img != ref).any(2).sum()))
+
+
+@pytest.mark.gpu
+def test_host_scene_uploads_render_the_same(gpu_ctx, tmp_path):
+    """A host scene's first upload prepares its meshes and keeps them packed
+    in pinned memory; later uploads copy that image.  Both, and the generic
+    description path (rt_scene_upload), must give the same frame."""
+    import ctypes
+    import rtrace_b200 as rt
+    from rtrace_b200 import _capi, workloads
+    path = workloads.make_noisy_icosphere(str(tmp_path), level=4, seed=3)
+    host = rt.HostScene.from_json_file(path)
+    r = rt.Renderer(200, 120)
+    r.anti_aliasing_mode = rt.AntiAliasingMode.NoJitter
+    imgs = []
+    for _ in range(3):
+        sc = rt.Scene.upload(host, gpu_ctx)
+        imgs.append(r.render(sc))
+        assert sc.device_bytes > 0
+        sc.close()
+    L = _capi.lib()
+    h = ctypes.c_void_p()
+    st = L.rt_scene_upload(gpu_ctx.handle, L.rt_host_scene_desc(host.handle), ctypes.byref(h))
+    assert st == 0, L.rt_last_error(gpu_ctx.handle)
+    generic = rt.Scene(h, gpu_ctx)
+    imgs.append(r.render(generic))
+    generic.close()
+    direct = r.render(rt.Scene.from_json_file(path, gpu_ctx))
+    for img in imgs:
+        assert np.array_equal(img, direct)
