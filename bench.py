@@ -207,6 +207,45 @@ def batch_run(rt, ctx, directory, steps):
     return out
 
 
+def large_mesh_run(rt, ctx, directory, reps):
+    """The large-mesh configuration: a 1024x1024 fractal-noise heightfield
+    (2,093,058 triangles, f32 STL), a mirror sphere (r 20, reflectivity
+    0.9), one disk light (16 rays), fog density 0.02, outline on, rendered
+    from its four auto-camera views at 3840x2160, no-jitter (outlines),
+    depth 10.  Reports the host load (JSON + STL + the reference k-d build),
+    the first upload (BVH build and device copy) and the device time per
+    frame."""
+    from rtrace_b200 import workloads
+    path = workloads.make_terrain(os.path.join(directory, "terrain"), n=1024, seed=11)
+    t0 = time.perf_counter()
+    host = rt.HostScene.from_json_file(path)
+    t1 = time.perf_counter()
+    scene = rt.Scene.upload(host, ctx)
+    t2 = time.perf_counter()
+    cams = rt.auto_cameras(path=path)
+    jobs = []
+    for view in ("left", "front", "top", "perspective"):
+        r = rt.Renderer(3840, 2160)
+        r.anti_aliasing_mode = rt.AntiAliasingMode.NoJitter
+        r.outline_config = scene.get_outline_config()
+        jobs.append(rt.Job(scene, r, cams[view]))
+    rt.render_batch(jobs, lanes=1, ctx=ctx)  # warm-up (scratch for 4K)
+    ms, rays, frames = 0.0, 0, 0
+    for _ in range(reps):
+        rt.render_batch(jobs, lanes=1, ctx=ctx)
+        for j in jobs:
+            ms += j.renderer.last_stats.device_ms
+            rays += j.renderer.last_stats.rays
+            frames += 1
+    out = {"workload": "terrain_1024_4k_4_auto_views", "triangles": 2 * 1023 * 1023,
+           "host_load_s": t1 - t0, "first_upload_s": t2 - t1, "device_bytes": scene.device_bytes,
+           "ms_per_frame": ms / frames, "mrays_per_s": rays / (ms * 1e-3) / 1e6, "rays_per_frame": rays // frames,
+           "timing": "CUDA events per render, 4 views x %d" % reps}
+    scene.close()
+    host.close()
+    return out
+
+
 def read_traffic():
     """Per-launch DRAM bytes of the shadow kernel from the committed ncu summary."""
     try:
@@ -288,6 +327,7 @@ def main():
     ap.add_argument("--cpu-seconds", type=float, default=15.0)
     ap.add_argument("--no-learned", action="store_true", help="skip the learned-vs-plain shadow comparison")
     ap.add_argument("--no-batch", action="store_true", help="skip the 256-job batch measurement")
+    ap.add_argument("--no-large", action="store_true", help="skip the 2-million-triangle terrain measurement")
     args = ap.parse_args()
     args.warmup = max(3, args.warmup)
     rank, world, local = env_int("RANK", 0), env_int("WORLD_SIZE", 1), env_int("LOCAL_RANK", 0)
@@ -413,6 +453,12 @@ def main():
                 learned = learned_vs_plain(rt, torch, ctx, d, min(args.steps, 10))
             except Exception as e:  # report, do not lose the headline line
                 learned = {"unavailable": "failed: %s" % e}
+        large = None
+        if world == 1 and not args.no_large:
+            try:
+                large = large_mesh_run(rt, ctx, d, 2)
+            except Exception as e:
+                large = {"unavailable": "failed: %s" % e}
         batch = None
         if world == 1 and not args.no_batch:
             try:
@@ -438,6 +484,7 @@ def main():
             "cpu_baseline": cpu,
             "learned_vs_plain": learned,
             "batch": batch,
+            "large_mesh": large,
             "clocks": clk,
         }
         print(json.dumps(line), flush=True)

@@ -49,6 +49,9 @@ struct rt_scene {
   // staging buffer and copied once (see upload())
   char* blk = nullptr;
   size_t blk_cap = 0, blk_used = 0;
+  char* arena = nullptr;  // the scene's device block (returned to the pool when freed)
+  size_t arena_bytes = 0;
+  ~rt_scene();
   std::vector<DirectCopy> direct;  // arena regions copied from pinned images
 };
 
@@ -257,12 +260,81 @@ rt_status upload_image(rt_ctx* ctx, rt_scene* sc, const char* src, size_t bytes,
   return RT_OK;
 }
 
+// Freed scene blocks, kept per device for the next upload of a similar
+// size (uploading and freeing a scene per frame then allocates nothing).
+// Bounded: at most kPoolBlocks blocks and kPoolBytes bytes per device.
+struct PoolBlock {
+  int device;
+  size_t bytes;
+  char* ptr;
+};
+std::mutex g_pool_mu;
+std::vector<PoolBlock> g_pool;
+const size_t kPoolBlocks = 8;
+const size_t kPoolBytes = (size_t)4 << 30;
+
+char* pool_take(int device, size_t bytes, size_t* got) {
+  std::lock_guard<std::mutex> g(g_pool_mu);
+  int best = -1;
+  for (int i = 0; i < (int)g_pool.size(); i++) {
+    const PoolBlock& b = g_pool[i];
+    if (b.device == device && b.bytes >= bytes && b.bytes <= 2 * bytes &&
+        (best < 0 || b.bytes < g_pool[best].bytes))
+      best = i;
+  }
+  if (best < 0) return nullptr;
+  char* p = g_pool[best].ptr;
+  *got = g_pool[best].bytes;
+  g_pool.erase(g_pool.begin() + best);
+  return p;
+}
+
+void pool_give(int device, char* p, size_t bytes) {
+  {
+    std::lock_guard<std::mutex> g(g_pool_mu);
+    size_t n = 0, total = 0;
+    for (const PoolBlock& b : g_pool)
+      if (b.device == device) {
+        n++;
+        total += b.bytes;
+      }
+    if (n < kPoolBlocks && total + bytes <= kPoolBytes) {
+      g_pool.push_back(PoolBlock{device, bytes, p});
+      return;
+    }
+  }
+  cudaFree(p);
+}
+
+}  // namespace
+
+// Frees the scene's own allocations and returns its block to the pool; no
+// kernel may still read the block when a later upload reuses it, hence the
+// device-wide synchronisation (which cudaFree would imply as well).
+rt_scene::~rt_scene() {
+  int prev = -1;
+  cudaGetDevice(&prev);
+  cudaSetDevice(device);
+  cudaDeviceSynchronize();
+  free_all(allocs);
+  if (arena) pool_give(device, arena, arena_bytes);
+  if (prev >= 0 && prev != device) cudaSetDevice(prev);
+}
+
+namespace {
+
 rt_status arena_open(rt_ctx* ctx, rt_scene* sc, size_t bytes) {
   rt_status st = arena_flush(ctx, sc);
   if (st != RT_OK) return st;
   bytes = (bytes + 255) & ~(size_t)255;
-  char* b = nullptr;
-  CK(dalloc(sc->allocs, &b, bytes));
+  size_t got = 0;
+  char* b = pool_take(ctx->device, bytes, &got);
+  if (!b) {
+    CK(cudaMalloc((void**)&b, bytes));
+    got = bytes;
+  }
+  sc->arena = b;
+  sc->arena_bytes = got;
   if (ctx->pin_cap < bytes) {
     if (ctx->pin) cudaFreeHost(ctx->pin);
     ctx->pin = nullptr;
@@ -1290,7 +1362,6 @@ rt_status rt_scene_camera_aspect(rt_ctx* ctx, const rt_scene* scene, double* out
 void rt_scene_free(rt_scene* scene) {
   if (!scene) return;
   cudaSetDevice(scene->device);
-  free_all(scene->allocs);
   delete scene;
 }
 

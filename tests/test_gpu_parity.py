@@ -115,15 +115,20 @@ def _gpu_mesh(ctx, sc, rays, use_kd, mode, tmax=float("inf")):
     return out
 
 
-@pytest.mark.parametrize("stl_name", ["plus.stl", "icosphere"])
+@pytest.mark.parametrize("stl_name", ["plus.stl", "icosphere", "heightfield"])
 @pytest.mark.parametrize("use_kd", [True, False])
 def test_mesh_queries_match_oracle(gpu_ctx, tmp_path, use_kd, stl_name):
     from tests.kd_rays import plus_rays
     if stl_name == "plus.stl":
         stl = os.path.join(oracle_lib.SCENES, "plus.stl")
-    else:
+    elif stl_name == "icosphere":
         stl = os.path.join(str(tmp_path), "ico.stl")
         v, f = workloads.noisy_icosphere(4, 3)
+        workloads.write_binary_stl(stl, v, f)
+    else:
+        # grid-aligned triangles: many edges lie exactly on k-d split planes
+        stl = os.path.join(str(tmp_path), "hf.stl")
+        v, f = workloads.heightfield(41, 5, height=4.0)
         workloads.write_binary_stl(stl, v, f)
     sc = rt.Scene.from_json_str(_mesh_scene(stl))
     rays = np.concatenate([plus_rays(stl, extra_random=3000), _surface_rays(stl, 3000, 9)])
@@ -154,6 +159,13 @@ def _synthetic_scenes(tmp):
                          "material": {"color": "#33AA77", "ambient": 0.1, "diffuse": 0.7, "specular": 0.3,
                                       "shininess": 16, "reflectivity": 0.4}})
     paths["mixed"] = workloads.write_scene(d, "mixed.json", s)
+    # the large-mesh configuration's scene at a small size
+    hv, hf = workloads.heightfield(25, 11)
+    workloads.write_binary_stl(os.path.join(d, "terrain.stl"), hv, hf)
+    t = workloads.terrain_scene("terrain.stl", 25)
+    t["objects"][1]["center"] = [0, 0, 12]
+    t["objects"][1]["radius"] = 4
+    paths["terrain"] = workloads.write_scene(d, "terrain.json", t)
     return paths
 
 
@@ -161,7 +173,7 @@ def _synthetic_scenes(tmp):
                                         ("stochastic", 4)])
 def test_modes_match_oracle(gpu_ctx, tmp_path, aa, samples):
     for name, path in _synthetic_scenes(tmp_path).items():
-        outline = name == "icosphere" and aa != "quincunx"
+        outline = name in ("icosphere", "terrain") and aa != "quincunx"
         (img, lin), st = gpu_render(path, 71, 43, aa, samples, outline=outline, linear=True)
         ref, rlin, cnt = oracle_lib.render(path, width=71, height=43, aa=aa, samples=samples, outline=outline,
                                            linear=True, counts=True)
