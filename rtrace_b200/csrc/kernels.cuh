@@ -367,27 +367,44 @@ __global__ void __launch_bounds__(128) k_emit(DFrame F, int level, long long c0)
         V3 up = fabs(cdir.x) < 0.9 ? mk(1.0, 0.0, 0.0) : mk(0.0, 1.0, 0.0);
         V3 bu = normalize(cross(up, cdir));
         V3 bv = normalize(cross(cdir, bu));
-        for (int smp = 0; smp < F.dsamp; smp++, s += CH) {
-          double dx = 0.0, dy = 0.0;
-          if (ok) {
-            for (int it = 0;; it++) {
-              if (it >= 4096 || !rng.range(-radius, radius, &dx) || !rng.range(-radius, radius, &dy)) {
-                atomicOr(F.err, ERR_WATCHDOG);
-                ok = false;
-                break;
-              }
-              if (dx * dx + dy * dy <= radius * radius) break;
-            }
+        // One rejection-sampling attempt per iteration; an accepted attempt
+        // emits the next sample.  Each lane draws exactly the numbers the
+        // reference's per-sample loop draws, in the same order, but the
+        // lanes of a warp stay in step (every attempt takes four words, so
+        // they also refill their ChaCha buffers together) instead of each
+        // sample waiting for the warp's slowest lane.
+        int smp = 0, it = 0;
+        while (ok && smp < F.dsamp) {
+          double dx, dy;
+          if (it >= 4096 || !rng.range(-radius, radius, &dx) || !rng.range(-radius, radius, &dy)) {
+            atomicOr(F.err, ERR_WATCHDOG);
+            ok = false;
+            break;
           }
-          V3 sp = lp + dx * bu + dy * bv;
-          // normalize(v) divides by norm(v): one square root for both
-          V3 sv = sp - hr.p;
-          double dist = norm(sv);
-          V3 sdir = sv / dist;
+          it++;
+          if (dx * dx + dy * dy <= radius * radius) {
+            V3 sp = lp + dx * bu + dy * bv;
+            // normalize(v) divides by norm(v): one square root for both
+            V3 sv = sp - hr.p;
+            double dist = norm(sv);
+            V3 sdir = sv / dist;
+            F.sh.dx[s] = sdir.x;
+            F.sh.dy[s] = sdir.y;
+            F.sh.dz[s] = sdir.z;
+            F.sh.dist[s] = dist;
+            s += CH;
+            smp++;
+            it = 0;
+          }
+        }
+        // after a failed range check or the watchdog: never traced
+        for (; smp < F.dsamp; smp++, s += CH) {
+          V3 sv = lp - hr.p;
+          V3 sdir = sv / norm(sv);
           F.sh.dx[s] = sdir.x;
           F.sh.dy[s] = sdir.y;
           F.sh.dz[s] = sdir.z;
-          F.sh.dist[s] = ok ? dist : -1.0;  // -1: never traced
+          F.sh.dist[s] = -1.0;
         }
       }
     }
