@@ -207,6 +207,35 @@ def batch_run(rt, ctx, directory, steps):
     return out
 
 
+def small_scene_run(rt, ctx, directory, reps, with_cpu):
+    """The small configuration: one sphere over a grid-textured reflective
+    plane, one point light, orthographic camera, 400x300 quincunx (the
+    library call; the CLI's diagonal rule would give a square image), depth
+    10, seed 0.  Device time per frame on the GPU and, when asked, the
+    whole frame on the CPU restatement (oracle, all host threads)."""
+    from rtrace_b200 import workloads
+    path = workloads.write_scene(directory, "sphere_grid.json", workloads.sphere_grid_scene())
+    scene = rt.Scene.from_json_file(path, ctx)
+    r = rt.Renderer(400, 300)
+    for _ in range(3):
+        r.render(scene)
+    ms, rays = 0.0, 0
+    for _ in range(reps):
+        r.render(scene)
+        ms += r.last_stats.device_ms
+        rays += r.last_stats.rays
+    out = {"workload": "sphere_grid_400x300_quincunx", "ms_per_frame": ms / reps,
+           "mrays_per_s": rays / (ms * 1e-3) / 1e6, "rays_per_frame": rays // reps}
+    if with_cpu:
+        from tests import oracle_lib
+        t = time.perf_counter()
+        oracle_lib.render(path, width=400, height=300, aa="quincunx", threads=os.cpu_count() or 1)
+        out["cpu_port_ms_per_frame"] = 1e3 * (time.perf_counter() - t)
+        out["cpu_port_cores"] = os.cpu_count() or 1
+    scene.close()
+    return out
+
+
 def large_mesh_run(rt, ctx, directory, reps):
     """The large-mesh configuration: a 1024x1024 fractal-noise heightfield
     (2,093,058 triangles, f32 STL), a mirror sphere (r 20, reflectivity
@@ -453,6 +482,12 @@ def main():
                 learned = learned_vs_plain(rt, torch, ctx, d, min(args.steps, 10))
             except Exception as e:  # report, do not lose the headline line
                 learned = {"unavailable": "failed: %s" % e}
+        small = None
+        if world == 1:
+            try:
+                small = small_scene_run(rt, ctx, d, 20, not args.no_cpu_baseline)
+            except Exception as e:
+                small = {"unavailable": "failed: %s" % e}
         large = None
         if world == 1 and not args.no_large:
             try:
@@ -485,6 +520,7 @@ def main():
             "learned_vs_plain": learned,
             "batch": batch,
             "large_mesh": large,
+            "small_scene": small,
             "clocks": clk,
         }
         print(json.dumps(line), flush=True)

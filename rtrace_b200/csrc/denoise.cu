@@ -122,8 +122,10 @@ struct ConvSmem {
   static constexpr int CPT = CIN / 8;                     // 16-byte channel chunks per pixel
   static constexpr int B_BYTES = 9 * CPT * COUT * 16;     // weights
   static constexpr int TAIL = 128;                        // barriers, TMEM slot, abort flag
+  static constexpr int BIAS = 128;                        // COUT floats
+  static constexpr int OUT = 4 * 32 * COUT * 2;           // epilogue staging: 32 pixels per warp
   static int a_bytes(int dil) { return 3 * CPT * halo_block(dil); }
-  static int total(int dil) { return 1024 + NSTAGE * a_bytes(dil) + B_BYTES + TAIL; }
+  static int total(int dil) { return 1024 + NSTAGE * a_bytes(dil) + B_BYTES + TAIL + BIAS + OUT; }
 };
 
 __device__ __forceinline__ void tma_load_4d(uint32_t dst, const CUtensorMap* map, int c0, int c1, int c2, int c3,
@@ -190,9 +192,12 @@ __global__ void __launch_bounds__(CONV_THREADS) k_conv3x3_tc(const __grid_consta
   volatile int* abort_flag = reinterpret_cast<volatile int*>(tail + 8 * (2 * NSTAGE + 2 * NACC) + 4);
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
 
+  float* s_bias = reinterpret_cast<float*>(tail + SM::TAIL);
+  unsigned char* s_out = tail + SM::TAIL + SM::BIAS;  // 4 warps x 32 pixels x COUT halves
   {
     uint4* dst = reinterpret_cast<uint4*>(base + NSTAGE * A_BYTES);
     for (int i = tid; i < SM::B_BYTES / 16; i += CONV_THREADS) dst[i] = wl[i];
+    for (int i = tid; i < COUT; i += CONV_THREADS) s_bias[i] = bias[i];
   }
   if (tid == 0) {
     for (int k = 0; k < NSTAGE; k++) {
@@ -322,25 +327,43 @@ __global__ void __launch_bounds__(CONV_THREADS) k_conv3x3_tc(const __grid_consta
       const long long py = tile / tiles_x;
       const int y = (int)(py % H), p = (int)(py / H);
       const int x = tx * TILE_M + tid;
-      if (x < W) {
-        if (MODE == 0) {
-          __half* o = out + (((long long)p * H + y) * (long long)W + x) * COUT;
+      if (MODE == 0) {
+        // Each warp stages its 32 pixels (COUT halves each) in shared
+        // memory, 16-byte chunks XOR-swizzled so that both the writes and
+        // the read-back are free of bank conflicts, then writes them out as
+        // contiguous 512-byte rows (the 32 pixels are contiguous in NHWC).
+        constexpr int CPX = COUT / 8;            // 16-byte chunks per pixel
+        constexpr int ROWB = COUT * 2;           // bytes per pixel
+        constexpr int PPL = 128 / ROWB;          // pixels per 128-byte bank window
+        unsigned char* wb = s_out + warp * 32 * ROWB;
 #pragma unroll
-          for (int c = 0; c < COUT; c += 8) {
-            __align__(16) __half h[8];
+        for (int c = 0; c < CPX; c++) {
+          __align__(16) __half h[8];
 #pragma unroll
-            for (int e = 0; e < 8; e++) {
-              float v = __uint_as_float(accv[c + e]) + __ldg(bias + c + e);
-              h[e] = __float2half_rn(v > 0.f ? v : 0.f);
-            }
-            *reinterpret_cast<uint4*>(o + c) = *reinterpret_cast<const uint4*>(h);
+          for (int e = 0; e < 8; e++) {
+            float v = __uint_as_float(accv[8 * c + e]) + s_bias[8 * c + e];
+            h[e] = __float2half_rn(v > 0.f ? v : 0.f);
           }
-        } else {
+          const int phys = c ^ ((lane / PPL) & (CPX - 1));
+          *reinterpret_cast<uint4*>(wb + lane * ROWB + phys * 16) = *reinterpret_cast<const uint4*>(h);
+        }
+        __syncwarp();
+        const int xw = tx * TILE_M + warp * 32;  // the warp's first pixel
+        __half* ow = out + (((long long)p * H + y) * (long long)W + xw) * COUT;
 #pragma unroll
-          for (int j = 0; j < DN_MAX_SLOTS; j++) {
-            float v = __uint_as_float(accv[j]) + __ldg(bias + j);
-            vis[(((long long)p * DN_MAX_SLOTS + j) * H + y) * (long long)W + x] = 1.f / (1.f + __expf(-v));
-          }
+        for (int k = 0; k < CPX; k++) {
+          const int o = k * 512 + lane * 16;  // byte offset in the warp's 32 * ROWB bytes
+          const int px = o / ROWB, ch = (o % ROWB) / 16;
+          const int phys = ch ^ ((px / PPL) & (CPX - 1));
+          const uint4 v = *reinterpret_cast<const uint4*>(wb + px * ROWB + phys * 16);
+          if (xw + px < W) *reinterpret_cast<uint4*>(reinterpret_cast<unsigned char*>(ow) + o) = v;
+        }
+        __syncwarp();
+      } else if (x < W) {
+#pragma unroll
+        for (int j = 0; j < DN_MAX_SLOTS; j++) {
+          float v = __uint_as_float(accv[j]) + s_bias[j];
+          vis[(((long long)p * DN_MAX_SLOTS + j) * H + y) * (long long)W + x] = 1.f / (1.f + __expf(-v));
         }
       }
     }
