@@ -900,24 +900,42 @@ __global__ void k_debug_disk(const uint64_t* seeds, long long n, double radius, 
   }
 }
 // mode 0: mesh_closest (BVH + verification), 1: exact k-d walk, 2: mesh_any
-__global__ void k_debug_mesh(DMesh M, int use_kd, int mode, const double* rays, long long n, double tmin,
-                             double tmax, double* out, int* err) {
-  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
-    const double* rr = rays + 6 * i;
-    V3 o = mk(rr[0], rr[1], rr[2]);
-    V3 d = normalize(mk(rr[3], rr[4], rr[5]));
+// Mesh queries for the parity tests: closest hit as the renderer runs it
+// (mode 0: BVH search + reference-leaf verification), the plain reference
+// k-d walk (mode 1), and any-hit as shadow rays run it (mode 2: packet
+// walk).  128 threads per block; every warp steps through the rays
+// together because the packet walks are warp collectives.
+__global__ void __launch_bounds__(128) k_debug_mesh(DMesh M, int use_kd, int mode, const double* rays, long long n,
+                                                    double tmin, double tmax, double* out, int* err) {
+  __shared__ int s_stack[4][RTB_STACK];
+  volatile int* stack = s_stack[threadIdx.x >> 5];
+  for (long long base = blockIdx.x * (long long)blockDim.x + (threadIdx.x & ~31); base < n;
+       base += (long long)gridDim.x * blockDim.x) {
+    const long long i = base + (threadIdx.x & 31);
+    const bool valid = i < n;
+    V3 o = mk(0.0, 0.0, 0.0), d = mk(0.0, 0.0, 1.0);
+    if (valid) {
+      const double* rr = rays + 6 * i;
+      o = mk(rr[0], rr[1], rr[2]);
+      d = normalize(mk(rr[3], rr[4], rr[5]));
+    }
     RayC r = make_rayc(o, d);
     double closest = tmax;
     int best = -1;
-    double* oo = out + 8 * i;
-    for (int k = 0; k < 8; k++) oo[k] = 0.0;
+    double* oo = out + 8 * (valid ? i : 0);
     if (mode == 2) {
-      oo[0] = mesh_any(M, r, tmin, tmax, use_kd != 0, err, nullptr) ? 1.0 : 0.0;
+      bool any = mesh_any_warp(M, r, tmin, tmax, valid, use_kd != 0, stack, err, nullptr);
+      if (valid) {
+        for (int k = 0; k < 8; k++) oo[k] = 0.0;
+        oo[0] = any ? 1.0 : 0.0;
+      }
       continue;
     }
-    bool hit = mode == 0 ? mesh_closest(M, r, tmin, closest, best, use_kd != 0, err, nullptr)
-                         : (mesh_bounds(M, r, tmin, closest) &&
-                            mesh_kd_walk<false>(M, r, tmin, closest, best, err, nullptr));
+    bool hit = valid && (mode == 0 ? mesh_closest(M, r, tmin, closest, best, use_kd != 0, err, nullptr)
+                                   : (mesh_bounds(M, r, tmin, closest) &&
+                                      mesh_kd_walk<false>(M, r, tmin, closest, best, err, nullptr)));
+    if (!valid) continue;
+    for (int k = 0; k < 8; k++) oo[k] = 0.0;
     if (hit) {
       const double2* E = M.brute + 5 * (size_t)best;
       double2 q1 = E[1], q2 = E[2], q3 = E[3], q4 = E[4];
