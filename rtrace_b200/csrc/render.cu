@@ -626,7 +626,7 @@ std::string prep_mesh(const rt_mesh_desc& md, MeshPrep* P) {
   // triangle BVH, the candidate search structure
   std::vector<BvhNode> bnodes;
   std::vector<int32_t> order;
-  build_bvh(tmin, tmax, 4, 1e-7 * (1.0 + scale), &bnodes, &order);
+  build_bvh(tmin, tmax, 8, 1e-7 * (1.0 + scale), &bnodes, &order);
   std::vector<double2> bvh, btris((size_t)nt * 5);
   put_bvh(bnodes, &bvh);
   for (long long k = 0; k < nt; k++)
@@ -826,7 +826,7 @@ rt_status do_upload(rt_ctx* ctx, const rt_scene_desc* d, rt_scene** out,
       }
       std::vector<BvhNode> bn;
       std::vector<int32_t> order;
-      build_bvh(bmin, bmax, 2, 1e-6 * (1.0 + scale), &bn, &order);
+      build_bvh(bmin, bmax, 8, 1e-6 * (1.0 + scale), &bn, &order);
       std::vector<double2> bvh;
       put_bvh(bn, &bvh);
       DSphGroup G{};
