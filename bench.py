@@ -213,19 +213,31 @@ def small_scene_run(rt, ctx, directory, reps, with_cpu):
     library call; the CLI's diagonal rule would give a square image), depth
     10, seed 0.  Device time per frame on the GPU and, when asked, the
     whole frame on the CPU restatement (oracle, all host threads)."""
-    from rtrace_b200 import workloads
+    from rtrace_b200 import _capi, workloads
     path = workloads.write_scene(directory, "sphere_grid.json", workloads.sphere_grid_scene())
     scene = rt.Scene.from_json_file(path, ctx)
     r = rt.Renderer(400, 300)
-    for _ in range(3):
-        r.render(scene)
-    ms, rays = 0.0, 0
-    for _ in range(reps):
-        r.render(scene)
-        ms += r.last_stats.device_ms
-        rays += r.last_stats.rays
-    out = {"workload": "sphere_grid_400x300_quincunx", "ms_per_frame": ms / reps,
-           "mrays_per_s": rays / (ms * 1e-3) / 1e6, "rays_per_frame": rays // reps}
+    out = {"workload": "sphere_grid_400x300_quincunx"}
+    # launched directly, then as a replayed CUDA graph (RT_FLAG_CUDA_GRAPH):
+    # the frame is ~50 short launches, so submission cost shows
+    for mode, flags in (("direct", 0), ("graph", _capi.RT_FLAG_CUDA_GRAPH)):
+        r.flags = flags
+        for _ in range(3):
+            r.render(scene)
+        ms, rays, call_ms = 0.0, 0, 0.0
+        for _ in range(reps):
+            r.render(scene)
+            ms += r.last_stats.device_ms
+            call_ms += r.last_stats.total_ms
+            rays += r.last_stats.rays
+        res = {"ms_per_frame": ms / reps, "mrays_per_s": rays / (ms * 1e-3) / 1e6, "call_ms": call_ms / reps,
+               "kernel_launches": r.last_stats.kernel_launches}
+        if mode == "direct":
+            out.update(res)
+            out["rays_per_frame"] = rays // reps
+        else:
+            res["replayed"] = r.last_stats.graph == 2
+            out["graph"] = res
     if with_cpu:
         from tests import oracle_lib
         t = time.perf_counter()

@@ -75,7 +75,7 @@ typedef struct rt_outline_config {
 
 /* Renderer fields (src/renderer.rs:37-47).  thread_count has no device
  * meaning and is not carried.  seed: `None` is rendered as 0, exactly as
- * `self.seed.unwrap_or(0)` does.  flags: RT_FLAG_* (profiling only). */
+ * `self.seed.unwrap_or(0)` does.  flags: RT_FLAG_* (profiling, graph replay). */
 typedef struct rt_render_params {
   uint32_t width;
   uint32_t height;
@@ -106,6 +106,12 @@ typedef struct rt_render_params {
  * (node visits, primitive tests).  Both slow the render slightly. */
 #define RT_FLAG_STAGE_TIMES 1u
 #define RT_FLAG_COUNT_WORK 2u
+/* Launch the frame as a CUDA graph.  The first render with a given set of
+ * launch arguments (scene, camera, image size, parameters, output pointer)
+ * captures its kernel sequence; later identical renders replay it in one
+ * submission.  Ignored with RT_FLAG_STAGE_TIMES and by rt_render_linear.
+ * The image is the same either way. */
+#define RT_FLAG_CUDA_GRAPH 4u
 
 /* Stages reported in rt_stats.stage_ms */
 enum { RT_STAGE_RAYGEN = 0, RT_STAGE_TRACE = 1, RT_STAGE_EMIT = 2, RT_STAGE_SHADOW = 3, RT_STAGE_RESOLVE = 4,
@@ -126,7 +132,7 @@ typedef struct rt_stats {
   uint64_t trace_nodes, trace_triangles, trace_spheres, trace_verifications;
   uint64_t shadow_nodes, shadow_triangles, shadow_spheres, shadow_verifications;
   uint32_t kernel_launches; /* kernels this render launched */
-  uint32_t reserved;
+  uint32_t graph;           /* RT_FLAG_CUDA_GRAPH: 1 captured by this call, 2 replayed; 0 launched directly */
   double device_ms; /* CUDA-event time of the device pipeline */
   double total_ms;  /* host wall time of the whole call */
   double stage_ms[RT_STAGE_COUNT]; /* RT_FLAG_STAGE_TIMES */

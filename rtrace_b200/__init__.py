@@ -88,6 +88,7 @@ class RenderStats:
     kernel_launches: int = 0
     stage_ms: dict = field(default_factory=dict)
     work: dict = field(default_factory=dict)
+    graph: int = 0  # RT_FLAG_CUDA_GRAPH: 1 captured by this render, 2 replayed
 
     @property
     def rays(self):
@@ -100,7 +101,7 @@ class RenderStats:
             "shadow_triangles", "shadow_spheres", "shadow_verifications")}
         stages = {name: float(st.stage_ms[i]) for i, name in enumerate(_capi.STAGES)}
         return cls(int(st.primary_rays), int(st.reflection_rays), int(st.shadow_rays), float(st.device_ms),
-                   float(st.total_ms), int(st.hits), int(st.kernel_launches), stages, work)
+                   float(st.total_ms), int(st.hits), int(st.kernel_launches), stages, work, int(st.graph))
 
 
 class Context:
@@ -287,7 +288,7 @@ class Renderer:
         self.anti_aliasing_mode = AntiAliasingMode.Quincunx
         self.seed = 0
         self.outline_config = None
-        self.flags = 0  # rtrace_b200._capi.RT_FLAG_* (profiling)
+        self.flags = 0  # rtrace_b200._capi.RT_FLAG_* (profiling, CUDA graph replay)
         # extensions (the reference always casts 16 rays per disk light)
         self.disk_samples = 16
         self.learned_shadows = False  # needs Context.load_denoiser first

@@ -83,6 +83,7 @@ class rt_render_params(ctypes.Structure):
 RT_OUTLINE_NOALLOC_MAX_PIXELS = 2048 * 2048
 RT_FLAG_STAGE_TIMES = 1
 RT_FLAG_COUNT_WORK = 2
+RT_FLAG_CUDA_GRAPH = 4
 STAGES = ["raygen", "trace", "emit", "shadow", "resolve", "fold", "post", "denoise"]
 
 
@@ -101,7 +102,7 @@ class rt_stats(ctypes.Structure):
         ("shadow_spheres", ctypes.c_uint64),
         ("shadow_verifications", ctypes.c_uint64),
         ("kernel_launches", ctypes.c_uint32),
-        ("reserved", ctypes.c_uint32),
+        ("graph", ctypes.c_uint32),
         ("device_ms", ctypes.c_double),
         ("total_ms", ctypes.c_double),
         ("stage_ms", ctypes.c_double * 8),

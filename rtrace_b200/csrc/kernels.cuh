@@ -133,6 +133,18 @@ __device__ __forceinline__ void camera_ray(const DCam& c, double u, double v, V3
   }
 }
 
+// Start of a frame: queue sizes and hit counts to zero except the level-0
+// queue, which holds the primary rays; work counters and the error word
+// cleared.  One block of 128 threads (levels <= RTB_MAX_LEVELS).  A kernel
+// rather than memsets and a host copy, so that the whole frame is device
+// work a CUDA graph can hold.
+__global__ void k_frame_init(DFrame F, int levels) {
+  for (int i = threadIdx.x; i < levels + 2; i += blockDim.x) F.counts[i] = i == 0 ? (int)F.n_primary : 0;
+  for (int i = threadIdx.x; i < levels + 1; i += blockDim.x) F.nhits[i] = 0;
+  if (threadIdx.x < 16) F.stats[threadIdx.x] = 0;
+  if (threadIdx.x == 0) *F.err = 0;
+}
+
 __global__ void k_raygen(DFrame F) {
   const uint64_t GOLD = 0x9E3779B97F4A7C15ULL;
   long long n = F.n_primary;

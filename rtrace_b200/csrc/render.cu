@@ -55,6 +55,16 @@ struct rt_scene {
   std::vector<DirectCopy> direct;  // arena regions copied from pinned images
 };
 
+// One captured render (RT_FLAG_CUDA_GRAPH): the launch sequence is fully
+// determined by the bytes of its key (every kernel argument, grid size and
+// the denoiser layers), so a render with the same key replays it.
+struct GraphEntry {
+  std::vector<unsigned char> key;
+  cudaGraphExec_t exec = nullptr;
+  uint32_t launches = 0;
+  uint64_t used = 0;  // LRU tick
+};
+
 struct rt_ctx {
   int device = 0;
   int num_sms = 148;
@@ -87,6 +97,8 @@ struct rt_ctx {
   char* pin = nullptr;  // pinned staging of scene uploads
   size_t pin_cap = 0;
   bool borrowed_net = false;  // a lane's net points at its parent's weights
+  std::vector<GraphEntry> graphs;  // captured renders, least recently used evicted
+  uint64_t graph_tick = 0;
 };
 
 namespace {
@@ -129,6 +141,16 @@ void free_all(std::vector<void*>& v) {
   v.clear();
 }
 
+// Captured renders name scratch buffers; they go whenever those are freed.
+// Callers have synchronised the stream, so no replay is in flight.
+void drop_graphs(rt_ctx* ctx) {
+  for (GraphEntry& g : ctx->graphs) cudaGraphExecDestroy(g.exec);
+  ctx->graphs.clear();
+}
+
+// Captured renders one context keeps (a few kB of host and device memory each).
+const size_t kMaxGraphs = 64;
+
 // Shadow-ray entries kept on the device at once (33 B each).
 const long long kShadowCap = 1LL << 26;
 
@@ -142,6 +164,7 @@ rt_status ensure_scratch(rt_ctx* ctx, long long n_rays, int levels, long long n_
   int Lv = std::max(levels, ctx->cap_levels);
   long long P = std::max(n_pix, ctx->cap_pixels);
   long long SH = std::max(n_shadow, ctx->cap_shadow), HS = std::max(n_hits_sh, ctx->cap_hits_sh);
+  drop_graphs(ctx);
   free_all(ctx->scratch);
   ctx->cap_rays = ctx->cap_levels = 0;
   ctx->cap_pixels = ctx->cap_shadow = ctx->cap_hits_sh = 0;
@@ -205,6 +228,7 @@ cudaError_t outline_smem_attr(int bytes) {
 rt_status ensure_dn_scratch(rt_ctx* ctx, long long n) {
   if (n <= ctx->dn_cap) return RT_OK;
   CK(cudaStreamSynchronize(ctx->stream));
+  drop_graphs(ctx);
   free_all(ctx->dn_scratch);
   ctx->dn_cap = 0;
   auto& o = ctx->dn_scratch;
@@ -1138,77 +1162,137 @@ rt_status render_impl(rt_ctx* ctx, const rt_scene* sc, const rt_render_params* P
     long long cap = (long long)nsm * per_sm;
     return (int)std::max<long long>(1, std::min(b, cap));
   };
-  CK(cudaMemsetAsync(ctx->d_counts, 0, (levels + 2) * sizeof(int), s));
-  CK(cudaMemsetAsync(ctx->d_nhits, 0, (levels + 1) * sizeof(int), s));
-  int n0 = (int)nprim;
-  CK(cudaMemcpyAsync(ctx->d_counts, &n0, sizeof(int), cudaMemcpyHostToDevice, s));
-  CK(cudaMemsetAsync(ctx->d_stats, 0, 16 * sizeof(unsigned long long), s));
-  CK(cudaMemsetAsync(ctx->d_err, 0, sizeof(int), s));
-  CK(cudaEventRecord(ctx->ev0, s));
-  Lc.begin();
-  if (max_depth > 0) {
-    k_raygen<<<blocks(nprim, 256, 16), 256, 0, s>>>(F);
+  const size_t o_shm = (size_t)(OT_X + 2 * o_radius) * (OT_Y + 2 * o_radius) * sizeof(double);
+  if (F.outline && o_shm > 48 * 1024) CK(outline_smem_attr((int)o_shm));
+  // The frame's device work, from queue reset to outline: launched directly,
+  // or captured into a CUDA graph.  Every argument it passes comes from F
+  // and the values the graph key lists below.
+  auto enqueue = [&]() -> rt_status {
+    k_frame_init<<<1, 128, 0, s>>>(F, levels);
     Lc.after(RT_STAGE_RAYGEN);
-    for (int l = 0; l < levels; l++) {
-      // per-level shadow layout (k_emit/k_shadow/k_resolve read it from F)
-      const int K = l == 0 ? K_0 : K_full;
-      const long long chunk = l == 0 ? chunk_0 : chunk_n;
-      F.K = K;
-      F.chunk_hits = chunk;
-      F.dsamp = (l == 0 && learned) ? lrays : dsamp;
-      const bool feat = l == 0 && F.feat_on;
-      const long long nchunks = (nprim + chunk - 1) / chunk;
-      if (count) k_trace<true><<<blocks(nprim, 128, 16), 128, 0, s>>>(F, l);
-      else k_trace<false><<<blocks(nprim, 128, 16), 128, 0, s>>>(F, l);
-      Lc.after(RT_STAGE_TRACE);
-      if (feat) {
-        CK(cudaMemsetAsync(F.feat, 0, (size_t)nprim * FEAT_CHANNELS * sizeof(__half), s));
-        if (F.vis_aov) CK(cudaMemsetAsync(F.vis_aov, 0, (size_t)nprim * DN_MAX_SLOTS * sizeof(float), s));
-      }
-      for (long long c = 0; c < nchunks; c++) {
-        long long c0 = c * chunk;
-        k_emit<<<blocks(chunk, 128, 16), 128, 0, s>>>(F, l, c0);
-        Lc.after(RT_STAGE_EMIT);
-        if (K > 0) {
-          if (count) k_shadow<true><<<blocks(chunk * K, 128, 32), 128, 0, s>>>(F, l, c0);
-          else k_shadow<false><<<blocks(chunk * K, 128, 32), 128, 0, s>>>(F, l, c0);
-          Lc.after(RT_STAGE_SHADOW);
-        }
+    if (max_depth > 0) {
+      k_raygen<<<blocks(nprim, 256, 16), 256, 0, s>>>(F);
+      Lc.after(RT_STAGE_RAYGEN);
+      for (int l = 0; l < levels; l++) {
+        // per-level shadow layout (k_emit/k_shadow/k_resolve read it from F)
+        const int K = l == 0 ? K_0 : K_full;
+        const long long chunk = l == 0 ? chunk_0 : chunk_n;
+        F.K = K;
+        F.chunk_hits = chunk;
+        F.dsamp = (l == 0 && learned) ? lrays : dsamp;
+        const bool feat = l == 0 && F.feat_on;
+        const long long nchunks = (nprim + chunk - 1) / chunk;
+        if (count) k_trace<true><<<blocks(nprim, 128, 16), 128, 0, s>>>(F, l);
+        else k_trace<false><<<blocks(nprim, 128, 16), 128, 0, s>>>(F, l);
+        Lc.after(RT_STAGE_TRACE);
         if (feat) {
-          k_features<<<blocks(chunk, 128, 16), 128, 0, s>>>(F, c0);
-          Lc.after(RT_STAGE_DENOISE);
+          CK(cudaMemsetAsync(F.feat, 0, (size_t)nprim * FEAT_CHANNELS * sizeof(__half), s));
+          if (F.vis_aov) CK(cudaMemsetAsync(F.vis_aov, 0, (size_t)nprim * DN_MAX_SLOTS * sizeof(float), s));
         }
-        if (l == 0 && learned) continue;  // resolved after the denoiser (one chunk)
-        k_resolve<<<blocks(chunk, 128, 16), 128, 0, s>>>(F, l, c0);
-        Lc.after(RT_STAGE_RESOLVE);
+        for (long long c = 0; c < nchunks; c++) {
+          long long c0 = c * chunk;
+          k_emit<<<blocks(chunk, 128, 16), 128, 0, s>>>(F, l, c0);
+          Lc.after(RT_STAGE_EMIT);
+          if (K > 0) {
+            if (count) k_shadow<true><<<blocks(chunk * K, 128, 32), 128, 0, s>>>(F, l, c0);
+            else k_shadow<false><<<blocks(chunk * K, 128, 32), 128, 0, s>>>(F, l, c0);
+            Lc.after(RT_STAGE_SHADOW);
+          }
+          if (feat) {
+            k_features<<<blocks(chunk, 128, 16), 128, 0, s>>>(F, c0);
+            Lc.after(RT_STAGE_DENOISE);
+          }
+          if (l == 0 && learned) continue;  // resolved after the denoiser (one chunk)
+          k_resolve<<<blocks(chunk, 128, 16), 128, 0, s>>>(F, l, c0);
+          Lc.after(RT_STAGE_RESOLVE);
+        }
+        if (l == 0 && learned) {
+          cudaError_t le = cudaSuccess;
+          int nl = denoise_run(ctx->net, F.feat, spp, H, W, ctx->d_act0, ctx->d_act1, F.vhat, F.err, s, nsm, &le);
+          for (int k = 0; k < nl; k++) Lc.after(RT_STAGE_DENOISE);
+          if (le != cudaSuccess) return cuda_fail(ctx, le, "denoiser launch");
+          k_resolve<<<blocks(chunk, 128, 16), 128, 0, s>>>(F, l, 0);
+          Lc.after(RT_STAGE_RESOLVE);
+        }
       }
-      if (l == 0 && learned) {
-        cudaError_t le = cudaSuccess;
-        int nl = denoise_run(ctx->net, F.feat, spp, H, W, ctx->d_act0, ctx->d_act1, F.vhat, F.err, s, nsm, &le);
-        for (int k = 0; k < nl; k++) Lc.after(RT_STAGE_DENOISE);
-        if (le != cudaSuccess) return cuda_fail(ctx, le, "denoiser launch");
-        k_resolve<<<blocks(chunk, 128, 16), 128, 0, s>>>(F, l, 0);
-        Lc.after(RT_STAGE_RESOLVE);
+      for (int l = levels - 2; l >= 0; l--) {
+        k_fold<<<blocks(nprim, 256, 16), 256, 0, s>>>(F, l);
+        Lc.after(RT_STAGE_FOLD);
       }
     }
-    for (int l = levels - 2; l >= 0; l--) {
-      k_fold<<<blocks(nprim, 256, 16), 256, 0, s>>>(F, l);
-      Lc.after(RT_STAGE_FOLD);
+    k_pixels<<<blocks(npix, 256, 16), 256, 0, s>>>(F);
+    Lc.after(RT_STAGE_POST);
+    if (F.outline) {
+      dim3 ob(OT_X, OT_Y), og((W + OT_X - 1) / OT_X, (H + OT_Y - 1) / OT_Y);
+      k_outline_mask<<<og, ob, 0, s>>>(F);
+      Lc.after(RT_STAGE_POST);
+      k_outline_apply<<<og, ob, o_shm, s>>>(F);
+      Lc.after(RT_STAGE_POST);
     }
+    CK(cudaGetLastError());
+    return RT_OK;
+  };
+  // CUDA graph: not with stage times (events between launches) nor with a
+  // linear output (a per-call buffer, so no key would ever repeat).
+  uint32_t graph_state = 0;
+  if ((P->flags & RT_FLAG_CUDA_GRAPH) && !Lc.timed && !linear_out) {
+    std::vector<unsigned char> key;
+    auto put = [&key](const void* p, size_t n) {
+      key.insert(key.end(), static_cast<const unsigned char*>(p), static_cast<const unsigned char*>(p) + n);
+    };
+    put(&F, sizeof F);
+    const long long kl[] = {nprim, npix, chunk_0, chunk_n, levels, max_depth, K_0, K_full, lrays, dsamp,
+                            learned, count, nsm, spp, H, W, (long long)o_shm};
+    put(kl, sizeof kl);
+    if (learned) {
+      const void* ap[] = {ctx->d_act0, ctx->d_act1};
+      put(ap, sizeof ap);
+      for (const DnLayer& dl : ctx->net.layers) {
+        const void* lp[] = {dl.w, dl.b};
+        const int li[] = {dl.cin, dl.cout, dl.dil, dl.act};
+        put(lp, sizeof lp);
+        put(li, sizeof li);
+      }
+    }
+    GraphEntry* hit = nullptr;
+    for (GraphEntry& g : ctx->graphs)
+      if (g.key == key) hit = &g;
+    if (!hit) {
+      cudaGraph_t g = nullptr;
+      CK(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
+      rt_status es = enqueue();
+      cudaError_t ce = cudaStreamEndCapture(s, &g);  // always ends the capture
+      if (es != RT_OK) {
+        if (g) cudaGraphDestroy(g);
+        return es;
+      }
+      if (ce != cudaSuccess) return cuda_fail(ctx, ce, "cudaStreamEndCapture");
+      cudaGraphExec_t ex = nullptr;
+      ce = cudaGraphInstantiate(&ex, g, 0);
+      cudaGraphDestroy(g);
+      if (ce != cudaSuccess) return cuda_fail(ctx, ce, "cudaGraphInstantiate");
+      if (ctx->graphs.size() >= kMaxGraphs) {
+        auto lru = std::min_element(ctx->graphs.begin(), ctx->graphs.end(),
+                                    [](const GraphEntry& a, const GraphEntry& b) { return a.used < b.used; });
+        cudaGraphExecDestroy(lru->exec);
+        ctx->graphs.erase(lru);
+      }
+      ctx->graphs.push_back(GraphEntry{std::move(key), ex, Lc.launches, 0});
+      hit = &ctx->graphs.back();
+      graph_state = 1;
+    } else {
+      Lc.launches = hit->launches;
+      graph_state = 2;
+    }
+    hit->used = ++ctx->graph_tick;
+    CK(cudaEventRecord(ctx->ev0, s));
+    CK(cudaGraphLaunch(hit->exec, s));
+  } else {
+    CK(cudaEventRecord(ctx->ev0, s));
+    Lc.begin();
+    rt_status es = enqueue();
+    if (es != RT_OK) return es;
   }
-  k_pixels<<<blocks(npix, 256, 16), 256, 0, s>>>(F);
-  Lc.after(RT_STAGE_POST);
-  if (F.outline) {
-    dim3 ob(OT_X, OT_Y), og((W + OT_X - 1) / OT_X, (H + OT_Y - 1) / OT_Y);
-    k_outline_mask<<<og, ob, 0, s>>>(F);
-    Lc.after(RT_STAGE_POST);
-    size_t shm = (size_t)(OT_X + 2 * F.o_radius) * (OT_Y + 2 * F.o_radius) * sizeof(double);
-    if (shm > 48 * 1024)
-      CK(outline_smem_attr((int)shm));
-    k_outline_apply<<<og, ob, shm, s>>>(F);
-    Lc.after(RT_STAGE_POST);
-  }
-  CK(cudaGetLastError());
   CK(cudaEventRecord(ctx->ev1, s));
   if (rgb_out && !direct)
     CK(cudaMemcpyAsync(rgb_out, d_rgb + 3 * keep_off, 3 * keep_pix,
@@ -1254,6 +1338,7 @@ rt_status render_impl(rt_ctx* ctx, const rt_scene* sc, const rt_render_params* P
       stats->shadow_verifications = hstats[9];
     }
     stats->kernel_launches = Lc.launches;
+    stats->graph = graph_state;
     stats->device_ms = ms;
     Lc.collect(stats->stage_ms);
     stats->total_ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
@@ -1301,6 +1386,7 @@ void rt_ctx_destroy(rt_ctx* ctx) {
   ctx->lanes.clear();
   if (ctx->pin) cudaFreeHost(ctx->pin);
   ctx->pin = nullptr;
+  drop_graphs(ctx);
   free_all(ctx->scratch);
   free_all(ctx->dn_scratch);
   if (!ctx->borrowed_net) denoise_free(&ctx->net);
@@ -1713,6 +1799,11 @@ rt_status rt_denoiser_load(rt_ctx* ctx, const void* blob, size_t bytes) {
   if (!ctx) return fail(nullptr, RT_ERR_INVALID_ARGUMENT, "null context");
   CK(cudaSetDevice(ctx->device));
   CK(cudaStreamSynchronize(ctx->stream));
+  drop_graphs(ctx);
+  for (rt_ctx* l : ctx->lanes) {
+    CK(cudaStreamSynchronize(l->stream));
+    drop_graphs(l);
+  }
   std::string e = denoise_load(blob, bytes, &ctx->net);
   if (!e.empty()) return fail(ctx, RT_ERR_INVALID_ARGUMENT, e);
   ctx->err.clear();

@@ -38,6 +38,7 @@ def _run_net(ctx, layers, feat):
     ctx.load_denoiser(denoiser.pack(layers))
     planes, H, W, _ = feat.shape
     vis = torch.full((planes, 2, H, W), -7.0, dtype=torch.float32, device=feat.device)
+    torch.cuda.synchronize()  # torch's fills run on torch's stream, the network on the context's
     L = rt._capi.lib()
     st = L.rt_denoiser_run(ctx.handle, feat.data_ptr(), planes, H, W, vis.data_ptr())
     assert st == 0, L.rt_last_error(ctx.handle)
@@ -128,6 +129,7 @@ def test_shadow_aov_is_visible_fraction(gpu_ctx):
     r.disk_samples = 16
     vis = torch.full((1, 2, 64, 96), -1.0, device=dev)
     feat = torch.zeros((1, 64, 96, 16), dtype=torch.float16, device=dev)
+    torch.cuda.synchronize()
     img = r.render_shadow_aov(scene, vis.data_ptr(), feat.data_ptr())
     assert np.array_equal(img, r.render(scene))  # the AOVs do not change the image
     valid = feat[..., 0] == 1
@@ -154,6 +156,7 @@ def test_learned_render_shades_with_the_network_output(gpu_ctx):
     r.learned_shadows = True
     vis = torch.zeros((2, 2, 72, 128), device=dev)
     feat = torch.zeros((2, 72, 128, 16), dtype=torch.float16, device=dev)
+    torch.cuda.synchronize()
     img = r.render_shadow_aov(scene, vis.data_ptr(), feat.data_ptr())
     st = r.last_stats
     # level 0 casts one ray per disk light
