@@ -148,8 +148,10 @@ void drop_graphs(rt_ctx* ctx) {
   ctx->graphs.clear();
 }
 
-// Captured renders one context keeps (a few kB of host and device memory each).
-const size_t kMaxGraphs = 64;
+// Captured renders one context keeps (tens of kB of host and device memory
+// each): enough for every job a batch lane renders, so that a repeated batch
+// replays instead of cycling through a too-small LRU.
+const size_t kMaxGraphs = 256;
 
 // Shadow-ray entries kept on the device at once (33 B each).
 const long long kShadowCap = 1LL << 26;
