@@ -297,6 +297,12 @@ rt_status rt_host_scene_load_json_file(const char* path, rt_host_scene** out);
 rt_status rt_auto_cameras_json_file(const char* path, rt_camera_config* out);
 rt_status rt_auto_cameras_json_str(const char* json, rt_camera_config* out);
 rt_status rt_host_scene_load_json_str(const char* json, rt_host_scene** out);
+/* The same loads with the k-d trees of meshes of 16,384 triangles or more
+ * built on ctx's device (rt_kd_build); the host scene is identical.
+ * rt_scene_load_json_file / _str build the same way.  Errors are reported
+ * through rt_last_error(ctx). */
+rt_status rt_host_scene_load_json_file_on(rt_ctx* ctx, const char* path, rt_host_scene** out);
+rt_status rt_host_scene_load_json_str_on(rt_ctx* ctx, const char* json, rt_host_scene** out);
 const rt_scene_desc* rt_host_scene_desc(const rt_host_scene* hs);
 void rt_host_scene_free(rt_host_scene* hs);
 
@@ -305,6 +311,19 @@ void rt_host_scene_free(rt_host_scene* hs);
  * k-d root paths and occurrence lists) and keeps it in the host scene;
  * later uploads of the same host scene, to any context, only copy it. */
 rt_status rt_host_scene_upload(rt_ctx* ctx, rt_host_scene* hs, rt_scene** out);
+/* KdTree::new(triangles, 16, 10) (src/mesh.rs:75-197, the tree
+ * Mesh::from_stl_file and the World build make) over n_triangles of 9
+ * doubles each (v0, v1, v2), as rt_mesh_desc wants it: nodes in preorder
+ * and the leaf lists.  With a context it is built on that device, one tree
+ * depth at a time; with ctx NULL on the host.  Both give the same bytes.
+ * A NaN centre in a node the reference sorts fails with RT_ERR_SCENE and
+ * the reference's panic message (its sort unwraps partial_cmp). */
+typedef struct rt_kd_tree rt_kd_tree;
+rt_status rt_kd_build(rt_ctx* ctx, const double* vertices, int64_t n_triangles, rt_kd_tree** out);
+const rt_kd_node_desc* rt_kd_tree_nodes(const rt_kd_tree* tree, int64_t* n_nodes);
+const int32_t* rt_kd_tree_index(const rt_kd_tree* tree, int64_t* n_index);
+void rt_kd_tree_free(rt_kd_tree* tree);
+
 /* Bytes rt_scene_upload copied to the device for this scene. */
 rt_status rt_scene_device_bytes(rt_ctx* ctx, const rt_scene* scene, uint64_t* out);
 

@@ -2367,6 +2367,62 @@ int oracle_hex_to_color(const char* hex, double* out) {
   return 0;
 }
 
+// KdTree::new(triangles, 16, 10) (build_recursive, src/mesh.rs:125-197)
+// over n triangles of 9 doubles (v0, v1, v2), flattened in preorder (left
+// child next) into 72-byte records {int32 axis (-1 leaf), right, first,
+// count; double split, bounds_min[3], bounds_max[3]} and the leaf lists in
+// leaf order: the layout the CUDA library's rt_kd_build returns.  Call with
+// null outputs to get the sizes, then again with buffers of those sizes.
+// Returns 0, or 1 with the panic message in err.
+int oracle_kd_build(const double* v, int64_t n, void* nodes_out, int32_t* idx_out, int64_t* n_nodes,
+                    int64_t* n_idx, char* err, int err_len) {
+  struct Rec {
+    int32_t axis, right, first, count;
+    double split, bmin[3], bmax[3];
+  };
+  static_assert(sizeof(Rec) == 72, "record layout");
+  std::vector<orc::Triangle> t((size_t)n);
+  for (int64_t i = 0; i < n; i++)
+    for (int k = 0; k < 3; k++) t[i].v[k] = orc::v3(v[9 * i + 3 * k], v[9 * i + 3 * k + 1], v[9 * i + 3 * k + 2]);
+  orc::KdTree kd;
+  try {
+    kd.construct(t);
+  } catch (const std::exception& e) {
+    snprintf(err, err_len, "%s", e.what());
+    return 1;
+  }
+  std::vector<Rec> recs;
+  std::vector<int32_t> idx;
+  std::function<void(const orc::KdNode*)> walk = [&](const orc::KdNode* nd) {
+    Rec r{};
+    for (int a = 0; a < 3; a++) {
+      r.bmin[a] = nd->bmin[a];
+      r.bmax[a] = nd->bmax[a];
+    }
+    size_t me = recs.size();
+    if (nd->leaf) {
+      r.axis = -1;
+      r.first = (int32_t)idx.size();
+      r.count = (int32_t)nd->tris.size();
+      for (size_t i : nd->tris) idx.push_back((int32_t)i);
+      recs.push_back(r);
+      return;
+    }
+    r.axis = nd->axis;
+    r.split = nd->split;
+    recs.push_back(r);
+    walk(nd->left.get());
+    recs[me].right = (int32_t)recs.size();
+    walk(nd->right.get());
+  };
+  if (kd.root) walk(kd.root.get());
+  *n_nodes = (int64_t)recs.size();
+  *n_idx = (int64_t)idx.size();
+  if (nodes_out) memcpy(nodes_out, recs.data(), recs.size() * sizeof(Rec));
+  if (idx_out) memcpy(idx_out, idx.data(), idx.size() * sizeof(int32_t));
+  return 0;
+}
+
 // serde_json's default f64 parsing of one JSON number literal.
 int oracle_json_f64(const char* text, double* out) {
   try {

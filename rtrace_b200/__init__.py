@@ -238,20 +238,41 @@ class HostScene:
         self.handle = handle
 
     @classmethod
-    def from_json_file(cls, path):
+    def from_json_file(cls, path, ctx=None):
+        """ctx: build the k-d trees of large meshes on that context's device
+        (the same trees as the host build)."""
         h = ctypes.c_void_p()
-        st = _capi.lib().rt_host_scene_load_json_file(str(path).encode(), ctypes.byref(h))
+        L = _capi.lib()
+        if ctx is None:
+            st = L.rt_host_scene_load_json_file(str(path).encode(), ctypes.byref(h))
+        else:
+            st = L.rt_host_scene_load_json_file_on(ctx.handle, str(path).encode(), ctypes.byref(h))
         if st != _capi.RT_OK:
-            _raise(st, None)
+            _raise(st, None if ctx is None else ctx.handle)
         return cls(h)
 
     @classmethod
-    def from_json_str(cls, text):
+    def from_json_str(cls, text, ctx=None):
         h = ctypes.c_void_p()
-        st = _capi.lib().rt_host_scene_load_json_str(text.encode(), ctypes.byref(h))
+        L = _capi.lib()
+        if ctx is None:
+            st = L.rt_host_scene_load_json_str(text.encode(), ctypes.byref(h))
+        else:
+            st = L.rt_host_scene_load_json_str_on(ctx.handle, text.encode(), ctypes.byref(h))
         if st != _capi.RT_OK:
-            _raise(st, None)
+            _raise(st, None if ctx is None else ctx.handle)
         return cls(h)
+
+    def meshes(self):
+        """Copies of each mesh's (vertices (n, 9) float64, k-d nodes, leaf
+        index list) as the flattened description holds them."""
+        d = _capi.lib().rt_host_scene_desc(self.handle).contents
+        out = []
+        for i in range(d.n_meshes):
+            m = d.meshes[i]
+            out.append((_array(m.vertices, np.float64, 9 * m.n_triangles).reshape(-1, 9),
+                        _array(m.nodes, KD_NODE_DTYPE, m.n_nodes), _array(m.tri_index, np.int32, m.n_tri_index)))
+        return out
 
     def close(self):
         if self.handle:
@@ -263,6 +284,37 @@ class HostScene:
             self.close()
         except Exception:
             pass
+
+
+KD_NODE_DTYPE = np.dtype(_capi.KD_NODE_FIELDS)
+
+
+def _array(ptr, dtype, n):
+    dtype = np.dtype(dtype)
+    if not n:
+        return np.zeros(0, dtype)
+    return np.frombuffer((ctypes.c_char * (int(n) * dtype.itemsize)).from_address(ptr), dtype).copy()
+
+
+def kd_build(vertices, ctx=None):
+    """rt_kd_build: KdTree::new(triangles, 16, 10) (src/mesh.rs:75-197) of
+    an (n, 9) float64 triangle array, on ctx's device or (ctx None) on the
+    host.  Returns (nodes, leaf index list): the nodes in preorder as a
+    KD_NODE_DTYPE array, the index list as int32."""
+    v = np.ascontiguousarray(vertices, dtype=np.float64).reshape(-1, 9)
+    L = _capi.lib()
+    t = ctypes.c_void_p()
+    h = None if ctx is None else ctx.handle
+    st = L.rt_kd_build(h, v.ctypes.data if len(v) else None, len(v), ctypes.byref(t))
+    if st != _capi.RT_OK:
+        _raise(st, h)
+    try:
+        nn, ni = ctypes.c_int64(), ctypes.c_int64()
+        pn = L.rt_kd_tree_nodes(t, ctypes.byref(nn))
+        pi = L.rt_kd_tree_index(t, ctypes.byref(ni))
+        return _array(pn, KD_NODE_DTYPE, nn.value), _array(pi, np.int32, ni.value)
+    finally:
+        L.rt_kd_tree_free(t)
 
 
 def fp64_rate(ctx=None):

@@ -136,6 +136,39 @@ _vp = ctypes.c_void_p
 _lib = None
 
 
+class rt_mesh_desc(ctypes.Structure):
+    _fields_ = [
+        ("vertices", ctypes.c_void_p),
+        ("n_triangles", ctypes.c_int64),
+        ("bounds_min", ctypes.c_double * 3),
+        ("bounds_max", ctypes.c_double * 3),
+        ("nodes", ctypes.c_void_p),
+        ("n_nodes", ctypes.c_int64),
+        ("tri_index", ctypes.c_void_p),
+        ("n_tri_index", ctypes.c_int64),
+    ]
+
+
+class rt_scene_desc(ctypes.Structure):
+    """The leading fields of rt_scene_desc, up to the meshes."""
+    _fields_ = [
+        ("camera", rt_camera_config),
+        ("objects", ctypes.c_void_p),
+        ("n_objects", ctypes.c_int32),
+        ("n_materials", ctypes.c_int32),
+        ("materials", ctypes.c_void_p),
+        ("lights", ctypes.c_void_p),
+        ("n_lights", ctypes.c_int32),
+        ("n_meshes", ctypes.c_int32),
+        ("meshes", ctypes.POINTER(rt_mesh_desc)),
+    ]
+
+
+# rt_kd_node_desc (72 bytes, no padding)
+KD_NODE_FIELDS = [("axis", "<i4"), ("right", "<i4"), ("first", "<i4"), ("count", "<i4"), ("split", "<f8"),
+                  ("bounds_min", "<f8", (3,)), ("bounds_max", "<f8", (3,))]
+
+
 def lib():
     """Loads the CUDA library (once); raises if it has not been built."""
     global _lib
@@ -176,7 +209,13 @@ def lib():
                                             ctypes.POINTER(rt_stats)]),
         "rt_host_scene_load_json_file": (ctypes.c_int, [ctypes.c_char_p, ctypes.POINTER(_vp)]),
         "rt_host_scene_load_json_str": (ctypes.c_int, [ctypes.c_char_p, ctypes.POINTER(_vp)]),
-        "rt_host_scene_desc": (_vp, [_vp]),
+        "rt_host_scene_load_json_file_on": (ctypes.c_int, [_vp, ctypes.c_char_p, ctypes.POINTER(_vp)]),
+        "rt_host_scene_load_json_str_on": (ctypes.c_int, [_vp, ctypes.c_char_p, ctypes.POINTER(_vp)]),
+        "rt_kd_build": (ctypes.c_int, [_vp, _vp, ctypes.c_int64, ctypes.POINTER(_vp)]),
+        "rt_kd_tree_nodes": (_vp, [_vp, ctypes.POINTER(ctypes.c_int64)]),
+        "rt_kd_tree_index": (_vp, [_vp, ctypes.POINTER(ctypes.c_int64)]),
+        "rt_kd_tree_free": (None, [_vp]),
+        "rt_host_scene_desc": (ctypes.POINTER(rt_scene_desc), [_vp]),
         "rt_host_scene_free": (None, [_vp]),
         "rt_scene_device_bytes": (ctypes.c_int, [_vp, _vp, ctypes.POINTER(ctypes.c_uint64)]),
         "rt_debug_fp64_rate": (ctypes.c_int, [_vp, ctypes.POINTER(ctypes.c_double)]),

@@ -21,6 +21,7 @@
 
 #include "../../include/rtrace_gpu.h"
 #include "bvh_build.hpp"
+#include "kd_build.hpp"
 #include "kernels.cuh"
 #include "scene_loader.hpp"
 
@@ -99,6 +100,7 @@ struct rt_ctx {
   bool borrowed_net = false;  // a lane's net points at its parent's weights
   std::vector<GraphEntry> graphs;  // captured renders, least recently used evicted
   uint64_t graph_tick = 0;
+  KdArena* kd_arena = nullptr;  // device memory of k-d builds, kept between them
 };
 
 namespace {
@@ -1351,6 +1353,21 @@ rt_status render_impl(rt_ctx* ctx, const rt_scene* sc, const rt_render_params* P
 
 }  // namespace
 
+// Meshes from this many triangles up build their k-d tree on the device when
+// a load has a context; smaller ones build faster on the host.
+const size_t kKdDeviceMin = 16384;
+
+KdBuildHook device_kd_hook(rt_ctx* ctx) {
+  KdBuildHook h;
+  h.min_triangles = kKdDeviceMin;
+  h.build = [ctx](const double* v, size_t n, std::vector<rt_kd_node_desc>* nodes, std::vector<int32_t>* idx) {
+    if (!ctx->kd_arena) ctx->kd_arena = kd_arena_new();
+    cudaError_t ce = cudaSuccess;
+    return kd_build_device(v, (int64_t)n, ctx->stream, ctx->kd_arena, nodes, idx, &ce);
+  };
+  return h;
+}
+
 // ==========================================================================
 // C ABI
 // ==========================================================================
@@ -1391,6 +1408,7 @@ void rt_ctx_destroy(rt_ctx* ctx) {
   drop_graphs(ctx);
   free_all(ctx->scratch);
   free_all(ctx->dn_scratch);
+  if (ctx->kd_arena) kd_arena_free(ctx->kd_arena);
   if (!ctx->borrowed_net) denoise_free(&ctx->net);
   for (cudaEvent_t e : ctx->stage_ev) cudaEventDestroy(e);
   if (ctx->ev0) cudaEventDestroy(ctx->ev0);
@@ -1417,21 +1435,63 @@ rt_status rt_scene_upload(rt_ctx* ctx, const rt_scene_desc* desc, rt_scene** out
 rt_status rt_scene_load_json_str(rt_ctx* ctx, const char* json, rt_scene** out) {
   if (!ctx || !json || !out) return fail(ctx, RT_ERR_INVALID_ARGUMENT, "null argument");
   *out = nullptr;
+  CK(cudaSetDevice(ctx->device));
   HostScene hs;
   std::string err;
-  if (!load_scene_json(json, ".", &hs, &err)) return fail(ctx, RT_ERR_SCENE, err);
+  KdBuildHook kd = device_kd_hook(ctx);
+  if (!load_scene_json(json, ".", &hs, &err, &kd)) return fail(ctx, RT_ERR_SCENE, err);
   return rt_scene_upload(ctx, &hs.desc, out);
 }
 
 rt_status rt_scene_load_json_file(rt_ctx* ctx, const char* path, rt_scene** out) {
   if (!ctx || !path || !out) return fail(ctx, RT_ERR_INVALID_ARGUMENT, "null argument");
   *out = nullptr;
+  CK(cudaSetDevice(ctx->device));
   std::string text, err;
   if (!read_text_file(path, &text, &err)) return fail(ctx, RT_ERR_IO, err);
   HostScene hs;
-  if (!load_scene_json(text, parent_dir(path), &hs, &err)) return fail(ctx, RT_ERR_SCENE, err);
+  KdBuildHook kd = device_kd_hook(ctx);
+  if (!load_scene_json(text, parent_dir(path), &hs, &err, &kd)) return fail(ctx, RT_ERR_SCENE, err);
   return rt_scene_upload(ctx, &hs.desc, out);
 }
+
+struct rt_kd_tree {
+  std::vector<rt_kd_node_desc> nodes;
+  std::vector<int32_t> idx;
+};
+
+rt_status rt_kd_build(rt_ctx* ctx, const double* vertices, int64_t n_triangles, rt_kd_tree** out) {
+  if (!out || (n_triangles > 0 && !vertices) || n_triangles < 0)
+    return fail(ctx, RT_ERR_INVALID_ARGUMENT, "null or invalid argument");
+  *out = nullptr;
+  auto t = std::make_unique<rt_kd_tree>();
+  std::string e;
+  if (ctx) {
+    CK(cudaSetDevice(ctx->device));
+    cudaError_t ce = cudaSuccess;
+    if (!ctx->kd_arena) ctx->kd_arena = kd_arena_new();
+    e = kd_build_device(vertices, n_triangles, ctx->stream, ctx->kd_arena, &t->nodes, &t->idx, &ce);
+    if (ce != cudaSuccess) return cuda_fail(ctx, ce, e.c_str());
+  } else {
+    e = kd_build_host(vertices, (size_t)n_triangles, &t->nodes, &t->idx);
+  }
+  if (!e.empty()) return fail(ctx, RT_ERR_SCENE, e);
+  if (ctx) ctx->err.clear();
+  *out = t.release();
+  return RT_OK;
+}
+
+const rt_kd_node_desc* rt_kd_tree_nodes(const rt_kd_tree* t, int64_t* n_nodes) {
+  if (n_nodes) *n_nodes = t ? (int64_t)t->nodes.size() : 0;
+  return t && !t->nodes.empty() ? t->nodes.data() : nullptr;
+}
+
+const int32_t* rt_kd_tree_index(const rt_kd_tree* t, int64_t* n_index) {
+  if (n_index) *n_index = t ? (int64_t)t->idx.size() : 0;
+  return t && !t->idx.empty() ? t->idx.data() : nullptr;
+}
+
+void rt_kd_tree_free(rt_kd_tree* t) { delete t; }
 
 rt_status rt_scene_outline_config(rt_ctx* ctx, const rt_scene* scene, rt_outline_config* out) {
   if (!scene || !out) return fail(ctx, RT_ERR_INVALID_ARGUMENT, "null argument");
@@ -1462,13 +1522,21 @@ struct rt_host_scene {
 };
 
 rt_status rt_host_scene_load_json_file(const char* path, rt_host_scene** out) {
-  rt_ctx* ctx = nullptr;
+  return rt_host_scene_load_json_file_on(nullptr, path, out);
+}
+
+rt_status rt_host_scene_load_json_file_on(rt_ctx* ctx, const char* path, rt_host_scene** out) {
   if (!path || !out) return fail(ctx, RT_ERR_INVALID_ARGUMENT, "null argument");
   *out = nullptr;
+  if (ctx) CK(cudaSetDevice(ctx->device));
   std::string text, err;
   if (!read_text_file(path, &text, &err)) return fail(ctx, RT_ERR_IO, err);
   auto h = std::make_unique<rt_host_scene>();
-  if (!load_scene_json(text, parent_dir(path), &h->hs, &err)) return fail(ctx, RT_ERR_SCENE, err);
+  KdBuildHook kd;
+  if (ctx) kd = device_kd_hook(ctx);
+  if (!load_scene_json(text, parent_dir(path), &h->hs, &err, ctx ? &kd : nullptr))
+    return fail(ctx, RT_ERR_SCENE, err);
+  if (ctx) ctx->err.clear();
   *out = h.release();
   return RT_OK;
 }
@@ -1499,12 +1567,19 @@ rt_status rt_auto_cameras_json_str(const char* json, rt_camera_config* out) {
 }
 
 rt_status rt_host_scene_load_json_str(const char* json, rt_host_scene** out) {
-  rt_ctx* ctx = nullptr;
+  return rt_host_scene_load_json_str_on(nullptr, json, out);
+}
+
+rt_status rt_host_scene_load_json_str_on(rt_ctx* ctx, const char* json, rt_host_scene** out) {
   if (!json || !out) return fail(ctx, RT_ERR_INVALID_ARGUMENT, "null argument");
   *out = nullptr;
+  if (ctx) CK(cudaSetDevice(ctx->device));
   std::string err;
   auto h = std::make_unique<rt_host_scene>();
-  if (!load_scene_json(json, ".", &h->hs, &err)) return fail(ctx, RT_ERR_SCENE, err);
+  KdBuildHook kd;
+  if (ctx) kd = device_kd_hook(ctx);
+  if (!load_scene_json(json, ".", &h->hs, &err, ctx ? &kd : nullptr)) return fail(ctx, RT_ERR_SCENE, err);
+  if (ctx) ctx->err.clear();
   *out = h.release();
   return RT_OK;
 }

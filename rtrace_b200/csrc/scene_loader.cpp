@@ -33,8 +33,13 @@ struct LoadError : std::runtime_error {
   using std::runtime_error::runtime_error;
 };
 
-inline double rmax(double a, double b) { return std::fmax(a, b); }
-inline double rmin(double a, double b) { return std::fmin(a, b); }
+// f64::max / f64::min: a NaN argument is ignored.  When the arguments
+// compare equal (+0 and -0) the reference's llvm.maxnum/minnum may return
+// either, and a compiled std::fmax/fmin differs from call site to call
+// site; these keep the first, as glibc's fmin/fmax do, everywhere (the
+// device k-d build uses the same rule, so both builds give the same bytes).
+inline double rmax(double a, double b) { return (b > a || a != a) ? b : a; }
+inline double rmin(double a, double b) { return (b < a || a != a) ? b : a; }
 inline double to_radians(double d) {
   const double k = M_PI / 180.0;
   return d * k;
@@ -723,7 +728,7 @@ struct KdBuilder {
   }
 };
 
-void make_mesh(const std::vector<Tri>& tris, HostMesh* m) {
+void make_mesh(const std::vector<Tri>& tris, HostMesh* m, const KdBuildHook* kd) {
   m->vertices.resize(tris.size() * 9);
   for (size_t i = 0; i < tris.size(); i++)
     for (int k = 0; k < 3; k++) {
@@ -744,6 +749,11 @@ void make_mesh(const std::vector<Tri>& tris, HostMesh* m) {
         mx[k] = rmax(mx[k], t.v[v][k]);
       }
   for (int k = 0; k < 3; k++) { m->bmin[k] = mn[k]; m->bmax[k] = mx[k]; }
+  if (kd && kd->build && tris.size() >= kd->min_triangles) {
+    std::string e = kd->build(m->vertices.data(), tris.size(), &m->nodes, &m->tri_index);
+    if (!e.empty()) throw LoadError(e);
+    return;
+  }
   KdBuilder kb(tris);
   std::vector<int32_t> all(tris.size());
   for (size_t i = 0; i < tris.size(); i++) all[i] = (int32_t)i;
@@ -832,6 +842,30 @@ std::vector<ObjIn> parse_objects(const J& j) {
 }  // namespace
 
 // --------------------------------------------------------- public API -----
+std::string kd_build_host(const double* vertices, size_t n, std::vector<rt_kd_node_desc>* nodes,
+                          std::vector<int32_t>* idx) {
+  nodes->clear();
+  idx->clear();
+  if (n == 0) return "";  // make_mesh builds no tree for an empty mesh
+  std::vector<Tri> tris(n);
+  for (size_t i = 0; i < n; i++)
+    for (int k = 0; k < 3; k++) tris[i].v[k] = {vertices[9 * i + 3 * k], vertices[9 * i + 3 * k + 1], vertices[9 * i + 3 * k + 2]};
+  try {
+    KdBuilder kb(tris);
+    std::vector<int32_t> all(n);
+    for (size_t i = 0; i < n; i++) all[i] = (int32_t)i;
+    double bmin[3], bmax[3];
+    kb.bounds(all, bmin, bmax);
+    KdOut out;
+    kb.build(std::move(all), bmin, bmax, 0, out);
+    *nodes = std::move(out.nodes);
+    *idx = std::move(out.idx);
+  } catch (const std::exception& e) {
+    return e.what();
+  }
+  return "";
+}
+
 bool hex_to_color(const std::string& in, double out[3], std::string* err) {
   size_t k = 0;
   while (k < in.size() && in[k] == '#') k++;
@@ -912,7 +946,8 @@ void HostScene::finalize() {
   desc.render_error = render_error.empty() ? nullptr : render_error.c_str();
 }
 
-bool load_scene_json(const std::string& text, const std::string& base_dir, HostScene* hs, std::string* err) {
+bool load_scene_json(const std::string& text, const std::string& base_dir, HostScene* hs, std::string* err,
+                     const KdBuildHook* kd) {
   try {
     J j = parse_json(text);
     if (j.k != J::OBJ) throw LoadError("invalid type: expected struct Scene");
@@ -1050,7 +1085,7 @@ bool load_scene_json(const std::string& text, const std::string& base_dir, HostS
           for (auto& tr : tris)
             for (int k = 0; k < 3; k++) tr.v[k] = xform_point(tm, tr.v[k]);
         auto hm = std::make_unique<HostMesh>();
-        make_mesh(tris, hm.get());
+        make_mesh(tris, hm.get(), kd);
         od.mesh = (int32_t)hs->meshes.size();
         hs->meshes.push_back(std::move(hm));
       }

@@ -3,6 +3,7 @@
 // producing the flattened rt_scene_desc the device path consumes.
 #pragma once
 
+#include <functional>
 #include <memory>
 #include <string>
 #include <vector>
@@ -30,9 +31,26 @@ struct HostScene {
   void finalize();  // point desc at the owned arrays
 };
 
+// A k-d builder that runs elsewhere (on a device): KdTree::new(tris, 16, 10)
+// over n triangles of 9 doubles each, with the host builder's preorder
+// layout.  build returns "" on success, else the error that fails the load.
+struct KdBuildHook {
+  size_t min_triangles = 0;  // smaller meshes build on the host
+  std::function<std::string(const double* vertices, size_t n, std::vector<rt_kd_node_desc>* nodes,
+                            std::vector<int32_t>* idx)>
+      build;
+};
+
 // Scene::from_json_str semantics with meshes resolved against base_dir
 // ("" = current directory).  Returns false with *err set on failure.
-bool load_scene_json(const std::string& text, const std::string& base_dir, HostScene* out, std::string* err);
+bool load_scene_json(const std::string& text, const std::string& base_dir, HostScene* out, std::string* err,
+                     const KdBuildHook* kd = nullptr);
+
+// The host k-d builder (KdTree::new(tris, 16, 10), src/mesh.rs:75-197) over
+// n triangles of 9 doubles each.  Returns "" or the reference's panic
+// message for a NaN centre in a node it sorts.
+std::string kd_build_host(const double* vertices, size_t n, std::vector<rt_kd_node_desc>* nodes,
+                          std::vector<int32_t>* idx);
 bool read_text_file(const std::string& path, std::string* out, std::string* err);
 std::string parent_dir(const std::string& path);
 

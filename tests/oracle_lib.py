@@ -65,8 +65,27 @@ def load():
     L.oracle_chacha_block.argtypes = [vp, ctypes.c_uint64, vp, ctypes.c_int, vp]
     L.oracle_outline.argtypes = [ctypes.c_uint32, ctypes.c_uint32] + [vp] * 8 + [ctypes.c_double] * 3 + \
         [vp, ctypes.c_int, ctypes.c_double, vp]
+    L.oracle_kd_build.argtypes = [vp, ctypes.c_int64, vp, vp, vp, vp, ctypes.c_char_p, ctypes.c_int]
+    L.oracle_kd_build.restype = ctypes.c_int
     _lib = L
     return L
+
+
+def kd_build(vertices):
+    """The oracle's KdTree::new(triangles, 16, 10) of an (n, 9) float64
+    array: (nodes as raw 72-byte preorder records, leaf index list)."""
+    import numpy as np
+    v = np.ascontiguousarray(vertices, dtype=np.float64).reshape(-1, 9)
+    L = load()
+    nn, ni = ctypes.c_int64(), ctypes.c_int64()
+    err = ctypes.create_string_buffer(512)
+    args = (v.ctypes.data if len(v) else None, len(v))
+    if L.oracle_kd_build(*args, None, None, ctypes.byref(nn), ctypes.byref(ni), err, 512):
+        raise OracleError(err.value.decode())
+    nodes = np.zeros(nn.value * 72, np.uint8)
+    idx = np.zeros(ni.value, np.int32)
+    L.oracle_kd_build(*args, nodes.ctypes.data, idx.ctypes.data, ctypes.byref(nn), ctypes.byref(ni), err, 512)
+    return nodes, idx
 
 
 class OracleError(Exception):
