@@ -27,10 +27,16 @@
 
 using namespace rtb;
 
+// A region of a scene's device block and where it is copied from at the
+// flush: a host array of its own (a pinned mesh image, or a mesh array
+// prepared by this upload), or the context's pinned staging buffer.
 struct DirectCopy {
   size_t off, take;
   const char* src;
   size_t bytes;
+};
+struct StagedCopy {
+  size_t off, pin_off, bytes;
 };
 
 struct rt_scene {
@@ -46,14 +52,15 @@ struct rt_scene {
   std::vector<DMesh> host_meshes;       // device pointers, for the debug entry point
   std::vector<int> obj_kind, obj_mesh;  // per World object
   int n_point_lights = 0, n_disk_lights = 0;
-  // upload arena: one device block, filled through the context's pinned
-  // staging buffer and copied once (see upload())
+  // upload arena: one device block; small arrays are staged in the
+  // context's pinned buffer, mesh arrays copied from their own host memory
   char* blk = nullptr;
-  size_t blk_cap = 0, blk_used = 0;
+  size_t blk_cap = 0, blk_used = 0, pin_used = 0;
   char* arena = nullptr;  // the scene's device block (returned to the pool when freed)
   size_t arena_bytes = 0;
   ~rt_scene();
-  std::vector<DirectCopy> direct;  // arena regions copied from pinned images
+  std::vector<DirectCopy> direct;
+  std::vector<StagedCopy> staged;  // runs of the staging buffer
 };
 
 // One captured render (RT_FLAG_CUDA_GRAPH): the launch sequence is fully
@@ -245,34 +252,30 @@ rt_status ensure_dn_scratch(rt_ctx* ctx, long long n) {
 }
 
 // Scene uploads go into one device block per scene (sized from the scene
-// description by arena_open), staged in the context's pinned buffer and
-// copied with one asynchronous transfer per block (arena_flush); arrays that
+// description by arena_open) and are copied with one asynchronous transfer
+// per run of staged arrays and one per mesh array (arena_flush); arrays that
 // do not fit get their own allocation.  One cudaMalloc and one cudaFree per
 // scene instead of one per array.
 rt_status arena_flush(rt_ctx* ctx, rt_scene* sc) {
   if (sc->blk && sc->blk_used) {
-    // staged ranges from the pinned staging buffer, regions reserved by
-    // upload_image straight from their own pinned source
-    size_t pos = 0;
-    for (const DirectCopy& d : sc->direct) {
-      if (d.off > pos) CK(cudaMemcpyAsync(sc->blk + pos, ctx->pin + pos, d.off - pos, cudaMemcpyHostToDevice, ctx->stream));
+    for (const StagedCopy& c : sc->staged)
+      CK(cudaMemcpyAsync(sc->blk + c.off, ctx->pin + c.pin_off, c.bytes, cudaMemcpyHostToDevice, ctx->stream));
+    for (const DirectCopy& d : sc->direct)
       if (d.bytes) CK(cudaMemcpyAsync(sc->blk + d.off, d.src, d.bytes, cudaMemcpyHostToDevice, ctx->stream));
-      pos = d.off + d.take;
-    }
-    if (sc->blk_used > pos)
-      CK(cudaMemcpyAsync(sc->blk + pos, ctx->pin + pos, sc->blk_used - pos, cudaMemcpyHostToDevice, ctx->stream));
     CK(cudaStreamSynchronize(ctx->stream));
   }
   sc->direct.clear();
+  sc->staged.clear();
   sc->blk = nullptr;
-  sc->blk_cap = sc->blk_used = 0;
+  sc->blk_cap = sc->blk_used = sc->pin_used = 0;
   return RT_OK;
 }
 
-// Reserves `bytes` of the arena for a pinned host image and copies it there
-// at the flush (no staging copy); a dedicated allocation and a direct copy
-// when the arena has no room.
-rt_status upload_image(rt_ctx* ctx, rt_scene* sc, const char* src, size_t bytes, char** dev) {
+// Reserves `bytes` of the arena for a host array and copies it there at
+// the flush, straight from `src` (which must live until then; pinned memory
+// copies fastest); a dedicated allocation and a synchronous copy when the
+// arena has no room.
+rt_status upload_direct(rt_ctx* ctx, rt_scene* sc, const char* src, size_t bytes, char** dev) {
   const size_t take = (std::max<size_t>(bytes, 16) + 255) & ~(size_t)255;
   if (sc->blk && sc->blk_used + take <= sc->blk_cap) {
     *dev = sc->blk + sc->blk_used;
@@ -351,10 +354,13 @@ rt_scene::~rt_scene() {
 
 namespace {
 
-rt_status arena_open(rt_ctx* ctx, rt_scene* sc, size_t bytes) {
+// Opens a scene block of `bytes`, of which at most `staged_bytes` are
+// staged through the context's pinned buffer.
+rt_status arena_open(rt_ctx* ctx, rt_scene* sc, size_t bytes, size_t staged_bytes) {
   rt_status st = arena_flush(ctx, sc);
   if (st != RT_OK) return st;
   bytes = (bytes + 255) & ~(size_t)255;
+  staged_bytes = (staged_bytes + 255) & ~(size_t)255;
   size_t got = 0;
   char* b = pool_take(ctx->device, bytes, &got);
   if (!b) {
@@ -363,12 +369,12 @@ rt_status arena_open(rt_ctx* ctx, rt_scene* sc, size_t bytes) {
   }
   sc->arena = b;
   sc->arena_bytes = got;
-  if (ctx->pin_cap < bytes) {
+  if (ctx->pin_cap < staged_bytes) {
     if (ctx->pin) cudaFreeHost(ctx->pin);
     ctx->pin = nullptr;
     ctx->pin_cap = 0;
-    CK(cudaMallocHost((void**)&ctx->pin, bytes));
-    ctx->pin_cap = bytes;
+    CK(cudaMallocHost((void**)&ctx->pin, staged_bytes));
+    ctx->pin_cap = staged_bytes;
   }
   sc->blk = b;
   sc->blk_cap = bytes;
@@ -380,10 +386,16 @@ template <class T>
 rt_status upload(rt_ctx* ctx, rt_scene* sc, const std::vector<T>& h, const T** out) {
   const size_t bytes = h.size() * sizeof(T);
   const size_t take = (std::max<size_t>(bytes, 16) + 255) & ~(size_t)255;
-  if (sc->blk && sc->blk_used + take <= sc->blk_cap) {
-    if (bytes) memcpy(ctx->pin + sc->blk_used, h.data(), bytes);
+  if (sc->blk && sc->blk_used + take <= sc->blk_cap && sc->pin_used + take <= ctx->pin_cap) {
+    if (bytes) memcpy(ctx->pin + sc->pin_used, h.data(), bytes);
     *out = reinterpret_cast<const T*>(sc->blk + sc->blk_used);
+    StagedCopy* last = sc->staged.empty() ? nullptr : &sc->staged.back();
+    if (last && last->off + last->bytes == sc->blk_used && last->pin_off + last->bytes == sc->pin_used)
+      last->bytes += take;  // contiguous with the previous staged array
+    else
+      sc->staged.push_back(StagedCopy{sc->blk_used, sc->pin_used, take});
     sc->blk_used += take;
+    sc->pin_used += take;
   } else {
     T* p = nullptr;
     CK(dalloc(sc->allocs, &p, h.size()));
@@ -392,6 +404,13 @@ rt_status upload(rt_ctx* ctx, rt_scene* sc, const std::vector<T>& h, const T** o
   }
   sc->uploaded_bytes += bytes;
   return RT_OK;
+}
+
+// Device bytes of a scene description other than its meshes' arrays (an
+// upper bound for what upload() stages).
+size_t scene_staged_bound(const rt_scene_desc* d) {
+  return (1 << 16) + (size_t)std::max(d->n_meshes, 0) * 256 + (size_t)std::max(d->n_objects, 0) * 512 +
+         (size_t)std::max(d->n_materials, 0) * 256 + (size_t)std::max(d->n_lights, 0) * 128 + 32 * 256;
 }
 
 // Device bytes a scene description needs (an upper bound for the arena).
@@ -554,6 +573,26 @@ void pack_prep(MeshPrep* P) {
 }
 
 // Returns an empty string, or why the description is invalid.
+// Host threads for a loop over n items (at least 64k items each).
+int host_parts(long long n) {
+  const long long hw = std::max(1u, std::thread::hardware_concurrency());
+  return (int)std::max(1LL, std::min(hw, n / 65536));
+}
+
+// f(begin, end, part) over host_parts(n) contiguous ranges of [0, n), each
+// on its own thread.
+template <class F>
+void parallel_ranges(long long n, F f) {
+  const int parts = host_parts(n);
+  if (parts == 1) {
+    f(0LL, n, 0);
+    return;
+  }
+  std::vector<std::thread> th;
+  for (int p = 0; p < parts; p++) th.emplace_back([&f, n, parts, p] { f(n * p / parts, n * (p + 1) / parts, p); });
+  for (auto& t : th) t.join();
+}
+
 std::string prep_mesh(const rt_mesh_desc& md, MeshPrep* P) {
   for (int k = 0; k < 3; k++) {
     P->bmin[k] = md.bounds_min[k];
@@ -569,28 +608,34 @@ std::string prep_mesh(const rt_mesh_desc& md, MeshPrep* P) {
   std::vector<double2> brute((size_t)nt * 5);
   std::vector<double4> normals((size_t)nt);
   std::vector<double> tmin((size_t)nt * 3), tmax((size_t)nt * 3);
-  double scale = 0.0;
-  for (long long t = 0; t < nt; t++) {
-    const double* v = md.vertices + 9 * t;
-    V3 v0 = mk(v[0], v[1], v[2]), v1 = mk(v[3], v[4], v[5]), v2 = mk(v[6], v[7], v[8]);
-    V3 e1 = v1 - v0, e2 = v2 - v0;
-    V3 n = cross(e1, e2);
-    int degenerate = norm(n) < 1e-8 ? 1 : 0;  // src/ray.rs:565-567
-    V3 nn = normalize(n);
-    normals[t] = double4{nn.x, nn.y, nn.z, 0.0};
-    double2* E = &brute[5 * t];
-    E[0] = double2{v0.x, v0.y};
-    E[1] = double2{v0.z, e1.x};
-    E[2] = double2{e1.y, e1.z};
-    E[3] = double2{e2.x, e2.y};
-    E[4] = double2{e2.z, pack2((int)t, degenerate)};
-    for (int k = 0; k < 3; k++) {
-      double a = v[k], b = v[3 + k], c = v[6 + k];
-      tmin[3 * t + k] = std::min(a, std::min(b, c));
-      tmax[3 * t + k] = std::max(a, std::max(b, c));
-      scale = std::max(scale, std::max(std::fabs(tmin[3 * t + k]), std::fabs(tmax[3 * t + k])));
+  std::vector<double> part_scale(host_parts(nt), 0.0);
+  parallel_ranges(nt, [&](long long t0, long long t1, int part) {
+    double scale = 0.0;
+    for (long long t = t0; t < t1; t++) {
+      const double* v = md.vertices + 9 * t;
+      V3 v0 = mk(v[0], v[1], v[2]), v1 = mk(v[3], v[4], v[5]), v2 = mk(v[6], v[7], v[8]);
+      V3 e1 = v1 - v0, e2 = v2 - v0;
+      V3 n = cross(e1, e2);
+      int degenerate = norm(n) < 1e-8 ? 1 : 0;  // src/ray.rs:565-567
+      V3 nn = normalize(n);
+      normals[t] = double4{nn.x, nn.y, nn.z, 0.0};
+      double2* E = &brute[5 * t];
+      E[0] = double2{v0.x, v0.y};
+      E[1] = double2{v0.z, e1.x};
+      E[2] = double2{e1.y, e1.z};
+      E[3] = double2{e2.x, e2.y};
+      E[4] = double2{e2.z, pack2((int)t, degenerate)};
+      for (int k = 0; k < 3; k++) {
+        double a = v[k], b = v[3 + k], c = v[6 + k];
+        tmin[3 * t + k] = std::min(a, std::min(b, c));
+        tmax[3 * t + k] = std::max(a, std::max(b, c));
+        scale = std::max(scale, std::max(std::fabs(tmin[3 * t + k]), std::fabs(tmax[3 * t + k])));
+      }
     }
-  }
+    part_scale[part] = scale;
+  });
+  double scale = 0.0;
+  for (double v : part_scale) scale = std::max(scale, v);
   // reference k-d tree: nodes, per-node root paths, leaf entries and the
   // per-triangle occurrences (leaf node, position in the leaf)
   std::vector<double2> nodes((size_t)md.n_nodes * 4);
@@ -657,8 +702,10 @@ std::string prep_mesh(const rt_mesh_desc& md, MeshPrep* P) {
   build_bvh(tmin, tmax, 8, 1e-7 * (1.0 + scale), &bnodes, &order);
   std::vector<double2> bvh, btris((size_t)nt * 5);
   put_bvh(bnodes, &bvh);
-  for (long long k = 0; k < nt; k++)
-    for (int j = 0; j < 5; j++) btris[5 * k + j] = brute[5 * (size_t)order[k] + j];
+  parallel_ranges(nt, [&](long long k0, long long k1, int) {
+    for (long long k = k0; k < k1; k++)
+      for (int j = 0; j < 5; j++) btris[5 * k + j] = brute[5 * (size_t)order[k] + j];
+  });
   P->bvh = std::move(bvh);
   P->btris = std::move(btris);
   P->brute = std::move(brute);
@@ -673,6 +720,15 @@ std::string prep_mesh(const rt_mesh_desc& md, MeshPrep* P) {
   return std::string();
 }
 
+template <class T>
+rt_status upload_array(rt_ctx* ctx, rt_scene* sc, const std::vector<T>& h, const T** out) {
+  char* dev = nullptr;
+  rt_status st = upload_direct(ctx, sc, reinterpret_cast<const char*>(h.data()), h.size() * sizeof(T), &dev);
+  *out = reinterpret_cast<const T*>(dev);
+  return st;
+}
+
+// Copies a prepared mesh into the scene's block.
 rt_status upload_prep(rt_ctx* ctx, rt_scene* sc, const MeshPrep& P, DMesh* out) {
   DMesh M{};
   for (int k = 0; k < 3; k++) {
@@ -683,7 +739,7 @@ rt_status upload_prep(rt_ctx* ctx, rt_scene* sc, const MeshPrep& P, DMesh* out) 
   M.n_tris = P.n_tris;
   if (P.image) {
     char* base = nullptr;
-    rt_status st = upload_image(ctx, sc, P.image, P.image_bytes, &base);
+    rt_status st = upload_direct(ctx, sc, P.image, P.image_bytes, &base);
     if (st != RT_OK) return st;
     M.bvh = reinterpret_cast<const double2*>(base + P.off[0]);
     M.btris = reinterpret_cast<const double2*>(base + P.off[1]);
@@ -697,29 +753,16 @@ rt_status upload_prep(rt_ctx* ctx, rt_scene* sc, const MeshPrep& P, DMesh* out) 
     *out = M;
     return RT_OK;
   }
+  // not packed: each array straight from P's own memory (P outlives the flush)
   rt_status st;
-  const double2* p2;
-  if ((st = upload(ctx, sc, P.bvh, &p2)) != RT_OK) return st;
-  M.bvh = p2;
-  if ((st = upload(ctx, sc, P.btris, &p2)) != RT_OK) return st;
-  M.btris = p2;
-  if ((st = upload(ctx, sc, P.brute, &p2)) != RT_OK) return st;
-  M.brute = p2;
-  const double4* p4;
-  if ((st = upload(ctx, sc, P.normals, &p4)) != RT_OK) return st;
-  M.normals = p4;
-  if ((st = upload(ctx, sc, P.nodes, &p2)) != RT_OK) return st;
-  M.nodes = p2;
-  const int* pi;
-  if ((st = upload(ctx, sc, P.leaf_tris, &pi)) != RT_OK) return st;
-  M.leaf_tris = pi;
-  const int2* pi2;
-  if ((st = upload(ctx, sc, P.leaf_path, &pi2)) != RT_OK) return st;
-  M.leaf_path = pi2;
-  if ((st = upload(ctx, sc, P.occ, &pi2)) != RT_OK) return st;
-  M.occ = pi2;
-  if ((st = upload(ctx, sc, P.occ_off, &pi)) != RT_OK) return st;
-  M.occ_off = pi;
+  if ((st = upload_array(ctx, sc, P.bvh, &M.bvh)) != RT_OK || (st = upload_array(ctx, sc, P.btris, &M.btris)) != RT_OK ||
+      (st = upload_array(ctx, sc, P.brute, &M.brute)) != RT_OK ||
+      (st = upload_array(ctx, sc, P.normals, &M.normals)) != RT_OK ||
+      (st = upload_array(ctx, sc, P.nodes, &M.nodes)) != RT_OK ||
+      (st = upload_array(ctx, sc, P.leaf_tris, &M.leaf_tris)) != RT_OK ||
+      (st = upload_array(ctx, sc, P.leaf_path, &M.leaf_path)) != RT_OK ||
+      (st = upload_array(ctx, sc, P.occ, &M.occ)) != RT_OK || (st = upload_array(ctx, sc, P.occ_off, &M.occ_off)) != RT_OK)
+    return st;
   M.n_nodes = P.n_nodes;
   M.n_tris = P.n_tris;
   *out = M;
@@ -753,10 +796,11 @@ rt_status do_upload(rt_ctx* ctx, const rt_scene_desc* d, rt_scene** out,
     if (d->meshes[m].n_triangles < 0 || d->meshes[m].n_nodes < 0 || d->meshes[m].n_tri_index < 0)
       return fail(ctx, RT_ERR_INVALID_ARGUMENT, "negative count");
   {
-    rt_status st = arena_open(ctx, sc.get(), scene_bytes_bound(d));
+    rt_status st = arena_open(ctx, sc.get(), scene_bytes_bound(d), scene_staged_bound(d));
     if (st != RT_OK) return st;
   }
   std::vector<DMesh> meshes(d->n_meshes);
+  std::vector<std::shared_ptr<MeshPrep>> keep;  // the copies read them until the flush
   if (preps && preps->size() != (size_t)d->n_meshes) preps->assign(d->n_meshes, nullptr);
   for (int m = 0; m < d->n_meshes; m++) {
     std::shared_ptr<MeshPrep> P = preps ? (*preps)[m] : nullptr;
@@ -764,11 +808,13 @@ rt_status do_upload(rt_ctx* ctx, const rt_scene_desc* d, rt_scene** out,
       P = std::make_shared<MeshPrep>();
       std::string e = prep_mesh(d->meshes[m], P.get());
       if (!e.empty()) return fail(ctx, RT_ERR_INVALID_ARGUMENT, e);
-      if (preps) {
-        pack_prep(P.get());
-        (*preps)[m] = P;
-      }
+      if (preps) (*preps)[m] = P;
+    } else if (!P->image) {
+      // uploaded again: from now on one pinned image, copied by DMA (the
+      // first upload skips the pinning, which costs more than its copy)
+      pack_prep(P.get());
     }
+    keep.push_back(P);
     rt_status st = upload_prep(ctx, sc.get(), *P, &meshes[m]);
     if (st != RT_OK) return st;
   }
