@@ -169,6 +169,12 @@ void build_bvh(const std::vector<double>& bmin, const std::vector<double>& bmax,
   nodes->resize(b.count((int)n));
   b.build(prims.data(), (int)n, 0, nodes->data(), 0, 0);
   for (size_t i = 0; i < n; i++) (*order)[i] = prims[i].id;
+  // each leaf's primitives in id order: a canonical layout (the device
+  // builder makes the same one; the order within a leaf changes no result)
+  for (const BvhNode& nd : *nodes) {
+    if (nd.lcnt > 0) std::sort(order->begin() + nd.lidx, order->begin() + nd.lidx + nd.lcnt);
+    if (nd.rcnt > 0) std::sort(order->begin() + nd.ridx, order->begin() + nd.ridx + nd.rcnt);
+  }
 }
 
 }  // namespace rtb

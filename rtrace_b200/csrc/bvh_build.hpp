@@ -26,9 +26,11 @@ struct BvhNode {
   int32_t lidx, lcnt, ridx, rcnt;
 };
 
-// Builds a BVH over n primitive boxes; returns nodes (root = 0) and the
-// primitive order (order[k] = primitive id stored at position k).  Boxes
-// are padded by `pad`.
+// Builds a BVH over n primitive boxes; returns nodes (root = 0, preorder,
+// left subtree first) and the primitive order (order[k] = primitive id
+// stored at position k, ids ascending within a leaf).  A node splits its
+// primitives at the median centroid (ties by id) of the axis with the
+// widest centroid extent; node boxes are padded by `pad`.
 void build_bvh(const std::vector<double>& bmin, const std::vector<double>& bmax, int leaf_size, double pad,
                std::vector<BvhNode>* nodes, std::vector<int32_t>* order);
 

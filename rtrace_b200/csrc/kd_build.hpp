@@ -8,11 +8,11 @@
 #include <vector>
 
 #include "../../include/rtrace_gpu.h"
+#include "build_arena.hpp"
 
 namespace rtb {
 
-// Device memory a context keeps for its k-d builds (freed with it).
-struct KdArena;
+// Device memory a context keeps for its builds (freed with it).
 KdArena* kd_arena_new();
 void kd_arena_free(KdArena* arena);
 

@@ -1,0 +1,41 @@
+// A large mesh's device search data, computed on the device: the work the
+// host preparation does (triangle records and normals, the triangle BVH,
+// the k-d occurrence lists), with the same results, byte for byte.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <string>
+
+#include "build_arena.hpp"
+
+namespace rtb {
+
+// Device destinations: bvh 7 x bvh_internal_nodes(n, leaf) double2,
+// btris and brute 5n double2, normals n double4, occ n_index int2,
+// occ_off n + 1 int.
+struct MeshPrepOut {
+  double2* bvh;
+  double2* btris;
+  double2* brute;
+  double4* normals;
+  int2* occ;
+  int* occ_off;
+};
+
+// Internal nodes of the median-split BVH over n primitives with leaves of
+// at most `leaf` (a function of n alone; at least 1 when n > 0).
+int bvh_internal_nodes(int n, int leaf);
+
+// h_vertices: 9n doubles (host); d_kd_nodes: the packed reference k-d
+// nodes on the device (4 double2 each, leaves {first, -1 - count} in the
+// last word); d_leaf_tris: the leaf lists on the device (n_index entries,
+// validated: every entry in [0, n), the leaves cover each entry once).
+// n > leaf.  Runs on stream s and returns when the results are written;
+// scratch (the vertices included) from arena.  Returns "" or the CUDA
+// failure (*cuda_err set).
+std::string prep_mesh_device(const double* h_vertices, int n, const double2* d_kd_nodes, int n_kd_nodes,
+                             const int* d_leaf_tris, int n_index, int leaf, cudaStream_t s, KdArena* arena,
+                             const MeshPrepOut& out, cudaError_t* cuda_err);
+
+}  // namespace rtb

@@ -22,6 +22,7 @@
 #include "../../include/rtrace_gpu.h"
 #include "bvh_build.hpp"
 #include "kd_build.hpp"
+#include "mesh_prep.hpp"
 #include "kernels.cuh"
 #include "scene_loader.hpp"
 
@@ -525,7 +526,10 @@ struct MeshPrep {
   std::vector<int> leaf_tris, occ_off;
   std::vector<int2> leaf_path, occ;
   double bmin[3], bmax[3];
-  int n_nodes = 0, n_tris = 0;
+  int n_nodes = 0, n_tris = 0, n_index = 0;
+  // Prepared on the device by the last upload: the records, normals, BVH
+  // and occurrence arrays are not on the host (only the k-d part is).
+  bool device_made = false;
   // Kept by a host scene, the nine arrays above are packed into one pinned
   // buffer (each at a 256-byte aligned offset) and the vectors released:
   // uploads then copy the image straight from pinned memory.
@@ -593,7 +597,16 @@ void parallel_ranges(long long n, F f) {
   for (auto& t : th) t.join();
 }
 
-std::string prep_mesh(const rt_mesh_desc& md, MeshPrep* P) {
+// Triangles per mesh BVH leaf (measured fastest of 2-16 on the mesh frame).
+const int kMeshLeaf = 8;
+// Meshes from this many triangles up are prepared on the device.
+const long long kPrepDeviceMin = 16384;
+
+// The part of a mesh's preparation that always runs on the host: checks,
+// the reference k-d nodes packed for the device with each node's root path,
+// the leaf lists.  Every leaf-list entry must name a triangle and belong to
+// exactly one leaf (as in every tree KdTree::new builds).
+std::string prep_mesh_kd(const rt_mesh_desc& md, MeshPrep* P) {
   for (int k = 0; k < 3; k++) {
     P->bmin[k] = md.bounds_min[k];
     P->bmax[k] = md.bounds_max[k];
@@ -604,6 +617,69 @@ std::string prep_mesh(const rt_mesh_desc& md, MeshPrep* P) {
     return "mesh too large";
   if ((nt > 0 && !md.vertices) || (md.n_nodes > 0 && !md.nodes) || (md.n_tri_index > 0 && !md.tri_index))
     return "null mesh array";
+  std::vector<double2> nodes((size_t)md.n_nodes * 4);
+  std::vector<int2> leaf_path((size_t)md.n_nodes, int2{0, 0});
+  std::vector<char> covered((size_t)md.n_tri_index, 0);
+  for (long long k = 0; k < md.n_nodes; k++) {
+    const rt_kd_node_desc& nd = md.nodes[k];
+    double2* N = &nodes[4 * k];
+    N[0] = double2{nd.bounds_min[0], nd.bounds_min[1]};
+    N[1] = double2{nd.bounds_min[2], nd.bounds_max[0]};
+    N[2] = double2{nd.bounds_max[1], nd.bounds_max[2]};
+    if (nd.axis < 0) {
+      if (nd.first < 0 || nd.count < 0 || (long long)nd.first + nd.count > md.n_tri_index)
+        return "k-d leaf range out of bounds";
+      for (int p = 0; p < nd.count; p++)
+        if (covered[nd.first + p]++) return "k-d leaves overlap";
+      N[3] = double2{0.0, pack2(nd.first, -1 - nd.count)};
+    } else {
+      if (nd.axis > 2 || nd.right <= k + 1 || nd.right >= md.n_nodes)
+        return "k-d node layout is not preorder";
+      N[3] = double2{nd.split, pack2(nd.right, nd.axis)};
+    }
+  }
+  for (char c : covered)
+    if (!c) return "k-d leaf lists have entries in no leaf";
+  if (md.n_nodes > 0) {
+    std::vector<std::pair<int, int2>> st;  // node, {path bits, depth}
+    st.push_back({0, int2{0, 0}});
+    std::vector<char> seen((size_t)md.n_nodes, 0);
+    while (!st.empty()) {
+      int k = st.back().first;
+      int2 pd = st.back().second;
+      st.pop_back();
+      if (seen[k]) return "k-d nodes do not form a tree";
+      seen[k] = 1;
+      leaf_path[k] = pd;
+      const rt_kd_node_desc& nd = md.nodes[k];
+      if (nd.axis >= 0) {
+        if (pd.y >= 31) return "k-d tree deeper than 31 levels";
+        st.push_back({k + 1, int2{pd.x, pd.y + 1}});
+        st.push_back({nd.right, int2{pd.x | (1 << pd.y), pd.y + 1}});
+      }
+    }
+  }
+  std::vector<int> leaf_tris((size_t)md.n_tri_index);
+  for (long long k = 0; k < md.n_tri_index; k++) {
+    int t = md.tri_index[k];
+    if (t < 0 || t >= nt) return "k-d leaf index out of range";
+    leaf_tris[k] = t;
+  }
+  P->nodes = std::move(nodes);
+  P->leaf_path = std::move(leaf_path);
+  P->leaf_tris = std::move(leaf_tris);
+  P->n_nodes = (int)md.n_nodes;
+  P->n_tris = (int)nt;
+  P->n_index = (int)md.n_tri_index;
+  return std::string();
+}
+
+// A mesh's whole preparation on the host: the k-d part, then the triangle
+// records and normals, the occurrence lists and the triangle BVH.
+std::string prep_mesh(const rt_mesh_desc& md, MeshPrep* P) {
+  std::string e = prep_mesh_kd(md, P);
+  if (!e.empty()) return e;
+  const long long nt = md.n_triangles;
   // triangle records and normals in original order
   std::vector<double2> brute((size_t)nt * 5);
   std::vector<double4> normals((size_t)nt);
@@ -636,53 +712,10 @@ std::string prep_mesh(const rt_mesh_desc& md, MeshPrep* P) {
   });
   double scale = 0.0;
   for (double v : part_scale) scale = std::max(scale, v);
-  // reference k-d tree: nodes, per-node root paths, leaf entries and the
-  // per-triangle occurrences (leaf node, position in the leaf)
-  std::vector<double2> nodes((size_t)md.n_nodes * 4);
-  std::vector<int2> leaf_path((size_t)md.n_nodes, int2{0, 0});
-  for (long long k = 0; k < md.n_nodes; k++) {
-    const rt_kd_node_desc& nd = md.nodes[k];
-    double2* N = &nodes[4 * k];
-    N[0] = double2{nd.bounds_min[0], nd.bounds_min[1]};
-    N[1] = double2{nd.bounds_min[2], nd.bounds_max[0]};
-    N[2] = double2{nd.bounds_max[1], nd.bounds_max[2]};
-    if (nd.axis < 0) {
-      if (nd.first < 0 || nd.count < 0 || (long long)nd.first + nd.count > md.n_tri_index)
-        return "k-d leaf range out of bounds";
-      N[3] = double2{0.0, pack2(nd.first, -1 - nd.count)};
-    } else {
-      if (nd.axis > 2 || nd.right <= k + 1 || nd.right >= md.n_nodes)
-        return "k-d node layout is not preorder";
-      N[3] = double2{nd.split, pack2(nd.right, nd.axis)};
-    }
-  }
-  if (md.n_nodes > 0) {
-    std::vector<std::pair<int, int2>> st;  // node, {path bits, depth}
-    st.push_back({0, int2{0, 0}});
-    std::vector<char> seen((size_t)md.n_nodes, 0);
-    while (!st.empty()) {
-      int k = st.back().first;
-      int2 pd = st.back().second;
-      st.pop_back();
-      if (seen[k]) return "k-d nodes do not form a tree";
-      seen[k] = 1;
-      leaf_path[k] = pd;
-      const rt_kd_node_desc& nd = md.nodes[k];
-      if (nd.axis >= 0) {
-        if (pd.y >= 31) return "k-d tree deeper than 31 levels";
-        st.push_back({k + 1, int2{pd.x, pd.y + 1}});
-        st.push_back({nd.right, int2{pd.x | (1 << pd.y), pd.y + 1}});
-      }
-    }
-  }
-  std::vector<int> leaf_tris((size_t)md.n_tri_index);
+  // per-triangle occurrences (leaf node, position in the leaf), by leaf
+  // node then position
   std::vector<int> occ_off((size_t)nt + 1, 0);
-  for (long long k = 0; k < md.n_tri_index; k++) {
-    int t = md.tri_index[k];
-    if (t < 0 || t >= nt) return "k-d leaf index out of range";
-    leaf_tris[k] = t;
-    occ_off[t + 1]++;
-  }
+  for (int t : P->leaf_tris) occ_off[t + 1]++;
   for (long long t = 0; t < nt; t++) occ_off[t + 1] += occ_off[t];
   std::vector<int2> occ((size_t)md.n_tri_index);
   {
@@ -699,7 +732,7 @@ std::string prep_mesh(const rt_mesh_desc& md, MeshPrep* P) {
   // triangle BVH, the candidate search structure
   std::vector<BvhNode> bnodes;
   std::vector<int32_t> order;
-  build_bvh(tmin, tmax, 8, 1e-7 * (1.0 + scale), &bnodes, &order);
+  build_bvh(tmin, tmax, kMeshLeaf, 1e-7 * (1.0 + scale), &bnodes, &order);
   std::vector<double2> bvh, btris((size_t)nt * 5);
   put_bvh(bnodes, &bvh);
   parallel_ranges(nt, [&](long long k0, long long k1, int) {
@@ -709,14 +742,9 @@ std::string prep_mesh(const rt_mesh_desc& md, MeshPrep* P) {
   P->bvh = std::move(bvh);
   P->btris = std::move(btris);
   P->brute = std::move(brute);
-  P->nodes = std::move(nodes);
   P->normals = std::move(normals);
-  P->leaf_tris = std::move(leaf_tris);
   P->occ_off = std::move(occ_off);
-  P->leaf_path = std::move(leaf_path);
   P->occ = std::move(occ);
-  P->n_nodes = (int)md.n_nodes;
-  P->n_tris = (int)nt;
   return std::string();
 }
 
@@ -726,6 +754,90 @@ rt_status upload_array(rt_ctx* ctx, rt_scene* sc, const std::vector<T>& h, const
   rt_status st = upload_direct(ctx, sc, reinterpret_cast<const char*>(h.data()), h.size() * sizeof(T), &dev);
   *out = reinterpret_cast<const T*>(dev);
   return st;
+}
+
+// A region of the scene's block that a kernel will fill (no copy).
+template <class T>
+rt_status reserve(rt_ctx* ctx, rt_scene* sc, size_t count, T** dev) {
+  const size_t bytes = count * sizeof(T);
+  const size_t take = (std::max<size_t>(bytes, 16) + 255) & ~(size_t)255;
+  if (sc->blk && sc->blk_used + take <= sc->blk_cap) {
+    *dev = reinterpret_cast<T*>(sc->blk + sc->blk_used);
+    sc->blk_used += take;
+  } else {
+    CK(dalloc(sc->allocs, dev, std::max<size_t>(count, 1)));
+  }
+  return RT_OK;
+}
+
+// A host array copied into the scene's block now, on the context's stream
+// (for data a kernel of this upload reads).
+template <class T>
+rt_status upload_now(rt_ctx* ctx, rt_scene* sc, const std::vector<T>& h, const T** out) {
+  T* dev = nullptr;
+  rt_status st = reserve(ctx, sc, h.size(), &dev);
+  if (st != RT_OK) return st;
+  if (!h.empty()) CK(cudaMemcpyAsync(dev, h.data(), h.size() * sizeof(T), cudaMemcpyHostToDevice, ctx->stream));
+  sc->uploaded_bytes += h.size() * sizeof(T);
+  *out = dev;
+  return RT_OK;
+}
+
+// Prepares a large mesh on the device straight into the scene's block: P
+// holds the k-d part (prep_mesh_kd).  keep_host: also copies the arrays
+// made on the device back into P, so that later uploads copy them.
+rt_status upload_prep_device(rt_ctx* ctx, rt_scene* sc, const rt_mesh_desc& md, MeshPrep* P, bool keep_host,
+                             DMesh* out) {
+  DMesh M{};
+  for (int k = 0; k < 3; k++) {
+    M.bmin[k] = P->bmin[k];
+    M.bmax[k] = P->bmax[k];
+  }
+  M.n_nodes = P->n_nodes;
+  M.n_tris = P->n_tris;
+  const int n = P->n_tris, nb = bvh_internal_nodes(n, kMeshLeaf);
+  rt_status st;
+  double2 *bvh, *btris, *brute;
+  double4* normals;
+  int2* occ;
+  int* occ_off;
+  if ((st = upload_now(ctx, sc, P->nodes, &M.nodes)) != RT_OK || (st = upload_now(ctx, sc, P->leaf_tris, &M.leaf_tris)) != RT_OK ||
+      (st = upload_now(ctx, sc, P->leaf_path, &M.leaf_path)) != RT_OK || (st = reserve(ctx, sc, 7 * (size_t)nb, &bvh)) != RT_OK ||
+      (st = reserve(ctx, sc, 5 * (size_t)n, &btris)) != RT_OK || (st = reserve(ctx, sc, 5 * (size_t)n, &brute)) != RT_OK ||
+      (st = reserve(ctx, sc, (size_t)n, &normals)) != RT_OK || (st = reserve(ctx, sc, (size_t)P->n_index, &occ)) != RT_OK ||
+      (st = reserve(ctx, sc, (size_t)n + 1, &occ_off)) != RT_OK)
+    return st;
+  if (!ctx->kd_arena) ctx->kd_arena = kd_arena_new();
+  cudaError_t ce = cudaSuccess;
+  std::string e = prep_mesh_device(md.vertices, n, M.nodes, P->n_nodes, M.leaf_tris, P->n_index, kMeshLeaf,
+                                   ctx->stream, ctx->kd_arena, MeshPrepOut{bvh, btris, brute, normals, occ, occ_off},
+                                   &ce);
+  if (ce != cudaSuccess) return cuda_fail(ctx, ce, e.c_str());
+  if (!e.empty()) return fail(ctx, RT_ERR_INVALID_ARGUMENT, e);
+  sc->uploaded_bytes += 9 * (size_t)n * sizeof(double);
+  M.bvh = bvh;
+  M.btris = btris;
+  M.brute = brute;
+  M.normals = normals;
+  M.occ = occ;
+  M.occ_off = occ_off;
+  if (keep_host) {
+    P->bvh.resize(7 * (size_t)nb);
+    P->btris.resize(5 * (size_t)n);
+    P->brute.resize(5 * (size_t)n);
+    P->normals.resize(n);
+    P->occ.resize(P->n_index);
+    P->occ_off.resize((size_t)n + 1);
+    CK(cudaMemcpy(P->bvh.data(), bvh, P->bvh.size() * sizeof(double2), cudaMemcpyDeviceToHost));
+    CK(cudaMemcpy(P->btris.data(), btris, P->btris.size() * sizeof(double2), cudaMemcpyDeviceToHost));
+    CK(cudaMemcpy(P->brute.data(), brute, P->brute.size() * sizeof(double2), cudaMemcpyDeviceToHost));
+    CK(cudaMemcpy(P->normals.data(), normals, P->normals.size() * sizeof(double4), cudaMemcpyDeviceToHost));
+    CK(cudaMemcpy(P->occ.data(), occ, P->occ.size() * sizeof(int2), cudaMemcpyDeviceToHost));
+    CK(cudaMemcpy(P->occ_off.data(), occ_off, P->occ_off.size() * sizeof(int), cudaMemcpyDeviceToHost));
+    P->device_made = false;
+  }
+  *out = M;
+  return RT_OK;
 }
 
 // Copies a prepared mesh into the scene's block.
@@ -803,19 +915,32 @@ rt_status do_upload(rt_ctx* ctx, const rt_scene_desc* d, rt_scene** out,
   std::vector<std::shared_ptr<MeshPrep>> keep;  // the copies read them until the flush
   if (preps && preps->size() != (size_t)d->n_meshes) preps->assign(d->n_meshes, nullptr);
   for (int m = 0; m < d->n_meshes; m++) {
+    const rt_mesh_desc& md = d->meshes[m];
     std::shared_ptr<MeshPrep> P = preps ? (*preps)[m] : nullptr;
+    rt_status st;
     if (!P) {
+      // first upload: large meshes are prepared on the device, into the block
       P = std::make_shared<MeshPrep>();
-      std::string e = prep_mesh(d->meshes[m], P.get());
+      const bool dev = md.n_triangles >= kPrepDeviceMin;
+      std::string e = dev ? prep_mesh_kd(md, P.get()) : prep_mesh(md, P.get());
       if (!e.empty()) return fail(ctx, RT_ERR_INVALID_ARGUMENT, e);
+      P->device_made = dev;
       if (preps) (*preps)[m] = P;
-    } else if (!P->image) {
-      // uploaded again: from now on one pinned image, copied by DMA (the
-      // first upload skips the pinning, which costs more than its copy)
-      pack_prep(P.get());
+      keep.push_back(P);
+      st = dev ? upload_prep_device(ctx, sc.get(), md, P.get(), false, &meshes[m])
+               : upload_prep(ctx, sc.get(), *P, &meshes[m]);
+    } else if (P->device_made) {
+      // uploaded again: prepared on the device once more, and this time
+      // the arrays stay on the host, as one pinned image for the uploads
+      // after this one (pinning costs more than a copy, so the first
+      // upload skips it)
+      st = upload_prep_device(ctx, sc.get(), md, P.get(), true, &meshes[m]);
+      if (st == RT_OK) pack_prep(P.get());
+    } else {
+      if (!P->image) pack_prep(P.get());
+      keep.push_back(P);
+      st = upload_prep(ctx, sc.get(), *P, &meshes[m]);
     }
-    keep.push_back(P);
-    rt_status st = upload_prep(ctx, sc.get(), *P, &meshes[m]);
     if (st != RT_OK) return st;
   }
   std::vector<int4> obj;
@@ -2027,6 +2152,59 @@ rt_status rt_debug_disk_offsets(rt_ctx* ctx, const uint64_t* light_seeds, int64_
   CK(cudaMemcpy(out, dout, (size_t)n * 32 * sizeof(double), cudaMemcpyDeviceToHost));
   free_all(tmp);
   if (herr) return fail(ctx, RT_ERR_DEVICE_WATCHDOG, "rejection sampling did not terminate");
+  return RT_OK;
+}
+
+rt_status rt_debug_mesh_prep(rt_ctx* ctx, const rt_mesh_desc* md, uint32_t* mismatch) {
+  if (!ctx || !md || !mismatch) return fail(ctx, RT_ERR_INVALID_ARGUMENT, "null argument");
+  *mismatch = 0;
+  if (md->n_triangles <= kMeshLeaf) return fail(ctx, RT_ERR_INVALID_ARGUMENT, "mesh too small for the device preparation");
+  CK(cudaSetDevice(ctx->device));
+  MeshPrep H, D;
+  std::string e = prep_mesh(*md, &H);
+  if (!e.empty()) return fail(ctx, RT_ERR_INVALID_ARGUMENT, e);
+  e = prep_mesh_kd(*md, &D);
+  if (!e.empty()) return fail(ctx, RT_ERR_INVALID_ARGUMENT, e);
+  const int n = D.n_tris, nb = bvh_internal_nodes(n, kMeshLeaf);
+  std::vector<void*> tmp;
+  double2 *dn, *bvh, *btris, *brute;
+  double4* normals;
+  int *dl, *occ_off;
+  int2* occ;
+  cudaError_t ce = cudaSuccess;
+  if ((ce = dalloc(tmp, &dn, D.nodes.size())) != cudaSuccess || (ce = dalloc(tmp, &dl, D.leaf_tris.size())) != cudaSuccess ||
+      (ce = dalloc(tmp, &bvh, 7 * (size_t)nb)) != cudaSuccess || (ce = dalloc(tmp, &btris, 5 * (size_t)n)) != cudaSuccess ||
+      (ce = dalloc(tmp, &brute, 5 * (size_t)n)) != cudaSuccess || (ce = dalloc(tmp, &normals, (size_t)n)) != cudaSuccess ||
+      (ce = dalloc(tmp, &occ, (size_t)D.n_index)) != cudaSuccess || (ce = dalloc(tmp, &occ_off, (size_t)n + 1)) != cudaSuccess) {
+    free_all(tmp);
+    return cuda_fail(ctx, ce, "cudaMalloc");
+  }
+  cudaMemcpy(dn, D.nodes.data(), D.nodes.size() * sizeof(double2), cudaMemcpyHostToDevice);
+  cudaMemcpy(dl, D.leaf_tris.data(), D.leaf_tris.size() * sizeof(int), cudaMemcpyHostToDevice);
+  if (!ctx->kd_arena) ctx->kd_arena = kd_arena_new();
+  e = prep_mesh_device(md->vertices, n, dn, D.n_nodes, dl, D.n_index, kMeshLeaf, ctx->stream, ctx->kd_arena,
+                       MeshPrepOut{bvh, btris, brute, normals, occ, occ_off}, &ce);
+  if (!e.empty()) {
+    free_all(tmp);
+    return ce != cudaSuccess ? cuda_fail(ctx, ce, e.c_str()) : fail(ctx, RT_ERR_INVALID_ARGUMENT, e);
+  }
+  auto same = [](const void* dev, const void* host, size_t bytes) {
+    std::vector<char> h(bytes);
+    if (bytes) cudaMemcpy(h.data(), dev, bytes, cudaMemcpyDeviceToHost);
+    return !bytes || memcmp(h.data(), host, bytes) == 0;
+  };
+  uint32_t m = 0;
+  if (H.bvh.size() != 7 * (size_t)nb || !same(bvh, H.bvh.data(), H.bvh.size() * sizeof(double2))) m |= 1;
+  if (!same(btris, H.btris.data(), H.btris.size() * sizeof(double2))) m |= 2;
+  if (!same(brute, H.brute.data(), H.brute.size() * sizeof(double2))) m |= 4;
+  if (!same(normals, H.normals.data(), H.normals.size() * sizeof(double4))) m |= 8;
+  if (!same(occ, H.occ.data(), H.occ.size() * sizeof(int2))) m |= 16;
+  if (!same(occ_off, H.occ_off.data(), H.occ_off.size() * sizeof(int))) m |= 32;
+  ce = cudaGetLastError();
+  free_all(tmp);
+  if (ce != cudaSuccess) return cuda_fail(ctx, ce, "mesh preparation check");
+  *mismatch = m;
+  ctx->err.clear();
   return RT_OK;
 }
 

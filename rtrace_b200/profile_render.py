@@ -2,10 +2,15 @@
 
     python -m rtrace_b200.profile_render --workload noisy_icosphere --width 960 --height 540 --reps 1
     python -m rtrace_b200.profile_render --workload ring_spheres --width 1920 --height 1080 --learned
+    python -m rtrace_b200.profile_render --kd-build terrain --reps 2
 
 Workloads (see rtrace_b200.workloads): sphere_grid (quincunx), noisy_icosphere
 (no-jitter + outline, the bench.py scene), ring_spheres (stochastic, 4 spp).
 Scene files are written to --dir (default: a temporary directory).
+--kd-build builds the k-d tree of a workload's mesh (terrain: the 1024x1024
+heightfield, 2,093,058 triangles; icosphere: the level-6 noisy icosphere)
+on the device --reps times after one warm-up build of 1,000 of its
+triangles, and checks it against the host build.
 """
 import argparse
 import json
@@ -25,8 +30,11 @@ def main(argv=None):
     ap.add_argument("--dir", default=None)
     ap.add_argument("--disk-samples", type=int, default=16, help="shadow rays per disk light (16: the reference)")
     ap.add_argument("--learned", action="store_true", help="learned soft shadows with the shipped denoiser weights")
+    ap.add_argument("--kd-build", default=None, choices=["terrain", "icosphere"])
     a = ap.parse_args(argv)
     d = a.dir or tempfile.mkdtemp(prefix="rtb_prof_")
+    if a.kd_build:
+        return kd_build(rt, workloads, a.kd_build, d, a.reps)
     if a.workload == "sphere_grid":
         path, aa, spp = workloads.write_scene(d, "sphere_grid.json", workloads.sphere_grid_scene()), 1, 1
     elif a.workload == "noisy_icosphere":
@@ -49,6 +57,28 @@ def main(argv=None):
     print(json.dumps({"workload": a.workload, "width": a.width, "height": a.height, "rays": st.rays,
                       "device_ms": st.device_ms}))
     return 0
+
+
+def kd_build(rt, workloads, which, d, reps):
+    import time
+    import numpy as np
+    if which == "terrain":
+        path = workloads.make_terrain(d, n=1024, seed=11)
+    else:
+        path = workloads.make_noisy_icosphere(d, level=6, seed=7)
+    host = rt.HostScene.from_json_file(path)
+    (v, nodes, idx), = host.meshes()
+    ctx = rt.default_context(0)
+    rt.kd_build(v[:1000], ctx=ctx)
+    times = []
+    for _ in range(reps):
+        t = time.perf_counter()
+        n2, i2 = rt.kd_build(v, ctx=ctx)
+        times.append((time.perf_counter() - t) * 1e3)
+    same = n2.tobytes() == nodes.tobytes() and np.array_equal(i2, idx)
+    print(json.dumps({"kd_build": which, "triangles": len(v), "nodes": len(nodes), "leaf_entries": len(idx),
+                      "device_ms": times, "same_as_host": same}))
+    return 0 if same else 1
 
 
 if __name__ == "__main__":
