@@ -619,15 +619,18 @@ std::vector<Tri> load_stl(const std::string& bytes) {
     memcpy(&f, &u, 4);
     return (double)f;
   };
-  size_t off = 84;
-  for (size_t k = 0; k < n; k++) {
-    off += 12;  // facet normal (unused by rendering)
-    for (int i = 0; i < 3; i++) {
-      out[k].v[i] = {f32(off), f32(off + 4), f32(off + 8)};
-      off += 12;
+  // 50-byte facets: normal (unused by rendering), three vertices, attribute
+  auto parse = [&](size_t k0, size_t k1) {
+    for (size_t k = k0; k < k1; k++) {
+      const size_t off = 84 + 50 * k + 12;
+      for (int i = 0; i < 3; i++) out[k].v[i] = {f32(off + 12 * i), f32(off + 12 * i + 4), f32(off + 12 * i + 8)};
     }
-    off += 2;
-  }
+  };
+  const size_t parts = std::min<size_t>(std::max(1u, std::thread::hardware_concurrency()), n / 65536 + 1);
+  std::vector<std::thread> th;
+  for (size_t p = 1; p < parts; p++) th.emplace_back(parse, n * p / parts, n * (p + 1) / parts);
+  parse(0, n / parts);
+  for (auto& t : th) t.join();
   return out;
 }
 
@@ -730,24 +733,37 @@ struct KdBuilder {
 
 void make_mesh(const std::vector<Tri>& tris, HostMesh* m, const KdBuildHook* kd) {
   m->vertices.resize(tris.size() * 9);
-  for (size_t i = 0; i < tris.size(); i++)
-    for (int k = 0; k < 3; k++) {
-      m->vertices[9 * i + 3 * k + 0] = tris[i].v[k].x;
-      m->vertices[9 * i + 3 * k + 1] = tris[i].v[k].y;
-      m->vertices[9 * i + 3 * k + 2] = tris[i].v[k].z;
-    }
   // Mesh::compute_bounds (src/mesh.rs:1017-1033)
   if (tris.empty()) {
     for (int k = 0; k < 3; k++) m->bmin[k] = m->bmax[k] = 0.0;
     return;
   }
+  // the vertex array and the bounds over contiguous ranges on host threads;
+  // the ranges' bounds combine in range order, which is the sequential
+  // fold (rmin/rmax keep the first of equal operands)
+  const size_t n = tris.size();
+  const size_t parts = std::min<size_t>(std::max(1u, std::thread::hardware_concurrency()), n / 65536 + 1);
+  std::vector<double> pmn(3 * parts, INF), pmx(3 * parts, -INF);
+  auto work = [&](size_t p) {
+    for (size_t i = n * p / parts; i < n * (p + 1) / parts; i++)
+      for (int v = 0; v < 3; v++)
+        for (int k = 0; k < 3; k++) {
+          const double c = tris[i].v[v][k];
+          m->vertices[9 * i + 3 * v + k] = c;
+          pmn[3 * p + k] = rmin(pmn[3 * p + k], c);
+          pmx[3 * p + k] = rmax(pmx[3 * p + k], c);
+        }
+  };
+  std::vector<std::thread> th;
+  for (size_t p = 1; p < parts; p++) th.emplace_back(work, p);
+  work(0);
+  for (auto& t : th) t.join();
   double mn[3] = {INF, INF, INF}, mx[3] = {-INF, -INF, -INF};
-  for (auto& t : tris)
-    for (int v = 0; v < 3; v++)
-      for (int k = 0; k < 3; k++) {
-        mn[k] = rmin(mn[k], t.v[v][k]);
-        mx[k] = rmax(mx[k], t.v[v][k]);
-      }
+  for (size_t p = 0; p < parts; p++)
+    for (int k = 0; k < 3; k++) {
+      mn[k] = rmin(mn[k], pmn[3 * p + k]);
+      mx[k] = rmax(mx[k], pmx[3 * p + k]);
+    }
   for (int k = 0; k < 3; k++) { m->bmin[k] = mn[k]; m->bmax[k] = mx[k]; }
   if (kd && kd->build && tris.size() >= kd->min_triangles) {
     std::string e = kd->build(m->vertices.data(), tris.size(), &m->nodes, &m->tri_index);
@@ -904,11 +920,19 @@ bool hex_to_color(const std::string& in, double out[3], std::string* err) {
 }
 
 bool read_text_file(const std::string& path, std::string* out, std::string* err) {
-  std::ifstream f(path, std::ios::binary);
+  std::ifstream f(path, std::ios::binary | std::ios::ate);
   if (!f) {
     *err = "No such file or directory (os error 2): " + path;
     return false;
   }
+  const std::streamoff size = f.tellg();
+  if (size >= 0) {  // one sized read (a 100 MB STL is read once, not copied through a stream)
+    out->resize((size_t)size);
+    f.seekg(0);
+    if (size == 0 || f.read(&(*out)[0], size)) return true;
+  }
+  f.clear();
+  f.seekg(0);
   std::stringstream ss;
   ss << f.rdbuf();
   *out = ss.str();
@@ -1080,7 +1104,7 @@ bool load_scene_json(const std::string& text, const std::string& base_dir, HostS
             for (int b = 0; b < 4; b++) od.transform[4 * a + b] = tm.m[a][b];
         }
       } else {
-        std::vector<Tri> tris = raw[i];
+        std::vector<Tri> tris = std::move(raw[i]);  // each mesh object reads its own file
         if (ht)
           for (auto& tr : tris)
             for (int k = 0; k < 3; k++) tr.v[k] = xform_point(tm, tr.v[k]);
