@@ -324,6 +324,19 @@ const rt_kd_node_desc* rt_kd_tree_nodes(const rt_kd_tree* tree, int64_t* n_nodes
 const int32_t* rt_kd_tree_index(const rt_kd_tree* tree, int64_t* n_index);
 void rt_kd_tree_free(rt_kd_tree* tree);
 
+/* PNG output (Renderer::render_to_file, src/renderer.rs:914-920): an
+ * 8-bit RGB image (width*height*3 bytes, top row first) as a PNG, encoded
+ * on the host's threads (adaptive row filters, the deflate stream cut into
+ * bands compressed in parallel).  The decoded pixels are the image; the
+ * file bytes differ from the reference's encoder.  rt_png_encode returns a
+ * buffer to release with rt_png_free; level is zlib's 0-9 (-1: default).
+ * rt_png_write writes at level 1 and fails with RT_ERR_IO when the file
+ * cannot be written. */
+rt_status rt_png_encode(const uint8_t* rgb, uint32_t width, uint32_t height, int32_t level, uint8_t** out,
+                        size_t* out_len);
+void rt_png_free(uint8_t* buffer);
+rt_status rt_png_write(const char* path, const uint8_t* rgb, uint32_t width, uint32_t height);
+
 /* Bytes rt_scene_upload copied to the device for this scene. */
 rt_status rt_scene_device_bytes(rt_ctx* ctx, const rt_scene* scene, uint64_t* out);
 

@@ -595,19 +595,25 @@ def auto_cameras(path=None, json_text=None):
 
 
 def write_png(path, img):
-    """Writes an (H, W, 3) uint8 array as an 8-bit RGB PNG."""
-    import struct
-    import zlib
+    """Writes an (H, W, 3) uint8 array as an 8-bit RGB PNG (rt_png_write:
+    encoded on the host's threads)."""
     img = np.ascontiguousarray(img, dtype=np.uint8)
     h, w, _ = img.shape
-    raw = np.zeros((h, 1 + 3 * w), np.uint8)
-    raw[:, 1:] = img.reshape(h, 3 * w)
+    st = _capi.lib().rt_png_write(str(path).encode(), img.ctypes.data, w, h)
+    if st != _capi.RT_OK:
+        raise OSError("cannot write %s (%s)" % (path, _capi.STATUS_NAMES.get(st, st)))
 
-    def chunk(tag, data):
-        c = struct.pack(">I", len(data)) + tag + data
-        return c + struct.pack(">I", zlib.crc32(tag + data) & 0xFFFFFFFF)
 
-    png = b"\x89PNG\r\n\x1a\n" + chunk(b"IHDR", struct.pack(">IIBBBBB", w, h, 8, 2, 0, 0, 0))
-    png += chunk(b"IDAT", zlib.compress(raw.tobytes(), 6)) + chunk(b"IEND", b"")
-    with open(path, "wb") as f:
-        f.write(png)
+def encode_png(img, level=-1):
+    """rt_png_encode: the PNG file bytes of an (H, W, 3) uint8 array."""
+    img = np.ascontiguousarray(img, dtype=np.uint8)
+    h, w, _ = img.shape
+    L = _capi.lib()
+    buf, n = ctypes.c_void_p(), ctypes.c_size_t()
+    st = L.rt_png_encode(img.ctypes.data, w, h, int(level), ctypes.byref(buf), ctypes.byref(n))
+    if st != _capi.RT_OK:
+        raise ValueError("PNG encoding failed (%s)" % _capi.STATUS_NAMES.get(st, st))
+    try:
+        return ctypes.string_at(buf, n.value)
+    finally:
+        L.rt_png_free(buf)

@@ -225,6 +225,10 @@ def lib():
                                                     _vp, _vp, _vp, _vp, ctypes.POINTER(rt_outline_config), _vp]),
         "rt_debug_stdrng_u32": (ctypes.c_int, [_vp, _vp, ctypes.c_int64, ctypes.c_int32, _vp]),
         "rt_debug_disk_offsets": (ctypes.c_int, [_vp, _vp, ctypes.c_int64, ctypes.c_double, _vp]),
+        "rt_png_encode": (ctypes.c_int, [_vp, ctypes.c_uint32, ctypes.c_uint32, ctypes.c_int32,
+                                         ctypes.POINTER(_vp), ctypes.POINTER(ctypes.c_size_t)]),
+        "rt_png_free": (None, [_vp]),
+        "rt_png_write": (ctypes.c_int, [ctypes.c_char_p, _vp, ctypes.c_uint32, ctypes.c_uint32]),
         "rt_debug_mesh_prep": (ctypes.c_int, [_vp, ctypes.POINTER(rt_mesh_desc), ctypes.POINTER(ctypes.c_uint32)]),
         "rt_debug_mesh_hit": (ctypes.c_int, [_vp, _vp, ctypes.c_int32, ctypes.c_int32, _vp, ctypes.c_int64,
                                              ctypes.c_double, ctypes.c_double, _vp]),

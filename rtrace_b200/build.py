@@ -71,7 +71,7 @@ def build(force=False, verbose=False):
         objs.append(obj)
     tmp = LIB + ".tmp"
     cmd = [nvcc, "-shared", "-gencode", "arch=compute_100a,code=sm_100a", "-o", tmp, *objs,
-           "-Xcompiler", "-fPIC"]
+           "-Xcompiler", "-fPIC", "-lz"]
     r = subprocess.run(cmd, capture_output=True, text=True)
     if r.returncode != 0:
         raise RuntimeError("link failed: %s\n%s%s" % (" ".join(cmd), r.stdout, r.stderr))

@@ -4,7 +4,6 @@ import json
 import math
 import os
 import struct
-import zlib
 
 import numpy as np
 import pytest
@@ -32,10 +31,8 @@ def test_png_writer_roundtrip(tmp_path):
     assert data[:8] == b"\x89PNG\r\n\x1a\n"
     w, h = struct.unpack(">II", data[16:24])
     assert (w, h) == (7, 5)
-    i = data.index(b"IDAT")
-    n = struct.unpack(">I", data[i - 4:i])[0]
-    raw = np.frombuffer(zlib.decompress(data[i + 4:i + 4 + n]), np.uint8).reshape(5, 1 + 21)
-    assert (raw[:, 0] == 0).all() and np.array_equal(raw[:, 1:].reshape(5, 7, 3), img)
+    from tests.test_png import decode_png
+    assert np.array_equal(decode_png(data), img)
 
 
 def test_workload_scenes_parse_in_oracle(tmp_path):
