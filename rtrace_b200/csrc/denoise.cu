@@ -109,11 +109,12 @@ constexpr int TILE_M = 128;
 constexpr int TMEM_COLS = 32;  // >= COUT, power of two >= 32
 constexpr int MAX_DIL = 64;    // 128 + 2 * dilation pixels must fit one TMA box (<= 256)
 
-// Shared memory of one CTA: NSTAGE input halos of a tile (3 rows of
-// TILE_M + 2 * dil pixels, one block of 16-byte rows per 8 channels), the
+// Shared memory of one CTA: a ring of NROW staged input rows (TILE_M +
+// 2 * dil pixels each, one block of 16-byte rows per 8 channels), the
 // weights, the pipeline's mbarriers, the TMEM address and an abort flag.
-constexpr int NSTAGE = 2;  // halo stages (TMA -> MMA)
+constexpr int NROW = 6;    // staged input rows (TMA -> MMA); a step reads 3
 constexpr int NACC = 2;    // TMEM accumulators (MMA -> epilogue)
+constexpr int SEG = 32;    // output rows a CTA walks down one column at a time
 constexpr int CONV_THREADS = 192;  // warps 0-3 epilogue, warp 4 TMA, warp 5 MMA
 __host__ __device__ constexpr int halo_px(int dil) { return TILE_M + 2 * dil; }
 __host__ __device__ constexpr int halo_block(int dil) { return ((halo_px(dil) * 16 + 127) / 128) * 128; }
@@ -121,12 +122,37 @@ template <int CIN, int COUT>
 struct ConvSmem {
   static constexpr int CPT = CIN / 8;                     // 16-byte channel chunks per pixel
   static constexpr int B_BYTES = 9 * CPT * COUT * 16;     // weights
-  static constexpr int TAIL = 128;                        // barriers, TMEM slot, abort flag
+  static constexpr int TAIL = 256;                        // barriers, TMEM slot, abort flag
+  static_assert(8 * (2 * NROW + 2 * NACC) + 8 <= TAIL, "the mbarriers, TMEM slot and abort flag overflow TAIL");
   static constexpr int BIAS = 128;                        // COUT floats
   static constexpr int OUT = 4 * 32 * COUT * 2;           // epilogue staging: 32 pixels per warp
-  static int a_bytes(int dil) { return 3 * CPT * halo_block(dil); }
-  static int total(int dil) { return 1024 + NSTAGE * a_bytes(dil) + B_BYTES + TAIL + BIAS + OUT; }
+  static int row_bytes(int dil) { return CPT * halo_block(dil); }
+  static int total(int dil) { return 1024 + NROW * row_bytes(dil) + B_BYTES + TAIL + BIAS + OUT; }
 };
+
+// Work of the convolution: segments of up to SEG output rows of one column
+// (plane p, 128-pixel tile tx, rows y = r, r + dil, r + 2 dil, ... of one
+// residue r mod dil).  Output row y reads input rows y - dil, y, y + dil,
+// so consecutive rows of a column share two of their three input rows: a
+// segment of L rows stages L + 2 input rows instead of 3L.
+struct ConvSeg {
+  int p, tx, r, k0, L;  // rows y = r + (k0 + t) * dil for t < L
+};
+__device__ __forceinline__ int conv_col_segs(int H, int dil) { return ((H + dil - 1) / dil + SEG - 1) / SEG; }
+__device__ __forceinline__ ConvSeg conv_seg(long long g, int H, int dil, int tiles_x) {
+  const int nseg = conv_col_segs(H, dil);
+  ConvSeg c;
+  const int q = (int)(g % nseg);
+  long long col = g / nseg;
+  c.r = (int)(col % dil);
+  col /= dil;
+  c.tx = (int)(col % tiles_x);
+  c.p = (int)(col / tiles_x);
+  c.k0 = q * SEG;
+  const int rows = (H - c.r + dil - 1) / dil;  // rows of residue r below H
+  c.L = max(0, min(SEG, rows - c.k0));
+  return c;
+}
 
 __device__ __forceinline__ void tma_load_4d(uint32_t dst, const CUtensorMap* map, int c0, int c1, int c2, int c3,
                                             uint32_t mbar) {
@@ -148,17 +174,20 @@ __device__ __forceinline__ void mbar_arrive(uint32_t mbar) {
 // MODE 0: ReLU, FP16 output [plane][H][W][COUT].  MODE 2: sigmoid of the
 // first DN_MAX_SLOTS channels, float output [plane][slot][H][W].
 //
-// Tiles are 128-pixel runs of one row; the CTA walks tiles blockIdx.x,
-// blockIdx.x + gridDim.x, ... with three roles working on different tiles:
-//   warp 4 (TMA): loads tile i's halo into stage i % NSTAGE with 3 * CIN / 8
-//     boxes (8 channels x halo_px pixels of one row; the hardware zero-fills
-//     outside the image and the plane), once the MMAs of tile i - NSTAGE
-//     have released the stage;
-//   warp 5 (MMA): once the halo has landed and the epilogue has drained
+// A step is one 128-pixel run of one output row; the CTA walks segments
+// blockIdx.x, blockIdx.x + gridDim.x, ... (see ConvSeg), a segment's steps
+// down its column, with three roles working on different steps:
+//   warp 4 (TMA): loads input row j (count over the CTA's whole walk) into
+//     ring slot j % NROW with CIN / 8 boxes (8 channels x halo_px pixels of
+//     one row; the hardware zero-fills outside the image and the plane),
+//     once the MMAs of row j - NROW's last step have released the slot;
+//   warp 5 (MMA): for step t of a segment whose first row is j0, once rows
+//     j0 + t .. j0 + t + 2 have landed and the epilogue has drained
 //     accumulator i % NACC, issues the 9 * CIN / 16 MMAs; tap (ky, kx) reads
-//     row ky's block from pixel kx * dil on (same staged data, descriptor
-//     start kx * dil * 16 bytes further); commits to the stage's "empty" and
-//     the accumulator's "full" barriers;
+//     row j0 + t + ky's slot from pixel kx * dil on (descriptor start
+//     kx * dil * 16 bytes further); commits to the accumulator's "full"
+//     barrier and to the "empty" barrier of row j0 + t (and, at a
+//     segment's last step, of its last two rows), each row's last use;
 //   warps 0-3 (epilogue): thread t reads accumulator row t (tcgen05.ld
 //     32x32b), releases the accumulator, adds the bias, applies the
 //     activation and stores.
@@ -179,28 +208,28 @@ __global__ void __launch_bounds__(CONV_THREADS) k_conv3x3_tc(const __grid_consta
   uint32_t pad = (1024u - (raw & 1023u)) & 1023u;
   unsigned char* base = smem_raw + pad;
   const int BLK = halo_block(dil);
-  const int A_BYTES = 3 * CPT * BLK;
-  const uint32_t sA = raw + pad;  // stage k at sA + k * A_BYTES
-  const uint32_t sB = sA + NSTAGE * A_BYTES;
-  unsigned char* tail = base + NSTAGE * A_BYTES + SM::B_BYTES;
-  const uint32_t bar0 = smem_u32(tail);  // full[NSTAGE], empty[NSTAGE], accf[NACC], acce[NACC]
+  const int ROWB = CPT * BLK;
+  const uint32_t sA = raw + pad;  // ring slot k at sA + k * ROWB
+  const uint32_t sB = sA + NROW * ROWB;
+  unsigned char* tail = base + NROW * ROWB + SM::B_BYTES;
+  const uint32_t bar0 = smem_u32(tail);  // full[NROW], empty[NROW], accf[NACC], acce[NACC]
   auto full_bar = [&](int k) { return bar0 + 8u * k; };
-  auto empty_bar = [&](int k) { return bar0 + 8u * (NSTAGE + k); };
-  auto accf_bar = [&](int k) { return bar0 + 8u * (2 * NSTAGE + k); };
-  auto acce_bar = [&](int k) { return bar0 + 8u * (2 * NSTAGE + NACC + k); };
-  uint32_t* tslot = reinterpret_cast<uint32_t*>(tail + 8 * (2 * NSTAGE + 2 * NACC));
-  volatile int* abort_flag = reinterpret_cast<volatile int*>(tail + 8 * (2 * NSTAGE + 2 * NACC) + 4);
+  auto empty_bar = [&](int k) { return bar0 + 8u * (NROW + k); };
+  auto accf_bar = [&](int k) { return bar0 + 8u * (2 * NROW + k); };
+  auto acce_bar = [&](int k) { return bar0 + 8u * (2 * NROW + NACC + k); };
+  uint32_t* tslot = reinterpret_cast<uint32_t*>(tail + 8 * (2 * NROW + 2 * NACC));
+  volatile int* abort_flag = reinterpret_cast<volatile int*>(tail + 8 * (2 * NROW + 2 * NACC) + 4);
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
 
   float* s_bias = reinterpret_cast<float*>(tail + SM::TAIL);
   unsigned char* s_out = tail + SM::TAIL + SM::BIAS;  // 4 warps x 32 pixels x COUT halves
   {
-    uint4* dst = reinterpret_cast<uint4*>(base + NSTAGE * A_BYTES);
+    uint4* dst = reinterpret_cast<uint4*>(base + NROW * ROWB);
     for (int i = tid; i < SM::B_BYTES / 16; i += CONV_THREADS) dst[i] = wl[i];
     for (int i = tid; i < COUT; i += CONV_THREADS) s_bias[i] = bias[i];
   }
   if (tid == 0) {
-    for (int k = 0; k < NSTAGE; k++) {
+    for (int k = 0; k < NROW; k++) {
       asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(full_bar(k)) : "memory");
       asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(empty_bar(k)) : "memory");
     }
@@ -225,145 +254,163 @@ __global__ void __launch_bounds__(CONV_THREADS) k_conv3x3_tc(const __grid_consta
   asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
   const uint32_t tmem = *tslot;
   constexpr uint32_t IDESC = umma_idesc(TILE_M, COUT);
-  const uint32_t tx_bytes = (uint32_t)(3 * CPT * halo_px(dil) * 16);
+  const uint32_t tx_bytes = (uint32_t)(CPT * halo_px(dil) * 16);  // one staged row
   const int tiles_x = (W + TILE_M - 1) / TILE_M;
-  const long long ntiles = (long long)planes * H * tiles_x;
+  const long long nsegs = (long long)planes * tiles_x * dil * conv_col_segs(H, dil);
   auto fail = [&]() {
     if (!*abort_flag) atomicOr(err, DN_ERR_WAIT);
     *abort_flag = 1;
   };
 
   if (warp == 4) {
-    // ---- TMA producer
+    // ---- TMA producer: the rows of each segment, r + (k0 - 1 + j) * dil
     if (lane == 0) {
       long long issued = 0;
-      for (long long tile = blockIdx.x; tile < ntiles && !*abort_flag; tile += gridDim.x, issued++) {
-        const int s = (int)(issued % NSTAGE);
-        const uint32_t ph = (uint32_t)((issued / NSTAGE) & 1);
-        if (!mbar_wait(empty_bar(s), ph ^ 1u)) {
-          fail();
-          break;
+      bool stop = false;
+      for (long long g = blockIdx.x; g < nsegs && !stop; g += gridDim.x) {
+        const ConvSeg c = conv_seg(g, H, dil, tiles_x);
+        for (int j = 0; j < (c.L > 0 ? c.L + 2 : 0); j++, issued++) {
+          const int k = (int)(issued % NROW);
+          if (*abort_flag || !mbar_wait(empty_bar(k), (uint32_t)((issued / NROW) & 1) ^ 1u)) {
+            fail();
+            stop = true;
+            break;
+          }
+          mbar_expect_tx(full_bar(k), tx_bytes);
+          const uint32_t st = sA + (uint32_t)(k * ROWB);
+          const int y = c.r + (c.k0 - 1 + j) * dil;
+          for (int cc = 0; cc < CPT; cc++)
+            tma_load_4d(st + (uint32_t)(cc * BLK), &in_map, 8 * cc, c.tx * TILE_M - dil, y, c.p, full_bar(k));
         }
-        const int tx = (int)(tile % tiles_x);
-        const long long py = tile / tiles_x;
-        const int y = (int)(py % H), p = (int)(py / H), x0 = tx * TILE_M;
-        mbar_expect_tx(full_bar(s), tx_bytes);
-        const uint32_t st = sA + (uint32_t)(s * A_BYTES);
-        for (int ky = 0; ky < 3; ky++)
-          for (int j = 0; j < CPT; j++)
-            tma_load_4d(st + (uint32_t)((ky * CPT + j) * BLK), &in_map, 8 * j, x0 - dil, y + (ky - 1) * dil, p,
-                        full_bar(s));
       }
       if (*abort_flag) {
-        // let the last NSTAGE loads land before the CTA's shared memory goes away
-        for (long long k = issued - NSTAGE; k < issued; k++)
-          if (k >= 0) mbar_wait(full_bar((int)(k % NSTAGE)), (uint32_t)((k / NSTAGE) & 1));
+        // let the last loads land before the CTA's shared memory goes away
+        for (long long k = issued - NROW; k < issued; k++)
+          if (k >= 0) mbar_wait(full_bar((int)(k % NROW)), (uint32_t)((k / NROW) & 1));
       }
     }
   } else if (warp == 5) {
     // ---- MMA issuer
     if (lane == 0) {
-      long long i = 0;
-      for (long long tile = blockIdx.x; tile < ntiles && !*abort_flag; tile += gridDim.x, i++) {
-        const int s = (int)(i % NSTAGE), a = (int)(i % NACC);
-        if (!mbar_wait(full_bar(s), (uint32_t)((i / NSTAGE) & 1)) ||
-            !mbar_wait(acce_bar(a), (uint32_t)((i / NACC) & 1) ^ 1u)) {
-          fail();
-          break;
-        }
-        asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-        const uint32_t st = sA + (uint32_t)(s * A_BYTES);
-        const uint32_t acc = tmem + (uint32_t)(a * TMEM_COLS);
-#pragma unroll
-        for (int t = 0; t < 9; t++) {
-          const int ky = t / 3, kx = t % 3;
-#pragma unroll
-          for (int s2 = 0; s2 < CIN / 16; s2++) {
-            uint64_t da = umma_desc(st + (uint32_t)((ky * CPT + 2 * s2) * BLK + kx * dil * 16), (uint32_t)BLK, 128);
-            uint64_t db = umma_desc(sB + (uint32_t)((t * CPT + 2 * s2) * COUT * 16), COUT * 16, 128);
-            mma_f16(acc, da, db, IDESC, (t > 0 || s2 > 0) ? 1u : 0u);
+      long long i = 0, j0 = 0;  // steps issued; the segment's first row
+      bool stop = false;
+      for (long long g = blockIdx.x; g < nsegs && !stop; g += gridDim.x) {
+        const ConvSeg c = conv_seg(g, H, dil, tiles_x);
+        if (c.L <= 0) continue;
+        for (int t = 0; t < c.L; t++, i++) {
+          const int a = (int)(i % NACC);
+          bool ok = !*abort_flag;
+          for (int ky = 0; ky < 3 && ok; ky++) {
+            const long long j = j0 + t + ky;
+            ok = mbar_wait(full_bar((int)(j % NROW)), (uint32_t)((j / NROW) & 1));
           }
+          if (!ok || !mbar_wait(acce_bar(a), (uint32_t)((i / NACC) & 1) ^ 1u)) {
+            fail();
+            stop = true;
+            break;
+          }
+          asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+          const uint32_t acc = tmem + (uint32_t)(a * TMEM_COLS);
+#pragma unroll
+          for (int tap = 0; tap < 9; tap++) {
+            const int ky = tap / 3, kx = tap % 3;
+            const uint32_t row = sA + (uint32_t)(((j0 + t + ky) % NROW) * ROWB);
+#pragma unroll
+            for (int s2 = 0; s2 < CIN / 16; s2++) {
+              uint64_t da = umma_desc(row + (uint32_t)(2 * s2 * BLK + kx * dil * 16), (uint32_t)BLK, 128);
+              uint64_t db = umma_desc(sB + (uint32_t)((tap * CPT + 2 * s2) * COUT * 16), COUT * 16, 128);
+              mma_f16(acc, da, db, IDESC, (tap > 0 || s2 > 0) ? 1u : 0u);
+            }
+          }
+          mma_commit(empty_bar((int)((j0 + t) % NROW)));
+          if (t == c.L - 1) {
+            mma_commit(empty_bar((int)((j0 + t + 1) % NROW)));
+            mma_commit(empty_bar((int)((j0 + t + 2) % NROW)));
+          }
+          mma_commit(accf_bar(a));
         }
-        mma_commit(empty_bar(s));
-        mma_commit(accf_bar(a));
+        j0 += c.L + 2;
       }
       if (*abort_flag && i > 0) mbar_wait(accf_bar((int)((i - 1) % NACC)), (uint32_t)(((i - 1) / NACC) & 1));
     }
   } else {
     // ---- epilogue (warps 0-3: thread tid <-> TMEM lane tid <-> pixel x0 + tid)
     long long i = 0;
-    for (long long tile = blockIdx.x; tile < ntiles; tile += gridDim.x, i++) {
-      const int a = (int)(i % NACC);
-      bool ok = true;
-      for (long long k = 0; k < kWaitLimit; k++) {
-        uint32_t done;
-        asm volatile(
-            "{\n\t.reg .pred p;\n\t"
-            "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
-            "selp.u32 %0, 1, 0, p;\n\t"
-            "}\n"
-            : "=r"(done)
-            : "r"(accf_bar(a)), "r"((uint32_t)((i / NACC) & 1))
-            : "memory");
-        if (done) break;
-        if (*abort_flag || k + 1 == kWaitLimit) {
-          ok = false;
+    bool stop = false;
+    for (long long g = blockIdx.x; g < nsegs && !stop; g += gridDim.x) {
+      const ConvSeg c = conv_seg(g, H, dil, tiles_x);
+      for (int t = 0; t < c.L; t++, i++) {
+        const int a = (int)(i % NACC);
+        bool ok = true;
+        for (long long k = 0; k < kWaitLimit; k++) {
+          uint32_t done;
+          asm volatile(
+              "{\n\t.reg .pred p;\n\t"
+              "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+              "selp.u32 %0, 1, 0, p;\n\t"
+              "}\n"
+              : "=r"(done)
+              : "r"(accf_bar(a)), "r"((uint32_t)((i / NACC) & 1))
+              : "memory");
+          if (done) break;
+          if (*abort_flag || k + 1 == kWaitLimit) {
+            ok = false;
+            break;
+          }
+        }
+        // the four warps agree before the warp-collective TMEM load
+        if (__any_sync(0xffffffffu, !ok)) ok = false;
+        if (!ok) {
+          if (lane == 0) fail();
+          stop = true;
           break;
         }
-      }
-      // the four warps agree before the warp-collective TMEM load
-      if (__any_sync(0xffffffffu, !ok)) ok = false;
-      if (!ok) {
-        if (lane == 0) fail();
-        break;
-      }
-      asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-      uint32_t accv[COUT];
-      tmem_ld<COUT>(tmem + (uint32_t)(a * TMEM_COLS) + ((uint32_t)(warp * 32) << 16), accv);
-      asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
-      asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
-      if (lane == 0) mbar_arrive(acce_bar(a));
-      const int tx = (int)(tile % tiles_x);
-      const long long py = tile / tiles_x;
-      const int y = (int)(py % H), p = (int)(py / H);
-      const int x = tx * TILE_M + tid;
-      if (MODE == 0) {
-        // Each warp stages its 32 pixels (COUT halves each) in shared
-        // memory, 16-byte chunks XOR-swizzled so that both the writes and
-        // the read-back are free of bank conflicts, then writes them out as
-        // contiguous 512-byte rows (the 32 pixels are contiguous in NHWC).
-        constexpr int CPX = COUT / 8;            // 16-byte chunks per pixel
-        constexpr int ROWB = COUT * 2;           // bytes per pixel
-        constexpr int PPL = 128 / ROWB;          // pixels per 128-byte bank window
-        unsigned char* wb = s_out + warp * 32 * ROWB;
-#pragma unroll
-        for (int c = 0; c < CPX; c++) {
-          __align__(16) __half h[8];
-#pragma unroll
-          for (int e = 0; e < 8; e++) {
-            float v = __uint_as_float(accv[8 * c + e]) + s_bias[8 * c + e];
-            h[e] = __float2half_rn(v > 0.f ? v : 0.f);
+        asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+        uint32_t accv[COUT];
+        tmem_ld<COUT>(tmem + (uint32_t)(a * TMEM_COLS) + ((uint32_t)(warp * 32) << 16), accv);
+        asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+        asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+        if (lane == 0) mbar_arrive(acce_bar(a));
+        const int tx = c.tx, p = c.p, y = c.r + (c.k0 + t) * dil;
+        const int x = tx * TILE_M + tid;
+        if (MODE == 0) {
+          // Each warp stages its 32 pixels (COUT halves each) in shared
+          // memory, 16-byte chunks XOR-swizzled so that both the writes and
+          // the read-back are free of bank conflicts, then writes them out as
+          // contiguous 512-byte rows (the 32 pixels are contiguous in NHWC).
+          constexpr int CPX = COUT / 8;            // 16-byte chunks per pixel
+          constexpr int ROWB = COUT * 2;           // bytes per pixel
+          constexpr int PPL = 128 / ROWB;          // pixels per 128-byte bank window
+          unsigned char* wb = s_out + warp * 32 * ROWB;
+  #pragma unroll
+          for (int c = 0; c < CPX; c++) {
+            __align__(16) __half h[8];
+  #pragma unroll
+            for (int e = 0; e < 8; e++) {
+              float v = __uint_as_float(accv[8 * c + e]) + s_bias[8 * c + e];
+              h[e] = __float2half_rn(v > 0.f ? v : 0.f);
+            }
+            const int phys = c ^ ((lane / PPL) & (CPX - 1));
+            *reinterpret_cast<uint4*>(wb + lane * ROWB + phys * 16) = *reinterpret_cast<const uint4*>(h);
           }
-          const int phys = c ^ ((lane / PPL) & (CPX - 1));
-          *reinterpret_cast<uint4*>(wb + lane * ROWB + phys * 16) = *reinterpret_cast<const uint4*>(h);
-        }
-        __syncwarp();
-        const int xw = tx * TILE_M + warp * 32;  // the warp's first pixel
-        __half* ow = out + (((long long)p * H + y) * (long long)W + xw) * COUT;
-#pragma unroll
-        for (int k = 0; k < CPX; k++) {
-          const int o = k * 512 + lane * 16;  // byte offset in the warp's 32 * ROWB bytes
-          const int px = o / ROWB, ch = (o % ROWB) / 16;
-          const int phys = ch ^ ((px / PPL) & (CPX - 1));
-          const uint4 v = *reinterpret_cast<const uint4*>(wb + px * ROWB + phys * 16);
-          if (xw + px < W) *reinterpret_cast<uint4*>(reinterpret_cast<unsigned char*>(ow) + o) = v;
-        }
-        __syncwarp();
-      } else if (x < W) {
-#pragma unroll
-        for (int j = 0; j < DN_MAX_SLOTS; j++) {
-          float v = __uint_as_float(accv[j]) + s_bias[j];
-          vis[(((long long)p * DN_MAX_SLOTS + j) * H + y) * (long long)W + x] = 1.f / (1.f + __expf(-v));
+          __syncwarp();
+          const int xw = tx * TILE_M + warp * 32;  // the warp's first pixel
+          __half* ow = out + (((long long)p * H + y) * (long long)W + xw) * COUT;
+  #pragma unroll
+          for (int k = 0; k < CPX; k++) {
+            const int o = k * 512 + lane * 16;  // byte offset in the warp's 32 * ROWB bytes
+            const int px = o / ROWB, ch = (o % ROWB) / 16;
+            const int phys = ch ^ ((px / PPL) & (CPX - 1));
+            const uint4 v = *reinterpret_cast<const uint4*>(wb + px * ROWB + phys * 16);
+            if (xw + px < W) *reinterpret_cast<uint4*>(reinterpret_cast<unsigned char*>(ow) + o) = v;
+          }
+          __syncwarp();
+        } else if (x < W) {
+  #pragma unroll
+          for (int j = 0; j < DN_MAX_SLOTS; j++) {
+            float v = __uint_as_float(accv[j]) + s_bias[j];
+            vis[(((long long)p * DN_MAX_SLOTS + j) * H + y) * (long long)W + x] = 1.f / (1.f + __expf(-v));
+          }
         }
       }
     }
@@ -431,8 +478,9 @@ cudaError_t launch_conv(const __half* in, int planes, int H, int W, int dil, con
   // persistent grid: 4 CTAs per SM (each holds 64 of the SM's 512 TMEM
   // columns; shared memory allows 2-6 resident); CTAs beyond the resident
   // ones start as others finish
-  long long ntiles = (long long)planes * H * ((W + TILE_M - 1) / TILE_M);
-  long long grid = std::min<long long>(ntiles, (long long)num_sms * 4);
+  const long long rows_per_col = (H + dil - 1) / dil;
+  const long long nsegs = (long long)planes * ((W + TILE_M - 1) / TILE_M) * dil * ((rows_per_col + SEG - 1) / SEG);
+  long long grid = std::min<long long>(nsegs, (long long)num_sms * 4);
   if (grid < 1) grid = 1;
   k_conv3x3_tc<CIN, COUT, MODE><<<(int)grid, CONV_THREADS, smem, s>>>(map, planes, H, W, dil, (const uint4*)w, b,
                                                                       out, vis, err);
