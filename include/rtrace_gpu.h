@@ -492,8 +492,10 @@ rt_status rt_debug_fp64_rate(rt_ctx* ctx, double* gops);
 rt_status rt_debug_mesh_hit(rt_ctx* ctx, const rt_scene* scene, int32_t object_index, int32_t use_kdtree,
                             const double* rays, int64_t n, double t_min, double t_max, double* out);
 /* Prepares a mesh description's device search data on the host and on
- * the device (the path uploads take for meshes of 16,384 triangles or
- * more) and compares them: bit k of *mismatch is set when array k differs
+ * the device (the path uploads take for meshes of 262,144 triangles or
+ * more; the host preparation of smaller meshes builds its BVH with a
+ * binned SAH instead, so the host side here uses the device's median
+ * split) and compares them: bit k of *mismatch is set when array k differs
  * (0 BVH, 1 records in BVH order, 2 records in mesh order, 3 normals,
  * 4 k-d occurrences, 5 occurrence offsets).  More than 8 triangles. */
 rt_status rt_debug_mesh_prep(rt_ctx* ctx, const rt_mesh_desc* mesh, uint32_t* mismatch);

@@ -1,5 +1,6 @@
-// Binary BVH build: top-down, split at the median centroid of the widest
-// centroid axis, leaves of at most `leaf_size` primitives.
+// Binary BVH builds: top-down, split at the median centroid of the widest
+// centroid axis (build_bvh) or at the binned surface-area optimum
+// (build_bvh_sah); leaves of at most `leaf_size` primitives.
 #include "bvh_build.hpp"
 
 #include <algorithm>
@@ -130,6 +131,137 @@ struct Builder {
   }
 };
 
+
+// Binned SAH build: 16 centroid bins per axis; a node splits at the bin
+// boundary with the smallest (left area x count + right area x count), the
+// first such on axis x, y, z in that order; a node whose centroids cannot
+// be binned apart splits at its median primitive id.  Leaves hold at most
+// `leaf` primitives.  The split sets depend only on the primitives, never
+// on their order, so the tree is deterministic.
+struct SahBuilder {
+  int leaf;
+  double pad;
+  static double area(const double mn[3], const double mx[3]) {
+    const double dx = mx[0] - mn[0], dy = mx[1] - mn[1], dz = mx[2] - mn[2];
+    return dx * dy + dy * dz + dz * dx;
+  }
+  static void bounds(const Prim* p, int n, double mn[3], double mx[3]) {
+    const double inf = std::numeric_limits<double>::infinity();
+    for (int k = 0; k < 3; k++) { mn[k] = inf; mx[k] = -inf; }
+    for (int i = 0; i < n; i++)
+      for (int k = 0; k < 3; k++) {
+        mn[k] = std::min(mn[k], p[i].lo[k]);
+        mx[k] = std::max(mx[k], p[i].hi[k]);
+      }
+  }
+  // Subtree over p[0, n) appended to out in preorder (node, left subtree,
+  // right subtree); returns its reference (node index in out, 0) or, for a
+  // leaf, (first primitive, count).
+  std::pair<int32_t, int32_t> build(Prim* p, int n, int32_t base, std::vector<BvhNode>& out, int depth) {
+    if (n <= leaf) return {base, n};
+    const double inf = std::numeric_limits<double>::infinity();
+    double cmin[3] = {inf, inf, inf}, cmax[3] = {-inf, -inf, -inf};
+    for (int i = 0; i < n; i++)
+      for (int k = 0; k < 3; k++) {
+        cmin[k] = std::min(cmin[k], p[i].c[k]);
+        cmax[k] = std::max(cmax[k], p[i].c[k]);
+      }
+    constexpr int B = 16;
+    double best = inf;
+    int best_axis = -1, best_b = -1;
+    for (int a = 0; a < 3; a++) {
+      const double ext = cmax[a] - cmin[a];
+      if (!(ext > 0)) continue;
+      int cnt[B] = {};
+      double bmn[B][3], bmx[B][3];
+      for (int b = 0; b < B; b++)
+        for (int k = 0; k < 3; k++) { bmn[b][k] = inf; bmx[b][k] = -inf; }
+      for (int i = 0; i < n; i++) {
+        const int b = std::min(std::max((int)((p[i].c[a] - cmin[a]) / ext * B), 0), B - 1);
+        cnt[b]++;
+        for (int k = 0; k < 3; k++) {
+          bmn[b][k] = std::min(bmn[b][k], p[i].lo[k]);
+          bmx[b][k] = std::max(bmx[b][k], p[i].hi[k]);
+        }
+      }
+      double rmn[B][3], rmx[B][3];
+      int rc[B] = {};
+      double mn[3] = {inf, inf, inf}, mx[3] = {-inf, -inf, -inf};
+      int c = 0;
+      for (int b = B - 1; b > 0; b--) {
+        for (int k = 0; k < 3; k++) { mn[k] = std::min(mn[k], bmn[b][k]); mx[k] = std::max(mx[k], bmx[b][k]); }
+        c += cnt[b];
+        for (int k = 0; k < 3; k++) { rmn[b][k] = mn[k]; rmx[b][k] = mx[k]; }
+        rc[b] = c;
+      }
+      for (int k = 0; k < 3; k++) { mn[k] = inf; mx[k] = -inf; }
+      c = 0;
+      for (int b = 0; b < B - 1; b++) {
+        for (int k = 0; k < 3; k++) { mn[k] = std::min(mn[k], bmn[b][k]); mx[k] = std::max(mx[k], bmx[b][k]); }
+        c += cnt[b];
+        if (c == 0 || rc[b + 1] == 0) continue;
+        const double cost = area(mn, mx) * c + area(rmn[b + 1], rmx[b + 1]) * rc[b + 1];
+        if (cost < best) {
+          best = cost;
+          best_axis = a;
+          best_b = b;
+        }
+      }
+    }
+    int mid;
+    if (best_axis >= 0) {
+      const int a = best_axis;
+      const double ext = cmax[a] - cmin[a];
+      mid = (int)(std::partition(p, p + n, [&](const Prim& q) {
+                    return std::min(std::max((int)((q.c[a] - cmin[a]) / ext * B), 0), B - 1) <= best_b;
+                  }) - p);
+    } else {
+      mid = n / 2;
+      std::nth_element(p, p + mid, p + n, [](const Prim& x, const Prim& y) { return x.id < y.id; });
+    }
+    const int32_t me = (int32_t)out.size();
+    out.emplace_back();
+    BvhNode nd{};
+    bounds(p, mid, nd.lmin, nd.lmax);
+    bounds(p + mid, n - mid, nd.rmin, nd.rmax);
+    for (int k = 0; k < 3; k++) {
+      nd.lmin[k] -= pad;
+      nd.lmax[k] += pad;
+      nd.rmin[k] -= pad;
+      nd.rmax[k] += pad;
+    }
+    std::pair<int32_t, int32_t> l, r;
+    if (n >= kParallelMin && depth < kParallelDepth) {
+      // both subtrees on threads into their own lists, appended left then
+      // right: the sequential build's preorder
+      std::vector<BvhNode> lo, ro;
+      auto fut = std::async(std::launch::async, [&] { return build(p, mid, base, lo, depth + 1); });
+      r = build(p + mid, n - mid, base + mid, ro, depth + 1);
+      l = fut.get();
+      auto append = [&](std::vector<BvhNode>& sub, std::pair<int32_t, int32_t>& ref) {
+        const int32_t off = (int32_t)out.size();
+        for (BvhNode& c : sub) {
+          if (c.lcnt == 0) c.lidx += off;
+          if (c.rcnt == 0) c.ridx += off;
+          out.push_back(c);
+        }
+        if (ref.second == 0) ref.first += off;
+      };
+      append(lo, l);
+      append(ro, r);
+    } else {
+      l = build(p, mid, base, out, depth + 1);
+      r = build(p + mid, n - mid, base + mid, out, depth + 1);
+    }
+    nd.lidx = l.first;
+    nd.lcnt = l.second;
+    nd.ridx = r.first;
+    nd.rcnt = r.second;
+    out[me] = nd;
+    return {me, 0};
+  }
+};
+
 }  // namespace
 
 void build_bvh(const std::vector<double>& bmin, const std::vector<double>& bmax, int leaf_size, double pad,
@@ -171,6 +303,33 @@ void build_bvh(const std::vector<double>& bmin, const std::vector<double>& bmax,
   for (size_t i = 0; i < n; i++) (*order)[i] = prims[i].id;
   // each leaf's primitives in id order: a canonical layout (the device
   // builder makes the same one; the order within a leaf changes no result)
+  for (const BvhNode& nd : *nodes) {
+    if (nd.lcnt > 0) std::sort(order->begin() + nd.lidx, order->begin() + nd.lidx + nd.lcnt);
+    if (nd.rcnt > 0) std::sort(order->begin() + nd.ridx, order->begin() + nd.ridx + nd.rcnt);
+  }
+}
+
+void build_bvh_sah(const std::vector<double>& bmin, const std::vector<double>& bmax, int leaf_size, double pad,
+                   std::vector<BvhNode>* nodes, std::vector<int32_t>* order) {
+  const size_t n = bmin.size() / 3;
+  nodes->clear();
+  order->resize(n);
+  std::vector<Prim> prims(n);
+  for (size_t i = 0; i < n; i++) {
+    for (int k = 0; k < 3; k++) {
+      prims[i].lo[k] = bmin[3 * i + k];
+      prims[i].hi[k] = bmax[3 * i + k];
+      prims[i].c[k] = 0.5 * (prims[i].lo[k] + prims[i].hi[k]);
+    }
+    prims[i].id = (int32_t)i;
+  }
+  if ((int)n <= leaf_size) {  // the median builder's single-leaf and empty layouts
+    build_bvh(bmin, bmax, leaf_size, pad, nodes, order);
+    return;
+  }
+  SahBuilder b{leaf_size, pad};
+  b.build(prims.data(), (int)n, 0, *nodes, 0);
+  for (size_t i = 0; i < n; i++) (*order)[i] = prims[i].id;
   for (const BvhNode& nd : *nodes) {
     if (nd.lcnt > 0) std::sort(order->begin() + nd.lidx, order->begin() + nd.lidx + nd.lcnt);
     if (nd.rcnt > 0) std::sort(order->begin() + nd.ridx, order->begin() + nd.ridx + nd.rcnt);

@@ -34,4 +34,11 @@ struct BvhNode {
 void build_bvh(const std::vector<double>& bmin, const std::vector<double>& bmax, int leaf_size, double pad,
                std::vector<BvhNode>* nodes, std::vector<int32_t>* order);
 
+// The same interface, layout and leaf order, with each node split at the
+// boundary of 16 centroid bins (per axis) that minimises the children's
+// surface area times primitive count: fewer node visits per ray than the
+// median split, at a build cost that keeps it on the host.
+void build_bvh_sah(const std::vector<double>& bmin, const std::vector<double>& bmax, int leaf_size, double pad,
+                   std::vector<BvhNode>* nodes, std::vector<int32_t>* order);
+
 }  // namespace rtb

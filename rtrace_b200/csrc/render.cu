@@ -599,8 +599,11 @@ void parallel_ranges(long long n, F f) {
 
 // Triangles per mesh BVH leaf (measured fastest of 2-16 on the mesh frame).
 const int kMeshLeaf = 8;
-// Meshes from this many triangles up are prepared on the device.
-const long long kPrepDeviceMin = 16384;
+// Meshes from this many triangles up are prepared on the device (median
+// split BVH, tens of ms for millions of triangles); smaller ones on the
+// host with a binned SAH BVH (about 7% fewer node visits per ray, 4% on the
+// 82k-triangle mesh frame).
+const long long kPrepDeviceMin = 262144;
 
 // The part of a mesh's preparation that always runs on the host: checks,
 // the reference k-d nodes packed for the device with each node's root path,
@@ -675,8 +678,9 @@ std::string prep_mesh_kd(const rt_mesh_desc& md, MeshPrep* P) {
 }
 
 // A mesh's whole preparation on the host: the k-d part, then the triangle
-// records and normals, the occurrence lists and the triangle BVH.
-std::string prep_mesh(const rt_mesh_desc& md, MeshPrep* P) {
+// records and normals, the occurrence lists and the triangle BVH (binned
+// SAH, or sah = false the median split the device builds).
+std::string prep_mesh(const rt_mesh_desc& md, MeshPrep* P, bool sah = true) {
   std::string e = prep_mesh_kd(md, P);
   if (!e.empty()) return e;
   const long long nt = md.n_triangles;
@@ -732,7 +736,10 @@ std::string prep_mesh(const rt_mesh_desc& md, MeshPrep* P) {
   // triangle BVH, the candidate search structure
   std::vector<BvhNode> bnodes;
   std::vector<int32_t> order;
-  build_bvh(tmin, tmax, kMeshLeaf, 1e-7 * (1.0 + scale), &bnodes, &order);
+  if (sah)
+    build_bvh_sah(tmin, tmax, kMeshLeaf, 1e-7 * (1.0 + scale), &bnodes, &order);
+  else
+    build_bvh(tmin, tmax, kMeshLeaf, 1e-7 * (1.0 + scale), &bnodes, &order);
   std::vector<double2> bvh, btris((size_t)nt * 5);
   put_bvh(bnodes, &bvh);
   parallel_ranges(nt, [&](long long k0, long long k1, int) {
@@ -2161,7 +2168,7 @@ rt_status rt_debug_mesh_prep(rt_ctx* ctx, const rt_mesh_desc* md, uint32_t* mism
   if (md->n_triangles <= kMeshLeaf) return fail(ctx, RT_ERR_INVALID_ARGUMENT, "mesh too small for the device preparation");
   CK(cudaSetDevice(ctx->device));
   MeshPrep H, D;
-  std::string e = prep_mesh(*md, &H);
+  std::string e = prep_mesh(*md, &H, false);
   if (!e.empty()) return fail(ctx, RT_ERR_INVALID_ARGUMENT, e);
   e = prep_mesh_kd(*md, &D);
   if (!e.empty()) return fail(ctx, RT_ERR_INVALID_ARGUMENT, e);

@@ -48,7 +48,7 @@ def _mesh(name):
 def test_device_preparation_equals_host(gpu_ctx, name):
     from rtrace_b200 import _capi
     v, nodes, idx = _mesh(name)
-    assert len(v) >= 16384  # the size from which uploads prepare on the device
+    assert len(v) >= 16384
     mask = ctypes.c_uint32(99)
     L = _capi.lib()
     st = L.rt_debug_mesh_prep(gpu_ctx.handle, ctypes.byref(_desc(v, nodes, idx)), ctypes.byref(mask))
@@ -57,11 +57,14 @@ def test_device_preparation_equals_host(gpu_ctx, name):
 
 
 @pytest.mark.gpu
-def test_upload_paths_render_the_same(gpu_ctx, tmp_path):
+def test_upload_paths_render_the_same(gpu_ctx, oracle, tmp_path):
     import rtrace_b200 as rt
-    path = workloads.make_noisy_icosphere(str(tmp_path), level=6)  # 81,920 triangles
+    from tests import oracle_lib
+    # 2 x 399^2 = 318,402 triangles: above the size from which uploads
+    # prepare meshes on the device
+    path = workloads.make_terrain(str(tmp_path), n=400, seed=4)
     host = rt.HostScene.from_json_file(path)
-    r = rt.Renderer(160, 90)
+    r = rt.Renderer(96, 54)
     r.anti_aliasing_mode = rt.AntiAliasingMode.NoJitter
     r.disk_samples = 4
     imgs, sizes = [], []
@@ -73,6 +76,7 @@ def test_upload_paths_render_the_same(gpu_ctx, tmp_path):
     want = r.render(rt.Scene.from_json_file(path, gpu_ctx))
     assert all(np.array_equal(i, want) for i in imgs)
     assert imgs[0].any()
+    assert np.array_equal(want, oracle_lib.render(path=path, width=96, height=54, aa="no-jitter", disk_samples=4))
     # the first two uploads copy the mesh's inputs, the third its prepared arrays
     assert sizes[0] == sizes[1] and sizes[2] > sizes[0]
 
