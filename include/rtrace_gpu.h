@@ -497,7 +497,10 @@ rt_status rt_debug_mesh_hit(rt_ctx* ctx, const rt_scene* scene, int32_t object_i
  * binned SAH instead, so the host side here uses the device's median
  * split) and compares them: bit k of *mismatch is set when array k differs
  * (0 BVH, 1 records in BVH order, 2 records in mesh order, 3 normals,
- * 4 k-d occurrences, 5 occurrence offsets).  More than 8 triangles. */
+ * 4 k-d occurrences, 5 occurrence offsets).  Bit 6: the arrays that an
+ * upload of a host-prepared mesh derives on the device from its BVH-order
+ * records and k-d tree (records in mesh order, normals, occurrences) differ
+ * from the host's.  More than 8 triangles. */
 rt_status rt_debug_mesh_prep(rt_ctx* ctx, const rt_mesh_desc* mesh, uint32_t* mismatch);
 
 #ifdef __cplusplus

@@ -11,6 +11,9 @@
 //     end.  Leaves end in id order (the host builder's canonical layout);
 //   * the k-d occurrence lists: every leaf entry as (triangle, leaf,
 //     position), stably sorted by triangle.
+// For a mesh prepared on the host, the arrays that follow from its BVH-order
+// records and its k-d tree (records in mesh order, normals, occurrences)
+// are derived here too, so an upload copies only the rest.
 // Sorts and scans are CUB's device-wide radix sort and scan.
 #include "mesh_prep.hpp"
 
@@ -216,6 +219,23 @@ __global__ void k_prep_gather(const int* __restrict__ order, int n, const double
     btris[i] = brute[5 * (long long)order[i / 5] + i % 5];
 }
 
+// Records in BVH order back to mesh order (each record carries its triangle
+// id), with each triangle's normal normalize(e1 x e2) from the record's
+// edges, the operations the host and k_prep_records perform.
+__global__ void k_prep_unpermute(const double2* __restrict__ btris, int n, double2* __restrict__ brute,
+                                 double4* __restrict__ normals) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    double2 r[5];
+    for (int k = 0; k < 5; k++) r[k] = btris[5 * (long long)i + k];
+    const int t = lo32(r[4].y);
+    if ((unsigned)t >= (unsigned)n) continue;  // not a record of this mesh
+    for (int k = 0; k < 5; k++) brute[5 * (long long)t + k] = r[k];
+    const V3 e1 = mk(r[1].y, r[2].x, r[2].y), e2 = mk(r[3].x, r[3].y, r[4].x);
+    const V3 nn = normalize(cross(e1, e2));
+    normals[t] = double4{nn.x, nn.y, nn.z, 0.0};
+  }
+}
+
 // Leaf entries per k-d node (0 for internal nodes).
 __global__ void k_prep_leaf_counts(const double2* __restrict__ kd, int nk, int* __restrict__ cnt) {
   for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < nk; k += gridDim.x * blockDim.x) {
@@ -260,6 +280,74 @@ struct Shape {
 struct Seg {
   int off, n, node;  // node: preorder index when it splits, -1 for a leaf
 };
+
+// CUB temporary storage from the arena, grown on demand (an outgrown block
+// stays in the arena until the next reset).
+struct CubTemp {
+  KdArena& A;
+  void* p = nullptr;
+  size_t cap = 0;
+  cudaError_t need(size_t bytes) {
+    if (bytes <= cap) return cudaSuccess;
+    char* t = nullptr;
+    cudaError_t e = A.get(&t, bytes);
+    if (e == cudaSuccess) {
+      p = t;
+      cap = bytes;
+    }
+    return e;
+  }
+};
+
+// The k-d occurrence lists: every leaf entry (leaf, position) stably sorted
+// by triangle, so each triangle's entries stay in (leaf, position) order,
+// and occ_off[t] = the first entry of triangle t (n + 1 offsets).  Queued
+// on s.
+cudaError_t occ_device(const double2* d_kd_nodes, int nk, const int* d_leaf_tris, int n_index, int n,
+                       cudaStream_t s, KdArena& A, CubTemp& temp, int2* occ, int* occ_off) {
+#define OCK(call)                          \
+  do {                                     \
+    cudaError_t e_ = (call);               \
+    if (e_ != cudaSuccess) return e_;      \
+  } while (0)
+  const int BS = 256;
+  int *d_cnt, *d_eoff, *d_tcount;
+  unsigned* d_tkey[2];
+  unsigned long long* d_val;
+  OCK(A.get(&d_cnt, (size_t)nk + 1));
+  OCK(A.get(&d_eoff, (size_t)nk + 1));
+  OCK(A.get(&d_tcount, (size_t)n + 1));
+  OCK(A.get(&d_tkey[0], (size_t)n_index));
+  OCK(A.get(&d_tkey[1], (size_t)n_index));
+  OCK(A.get(&d_val, (size_t)n_index));
+  OCK(cudaMemsetAsync(d_tcount, 0, (n + 1) * sizeof(int), s));
+  OCK(cudaMemsetAsync(d_cnt + nk, 0, sizeof(int), s));
+  if (nk > 0) k_prep_leaf_counts<<<grid_for(nk, BS), BS, 0, s>>>(d_kd_nodes, nk, d_cnt);
+  OCK(cudaGetLastError());
+  size_t tb = 0;
+  OCK(cub::DeviceScan::ExclusiveSum(nullptr, tb, d_cnt, d_eoff, nk + 1, s));
+  OCK(temp.need(tb));
+  tb = temp.cap;
+  OCK(cub::DeviceScan::ExclusiveSum(temp.p, tb, d_cnt, d_eoff, nk + 1, s));
+  if (nk > 0)
+    k_prep_occ_entries<<<(int)((32LL * nk + 255) / 256), 256, 0, s>>>(d_kd_nodes, nk, d_eoff, d_leaf_tris,
+                                                                        d_tkey[0], d_val, d_tcount);
+  OCK(cudaGetLastError());
+  const int tri_bits = bits_for(n);
+  unsigned long long* occ64 = reinterpret_cast<unsigned long long*>(occ);
+  tb = 0;
+  OCK(cub::DeviceRadixSort::SortPairs(nullptr, tb, d_tkey[0], d_tkey[1], d_val, occ64, n_index, 0, tri_bits, s));
+  OCK(temp.need(tb));
+  tb = temp.cap;
+  OCK(cub::DeviceRadixSort::SortPairs(temp.p, tb, d_tkey[0], d_tkey[1], d_val, occ64, n_index, 0, tri_bits, s));
+  tb = 0;
+  OCK(cub::DeviceScan::ExclusiveSum(nullptr, tb, d_tcount, occ_off, n + 1, s));
+  OCK(temp.need(tb));
+  tb = temp.cap;
+  OCK(cub::DeviceScan::ExclusiveSum(temp.p, tb, d_tcount, occ_off, n + 1, s));
+#undef OCK
+  return cudaSuccess;
+}
 
 }  // namespace
 
@@ -441,42 +529,28 @@ std::string prep_mesh_device(const double* h_vertices, int n, const double2* d_k
   PCK(cudaGetLastError());
 
   // ---- k-d occurrences
-  int *d_cnt, *d_eoff, *d_tcount;
-  unsigned *d_tkey[2];
-  unsigned long long* d_val;
-  PCK(A.get(&d_cnt, (size_t)n_kd_nodes + 1));
-  PCK(A.get(&d_eoff, (size_t)n_kd_nodes + 1));
-  PCK(A.get(&d_tcount, (size_t)n + 1));
-  PCK(A.get(&d_tkey[0], (size_t)n_index));
-  PCK(A.get(&d_tkey[1], (size_t)n_index));
-  PCK(A.get(&d_val, (size_t)n_index));
-  PCK(cudaMemsetAsync(d_tcount, 0, (n + 1) * sizeof(int), s));
-  PCK(cudaMemsetAsync(d_cnt + n_kd_nodes, 0, sizeof(int), s));
-  k_prep_leaf_counts<<<grid_for(n_kd_nodes, BS), BS, 0, s>>>(d_kd_nodes, n_kd_nodes, d_cnt);
-  PCK(cudaGetLastError());
-  size_t tb = 0;
-  PCK(cub::DeviceScan::ExclusiveSum(nullptr, tb, d_cnt, d_eoff, n_kd_nodes + 1, s));
-  PCK(temp(tb));
-  tb = temp_cap;
-  PCK(cub::DeviceScan::ExclusiveSum(d_temp, tb, d_cnt, d_eoff, n_kd_nodes + 1, s));
-  if (n_kd_nodes > 0)
-    k_prep_occ_entries<<<(int)((32LL * n_kd_nodes + 255) / 256), 256, 0, s>>>(d_kd_nodes, n_kd_nodes, d_eoff,
-                                                                                d_leaf_tris, d_tkey[0], d_val,
-                                                                                d_tcount);
-  PCK(cudaGetLastError());
-  tb = 0;
-  unsigned long long* occ64 = reinterpret_cast<unsigned long long*>(out.occ);
-  PCK(cub::DeviceRadixSort::SortPairs(nullptr, tb, d_tkey[0], d_tkey[1], d_val, occ64, n_index, 0, rank_bits, s));
-  PCK(temp(tb));
-  tb = temp_cap;
-  PCK(cub::DeviceRadixSort::SortPairs(d_temp, tb, d_tkey[0], d_tkey[1], d_val, occ64, n_index, 0, rank_bits, s));
-  tb = 0;
-  PCK(cub::DeviceScan::ExclusiveSum(nullptr, tb, d_tcount, out.occ_off, n + 1, s));
-  PCK(temp(tb));
-  tb = temp_cap;
-  PCK(cub::DeviceScan::ExclusiveSum(d_temp, tb, d_tcount, out.occ_off, n + 1, s));
+  CubTemp occ_temp{A};
+  PCK(occ_device(d_kd_nodes, n_kd_nodes, d_leaf_tris, n_index, n, s, A, occ_temp, out.occ, out.occ_off));
   PCK(cudaStreamSynchronize(s));
 #undef PCK
+  return "";
+}
+
+std::string derive_mesh_device(const double2* d_btris, int n, const double2* d_kd_nodes, int n_kd_nodes,
+                               const int* d_leaf_tris, int n_index, cudaStream_t s, KdArena* arena,
+                               double2* brute, double4* normals, int2* occ, int* occ_off, cudaError_t* cuda_err) {
+  *cuda_err = cudaSuccess;
+  KdArena& A = *arena;
+  A.reset();
+  const int BS = 256;
+  if (n > 0) k_prep_unpermute<<<grid_for(n, BS), BS, 0, s>>>(d_btris, n, brute, normals);
+  cudaError_t e = cudaGetLastError();
+  CubTemp temp{A};
+  if (e == cudaSuccess) e = occ_device(d_kd_nodes, n_kd_nodes, d_leaf_tris, n_index, n, s, A, temp, occ, occ_off);
+  if (e != cudaSuccess) {
+    *cuda_err = e;
+    return std::string("mesh arrays from the records: ") + cudaGetErrorString(e);
+  }
   return "";
 }
 

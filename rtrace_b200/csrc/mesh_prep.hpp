@@ -38,4 +38,14 @@ std::string prep_mesh_device(const double* h_vertices, int n, const double2* d_k
                              const int* d_leaf_tris, int n_index, int leaf, cudaStream_t s, KdArena* arena,
                              const MeshPrepOut& out, cudaError_t* cuda_err);
 
+// The arrays of a host-prepared mesh that follow from its records in BVH
+// order and its k-d tree, with the host preparation's bytes: the records
+// in mesh order, the normals and the k-d occurrence lists.  d_btris: 5n
+// double2 (each record's triangle id in [0, n)); d_kd_nodes, d_leaf_tris
+// as for prep_mesh_device.  Destinations as in MeshPrepOut.  Queues the
+// work on stream s (scratch from arena) and returns without waiting.
+std::string derive_mesh_device(const double2* d_btris, int n, const double2* d_kd_nodes, int n_kd_nodes,
+                               const int* d_leaf_tris, int n_index, cudaStream_t s, KdArena* arena,
+                               double2* brute, double4* normals, int2* occ, int* occ_off, cudaError_t* cuda_err);
+
 }  // namespace rtb

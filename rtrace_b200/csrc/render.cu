@@ -39,6 +39,21 @@ struct DirectCopy {
 struct StagedCopy {
   size_t off, pin_off, bytes;
 };
+// A host-prepared mesh whose records in mesh order, normals and occurrence
+// lists the device derives from its copied arrays (derive_mesh_device), at
+// the flush once the copies are queued.
+struct MeshDerive {
+  const double2* btris;
+  int n;
+  const double2* nodes;
+  int n_nodes;
+  const int* leaf_tris;
+  int n_index;
+  double2* brute;
+  double4* normals;
+  int2* occ;
+  int* occ_off;
+};
 
 struct rt_scene {
   rt_ctx* ctx = nullptr;
@@ -62,6 +77,7 @@ struct rt_scene {
   ~rt_scene();
   std::vector<DirectCopy> direct;
   std::vector<StagedCopy> staged;  // runs of the staging buffer
+  std::vector<MeshDerive> derive;
 };
 
 // One captured render (RT_FLAG_CUDA_GRAPH): the launch sequence is fully
@@ -258,13 +274,25 @@ rt_status ensure_dn_scratch(rt_ctx* ctx, long long n) {
 // do not fit get their own allocation.  One cudaMalloc and one cudaFree per
 // scene instead of one per array.
 rt_status arena_flush(rt_ctx* ctx, rt_scene* sc) {
+  bool queued = false;
   if (sc->blk && sc->blk_used) {
     for (const StagedCopy& c : sc->staged)
       CK(cudaMemcpyAsync(sc->blk + c.off, ctx->pin + c.pin_off, c.bytes, cudaMemcpyHostToDevice, ctx->stream));
     for (const DirectCopy& d : sc->direct)
       if (d.bytes) CK(cudaMemcpyAsync(sc->blk + d.off, d.src, d.bytes, cudaMemcpyHostToDevice, ctx->stream));
-    CK(cudaStreamSynchronize(ctx->stream));
+    queued = true;
   }
+  std::vector<MeshDerive> derive;
+  derive.swap(sc->derive);
+  for (const MeshDerive& m : derive) {
+    if (!ctx->kd_arena) ctx->kd_arena = kd_arena_new();
+    cudaError_t ce = cudaSuccess;
+    std::string e = derive_mesh_device(m.btris, m.n, m.nodes, m.n_nodes, m.leaf_tris, m.n_index, ctx->stream,
+                                       ctx->kd_arena, m.brute, m.normals, m.occ, m.occ_off, &ce);
+    if (!e.empty()) return cuda_fail(ctx, ce, e.c_str());
+    queued = true;
+  }
+  if (queued) CK(cudaStreamSynchronize(ctx->stream));
   sc->direct.clear();
   sc->staged.clear();
   sc->blk = nullptr;
@@ -519,7 +547,10 @@ void put_bvh(const std::vector<BvhNode>& nodes, std::vector<double2>* out) {
 // Everything the device needs for one mesh, computed on the host: triangle
 // records in original and BVH order, normals, the reference k-d tree with
 // root paths and occurrence lists, the BVH.  Pure function of the mesh
-// description, so a host scene can keep it across uploads.
+// description, so a host scene can keep it across uploads.  An upload
+// copies the BVH, the BVH-order records and the k-d part; the device
+// derives the records in mesh order, the normals and the occurrence lists
+// from them (derive_mesh_device), so only prep_mesh(full = true) fills those.
 struct MeshPrep {
   std::vector<double2> bvh, btris, brute, nodes;
   std::vector<double4> normals;
@@ -530,28 +561,28 @@ struct MeshPrep {
   // Prepared on the device by the last upload: the records, normals, BVH
   // and occurrence arrays are not on the host (only the k-d part is).
   bool device_made = false;
-  // Kept by a host scene, the nine arrays above are packed into one pinned
-  // buffer (each at a 256-byte aligned offset) and the vectors released:
-  // uploads then copy the image straight from pinned memory.
+  // Kept by a host scene, the five uploaded arrays are packed into one
+  // pinned buffer (each at a 256-byte aligned offset; bvh, btris, nodes,
+  // leaf_tris, leaf_path) and the vectors released: uploads then copy the
+  // image straight from pinned memory.
+  static const int kImageArrays = 5;
   char* image = nullptr;
   size_t image_bytes = 0;
-  size_t off[9] = {}, len[9] = {};
+  size_t off[kImageArrays] = {}, len[kImageArrays] = {};
   ~MeshPrep() {
     if (image) cudaFreeHost(image);
   }
 };
 
-// Packs P's arrays into a pinned image (see MeshPrep); leaves P as it is if
-// pinned memory cannot be had.
+// Packs P's uploaded arrays into a pinned image (see MeshPrep); leaves P as
+// it is if pinned memory cannot be had.
 void pack_prep(MeshPrep* P) {
-  const void* src[9] = {P->bvh.data(), P->btris.data(), P->brute.data(), P->normals.data(), P->nodes.data(),
-                        P->leaf_tris.data(), P->leaf_path.data(), P->occ.data(), P->occ_off.data()};
-  size_t n[9] = {P->bvh.size() * sizeof(double2), P->btris.size() * sizeof(double2),
-                 P->brute.size() * sizeof(double2), P->normals.size() * sizeof(double4),
-                 P->nodes.size() * sizeof(double2), P->leaf_tris.size() * sizeof(int),
-                 P->leaf_path.size() * sizeof(int2), P->occ.size() * sizeof(int2), P->occ_off.size() * sizeof(int)};
+  const int K = MeshPrep::kImageArrays;
+  const void* src[K] = {P->bvh.data(), P->btris.data(), P->nodes.data(), P->leaf_tris.data(), P->leaf_path.data()};
+  size_t n[K] = {P->bvh.size() * sizeof(double2), P->btris.size() * sizeof(double2), P->nodes.size() * sizeof(double2),
+                 P->leaf_tris.size() * sizeof(int), P->leaf_path.size() * sizeof(int2)};
   size_t total = 0;
-  for (int k = 0; k < 9; k++) {
+  for (int k = 0; k < K; k++) {
     P->off[k] = total;
     P->len[k] = n[k];
     total += (std::max<size_t>(n[k], 16) + 255) & ~(size_t)255;
@@ -561,7 +592,7 @@ void pack_prep(MeshPrep* P) {
     cudaGetLastError();
     return;
   }
-  for (int k = 0; k < 9; k++)
+  for (int k = 0; k < K; k++)
     if (n[k]) memcpy(img + P->off[k], src[k], n[k]);
   P->image = img;
   P->image_bytes = total;
@@ -678,15 +709,17 @@ std::string prep_mesh_kd(const rt_mesh_desc& md, MeshPrep* P) {
 }
 
 // A mesh's whole preparation on the host: the k-d part, then the triangle
-// records and normals, the occurrence lists and the triangle BVH (binned
-// SAH, or sah = false the median split the device builds).
-std::string prep_mesh(const rt_mesh_desc& md, MeshPrep* P, bool sah = true) {
+// records, the triangle BVH (binned SAH, or sah = false the median split
+// the device builds) and the records in BVH order; full = true also keeps
+// the records in mesh order, the normals and the occurrence lists, which
+// uploads derive on the device.
+std::string prep_mesh(const rt_mesh_desc& md, MeshPrep* P, bool sah = true, bool full = false) {
   std::string e = prep_mesh_kd(md, P);
   if (!e.empty()) return e;
   const long long nt = md.n_triangles;
   // triangle records and normals in original order
   std::vector<double2> brute((size_t)nt * 5);
-  std::vector<double4> normals((size_t)nt);
+  std::vector<double4> normals(full ? (size_t)nt : 0);
   std::vector<double> tmin((size_t)nt * 3), tmax((size_t)nt * 3);
   std::vector<double> part_scale(host_parts(nt), 0.0);
   parallel_ranges(nt, [&](long long t0, long long t1, int part) {
@@ -697,8 +730,10 @@ std::string prep_mesh(const rt_mesh_desc& md, MeshPrep* P, bool sah = true) {
       V3 e1 = v1 - v0, e2 = v2 - v0;
       V3 n = cross(e1, e2);
       int degenerate = norm(n) < 1e-8 ? 1 : 0;  // src/ray.rs:565-567
-      V3 nn = normalize(n);
-      normals[t] = double4{nn.x, nn.y, nn.z, 0.0};
+      if (full) {
+        V3 nn = normalize(n);
+        normals[t] = double4{nn.x, nn.y, nn.z, 0.0};
+      }
       double2* E = &brute[5 * t];
       E[0] = double2{v0.x, v0.y};
       E[1] = double2{v0.z, e1.x};
@@ -718,11 +753,13 @@ std::string prep_mesh(const rt_mesh_desc& md, MeshPrep* P, bool sah = true) {
   for (double v : part_scale) scale = std::max(scale, v);
   // per-triangle occurrences (leaf node, position in the leaf), by leaf
   // node then position
-  std::vector<int> occ_off((size_t)nt + 1, 0);
-  for (int t : P->leaf_tris) occ_off[t + 1]++;
-  for (long long t = 0; t < nt; t++) occ_off[t + 1] += occ_off[t];
-  std::vector<int2> occ((size_t)md.n_tri_index);
-  {
+  std::vector<int> occ_off;
+  std::vector<int2> occ;
+  if (full) {
+    occ_off.assign((size_t)nt + 1, 0);
+    for (int t : P->leaf_tris) occ_off[t + 1]++;
+    for (long long t = 0; t < nt; t++) occ_off[t + 1] += occ_off[t];
+    occ.resize((size_t)md.n_tri_index);
     std::vector<int> fill(occ_off.begin(), occ_off.end() - 1);
     for (long long k = 0; k < md.n_nodes; k++) {
       const rt_kd_node_desc& nd = md.nodes[k];
@@ -748,10 +785,12 @@ std::string prep_mesh(const rt_mesh_desc& md, MeshPrep* P, bool sah = true) {
   });
   P->bvh = std::move(bvh);
   P->btris = std::move(btris);
-  P->brute = std::move(brute);
-  P->normals = std::move(normals);
-  P->occ_off = std::move(occ_off);
-  P->occ = std::move(occ);
+  if (full) {
+    P->brute = std::move(brute);
+    P->normals = std::move(normals);
+    P->occ_off = std::move(occ_off);
+    P->occ = std::move(occ);
+  }
   return std::string();
 }
 
@@ -791,8 +830,9 @@ rt_status upload_now(rt_ctx* ctx, rt_scene* sc, const std::vector<T>& h, const T
 }
 
 // Prepares a large mesh on the device straight into the scene's block: P
-// holds the k-d part (prep_mesh_kd).  keep_host: also copies the arrays
-// made on the device back into P, so that later uploads copy them.
+// holds the k-d part (prep_mesh_kd).  keep_host: also copies the BVH and
+// the BVH-order records back into P, so that later uploads copy them
+// (upload_prep).
 rt_status upload_prep_device(rt_ctx* ctx, rt_scene* sc, const rt_mesh_desc& md, MeshPrep* P, bool keep_host,
                              DMesh* out) {
   DMesh M{};
@@ -829,25 +869,19 @@ rt_status upload_prep_device(rt_ctx* ctx, rt_scene* sc, const rt_mesh_desc& md, 
   M.occ = occ;
   M.occ_off = occ_off;
   if (keep_host) {
+    // what upload_prep copies; it derives the rest
     P->bvh.resize(7 * (size_t)nb);
     P->btris.resize(5 * (size_t)n);
-    P->brute.resize(5 * (size_t)n);
-    P->normals.resize(n);
-    P->occ.resize(P->n_index);
-    P->occ_off.resize((size_t)n + 1);
     CK(cudaMemcpy(P->bvh.data(), bvh, P->bvh.size() * sizeof(double2), cudaMemcpyDeviceToHost));
     CK(cudaMemcpy(P->btris.data(), btris, P->btris.size() * sizeof(double2), cudaMemcpyDeviceToHost));
-    CK(cudaMemcpy(P->brute.data(), brute, P->brute.size() * sizeof(double2), cudaMemcpyDeviceToHost));
-    CK(cudaMemcpy(P->normals.data(), normals, P->normals.size() * sizeof(double4), cudaMemcpyDeviceToHost));
-    CK(cudaMemcpy(P->occ.data(), occ, P->occ.size() * sizeof(int2), cudaMemcpyDeviceToHost));
-    CK(cudaMemcpy(P->occ_off.data(), occ_off, P->occ_off.size() * sizeof(int), cudaMemcpyDeviceToHost));
     P->device_made = false;
   }
   *out = M;
   return RT_OK;
 }
 
-// Copies a prepared mesh into the scene's block.
+// Copies a prepared mesh into the scene's block: the BVH, the BVH-order
+// records and the k-d part; the rest is derived on the device at the flush.
 rt_status upload_prep(rt_ctx* ctx, rt_scene* sc, const MeshPrep& P, DMesh* out) {
   DMesh M{};
   for (int k = 0; k < 3; k++) {
@@ -856,34 +890,37 @@ rt_status upload_prep(rt_ctx* ctx, rt_scene* sc, const MeshPrep& P, DMesh* out) 
   }
   M.n_nodes = P.n_nodes;
   M.n_tris = P.n_tris;
+  rt_status st;
   if (P.image) {
     char* base = nullptr;
-    rt_status st = upload_direct(ctx, sc, P.image, P.image_bytes, &base);
-    if (st != RT_OK) return st;
+    if ((st = upload_direct(ctx, sc, P.image, P.image_bytes, &base)) != RT_OK) return st;
     M.bvh = reinterpret_cast<const double2*>(base + P.off[0]);
     M.btris = reinterpret_cast<const double2*>(base + P.off[1]);
-    M.brute = reinterpret_cast<const double2*>(base + P.off[2]);
-    M.normals = reinterpret_cast<const double4*>(base + P.off[3]);
-    M.nodes = reinterpret_cast<const double2*>(base + P.off[4]);
-    M.leaf_tris = reinterpret_cast<const int*>(base + P.off[5]);
-    M.leaf_path = reinterpret_cast<const int2*>(base + P.off[6]);
-    M.occ = reinterpret_cast<const int2*>(base + P.off[7]);
-    M.occ_off = reinterpret_cast<const int*>(base + P.off[8]);
-    *out = M;
-    return RT_OK;
+    M.nodes = reinterpret_cast<const double2*>(base + P.off[2]);
+    M.leaf_tris = reinterpret_cast<const int*>(base + P.off[3]);
+    M.leaf_path = reinterpret_cast<const int2*>(base + P.off[4]);
+  } else {
+    // not packed: each array straight from P's own memory (P outlives the flush)
+    if ((st = upload_array(ctx, sc, P.bvh, &M.bvh)) != RT_OK || (st = upload_array(ctx, sc, P.btris, &M.btris)) != RT_OK ||
+        (st = upload_array(ctx, sc, P.nodes, &M.nodes)) != RT_OK ||
+        (st = upload_array(ctx, sc, P.leaf_tris, &M.leaf_tris)) != RT_OK ||
+        (st = upload_array(ctx, sc, P.leaf_path, &M.leaf_path)) != RT_OK)
+      return st;
   }
-  // not packed: each array straight from P's own memory (P outlives the flush)
-  rt_status st;
-  if ((st = upload_array(ctx, sc, P.bvh, &M.bvh)) != RT_OK || (st = upload_array(ctx, sc, P.btris, &M.btris)) != RT_OK ||
-      (st = upload_array(ctx, sc, P.brute, &M.brute)) != RT_OK ||
-      (st = upload_array(ctx, sc, P.normals, &M.normals)) != RT_OK ||
-      (st = upload_array(ctx, sc, P.nodes, &M.nodes)) != RT_OK ||
-      (st = upload_array(ctx, sc, P.leaf_tris, &M.leaf_tris)) != RT_OK ||
-      (st = upload_array(ctx, sc, P.leaf_path, &M.leaf_path)) != RT_OK ||
-      (st = upload_array(ctx, sc, P.occ, &M.occ)) != RT_OK || (st = upload_array(ctx, sc, P.occ_off, &M.occ_off)) != RT_OK)
+  const int n = P.n_tris;
+  double2* brute;
+  double4* normals;
+  int2* occ;
+  int* occ_off;
+  if ((st = reserve(ctx, sc, 5 * (size_t)n, &brute)) != RT_OK || (st = reserve(ctx, sc, (size_t)n, &normals)) != RT_OK ||
+      (st = reserve(ctx, sc, (size_t)P.n_index, &occ)) != RT_OK ||
+      (st = reserve(ctx, sc, (size_t)n + 1, &occ_off)) != RT_OK)
     return st;
-  M.n_nodes = P.n_nodes;
-  M.n_tris = P.n_tris;
+  sc->derive.push_back(MeshDerive{M.btris, n, M.nodes, P.n_nodes, M.leaf_tris, P.n_index, brute, normals, occ, occ_off});
+  M.brute = brute;
+  M.normals = normals;
+  M.occ = occ;
+  M.occ_off = occ_off;
   *out = M;
   return RT_OK;
 }
@@ -2168,7 +2205,7 @@ rt_status rt_debug_mesh_prep(rt_ctx* ctx, const rt_mesh_desc* md, uint32_t* mism
   if (md->n_triangles <= kMeshLeaf) return fail(ctx, RT_ERR_INVALID_ARGUMENT, "mesh too small for the device preparation");
   CK(cudaSetDevice(ctx->device));
   MeshPrep H, D;
-  std::string e = prep_mesh(*md, &H, false);
+  std::string e = prep_mesh(*md, &H, false, true);
   if (!e.empty()) return fail(ctx, RT_ERR_INVALID_ARGUMENT, e);
   e = prep_mesh_kd(*md, &D);
   if (!e.empty()) return fail(ctx, RT_ERR_INVALID_ARGUMENT, e);
@@ -2186,8 +2223,9 @@ rt_status rt_debug_mesh_prep(rt_ctx* ctx, const rt_mesh_desc* md, uint32_t* mism
     free_all(tmp);
     return cuda_fail(ctx, ce, "cudaMalloc");
   }
-  cudaMemcpy(dn, D.nodes.data(), D.nodes.size() * sizeof(double2), cudaMemcpyHostToDevice);
-  cudaMemcpy(dl, D.leaf_tris.data(), D.leaf_tris.size() * sizeof(int), cudaMemcpyHostToDevice);
+  // on the context's stream (non-blocking), which the preparations below use
+  cudaMemcpyAsync(dn, D.nodes.data(), D.nodes.size() * sizeof(double2), cudaMemcpyHostToDevice, ctx->stream);
+  cudaMemcpyAsync(dl, D.leaf_tris.data(), D.leaf_tris.size() * sizeof(int), cudaMemcpyHostToDevice, ctx->stream);
   if (!ctx->kd_arena) ctx->kd_arena = kd_arena_new();
   e = prep_mesh_device(md->vertices, n, dn, D.n_nodes, dl, D.n_index, kMeshLeaf, ctx->stream, ctx->kd_arena,
                        MeshPrepOut{bvh, btris, brute, normals, occ, occ_off}, &ce);
@@ -2207,6 +2245,28 @@ rt_status rt_debug_mesh_prep(rt_ctx* ctx, const rt_mesh_desc* md, uint32_t* mism
   if (!same(normals, H.normals.data(), H.normals.size() * sizeof(double4))) m |= 8;
   if (!same(occ, H.occ.data(), H.occ.size() * sizeof(int2))) m |= 16;
   if (!same(occ_off, H.occ_off.data(), H.occ_off.size() * sizeof(int))) m |= 32;
+  // the arrays an upload of the host preparation derives on the device,
+  // from the host's BVH-order records, into the same buffers
+  cudaStream_t s = ctx->stream;
+  if ((ce = cudaMemcpyAsync(btris, H.btris.data(), H.btris.size() * sizeof(double2), cudaMemcpyHostToDevice, s)) ==
+          cudaSuccess &&
+      (ce = cudaMemsetAsync(brute, 0xff, H.brute.size() * sizeof(double2), s)) == cudaSuccess &&
+      (ce = cudaMemsetAsync(normals, 0xff, H.normals.size() * sizeof(double4), s)) == cudaSuccess &&
+      (ce = cudaMemsetAsync(occ, 0xff, H.occ.size() * sizeof(int2), s)) == cudaSuccess &&
+      (ce = cudaMemsetAsync(occ_off, 0xff, H.occ_off.size() * sizeof(int), s)) == cudaSuccess) {
+    e = derive_mesh_device(btris, n, dn, D.n_nodes, dl, D.n_index, s, ctx->kd_arena, brute, normals, occ, occ_off,
+                           &ce);
+    if (e.empty() && (ce = cudaStreamSynchronize(s)) == cudaSuccess &&
+        (!same(brute, H.brute.data(), H.brute.size() * sizeof(double2)) ||
+         !same(normals, H.normals.data(), H.normals.size() * sizeof(double4)) ||
+         !same(occ, H.occ.data(), H.occ.size() * sizeof(int2)) ||
+         !same(occ_off, H.occ_off.data(), H.occ_off.size() * sizeof(int))))
+      m |= 64;
+  }
+  if (ce != cudaSuccess) {
+    free_all(tmp);
+    return cuda_fail(ctx, ce, "mesh derivation check");
+  }
   ce = cudaGetLastError();
   free_all(tmp);
   if (ce != cudaSuccess) return cuda_fail(ctx, ce, "mesh preparation check");
