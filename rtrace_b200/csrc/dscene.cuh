@@ -23,7 +23,8 @@
 //   * Shadow rays only ask `world.hit(..).is_some()`; every per-object
 //     test is monotone in t_max, so any accepting object suffices.
 // Boxes are padded and pruning uses a relative margin, so a box never
-// rejects a primitive the exact test would accept.
+// rejects a primitive the exact test would accept.  Mesh BVH boxes are
+// tested in single precision with margins that keep this (RayF).
 #pragma once
 
 #include "dmath.cuh"
@@ -63,6 +64,7 @@ struct DCube {
 struct DMesh {
   double bmin[3], bmax[3];
   const double2* bvh;      // triangle BVH nodes
+  const float4* fbvh;      // the same BVH in single precision (FNode), which the walks test
   const double2* btris;    // triangle records in BVH leaf order
   const double2* brute;    // triangle records in original order
   const double4* normals;  // normalize(e1 x e2) per triangle
@@ -504,22 +506,130 @@ __device__ __forceinline__ BNode load_bnode(const double2* base, int node) {
   return n;
 }
 
+// A BVH node in single precision: the double node's child boxes rounded
+// outwards to floats, the same child references.  Layout: fbvh[0].x is
+// the largest |coordinate| of any child box (the scale the slab constants
+// below need); node k is fbvh[1 + 4k .. 4 + 4k] = {lmn.xyz, lmx.x},
+// {lmx.yz, rmn.xy}, {rmn.z, rmx.xyz}, {lidx, lcnt, ridx, rcnt as int bits}.
+struct FNode {
+  float lmn[3], lmx[3], rmn[3], rmx[3];
+  int lidx, lcnt, ridx, rcnt;
+};
+__device__ __forceinline__ FNode load_fnode(const float4* fbvh, int node) {
+  const float4* N = fbvh + 1 + 4 * (size_t)node;
+  const float4 a = __ldg(N + 0), b = __ldg(N + 1), c = __ldg(N + 2), d = __ldg(N + 3);
+  FNode n;
+  n.lmn[0] = a.x; n.lmn[1] = a.y; n.lmn[2] = a.z;
+  n.lmx[0] = a.w; n.lmx[1] = b.x; n.lmx[2] = b.y;
+  n.rmn[0] = b.z; n.rmn[1] = b.w; n.rmn[2] = c.x;
+  n.rmx[0] = c.y; n.rmx[1] = c.z; n.rmx[2] = c.w;
+  n.lidx = __float_as_int(d.x);
+  n.lcnt = __float_as_int(d.y);
+  n.ridx = __float_as_int(d.z);
+  n.rcnt = __float_as_int(d.w);
+  return n;
+}
+
+// A ray's single-precision slab constants.  Entry distances are taken from
+// hi = o + delta rounded up, exit distances from lo = o - delta rounded
+// down: the distances of the box grown by delta on every side.  One float
+// subtraction and one product with the rounded reciprocal move a computed
+// slab plane by at most 3.0002 * 2^-24 * (|box coordinate| + |hi|), so
+// delta = 3e-7 * (scale + max |o|) keeps every computed interval around
+// the exact interval of the float box (which holds the double box): a box
+// the exact ray meets is never rejected.  An axis with d = 0 has an
+// infinite reciprocal: the slab is everything or nothing (0 * inf = NaN
+// only when the origin lies outside the unpadded box, where either answer
+// is right).  all: the constants cannot bound the rounding (NaN, an origin
+// or scale beyond 1e30, a component of d nonzero but below 1e-30, whose
+// reciprocal would overflow), so every box is accepted.
+struct RayF {
+  float lo[3], hi[3], inv[3];
+  bool all;
+};
+__device__ __forceinline__ RayF make_rayf(const RayC& r, float scale) {
+  RayF f;
+  bool bad = !(scale < 1e30f);
+  double om = 0.0;
+#pragma unroll
+  for (int a = 0; a < 3; a++) {
+    const double o = r.o[a], d = r.d[a];
+    bad = bad || !(fabs(o) < 1e30) || d != d || (d != 0.0 && fabs(d) < 1e-30);
+    om = fmax(om, fabs(o));
+  }
+  const double delta = 3e-7 * ((double)scale + om) + 1e-30;
+#pragma unroll
+  for (int a = 0; a < 3; a++) {
+    f.lo[a] = __double2float_rd(r.o[a] - delta);
+    f.hi[a] = __double2float_ru(r.o[a] + delta);
+    f.inv[a] = __double2float_rn(r.inv[a]);
+  }
+  f.all = bad;
+  return f;
+}
+
+// box_hit in single precision: never rejects a box that box_hit's exact
+// counterpart accepts (see RayF); tmax is the rounded-up pruning bound.
+__device__ __forceinline__ bool box_hit_f(const float* mn, const float* mx, const RayF& f, float tmax, float* te) {
+  float tl = -__int_as_float(0x7f800000), th = __int_as_float(0x7f800000);
+#pragma unroll
+  for (int a = 0; a < 3; a++) {
+    const float t0 = (mn[a] - f.hi[a]) * f.inv[a];
+    const float t1 = (mx[a] - f.lo[a]) * f.inv[a];
+    tl = fmaxf(tl, fminf(t0, t1));
+    th = fminf(th, fmaxf(t0, t1));
+  }
+  *te = tl;
+  return f.all || (tl <= th && th >= 0.0f && !(tl > tmax));
+}
+
+// Node sources of the BVH walks: a BVH's nodes and one ray's box test, in
+// double (sphere runs) or single precision (meshes).  bound(t) turns a
+// pruning distance into the form test() takes.
+struct DNodes {
+  typedef BNode Node;
+  typedef double T;
+  const double2* bvh;
+  const RayC* r;
+  __device__ __forceinline__ Node load(int k) const { return load_bnode(bvh, k); }
+  __device__ __forceinline__ double bound(double t) const { return t; }
+  __device__ __forceinline__ bool test(const T* mn, const T* mx, double b, T* te) const {
+    return box_hit(mn, mx, *r, b, te);
+  }
+};
+struct FNodes {
+  typedef FNode Node;
+  typedef float T;
+  const float4* fbvh;
+  RayF f;
+  __device__ __forceinline__ Node load(int k) const { return load_fnode(fbvh, k); }
+  // box_hit's t * RTB_PRUNE_REL + RTB_PRUNE_ABS, rounded up
+  __device__ __forceinline__ float bound(double t) const {
+    return __double2float_ru(t * RTB_PRUNE_REL + RTB_PRUNE_ABS);
+  }
+  __device__ __forceinline__ bool test(const T* mn, const T* mx, float b, T* te) const {
+    return box_hit_f(mn, mx, f, b, te);
+  }
+};
+__device__ __forceinline__ FNodes mesh_nodes(const DMesh& M, const RayC& r) {
+  return FNodes{M.fbvh, make_rayf(r, __ldg(M.fbvh).x)};
+}
+
 // Generic BVH walk.  visit_leaf(first, count) tests a leaf's primitives and
 // returns true to stop; bound() is the current pruning t.  Children are
 // visited nearest first.
-template <class Leaf, class Bound>
-__device__ __forceinline__ bool bvh_walk(const double2* bvh, const RayC& r, Leaf visit_leaf, Bound bound, int* err,
-                                         Work* w) {
+template <class Nodes, class Leaf, class Bound>
+__device__ __forceinline__ bool bvh_walk(const Nodes& src, Leaf visit_leaf, Bound bound, int* err, Work* w) {
   int stack[RTB_STACK];
   int sp = 0;
   int node = 0;
   for (;;) {
-    BNode n = load_bnode(bvh, node);
+    const typename Nodes::Node n = src.load(node);
     if (w) w->nodes++;
-    double tl = 0, tr = 0;
-    double b = bound();
-    bool hl = n.lcnt >= 0 && box_hit(n.lmn, n.lmx, r, b, &tl);
-    bool hr = n.rcnt >= 0 && box_hit(n.rmn, n.rmx, r, b, &tr);
+    typename Nodes::T tl = 0, tr = 0;
+    const auto b = src.bound(bound());
+    bool hl = n.lcnt >= 0 && src.test(n.lmn, n.lmx, b, &tl);
+    bool hr = n.rcnt >= 0 && src.test(n.rmn, n.rmx, b, &tr);
     bool swap = hl && hr && tr < tl;
     int aidx = swap ? n.ridx : n.lidx, acnt = swap ? n.rcnt : n.lcnt;
     int bidx = swap ? n.lidx : n.ridx, bcnt = swap ? n.lcnt : n.rcnt;
@@ -567,7 +677,7 @@ __device__ bool mesh_closest(const DMesh& M, const RayC& r, double tmin, double&
   int nt = 0;
   bool overflow = false;
   bvh_walk(
-      M.bvh, r,
+      mesh_nodes(M, r),
       [&](int first, int cnt) {
         for (int k = 0; k < cnt; k++) {
           const double2* E = M.btris + 5 * (size_t)(first + k);
@@ -640,7 +750,7 @@ __device__ bool mesh_closest(const DMesh& M, const RayC& r, double tmin, double&
 __device__ bool mesh_any(const DMesh& M, const RayC& r, double tmin, double tmax, bool use_kd, int* err, Work* w) {
   if (!mesh_bounds(M, r, tmin, tmax)) return false;
   return bvh_walk(
-      M.bvh, r,
+      mesh_nodes(M, r),
       [&](int first, int cnt) {
         for (int k = 0; k < cnt; k++) {
           const double2* E = M.btris + 5 * (size_t)(first + k);
@@ -668,7 +778,7 @@ __device__ bool group_hit(const DScene& S, const DSphGroup& G, const RayC& r, do
   double bt = closest;
   int bi = -1;
   bool stop = bvh_walk(
-      G.bvh, r,
+      DNodes{G.bvh, &r},
       [&](int first, int cnt) {
         for (int k = 0; k < cnt; k++) {
           int sidx = __ldg(G.order + first + k);  // position in the run
@@ -804,9 +914,9 @@ __device__ __forceinline__ bool world_any(const DScene& S, const RayC& r, double
 // `stack` is the warp's RTB_STACK-entry traversal stack in shared memory:
 // every lane writes the same value to the same entry and reads back only
 // values it wrote itself, so it needs no synchronisation.
-template <class Leaf>
-__device__ __forceinline__ bool bvh_any_warp(const double2* bvh, const RayC& r, double tmax, bool active,
-                                             Leaf visit_leaf, volatile int* stack, int* err, Work* w) {
+template <class Nodes, class Leaf>
+__device__ __forceinline__ bool bvh_any_warp(const Nodes& src, double tmax, bool active, Leaf visit_leaf,
+                                             volatile int* stack, int* err, Work* w) {
   const unsigned FULL = 0xffffffffu;
   bool found = false;
   if (!__any_sync(FULL, active)) return false;
@@ -817,12 +927,13 @@ __device__ __forceinline__ bool bvh_any_warp(const double2* bvh, const RayC& r, 
   // hold the single-ray work rather than the packet's shared visits
   bool mine = true;
   unsigned long long mine_bits = 0;
+  const auto b = src.bound(tmax);
   for (;;) {
-    BNode n = load_bnode(bvh, node);
+    const typename Nodes::Node n = src.load(node);
     if (w && active && mine) w->nodes++;
-    double tl = 0, tr = 0;
-    bool hl = active && n.lcnt >= 0 && box_hit(n.lmn, n.lmx, r, tmax, &tl);
-    bool hr = active && n.rcnt >= 0 && box_hit(n.rmn, n.rmx, r, tmax, &tr);
+    typename Nodes::T tl = 0, tr = 0;
+    bool hl = active && n.lcnt >= 0 && src.test(n.lmn, n.lmx, b, &tl);
+    bool hr = active && n.rcnt >= 0 && src.test(n.rmn, n.rmx, b, &tr);
     if (w) {
       hl = hl && mine;
       hr = hr && mine;
@@ -878,7 +989,7 @@ __device__ __forceinline__ bool mesh_any_warp(const DMesh& M, const RayC& r, dou
                                               bool use_kd, volatile int* stack, int* err, Work* w) {
   active = active && mesh_bounds(M, r, tmin, tmax);
   return bvh_any_warp(
-      M.bvh, r, tmax, active,
+      mesh_nodes(M, r), tmax, active,
       [&](int first, int cnt) {
         for (int k = 0; k < cnt; k++) {
           const double2* E = M.btris + 5 * (size_t)(first + k);
@@ -900,7 +1011,7 @@ __device__ __forceinline__ bool mesh_any_warp(const DMesh& M, const RayC& r, dou
 __device__ __forceinline__ bool group_any_warp(const DScene& S, const DSphGroup& G, const RayC& r, double tmin,
                                                double tmax, bool active, volatile int* stack, int* err, Work* w) {
   return bvh_any_warp(
-      G.bvh, r, tmax, active,
+      DNodes{G.bvh, &r}, tmax, active,
       [&](int first, int cnt) {
         for (int k = 0; k < cnt; k++) {
           int sidx = __ldg(G.order + first + k);

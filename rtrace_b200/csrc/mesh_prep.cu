@@ -219,6 +219,44 @@ __global__ void k_prep_gather(const int* __restrict__ order, int n, const double
     btris[i] = brute[5 * (long long)order[i / 5] + i % 5];
 }
 
+// Single-precision copy of a BVH (FNode layout): child boxes rounded
+// outwards, child references as they are, and in fbvh[0].x the largest
+// |coordinate| of any present child's box, by atomicMax on the bits
+// (non-negative floats order like their encodings; fbvh[0] zeroed first).
+__global__ void k_prep_fbvh(const double2* __restrict__ bvh, int nb, float4* __restrict__ fbvh) {
+  float scale = 0.0f;
+  for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < nb; k += gridDim.x * blockDim.x) {
+    const double2* N = bvh + 7 * (long long)k;
+    double b[12];
+    for (int j = 0; j < 6; j++) {
+      const double2 v = N[j];
+      b[2 * j] = v.x;
+      b[2 * j + 1] = v.y;
+    }
+    const double2 refs = N[6];
+    float f[12];
+    for (int j = 0; j < 12; j++) {
+      // b: lmn xyz, lmx xyz, rmn xyz, rmx xyz
+      const bool lower = (j / 3) % 2 == 0;
+      f[j] = lower ? __double2float_rd(b[j]) : __double2float_ru(b[j]);
+    }
+    for (int j = 0; j < 12; j++) {
+      const float m = fabsf(f[j]);
+      // present children only; a NaN coordinate makes the scale NaN
+      if (hi32(j < 6 ? refs.x : refs.y) >= 0 && (m > scale || m != m) && scale == scale) scale = m;
+    }
+    float4* F = fbvh + 1 + 4 * (long long)k;
+    F[0] = make_float4(f[0], f[1], f[2], f[3]);
+    F[1] = make_float4(f[4], f[5], f[6], f[7]);
+    F[2] = make_float4(f[8], f[9], f[10], f[11]);
+    F[3] = make_float4(__int_as_float(lo32(refs.x)), __int_as_float(hi32(refs.x)), __int_as_float(lo32(refs.y)),
+                       __int_as_float(hi32(refs.y)));
+  }
+  // a NaN scale becomes +inf, which disables the float tests (RayF::all)
+  if (scale != scale) scale = __int_as_float(0x7f800000);
+  atomicMax(reinterpret_cast<unsigned*>(fbvh), __float_as_uint(scale));
+}
+
 // Records in BVH order back to mesh order (each record carries its triangle
 // id), with each triangle's normal normalize(e1 x e2) from the record's
 // edges, the operations the host and k_prep_records perform.
@@ -528,6 +566,12 @@ std::string prep_mesh_device(const double* h_vertices, int n, const double2* d_k
   k_prep_gather<<<grid_for(5LL * n, BS), BS, 0, s>>>(d_perm[0], n, out.brute, out.btris);
   PCK(cudaGetLastError());
 
+  // ---- the single-precision BVH of shadow rays
+  const int nb = bvh_internal_nodes(n, leaf);
+  PCK(cudaMemsetAsync(out.fbvh, 0, sizeof(float4), s));
+  k_prep_fbvh<<<grid_for(nb, BS), BS, 0, s>>>(out.bvh, nb, out.fbvh);
+  PCK(cudaGetLastError());
+
   // ---- k-d occurrences
   CubTemp occ_temp{A};
   PCK(occ_device(d_kd_nodes, n_kd_nodes, d_leaf_tris, n_index, n, s, A, occ_temp, out.occ, out.occ_off));
@@ -536,15 +580,18 @@ std::string prep_mesh_device(const double* h_vertices, int n, const double2* d_k
   return "";
 }
 
-std::string derive_mesh_device(const double2* d_btris, int n, const double2* d_kd_nodes, int n_kd_nodes,
-                               const int* d_leaf_tris, int n_index, cudaStream_t s, KdArena* arena,
-                               double2* brute, double4* normals, int2* occ, int* occ_off, cudaError_t* cuda_err) {
+std::string derive_mesh_device(const double2* d_bvh, int nb, const double2* d_btris, int n,
+                               const double2* d_kd_nodes, int n_kd_nodes, const int* d_leaf_tris, int n_index,
+                               cudaStream_t s, KdArena* arena, float4* fbvh, double2* brute, double4* normals,
+                               int2* occ, int* occ_off, cudaError_t* cuda_err) {
   *cuda_err = cudaSuccess;
   KdArena& A = *arena;
   A.reset();
   const int BS = 256;
-  if (n > 0) k_prep_unpermute<<<grid_for(n, BS), BS, 0, s>>>(d_btris, n, brute, normals);
-  cudaError_t e = cudaGetLastError();
+  cudaError_t e = cudaMemsetAsync(fbvh, 0, sizeof(float4), s);
+  if (e == cudaSuccess && nb > 0) k_prep_fbvh<<<grid_for(nb, BS), BS, 0, s>>>(d_bvh, nb, fbvh);
+  if (e == cudaSuccess && n > 0) k_prep_unpermute<<<grid_for(n, BS), BS, 0, s>>>(d_btris, n, brute, normals);
+  if (e == cudaSuccess) e = cudaGetLastError();
   CubTemp temp{A};
   if (e == cudaSuccess) e = occ_device(d_kd_nodes, n_kd_nodes, d_leaf_tris, n_index, n, s, A, temp, occ, occ_off);
   if (e != cudaSuccess) {

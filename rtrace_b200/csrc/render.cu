@@ -43,6 +43,9 @@ struct StagedCopy {
 // lists the device derives from its copied arrays (derive_mesh_device), at
 // the flush once the copies are queued.
 struct MeshDerive {
+  const double2* bvh;
+  int nb;
+  float4* fbvh;
   const double2* btris;
   int n;
   const double2* nodes;
@@ -287,8 +290,9 @@ rt_status arena_flush(rt_ctx* ctx, rt_scene* sc) {
   for (const MeshDerive& m : derive) {
     if (!ctx->kd_arena) ctx->kd_arena = kd_arena_new();
     cudaError_t ce = cudaSuccess;
-    std::string e = derive_mesh_device(m.btris, m.n, m.nodes, m.n_nodes, m.leaf_tris, m.n_index, ctx->stream,
-                                       ctx->kd_arena, m.brute, m.normals, m.occ, m.occ_off, &ce);
+    std::string e = derive_mesh_device(m.bvh, m.nb, m.btris, m.n, m.nodes, m.n_nodes, m.leaf_tris, m.n_index,
+                                       ctx->stream, ctx->kd_arena, m.fbvh, m.brute, m.normals, m.occ, m.occ_off,
+                                       &ce);
     if (!e.empty()) return cuda_fail(ctx, ce, e.c_str());
     queued = true;
   }
@@ -448,9 +452,11 @@ size_t scene_bytes_bound(const rt_scene_desc* d) {
   for (int m = 0; m < d->n_meshes; m++) {
     const rt_mesh_desc& md = d->meshes[m];
     size_t nt = (size_t)std::max<int64_t>(md.n_triangles, 0);
-    // triangle records twice (80 B), normals (32), BVH nodes (<= nt/2, 112 B),
-    // k-d nodes (64 + 8), leaf entries and occurrences (4 + 8), padding
-    b += nt * (80 * 2 + 32 + 64) + (size_t)std::max<int64_t>(md.n_nodes, 0) * 72 +
+    // triangle records twice (80 B), normals (32), BVH nodes in double and
+    // single precision (<= nt/2 nodes, 112 + 64 B, with a median split;
+    // an SAH tree with more spills to its own allocation), k-d nodes
+    // (64 + 8), leaf entries and occurrences (4 + 8), padding
+    b += nt * (80 * 2 + 32 + 88) + (size_t)std::max<int64_t>(md.n_nodes, 0) * 72 +
          (size_t)std::max<int64_t>(md.n_tri_index, 0) * 12 + 8 * 256;
   }
   // objects, spheres (+ run BVHs), planes, cubes, materials, lights
@@ -845,11 +851,13 @@ rt_status upload_prep_device(rt_ctx* ctx, rt_scene* sc, const rt_mesh_desc& md, 
   const int n = P->n_tris, nb = bvh_internal_nodes(n, kMeshLeaf);
   rt_status st;
   double2 *bvh, *btris, *brute;
+  float4* fbvh;
   double4* normals;
   int2* occ;
   int* occ_off;
   if ((st = upload_now(ctx, sc, P->nodes, &M.nodes)) != RT_OK || (st = upload_now(ctx, sc, P->leaf_tris, &M.leaf_tris)) != RT_OK ||
       (st = upload_now(ctx, sc, P->leaf_path, &M.leaf_path)) != RT_OK || (st = reserve(ctx, sc, 7 * (size_t)nb, &bvh)) != RT_OK ||
+      (st = reserve(ctx, sc, 1 + 4 * (size_t)nb, &fbvh)) != RT_OK ||
       (st = reserve(ctx, sc, 5 * (size_t)n, &btris)) != RT_OK || (st = reserve(ctx, sc, 5 * (size_t)n, &brute)) != RT_OK ||
       (st = reserve(ctx, sc, (size_t)n, &normals)) != RT_OK || (st = reserve(ctx, sc, (size_t)P->n_index, &occ)) != RT_OK ||
       (st = reserve(ctx, sc, (size_t)n + 1, &occ_off)) != RT_OK)
@@ -857,12 +865,13 @@ rt_status upload_prep_device(rt_ctx* ctx, rt_scene* sc, const rt_mesh_desc& md, 
   if (!ctx->kd_arena) ctx->kd_arena = kd_arena_new();
   cudaError_t ce = cudaSuccess;
   std::string e = prep_mesh_device(md.vertices, n, M.nodes, P->n_nodes, M.leaf_tris, P->n_index, kMeshLeaf,
-                                   ctx->stream, ctx->kd_arena, MeshPrepOut{bvh, btris, brute, normals, occ, occ_off},
-                                   &ce);
+                                   ctx->stream, ctx->kd_arena,
+                                   MeshPrepOut{bvh, fbvh, btris, brute, normals, occ, occ_off}, &ce);
   if (ce != cudaSuccess) return cuda_fail(ctx, ce, e.c_str());
   if (!e.empty()) return fail(ctx, RT_ERR_INVALID_ARGUMENT, e);
   sc->uploaded_bytes += 9 * (size_t)n * sizeof(double);
   M.bvh = bvh;
+  M.fbvh = fbvh;
   M.btris = btris;
   M.brute = brute;
   M.normals = normals;
@@ -908,15 +917,20 @@ rt_status upload_prep(rt_ctx* ctx, rt_scene* sc, const MeshPrep& P, DMesh* out) 
       return st;
   }
   const int n = P.n_tris;
+  const int nb = (int)((P.image ? P.len[0] : P.bvh.size() * sizeof(double2)) / (7 * sizeof(double2)));
+  float4* fbvh;
   double2* brute;
   double4* normals;
   int2* occ;
   int* occ_off;
-  if ((st = reserve(ctx, sc, 5 * (size_t)n, &brute)) != RT_OK || (st = reserve(ctx, sc, (size_t)n, &normals)) != RT_OK ||
+  if ((st = reserve(ctx, sc, 1 + 4 * (size_t)nb, &fbvh)) != RT_OK ||
+      (st = reserve(ctx, sc, 5 * (size_t)n, &brute)) != RT_OK || (st = reserve(ctx, sc, (size_t)n, &normals)) != RT_OK ||
       (st = reserve(ctx, sc, (size_t)P.n_index, &occ)) != RT_OK ||
       (st = reserve(ctx, sc, (size_t)n + 1, &occ_off)) != RT_OK)
     return st;
-  sc->derive.push_back(MeshDerive{M.btris, n, M.nodes, P.n_nodes, M.leaf_tris, P.n_index, brute, normals, occ, occ_off});
+  sc->derive.push_back(MeshDerive{M.bvh, nb, fbvh, M.btris, n, M.nodes, P.n_nodes, M.leaf_tris, P.n_index, brute,
+                                  normals, occ, occ_off});
+  M.fbvh = fbvh;
   M.brute = brute;
   M.normals = normals;
   M.occ = occ;
@@ -2212,12 +2226,14 @@ rt_status rt_debug_mesh_prep(rt_ctx* ctx, const rt_mesh_desc* md, uint32_t* mism
   const int n = D.n_tris, nb = bvh_internal_nodes(n, kMeshLeaf);
   std::vector<void*> tmp;
   double2 *dn, *bvh, *btris, *brute;
+  float4* fbvh;
   double4* normals;
   int *dl, *occ_off;
   int2* occ;
   cudaError_t ce = cudaSuccess;
   if ((ce = dalloc(tmp, &dn, D.nodes.size())) != cudaSuccess || (ce = dalloc(tmp, &dl, D.leaf_tris.size())) != cudaSuccess ||
-      (ce = dalloc(tmp, &bvh, 7 * (size_t)nb)) != cudaSuccess || (ce = dalloc(tmp, &btris, 5 * (size_t)n)) != cudaSuccess ||
+      (ce = dalloc(tmp, &bvh, 7 * (size_t)nb)) != cudaSuccess || (ce = dalloc(tmp, &fbvh, 1 + 4 * (size_t)nb)) != cudaSuccess ||
+      (ce = dalloc(tmp, &btris, 5 * (size_t)n)) != cudaSuccess ||
       (ce = dalloc(tmp, &brute, 5 * (size_t)n)) != cudaSuccess || (ce = dalloc(tmp, &normals, (size_t)n)) != cudaSuccess ||
       (ce = dalloc(tmp, &occ, (size_t)D.n_index)) != cudaSuccess || (ce = dalloc(tmp, &occ_off, (size_t)n + 1)) != cudaSuccess) {
     free_all(tmp);
@@ -2228,7 +2244,7 @@ rt_status rt_debug_mesh_prep(rt_ctx* ctx, const rt_mesh_desc* md, uint32_t* mism
   cudaMemcpyAsync(dl, D.leaf_tris.data(), D.leaf_tris.size() * sizeof(int), cudaMemcpyHostToDevice, ctx->stream);
   if (!ctx->kd_arena) ctx->kd_arena = kd_arena_new();
   e = prep_mesh_device(md->vertices, n, dn, D.n_nodes, dl, D.n_index, kMeshLeaf, ctx->stream, ctx->kd_arena,
-                       MeshPrepOut{bvh, btris, brute, normals, occ, occ_off}, &ce);
+                       MeshPrepOut{bvh, fbvh, btris, brute, normals, occ, occ_off}, &ce);
   if (!e.empty()) {
     free_all(tmp);
     return ce != cudaSuccess ? cuda_fail(ctx, ce, e.c_str()) : fail(ctx, RT_ERR_INVALID_ARGUMENT, e);
@@ -2254,8 +2270,8 @@ rt_status rt_debug_mesh_prep(rt_ctx* ctx, const rt_mesh_desc* md, uint32_t* mism
       (ce = cudaMemsetAsync(normals, 0xff, H.normals.size() * sizeof(double4), s)) == cudaSuccess &&
       (ce = cudaMemsetAsync(occ, 0xff, H.occ.size() * sizeof(int2), s)) == cudaSuccess &&
       (ce = cudaMemsetAsync(occ_off, 0xff, H.occ_off.size() * sizeof(int), s)) == cudaSuccess) {
-    e = derive_mesh_device(btris, n, dn, D.n_nodes, dl, D.n_index, s, ctx->kd_arena, brute, normals, occ, occ_off,
-                           &ce);
+    e = derive_mesh_device(bvh, nb, btris, n, dn, D.n_nodes, dl, D.n_index, s, ctx->kd_arena, fbvh, brute, normals,
+                           occ, occ_off, &ce);
     if (e.empty() && (ce = cudaStreamSynchronize(s)) == cudaSuccess &&
         (!same(brute, H.brute.data(), H.brute.size() * sizeof(double2)) ||
          !same(normals, H.normals.data(), H.normals.size() * sizeof(double4)) ||

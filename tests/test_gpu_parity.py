@@ -145,6 +145,67 @@ def test_mesh_queries_match_oracle(gpu_ctx, tmp_path, use_kd, stl_name):
     assert np.array_equal(outa[:, 0], refa[:, 0])
 
 
+def _culling_rays(centre, radius, rng):
+    """Rays aimed at the margins of single-precision box culling: exactly
+    axis-parallel rays and rays with one zero component through the mesh,
+    origins a million units away aimed at it, and direction components
+    below 1e-30."""
+    rays = []
+    for axis in range(3):
+        for sign in (1.0, -1.0):
+            o = centre + rng.uniform(-radius, radius, (150, 3))
+            o[:, axis] = centre[axis] - sign * 3 * radius
+            d = np.zeros((150, 3))
+            d[:, axis] = sign
+            rays.append(np.concatenate([o, d], 1))
+        o = centre + rng.uniform(-1.5 * radius, 1.5 * radius, (150, 3))
+        d = rng.normal(size=(150, 3))
+        d[:, axis] = 0.0
+        rays.append(np.concatenate([o, d], 1))
+    u = rng.normal(size=(300, 3))
+    u /= np.linalg.norm(u, axis=1, keepdims=True)
+    o = centre + 1e6 * u
+    aim = centre + rng.uniform(-radius, radius, (300, 3))
+    rays.append(np.concatenate([o, aim - o], 1))
+    o = centre + rng.uniform(-radius, radius, (150, 3))
+    o[:, 0] = centre[0] - 3 * radius
+    d = np.stack([np.ones(150), rng.normal(size=150) * 1e-35, rng.normal(size=150) * 0.3], 1)
+    rays.append(np.concatenate([o, d], 1))
+    return np.concatenate(rays)
+
+
+@pytest.mark.parametrize("use_kd", [True, False])
+def test_shadow_box_culling_margins(gpu_ctx, tmp_path, use_kd):
+    """Shadow rays cull mesh boxes in single precision, with margins taken
+    from the ray origin and the mesh's coordinate scale.  The any-hit answer
+    must stay the reference's on a mesh 25,000 units from the origin (float
+    spacing there is 2e-3 against triangles of 0.15) and on rays that put
+    those margins to the test."""
+    stl = os.path.join(str(tmp_path), "far.stl")
+    v, f = workloads.noisy_icosphere(3, 5)
+    v = v + np.array([1.0e4, -2.5e4, 3.0e3])
+    workloads.write_binary_stl(stl, v, f)
+    sc = rt.Scene.from_json_str(_mesh_scene(stl))
+    rng = np.random.default_rng(21)
+    centre = v.mean(0)
+    rays = np.concatenate([_surface_rays(stl, 2000, 13), _culling_rays(centre, 1.0, rng)])
+    for tmax in (0.7, 4.0, float("inf")):
+        refa = oracle_lib.mesh_hit(stl, rays, use_kdtree=use_kd, tmax=tmax)
+        outa = _gpu_mesh(gpu_ctx, sc, rays, use_kd, 2, tmax)
+        bad = np.nonzero(outa[:, 0] != refa[:, 0])[0]
+        assert len(bad) == 0, (tmax, len(bad), rays[bad[:3]].tolist())
+        assert 0 < refa[:, 0].sum() < len(rays)
+    # the same rays around the origin, where the margins are tightest
+    stl0 = os.path.join(str(tmp_path), "near.stl")
+    v0 = v - v.mean(0)
+    workloads.write_binary_stl(stl0, v0, f)
+    sc0 = rt.Scene.from_json_str(_mesh_scene(stl0))
+    rays0 = np.concatenate([_surface_rays(stl0, 2000, 14), _culling_rays(v0.mean(0), 1.0, rng)])
+    refa = oracle_lib.mesh_hit(stl0, rays0, use_kdtree=use_kd, tmax=4.0)
+    outa = _gpu_mesh(gpu_ctx, sc0, rays0, use_kd, 2, 4.0)
+    assert np.array_equal(outa[:, 0], refa[:, 0])
+
+
 def _synthetic_scenes(tmp):
     d = str(tmp)
     paths = {"sphere_grid": workloads.write_scene(d, "sphere_grid.json", workloads.sphere_grid_scene()),
