@@ -80,6 +80,7 @@ struct DMesh {
 // A run of consecutive spheres [first_obj, first_obj + count) in the World.
 struct DSphGroup {
   const double2* bvh;  // BVH nodes over the run; leaves index `order`
+  const float4* fbvh;  // the same BVH in single precision (FNode), which the walks test
   const int* order;    // BVH position -> position in the run
   int first_sphere;    // index of the run's first sphere in DScene::sph
   int first_obj;       // World index of the run's first sphere
@@ -614,6 +615,9 @@ struct FNodes {
 __device__ __forceinline__ FNodes mesh_nodes(const DMesh& M, const RayC& r) {
   return FNodes{M.fbvh, make_rayf(r, __ldg(M.fbvh).x)};
 }
+__device__ __forceinline__ FNodes group_nodes(const DSphGroup& G, const RayC& r) {
+  return FNodes{G.fbvh, make_rayf(r, __ldg(G.fbvh).x)};
+}
 
 // Generic BVH walk.  visit_leaf(first, count) tests a leaf's primitives and
 // returns true to stop; bound() is the current pruning t.  Children are
@@ -778,7 +782,7 @@ __device__ bool group_hit(const DScene& S, const DSphGroup& G, const RayC& r, do
   double bt = closest;
   int bi = -1;
   bool stop = bvh_walk(
-      DNodes{G.bvh, &r},
+      group_nodes(G, r),
       [&](int first, int cnt) {
         for (int k = 0; k < cnt; k++) {
           int sidx = __ldg(G.order + first + k);  // position in the run
@@ -1011,7 +1015,7 @@ __device__ __forceinline__ bool mesh_any_warp(const DMesh& M, const RayC& r, dou
 __device__ __forceinline__ bool group_any_warp(const DScene& S, const DSphGroup& G, const RayC& r, double tmin,
                                                double tmax, bool active, volatile int* stack, int* err, Work* w) {
   return bvh_any_warp(
-      DNodes{G.bvh, &r}, tmax, active,
+      group_nodes(G, r), tmax, active,
       [&](int first, int cnt) {
         for (int k = 0; k < cnt; k++) {
           int sidx = __ldg(G.order + first + k);

@@ -9,10 +9,12 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <cfloat>
 #include <chrono>
 #include <cmath>
 #include <cstdio>
 #include <cstring>
+#include <limits>
 #include <memory>
 #include <mutex>
 #include <string>
@@ -548,6 +550,51 @@ void put_bvh(const std::vector<BvhNode>& nodes, std::vector<double2>* out) {
     N[5] = double2{n.rmax[1], n.rmax[2]};
     N[6] = double2{pack2(n.lidx, n.lcnt), pack2(n.ridx, n.rcnt)};
   }
+}
+
+// A double rounded down (up) to a float: the float box holds the double one.
+float float_down(double x) {
+  if (x != x) return std::numeric_limits<float>::quiet_NaN();
+  if (x >= (double)FLT_MAX) return FLT_MAX;
+  if (x < -(double)FLT_MAX) return -std::numeric_limits<float>::infinity();
+  float f = (float)x;
+  return (double)f > x ? std::nextafter(f, -std::numeric_limits<float>::infinity()) : f;
+}
+float float_up(double x) { return -float_down(-x); }
+
+// The single-precision copy of a BVH that the device walks test (the FNode
+// layout of dscene.cuh, as mesh_prep.cu's k_prep_fbvh writes it for
+// meshes): child boxes rounded outwards, references as they are, and in
+// element 0 the largest |coordinate| of a present child's box (+inf when
+// one is NaN, which turns the float tests off).
+void put_fbvh(const std::vector<BvhNode>& nodes, std::vector<float4>* out) {
+  out->assign(1 + 4 * nodes.size(), float4{0.f, 0.f, 0.f, 0.f});
+  float scale = 0.0f;
+  for (size_t k = 0; k < nodes.size(); k++) {
+    const BvhNode& n = nodes[k];
+    float f[12];
+    for (int a = 0; a < 3; a++) {
+      f[a] = float_down(n.lmin[a]);
+      f[3 + a] = float_up(n.lmax[a]);
+      f[6 + a] = float_down(n.rmin[a]);
+      f[9 + a] = float_up(n.rmax[a]);
+    }
+    for (int j = 0; j < 12; j++) {
+      const float m = std::fabs(f[j]);
+      if ((j < 6 ? n.lcnt : n.rcnt) >= 0 && (m > scale || m != m) && scale == scale) scale = m;
+    }
+    float4* F = &(*out)[1 + 4 * k];
+    auto bits = [](int v) {
+      float x;
+      memcpy(&x, &v, sizeof x);
+      return x;
+    };
+    F[0] = float4{f[0], f[1], f[2], f[3]};
+    F[1] = float4{f[4], f[5], f[6], f[7]};
+    F[2] = float4{f[8], f[9], f[10], f[11]};
+    F[3] = float4{bits(n.lidx), bits(n.lcnt), bits(n.ridx), bits(n.rcnt)};
+  }
+  (*out)[0].x = scale == scale ? scale : std::numeric_limits<float>::infinity();
 }
 
 // Everything the device needs for one mesh, computed on the host: triangle
@@ -1086,10 +1133,15 @@ rt_status do_upload(rt_ctx* ctx, const rt_scene_desc* d, rt_scene** out,
       build_bvh(bmin, bmax, 8, 1e-6 * (1.0 + scale), &bn, &order);
       std::vector<double2> bvh;
       put_bvh(bn, &bvh);
+      std::vector<float4> fbvh;
+      put_fbvh(bn, &fbvh);
       DSphGroup G{};
       const double2* pb;
+      const float4* pf;
       rt_status st = upload(ctx, sc.get(), bvh, &pb);
       if (st != RT_OK) return st;
+      if ((st = upload(ctx, sc.get(), fbvh, &pf)) != RT_OK) return st;
+      G.fbvh = pf;
       std::vector<int> ord(order.begin(), order.end());
       const int* po;
       st = upload(ctx, sc.get(), ord, &po);
