@@ -43,14 +43,16 @@ TRAFFIC_FILE = os.path.join(ROOT, "profiles", "k_shadow_noisy_icosphere_1080p.md
 
 # Algorithmic bytes per unit of work of the any-hit (shadow) kernel: every
 # shadow ray reads its direction and distance (32 B) and its hit's origin
-# (24 B) and writes one visibility byte; each BVH node visit reads one node
-# (112 B), each triangle test one triangle record (80 B), each sphere test
-# one sphere (40 B), each verification unit one 16-byte k-d record.
-B_RAY, B_NODE, B_TRI, B_SPH, B_VERIFY = 57, 112, 80, 40, 16
+# (24 B) and writes one visibility byte; each BVH node visit reads one
+# single-precision node (64 B: two child boxes and their references), each
+# triangle test one triangle record (80 B), each sphere test one sphere
+# (40 B), each verification unit one 16-byte k-d record.
+B_RAY, B_NODE, B_TRI, B_SPH, B_VERIFY = 57, 64, 80, 40, 16
 # FP64 operations per unit (adds, multiplies, divisions and square roots of
-# the restated reference formulas): box pair 36, Moller-Trumbore 40,
-# sphere test 22, verification unit 2.
-F_NODE, F_TRI, F_SPH, F_VERIFY = 36, 40, 22, 2
+# the restated reference formulas): Moller-Trumbore 40, sphere test 22,
+# verification unit 2.  Node visits test their boxes in single precision
+# (24 FP32 operations for the pair) and count no FP64 operations.
+F_NODE, F_TRI, F_SPH, F_VERIFY = 0, 40, 22, 2
 
 
 def env_int(name, default):
