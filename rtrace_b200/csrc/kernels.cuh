@@ -423,9 +423,11 @@ __global__ void __launch_bounds__(128) k_emit(DFrame F, int level, long long c0)
   }
 }
 
-// world.hit(&shadow_ray, 0.001, distance).is_some() per shadow ray
+// world.hit(&shadow_ray, 0.001, distance).is_some() per shadow ray.  Seven
+// blocks of 128 per SM (72 registers): 1-2% faster on the bench frame than
+// 8 (64 registers, more spills) or 6.
 template <bool COUNT>
-__global__ void __launch_bounds__(128, 8) k_shadow(DFrame F, int level, long long c0) {
+__global__ void __launch_bounds__(128, 7) k_shadow(DFrame F, int level, long long c0) {
   long long nh = F.nhits[level];
   long long c1 = c0 + F.chunk_hits < nh ? c0 + F.chunk_hits : nh;
   const int K = F.K;
