@@ -681,8 +681,10 @@ void parallel_ranges(long long n, F f) {
   for (auto& t : th) t.join();
 }
 
-// Triangles per mesh BVH leaf (measured fastest of 2-16 on the mesh frame).
-const int kMeshLeaf = 8;
+// Triangles per mesh BVH leaf.  With single-precision box tests 4 is
+// fastest on the 82k-triangle mesh frame (7.21 ms; 2: 7.31, 3: 7.26,
+// 5: 7.28, 6: 7.30, 8: 7.39, 12: 7.68); with double boxes it was 8.
+const int kMeshLeaf = 4;
 // Meshes from this many triangles up are prepared on the device (median
 // split BVH, tens of ms for millions of triangles); smaller ones on the
 // host with a binned SAH BVH (about 7% fewer node visits per ray, 4% on the
