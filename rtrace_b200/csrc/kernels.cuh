@@ -468,8 +468,11 @@ __global__ void __launch_bounds__(128, 7) k_shadow(DFrame F, int level, long lon
 }
 
 // phong_lighting's sum, fog and the reflection ray (src/lighting.rs:220-288,
-// 297-319, 437-496) for hits [c0, c1).
-__global__ void __launch_bounds__(128) k_resolve(DFrame F, int level, long long c0) {
+// 297-319, 437-496) for hits [c0, c1).  Eight blocks of 128 per SM (64
+// registers, some spilled): the kernel streams the shadow buffer, and the
+// extra warps hide more of its latency than the spills cost (bench frame
+// 7.0 ms against 7.23 ms at 128 registers; 6, 10 and 12 blocks were slower).
+__global__ void __launch_bounds__(128, 8) k_resolve(DFrame F, int level, long long c0) {
   const DScene& S = F.S;
   long long nh = F.nhits[level];
   long long c1 = c0 + F.chunk_hits < nh ? c0 + F.chunk_hits : nh;
