@@ -71,6 +71,7 @@ struct DMesh {
   const double2* nodes;    // reference k-d tree, preorder
   const int* leaf_tris;    // k-d leaf triangle lists, leaf order (KdNode::Leaf.triangles)
   const int2* leaf_path;   // per k-d node: {path bits (bit k: right at depth k), depth}
+  const double2* cells;    // per k-d leaf: its cell lo < p <= hi (3 double2: lo.xyz, hi.xyz)
   const int* occ_off;      // per triangle: occurrences [occ_off[t], occ_off[t+1])
   const int2* occ;         // {k-d leaf node, position in the leaf}
   int n_nodes;
@@ -390,16 +391,52 @@ __device__ __forceinline__ int kd_locate_visited(const DMesh& M, const RayC& r, 
   return -1;
 }
 
-// Whether the reference tests triangle `tri` (hit at t) for this ray.  The
-// leaf whose cell holds the hit point is tried first; when it holds the
-// triangle and is visited, that settles it (need_order == false).
+// Whether the reference tests triangle `tri` (hit at t) for this ray, for
+// the leaf whose cell holds the hit point p = o + t d: true when that leaf
+// holds the triangle and the reference visits it.  false leaves the
+// question to tri_first_visit (every leaf holding the triangle).
+//
+// p's leaf is found among the triangle's own leaves by their cells (the
+// points whose descent, left iff p[axis] <= split, ends there), which is
+// exactly where kd_locate_visited's descent would end.  The visiting rules
+// on the way need no descent either, for t > 0:
+//   * a split on an axis the reference treats as parallel lets the ray
+//     into the origin's side only, so the origin must lie in the cell on
+//     that axis too;
+//   * on any other axis p's side is the near side (always visited) or the
+//     far side, and then split_ahead holds: p = fl(o + fl(t d)) with t > 0
+//     can only end on the other side of the split from o if d points
+//     there (rounding is monotone), which is split_ahead's sign test.
+// So the leaf is visited iff those origin checks and its slab test pass.
 __device__ __forceinline__ bool tri_visited_fast(const DMesh& M, const RayC& r, int tri, double t, Work* w) {
-  unsigned key;
-  int leaf = kd_locate_visited(M, r, r.o + t * r.d, &key, w);
-  if (leaf < 0) return false;
-  int b = __ldg(M.occ_off + tri), e = __ldg(M.occ_off + tri + 1);
-  for (int k = b; k < e; k++)
-    if (__ldg(M.occ + k).x == leaf) return true;
+  const V3 p = r.o + t * r.d;
+  const int b = __ldg(M.occ_off + tri), e = __ldg(M.occ_off + tri + 1);
+  if (!(t > 0.0)) {
+    unsigned key;
+    const int leaf = kd_locate_visited(M, r, p, &key, w);
+    if (leaf < 0) return false;
+    for (int k = b; k < e; k++)
+      if (__ldg(M.occ + k).x == leaf) return true;
+    return false;
+  }
+  for (int k = b; k < e; k++) {
+    const int leaf = __ldg(M.occ + k).x;
+    const double2* C = M.cells + 3 * (size_t)leaf;
+    const double2 c0 = __ldg(C), c1 = __ldg(C + 1), c2 = __ldg(C + 2);
+    const double lo[3] = {c0.x, c0.y, c1.x}, hi[3] = {c1.y, c2.x, c2.y};
+    if (w) w->verify += 4;
+    bool in = true;
+#pragma unroll
+    for (int a = 0; a < 3; a++) in = in && p[a] > lo[a] && p[a] <= hi[a];
+    if (!in) continue;
+    // the cells of a tree's leaves do not overlap: this is p's leaf
+#pragma unroll
+    for (int a = 0; a < 3; a++)
+      if ((r.par & (1 << a)) && !(r.o[a] > lo[a] && r.o[a] <= hi[a])) return false;
+    if (w) w->verify += 3;
+    double te;
+    return kd_slab(M.nodes + 4 * (size_t)leaf, r, &te);
+  }
   return false;
 }
 

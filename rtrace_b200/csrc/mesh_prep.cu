@@ -274,6 +274,49 @@ __global__ void k_prep_unpermute(const double2* __restrict__ btris, int n, doubl
   }
 }
 
+// The cell of each k-d leaf: the points whose descent (left iff
+// p[axis] <= split) ends there, lo < p <= hi per axis, from the splits on
+// its root path (leaf_path: bit j = right at depth j).  A right turn raises
+// lo to the split, a left turn lowers hi to it.  A leaf whose path meets a
+// NaN split (which sends every point right), or does not lead to it, gets
+// lo = +inf: no point is in it, and the caller falls back to a descent.
+// Internal nodes get an empty cell as well.
+__global__ void k_prep_cells(const double2* __restrict__ kd, int nk, const int2* __restrict__ leaf_path,
+                             double2* __restrict__ cells) {
+  const double INF = __longlong_as_double(0x7ff0000000000000LL);
+  for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < nk; k += gridDim.x * blockDim.x) {
+    double lo[3] = {-INF, -INF, -INF}, hi[3] = {INF, INF, INF};
+    bool ok = hi32(kd[4 * (long long)k + 3].y) < 0;  // leaves only
+    if (ok) {
+      const int2 pd = leaf_path[k];
+      int node = 0;
+      for (int j = 0; ok && j < pd.y && j < 31; j++) {
+        const double2 n3 = kd[4 * (long long)node + 3];
+        const int right = lo32(n3.y), axis = hi32(n3.y);
+        const double split = n3.x;
+        if (axis < 0 || axis > 2 || split != split) {
+          ok = false;
+          break;
+        }
+        if ((pd.x >> j) & 1) {
+          lo[axis] = fmax(lo[axis], split);
+          node = right;
+        } else {
+          hi[axis] = fmin(hi[axis], split);
+          node = node + 1;
+        }
+        if (node < 0 || node >= nk) ok = false;
+      }
+      ok = ok && node == k;
+    }
+    if (!ok) lo[0] = INF;
+    double2* C = cells + 3 * (long long)k;
+    C[0] = double2{lo[0], lo[1]};
+    C[1] = double2{lo[2], hi[0]};
+    C[2] = double2{hi[1], hi[2]};
+  }
+}
+
 // Leaf entries per k-d node (0 for internal nodes).
 __global__ void k_prep_leaf_counts(const double2* __restrict__ kd, int nk, int* __restrict__ cnt) {
   for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < nk; k += gridDim.x * blockDim.x) {
@@ -395,8 +438,8 @@ int bvh_internal_nodes(int n, int leaf) {
 }
 
 std::string prep_mesh_device(const double* h_vertices, int n, const double2* d_kd_nodes, int n_kd_nodes,
-                             const int* d_leaf_tris, int n_index, int leaf, cudaStream_t s, KdArena* arena,
-                             const MeshPrepOut& out, cudaError_t* cuda_err) {
+                             const int* d_leaf_tris, const int2* d_leaf_path, int n_index, int leaf, cudaStream_t s,
+                             KdArena* arena, const MeshPrepOut& out, cudaError_t* cuda_err) {
   *cuda_err = cudaSuccess;
   if (n <= leaf) return "mesh too small for the device preparation";
 #define PCK(call)                                                               \
@@ -566,10 +609,12 @@ std::string prep_mesh_device(const double* h_vertices, int n, const double2* d_k
   k_prep_gather<<<grid_for(5LL * n, BS), BS, 0, s>>>(d_perm[0], n, out.brute, out.btris);
   PCK(cudaGetLastError());
 
-  // ---- the single-precision BVH of shadow rays
+  // ---- the single-precision BVH, the k-d leaf cells
   const int nb = bvh_internal_nodes(n, leaf);
   PCK(cudaMemsetAsync(out.fbvh, 0, sizeof(float4), s));
   k_prep_fbvh<<<grid_for(nb, BS), BS, 0, s>>>(out.bvh, nb, out.fbvh);
+  if (n_kd_nodes > 0)
+    k_prep_cells<<<grid_for(n_kd_nodes, BS), BS, 0, s>>>(d_kd_nodes, n_kd_nodes, d_leaf_path, out.cells);
   PCK(cudaGetLastError());
 
   // ---- k-d occurrences
@@ -581,15 +626,18 @@ std::string prep_mesh_device(const double* h_vertices, int n, const double2* d_k
 }
 
 std::string derive_mesh_device(const double2* d_bvh, int nb, const double2* d_btris, int n,
-                               const double2* d_kd_nodes, int n_kd_nodes, const int* d_leaf_tris, int n_index,
-                               cudaStream_t s, KdArena* arena, float4* fbvh, double2* brute, double4* normals,
-                               int2* occ, int* occ_off, cudaError_t* cuda_err) {
+                               const double2* d_kd_nodes, int n_kd_nodes, const int* d_leaf_tris,
+                               const int2* d_leaf_path, int n_index, cudaStream_t s, KdArena* arena, float4* fbvh,
+                               double2* cells, double2* brute, double4* normals, int2* occ, int* occ_off,
+                               cudaError_t* cuda_err) {
   *cuda_err = cudaSuccess;
   KdArena& A = *arena;
   A.reset();
   const int BS = 256;
   cudaError_t e = cudaMemsetAsync(fbvh, 0, sizeof(float4), s);
   if (e == cudaSuccess && nb > 0) k_prep_fbvh<<<grid_for(nb, BS), BS, 0, s>>>(d_bvh, nb, fbvh);
+  if (e == cudaSuccess && n_kd_nodes > 0)
+    k_prep_cells<<<grid_for(n_kd_nodes, BS), BS, 0, s>>>(d_kd_nodes, n_kd_nodes, d_leaf_path, cells);
   if (e == cudaSuccess && n > 0) k_prep_unpermute<<<grid_for(n, BS), BS, 0, s>>>(d_btris, n, brute, normals);
   if (e == cudaSuccess) e = cudaGetLastError();
   CubTemp temp{A};

@@ -53,7 +53,9 @@ struct MeshDerive {
   const double2* nodes;
   int n_nodes;
   const int* leaf_tris;
+  const int2* leaf_path;
   int n_index;
+  double2* cells;
   double2* brute;
   double4* normals;
   int2* occ;
@@ -292,9 +294,9 @@ rt_status arena_flush(rt_ctx* ctx, rt_scene* sc) {
   for (const MeshDerive& m : derive) {
     if (!ctx->kd_arena) ctx->kd_arena = kd_arena_new();
     cudaError_t ce = cudaSuccess;
-    std::string e = derive_mesh_device(m.bvh, m.nb, m.btris, m.n, m.nodes, m.n_nodes, m.leaf_tris, m.n_index,
-                                       ctx->stream, ctx->kd_arena, m.fbvh, m.brute, m.normals, m.occ, m.occ_off,
-                                       &ce);
+    std::string e = derive_mesh_device(m.bvh, m.nb, m.btris, m.n, m.nodes, m.n_nodes, m.leaf_tris, m.leaf_path,
+                                       m.n_index, ctx->stream, ctx->kd_arena, m.fbvh, m.cells, m.brute, m.normals,
+                                       m.occ, m.occ_off, &ce);
     if (!e.empty()) return cuda_fail(ctx, ce, e.c_str());
     queued = true;
   }
@@ -457,8 +459,9 @@ size_t scene_bytes_bound(const rt_scene_desc* d) {
     // triangle records twice (80 B), normals (32), BVH nodes in double and
     // single precision (<= nt/2 nodes, 112 + 64 B, with a median split;
     // an SAH tree with more spills to its own allocation), k-d nodes
-    // (64 + 8), leaf entries and occurrences (4 + 8), padding
-    b += nt * (80 * 2 + 32 + 88) + (size_t)std::max<int64_t>(md.n_nodes, 0) * 72 +
+    // (64 + 8) and leaf cells (48), leaf entries and occurrences (4 + 8),
+    // padding
+    b += nt * (80 * 2 + 32 + 88) + (size_t)std::max<int64_t>(md.n_nodes, 0) * 120 +
          (size_t)std::max<int64_t>(md.n_tri_index, 0) * 12 + 8 * 256;
   }
   // objects, spheres (+ run BVHs), planes, cubes, materials, lights
@@ -899,7 +902,7 @@ rt_status upload_prep_device(rt_ctx* ctx, rt_scene* sc, const rt_mesh_desc& md, 
   M.n_tris = P->n_tris;
   const int n = P->n_tris, nb = bvh_internal_nodes(n, kMeshLeaf);
   rt_status st;
-  double2 *bvh, *btris, *brute;
+  double2 *bvh, *btris, *brute, *cells;
   float4* fbvh;
   double4* normals;
   int2* occ;
@@ -907,20 +910,22 @@ rt_status upload_prep_device(rt_ctx* ctx, rt_scene* sc, const rt_mesh_desc& md, 
   if ((st = upload_now(ctx, sc, P->nodes, &M.nodes)) != RT_OK || (st = upload_now(ctx, sc, P->leaf_tris, &M.leaf_tris)) != RT_OK ||
       (st = upload_now(ctx, sc, P->leaf_path, &M.leaf_path)) != RT_OK || (st = reserve(ctx, sc, 7 * (size_t)nb, &bvh)) != RT_OK ||
       (st = reserve(ctx, sc, 1 + 4 * (size_t)nb, &fbvh)) != RT_OK ||
+      (st = reserve(ctx, sc, 3 * (size_t)P->n_nodes, &cells)) != RT_OK ||
       (st = reserve(ctx, sc, 5 * (size_t)n, &btris)) != RT_OK || (st = reserve(ctx, sc, 5 * (size_t)n, &brute)) != RT_OK ||
       (st = reserve(ctx, sc, (size_t)n, &normals)) != RT_OK || (st = reserve(ctx, sc, (size_t)P->n_index, &occ)) != RT_OK ||
       (st = reserve(ctx, sc, (size_t)n + 1, &occ_off)) != RT_OK)
     return st;
   if (!ctx->kd_arena) ctx->kd_arena = kd_arena_new();
   cudaError_t ce = cudaSuccess;
-  std::string e = prep_mesh_device(md.vertices, n, M.nodes, P->n_nodes, M.leaf_tris, P->n_index, kMeshLeaf,
-                                   ctx->stream, ctx->kd_arena,
-                                   MeshPrepOut{bvh, fbvh, btris, brute, normals, occ, occ_off}, &ce);
+  std::string e = prep_mesh_device(md.vertices, n, M.nodes, P->n_nodes, M.leaf_tris, M.leaf_path, P->n_index,
+                                   kMeshLeaf, ctx->stream, ctx->kd_arena,
+                                   MeshPrepOut{bvh, fbvh, cells, btris, brute, normals, occ, occ_off}, &ce);
   if (ce != cudaSuccess) return cuda_fail(ctx, ce, e.c_str());
   if (!e.empty()) return fail(ctx, RT_ERR_INVALID_ARGUMENT, e);
   sc->uploaded_bytes += 9 * (size_t)n * sizeof(double);
   M.bvh = bvh;
   M.fbvh = fbvh;
+  M.cells = cells;
   M.btris = btris;
   M.brute = brute;
   M.normals = normals;
@@ -968,18 +973,20 @@ rt_status upload_prep(rt_ctx* ctx, rt_scene* sc, const MeshPrep& P, DMesh* out) 
   const int n = P.n_tris;
   const int nb = (int)((P.image ? P.len[0] : P.bvh.size() * sizeof(double2)) / (7 * sizeof(double2)));
   float4* fbvh;
-  double2* brute;
+  double2 *cells, *brute;
   double4* normals;
   int2* occ;
   int* occ_off;
   if ((st = reserve(ctx, sc, 1 + 4 * (size_t)nb, &fbvh)) != RT_OK ||
+      (st = reserve(ctx, sc, 3 * (size_t)P.n_nodes, &cells)) != RT_OK ||
       (st = reserve(ctx, sc, 5 * (size_t)n, &brute)) != RT_OK || (st = reserve(ctx, sc, (size_t)n, &normals)) != RT_OK ||
       (st = reserve(ctx, sc, (size_t)P.n_index, &occ)) != RT_OK ||
       (st = reserve(ctx, sc, (size_t)n + 1, &occ_off)) != RT_OK)
     return st;
-  sc->derive.push_back(MeshDerive{M.bvh, nb, fbvh, M.btris, n, M.nodes, P.n_nodes, M.leaf_tris, P.n_index, brute,
-                                  normals, occ, occ_off});
+  sc->derive.push_back(MeshDerive{M.bvh, nb, fbvh, M.btris, n, M.nodes, P.n_nodes, M.leaf_tris, M.leaf_path,
+                                  P.n_index, cells, brute, normals, occ, occ_off});
   M.fbvh = fbvh;
+  M.cells = cells;
   M.brute = brute;
   M.normals = normals;
   M.occ = occ;
@@ -2287,13 +2294,15 @@ rt_status rt_debug_mesh_prep(rt_ctx* ctx, const rt_mesh_desc* md, uint32_t* mism
   if (!e.empty()) return fail(ctx, RT_ERR_INVALID_ARGUMENT, e);
   const int n = D.n_tris, nb = bvh_internal_nodes(n, kMeshLeaf);
   std::vector<void*> tmp;
-  double2 *dn, *bvh, *btris, *brute;
+  double2 *dn, *bvh, *btris, *brute, *cells;
   float4* fbvh;
   double4* normals;
   int *dl, *occ_off;
-  int2* occ;
+  int2 *occ, *dp;
   cudaError_t ce = cudaSuccess;
   if ((ce = dalloc(tmp, &dn, D.nodes.size())) != cudaSuccess || (ce = dalloc(tmp, &dl, D.leaf_tris.size())) != cudaSuccess ||
+      (ce = dalloc(tmp, &dp, D.leaf_path.size())) != cudaSuccess ||
+      (ce = dalloc(tmp, &cells, 3 * (size_t)D.n_nodes)) != cudaSuccess ||
       (ce = dalloc(tmp, &bvh, 7 * (size_t)nb)) != cudaSuccess || (ce = dalloc(tmp, &fbvh, 1 + 4 * (size_t)nb)) != cudaSuccess ||
       (ce = dalloc(tmp, &btris, 5 * (size_t)n)) != cudaSuccess ||
       (ce = dalloc(tmp, &brute, 5 * (size_t)n)) != cudaSuccess || (ce = dalloc(tmp, &normals, (size_t)n)) != cudaSuccess ||
@@ -2304,9 +2313,10 @@ rt_status rt_debug_mesh_prep(rt_ctx* ctx, const rt_mesh_desc* md, uint32_t* mism
   // on the context's stream (non-blocking), which the preparations below use
   cudaMemcpyAsync(dn, D.nodes.data(), D.nodes.size() * sizeof(double2), cudaMemcpyHostToDevice, ctx->stream);
   cudaMemcpyAsync(dl, D.leaf_tris.data(), D.leaf_tris.size() * sizeof(int), cudaMemcpyHostToDevice, ctx->stream);
+  cudaMemcpyAsync(dp, D.leaf_path.data(), D.leaf_path.size() * sizeof(int2), cudaMemcpyHostToDevice, ctx->stream);
   if (!ctx->kd_arena) ctx->kd_arena = kd_arena_new();
-  e = prep_mesh_device(md->vertices, n, dn, D.n_nodes, dl, D.n_index, kMeshLeaf, ctx->stream, ctx->kd_arena,
-                       MeshPrepOut{bvh, fbvh, btris, brute, normals, occ, occ_off}, &ce);
+  e = prep_mesh_device(md->vertices, n, dn, D.n_nodes, dl, dp, D.n_index, kMeshLeaf, ctx->stream, ctx->kd_arena,
+                       MeshPrepOut{bvh, fbvh, cells, btris, brute, normals, occ, occ_off}, &ce);
   if (!e.empty()) {
     free_all(tmp);
     return ce != cudaSuccess ? cuda_fail(ctx, ce, e.c_str()) : fail(ctx, RT_ERR_INVALID_ARGUMENT, e);
@@ -2332,8 +2342,8 @@ rt_status rt_debug_mesh_prep(rt_ctx* ctx, const rt_mesh_desc* md, uint32_t* mism
       (ce = cudaMemsetAsync(normals, 0xff, H.normals.size() * sizeof(double4), s)) == cudaSuccess &&
       (ce = cudaMemsetAsync(occ, 0xff, H.occ.size() * sizeof(int2), s)) == cudaSuccess &&
       (ce = cudaMemsetAsync(occ_off, 0xff, H.occ_off.size() * sizeof(int), s)) == cudaSuccess) {
-    e = derive_mesh_device(bvh, nb, btris, n, dn, D.n_nodes, dl, D.n_index, s, ctx->kd_arena, fbvh, brute, normals,
-                           occ, occ_off, &ce);
+    e = derive_mesh_device(bvh, nb, btris, n, dn, D.n_nodes, dl, dp, D.n_index, s, ctx->kd_arena, fbvh, cells, brute,
+                           normals, occ, occ_off, &ce);
     if (e.empty() && (ce = cudaStreamSynchronize(s)) == cudaSuccess &&
         (!same(brute, H.brute.data(), H.brute.size() * sizeof(double2)) ||
          !same(normals, H.normals.data(), H.normals.size() * sizeof(double4)) ||
