@@ -359,84 +359,49 @@ __device__ __forceinline__ bool kd_leaf_visited(const DMesh& M, const RayC& r, i
   return true;
 }
 
-// Descends the reference's k-d tree towards the leaf whose cell holds point
-// p (a candidate's hit point), checking the reference's visiting rules on
-// the way.  Returns that leaf if the reference tests it, else -1.
-__device__ __forceinline__ int kd_locate_visited(const DMesh& M, const RayC& r, V3 p, unsigned* key, Work* w) {
-  int node = 0;
-  unsigned k_out = 0;
-  for (int depth = 0; depth < 32; depth++) {
-    double2 n3 = __ldg(M.nodes + 4 * (size_t)node + 3);
-    if (w) w->verify++;
-    int right = lo32(n3.y), axis = hi32(n3.y);
-    if (axis < 0) {
-      if (w) w->verify += 3;
-      double te;
-      if (!kd_slab(M.nodes + 4 * (size_t)node, r, &te)) return -1;
-      *key = k_out;
-      return node;
-    }
-    double split = n3.x;
-    bool go_right = !(p[axis] <= split);
-    double op = r.o[axis];
-    bool left_side = op <= split;
-    if (r.par & (1 << axis)) {
-      if (go_right == left_side) return -1;
-    } else if (go_right == left_side) {
-      if (!split_ahead(split, op, r.d[axis])) return -1;
-      k_out |= 1u << (31 - depth);
-    }
-    node = go_right ? right : node + 1;
+// kd_leaf_visited's answer without its root-to-leaf walk, from the leaf's
+// cell: per axis, lo = the largest split the path turns right at and hi =
+// the smallest it turns left at (k_prep_cells).  The walk fails at a
+// right turn at split s only when o <= s and split_ahead(s, o, d) fails,
+// and that happens at some right turn of an axis exactly when
+// !(o > lo || d > 0 || (o == lo && d == d)); at a left turn only when
+// o > s and d is not negative, i.e. when !(o <= hi || d < 0).  On an axis
+// the reference treats as parallel, the origin must be on the leaf's side
+// of every split: lo < o <= hi.  Then the leaf's slab test.  A cell that
+// could not be built (NaN split on the path, marked by a NaN lo) or a
+// non-finite origin takes the walk.
+__device__ __forceinline__ bool kd_leaf_visited_cell(const DMesh& M, const RayC& r, int leaf, Work* w) {
+  const double2* C = M.cells + 3 * (size_t)leaf;
+  const double2 c0 = __ldg(C), c1 = __ldg(C + 1), c2 = __ldg(C + 2);
+  const double lo[3] = {c0.x, c0.y, c1.x}, hi[3] = {c1.y, c2.x, c2.y};
+  if (w) w->verify += 4;
+  const bool finite_o = fabs(r.o.x) < RTB_INF && fabs(r.o.y) < RTB_INF && fabs(r.o.z) < RTB_INF;
+  if (lo[0] != lo[0] || !finite_o) {
+    if (w) w->verify += (unsigned)__ldg(M.leaf_path + leaf).y;
+    unsigned key;
+    return kd_leaf_visited(M, r, leaf, &key);
   }
-  return -1;
+#pragma unroll
+  for (int a = 0; a < 3; a++) {
+    const double o = r.o[a], d = r.d[a];
+    if (r.par & (1 << a)) {
+      if (!(o > lo[a] && o <= hi[a])) return false;
+    } else {
+      if (!(o > lo[a] || d > 0.0 || (o == lo[a] && d == d))) return false;
+      if (!(o <= hi[a] || d < 0.0)) return false;
+    }
+  }
+  if (w) w->verify += 3;
+  double te;
+  return kd_slab(M.nodes + 4 * (size_t)leaf, r, &te);
 }
 
-// Whether the reference tests triangle `tri` (hit at t) for this ray, for
-// the leaf whose cell holds the hit point p = o + t d: true when that leaf
-// holds the triangle and the reference visits it.  false leaves the
-// question to tri_first_visit (every leaf holding the triangle).
-//
-// p's leaf is found among the triangle's own leaves by their cells (the
-// points whose descent, left iff p[axis] <= split, ends there), which is
-// exactly where kd_locate_visited's descent would end.  The visiting rules
-// on the way need no descent either, for t > 0:
-//   * a split on an axis the reference treats as parallel lets the ray
-//     into the origin's side only, so the origin must lie in the cell on
-//     that axis too;
-//   * on any other axis p's side is the near side (always visited) or the
-//     far side, and then split_ahead holds: p = fl(o + fl(t d)) with t > 0
-//     can only end on the other side of the split from o if d points
-//     there (rounding is monotone), which is split_ahead's sign test.
-// So the leaf is visited iff those origin checks and its slab test pass.
-__device__ __forceinline__ bool tri_visited_fast(const DMesh& M, const RayC& r, int tri, double t, Work* w) {
-  const V3 p = r.o + t * r.d;
+// Whether the reference tests triangle `tri` for this ray: whether it
+// visits some k-d leaf holding it.
+__device__ __forceinline__ bool tri_visited(const DMesh& M, const RayC& r, int tri, Work* w) {
   const int b = __ldg(M.occ_off + tri), e = __ldg(M.occ_off + tri + 1);
-  if (!(t > 0.0)) {
-    unsigned key;
-    const int leaf = kd_locate_visited(M, r, p, &key, w);
-    if (leaf < 0) return false;
-    for (int k = b; k < e; k++)
-      if (__ldg(M.occ + k).x == leaf) return true;
-    return false;
-  }
-  for (int k = b; k < e; k++) {
-    const int leaf = __ldg(M.occ + k).x;
-    const double2* C = M.cells + 3 * (size_t)leaf;
-    const double2 c0 = __ldg(C), c1 = __ldg(C + 1), c2 = __ldg(C + 2);
-    const double lo[3] = {c0.x, c0.y, c1.x}, hi[3] = {c1.y, c2.x, c2.y};
-    if (w) w->verify += 4;
-    bool in = true;
-#pragma unroll
-    for (int a = 0; a < 3; a++) in = in && p[a] > lo[a] && p[a] <= hi[a];
-    if (!in) continue;
-    // the cells of a tree's leaves do not overlap: this is p's leaf
-#pragma unroll
-    for (int a = 0; a < 3; a++)
-      if ((r.par & (1 << a)) && !(r.o[a] > lo[a] && r.o[a] <= hi[a])) return false;
-    if (w) w->verify += 3;
-    double te;
-    return kd_slab(M.nodes + 4 * (size_t)leaf, r, &te);
-  }
+  for (int k = b; k < e; k++)
+    if (kd_leaf_visited_cell(M, r, __ldg(M.occ + k).x, w)) return true;
   return false;
 }
 
@@ -760,7 +725,7 @@ __device__ bool mesh_closest(const DMesh& M, const RayC& r, double tmin, double&
     best_tri = bi;
     return true;
   }
-  if (nt == 1 && tri_visited_fast(M, r, ties[0], bt, w)) {
+  if (nt == 1 && tri_visited(M, r, ties[0], w)) {
     closest = bt;
     best_tri = ties[0];
     return true;
@@ -799,9 +764,7 @@ __device__ bool mesh_any(const DMesh& M, const RayC& r, double tmin, double tmax
           if (w) w->tris++;
           if (tri_t(E, r, tmin, tmax, &t)) {
             if (!use_kd) return true;
-            int tri = lo32(__ldg(E + 4).y);
-            unsigned long long o;
-            if (tri_visited_fast(M, r, tri, t, w) || tri_first_visit(M, r, tri, &o, w)) return true;
+            if (tri_visited(M, r, lo32(__ldg(E + 4).y), w)) return true;
           }
         }
         return false;
@@ -1038,9 +1001,7 @@ __device__ __forceinline__ bool mesh_any_warp(const DMesh& M, const RayC& r, dou
           if (w) w->tris++;
           if (tri_t(E, r, tmin, tmax, &t)) {
             if (!use_kd) return true;
-            int tri = lo32(__ldg(E + 4).y);
-            unsigned long long o;
-            if (tri_visited_fast(M, r, tri, t, w) || tri_first_visit(M, r, tri, &o, w)) return true;
+            if (tri_visited(M, r, lo32(__ldg(E + 4).y), w)) return true;
           }
         }
         return false;

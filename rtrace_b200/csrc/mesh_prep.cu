@@ -274,13 +274,12 @@ __global__ void k_prep_unpermute(const double2* __restrict__ btris, int n, doubl
   }
 }
 
-// The cell of each k-d leaf: the points whose descent (left iff
-// p[axis] <= split) ends there, lo < p <= hi per axis, from the splits on
-// its root path (leaf_path: bit j = right at depth j).  A right turn raises
-// lo to the split, a left turn lowers hi to it.  A leaf whose path meets a
-// NaN split (which sends every point right), or does not lead to it, gets
-// lo = +inf: no point is in it, and the caller falls back to a descent.
-// Internal nodes get an empty cell as well.
+// The cell of each k-d leaf from the splits on its root path (leaf_path:
+// bit j = right at depth j): per axis, lo = the largest split the path
+// turns right at and hi = the smallest it turns left at (-inf / +inf when
+// there is none), so the leaf's cell is lo < p <= hi.  A leaf whose path
+// meets a NaN split, or does not lead to it, gets a NaN lo, which sends
+// callers back to the walk.  Internal nodes get the same mark.
 __global__ void k_prep_cells(const double2* __restrict__ kd, int nk, const int2* __restrict__ leaf_path,
                              double2* __restrict__ cells) {
   const double INF = __longlong_as_double(0x7ff0000000000000LL);
@@ -309,7 +308,7 @@ __global__ void k_prep_cells(const double2* __restrict__ kd, int nk, const int2*
       }
       ok = ok && node == k;
     }
-    if (!ok) lo[0] = INF;
+    if (!ok) lo[0] = __longlong_as_double(0x7ff8000000000000LL);
     double2* C = cells + 3 * (long long)k;
     C[0] = double2{lo[0], lo[1]};
     C[1] = double2{lo[2], hi[0]};
