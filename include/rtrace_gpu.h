@@ -488,7 +488,12 @@ rt_status rt_debug_disk_offsets(rt_ctx* ctx, const uint64_t* light_seeds, int64_
 rt_status rt_debug_fp64_rate(rt_ctx* ctx, double* gops);
 /* MeshObject::hit (src/ray.rs:614-675) of mesh `mesh_object` of a loaded
  * scene for n rays (6 doubles each: origin, direction).  out: 8 doubles per
- * ray [hit, t, point xyz, normal xyz]. */
+ * ray [hit, t, point xyz, normal xyz].  use_kdtree: bit 0 the Renderer
+ * field; bits 1-2 the query: 0 closest hit as rendered, 1 the reference's
+ * own k-d walk, 2 any hit below t_max as shadow rays run it, 3 for every
+ * k-d leaf the visit test from the leaf's cell against the walk from the
+ * root (out: [leaves where they differ, leaves where they agree, leaves
+ * the walk visits, 0...]). */
 rt_status rt_debug_mesh_hit(rt_ctx* ctx, const rt_scene* scene, int32_t object_index, int32_t use_kdtree,
                             const double* rays, int64_t n, double t_min, double t_max, double* out);
 /* Prepares a mesh description's device search data on the host and on

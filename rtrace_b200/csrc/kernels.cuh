@@ -918,12 +918,13 @@ __global__ void k_debug_disk(const uint64_t* seeds, long long n, double radius, 
     }
   }
 }
-// mode 0: mesh_closest (BVH + verification), 1: exact k-d walk, 2: mesh_any
 // Mesh queries for the parity tests: closest hit as the renderer runs it
 // (mode 0: BVH search + reference-leaf verification), the plain reference
-// k-d walk (mode 1), and any-hit as shadow rays run it (mode 2: packet
-// walk).  128 threads per block; every warp steps through the rays
-// together because the packet walks are warp collectives.
+// k-d walk (mode 1), any-hit as shadow rays run it (mode 2: packet walk),
+// and for every k-d leaf the cell-based visit test against the root walk
+// (mode 3: out = {leaves where they differ, where they agree, leaves the
+// walk visits}).  128 threads per block; every warp steps through the
+// rays together because the packet walks are warp collectives.
 __global__ void __launch_bounds__(128) k_debug_mesh(DMesh M, int use_kd, int mode, const double* rays, long long n,
                                                     double tmin, double tmax, double* out, int* err) {
   __shared__ int s_stack[4][RTB_STACK];
@@ -942,6 +943,25 @@ __global__ void __launch_bounds__(128) k_debug_mesh(DMesh M, int use_kd, int mod
     double closest = tmax;
     int best = -1;
     double* oo = out + 8 * (valid ? i : 0);
+    if (mode == 3) {
+      // every k-d leaf: the cell-based visit test against the root walk
+      if (valid) {
+        double agree = 0.0, visited = 0.0, differ = 0.0;
+        for (int k = 0; k < M.n_nodes; k++) {
+          if (hi32(__ldg(M.nodes + 4 * (size_t)k + 3).y) >= 0) continue;
+          unsigned key;
+          const bool a = kd_leaf_visited_cell(M, r, k, nullptr), b = kd_leaf_visited(M, r, k, &key);
+          if (a == b) agree += 1.0;
+          else differ += 1.0;
+          if (b) visited += 1.0;
+        }
+        for (int k = 0; k < 8; k++) oo[k] = 0.0;
+        oo[0] = differ;
+        oo[1] = agree;
+        oo[2] = visited;
+      }
+      continue;
+    }
     if (mode == 2) {
       bool any = mesh_any_warp(M, r, tmin, tmax, valid, use_kd != 0, stack, err, nullptr);
       if (valid) {

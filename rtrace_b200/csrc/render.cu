@@ -2370,9 +2370,9 @@ rt_status rt_debug_mesh_hit(rt_ctx* ctx, const rt_scene* scene, int32_t object_i
       scene->obj_kind[object_index] != RT_OBJ_MESH)
     return fail(ctx, RT_ERR_INVALID_ARGUMENT, "object is not a mesh");
   // bit 0: use_kdtree as the Renderer field; bits 1-2: the query
-  // (0 closest hit, 1 the plain k-d walk, 2 any hit)
+  // (0 closest hit, 1 the plain k-d walk, 2 any hit, 3 the k-d leaf visit
+  // tests compared)
   int mode = (use_kdtree >> 1) & 3;
-  if (mode > 2) return fail(ctx, RT_ERR_INVALID_ARGUMENT, "bad query mode");
   if (n == 0) return RT_OK;
   CK(cudaSetDevice(ctx->device));
   DMesh M = scene->host_meshes[scene->obj_mesh[object_index]];

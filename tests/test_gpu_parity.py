@@ -328,3 +328,34 @@ def test_host_scene_uploads_render_the_same(gpu_ctx, tmp_path):
     direct = r.render(rt.Scene.from_json_file(path, gpu_ctx))
     for img in imgs:
         assert np.array_equal(img, direct)
+
+
+@pytest.mark.parametrize("stl_name", ["plus.stl", "heightfield", "far_icosphere"])
+def test_leaf_visits_from_cells_match_root_walk(gpu_ctx, tmp_path, stl_name):
+    """Verification decides whether the reference visits a k-d leaf from the
+    leaf's cell (the splits on its root path) instead of walking from the
+    root.  For every leaf and every ray the two must agree: rays from the
+    k-d edge-case generator (axis-aligned, on split planes), surface rays,
+    and the culling rays (zero and tiny direction components, far origins)."""
+    from tests.kd_rays import plus_rays
+    rng = np.random.default_rng(31)
+    if stl_name == "plus.stl":
+        stl = os.path.join(oracle_lib.SCENES, "plus.stl")
+        centre, radius = np.zeros(3), 1.0
+    elif stl_name == "heightfield":
+        stl = os.path.join(str(tmp_path), "hf.stl")
+        v, f = workloads.heightfield(17, 5, height=4.0)
+        workloads.write_binary_stl(stl, v, f)
+        centre, radius = v.mean(0), 2.0
+    else:
+        stl = os.path.join(str(tmp_path), "far.stl")
+        v, f = workloads.noisy_icosphere(2, 5)
+        v = v + np.array([1.0e4, -2.5e4, 3.0e3])
+        workloads.write_binary_stl(stl, v, f)
+        centre, radius = v.mean(0), 1.0
+    sc = rt.Scene.from_json_str(_mesh_scene(stl))
+    rays = np.concatenate([plus_rays(stl, extra_random=600), _surface_rays(stl, 600, 33),
+                           _culling_rays(centre, radius, rng)])
+    out = _gpu_mesh(gpu_ctx, sc, rays, True, 3)
+    assert out[:, 0].sum() == 0, (int(out[:, 0].sum()), rays[np.nonzero(out[:, 0])[0][:3]].tolist())
+    assert out[:, 1].min() > 0 and out[:, 2].sum() > 0
