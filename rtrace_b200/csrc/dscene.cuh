@@ -298,27 +298,6 @@ __device__ __forceinline__ bool kd_slab(const double2* N, const RayC& r, double*
   return th >= 0.0;
 }
 
-// Ray/box entry for BVH culling (padded boxes; not a reference test).
-__device__ __forceinline__ bool box_hit(const double* mn, const double* mx, const RayC& r, double tmax,
-                                        double* te) {
-  double tl = -RTB_INF, th = RTB_INF;
-#pragma unroll
-  for (int a = 0; a < 3; a++) {
-    double o = r.o[a];
-    if (r.d[a] == 0.0) {
-      if (o < mn[a] || o > mx[a]) return false;
-    } else {
-      double inv = r.inv[a];
-      double t0 = (mn[a] - o) * inv;
-      double t1 = (mx[a] - o) * inv;
-      tl = rmax(tl, rmin(t0, t1));
-      th = rmin(th, rmax(t0, t1));
-    }
-  }
-  *te = tl;
-  return tl <= th && th >= 0.0 && !(tl > tmax * RTB_PRUNE_REL + RTB_PRUNE_ABS);
-}
-
 // `(split - origin) / dir >= 0.0` without the division (src/mesh.rs:441,
 // :448).  Here |dir| >= 1e-9 and |dir| <= 1 (a unit direction), so a
 // non-zero numerator gives a quotient of magnitude at least the smallest
@@ -488,27 +467,6 @@ __device__ bool mesh_kd_walk(const DMesh& M, const RayC& r, double tmin, double&
   return found;
 }
 
-// Loads one BVH node: child boxes and child references.
-struct BNode {
-  double lmn[3], lmx[3], rmn[3], rmx[3];
-  int lidx, lcnt, ridx, rcnt;
-};
-__device__ __forceinline__ BNode load_bnode(const double2* base, int node) {
-  const double2* N = base + 7 * (size_t)node;
-  double2 b0 = __ldg(N + 0), b1 = __ldg(N + 1), b2 = __ldg(N + 2), b3 = __ldg(N + 3), b4 = __ldg(N + 4),
-          b5 = __ldg(N + 5), b6 = __ldg(N + 6);
-  BNode n;
-  n.lmn[0] = b0.x; n.lmn[1] = b0.y; n.lmn[2] = b1.x;
-  n.lmx[0] = b1.y; n.lmx[1] = b2.x; n.lmx[2] = b2.y;
-  n.rmn[0] = b3.x; n.rmn[1] = b3.y; n.rmn[2] = b4.x;
-  n.rmx[0] = b4.y; n.rmx[1] = b5.x; n.rmx[2] = b5.y;
-  n.lidx = lo32(b6.x);
-  n.lcnt = hi32(b6.x);
-  n.ridx = lo32(b6.y);
-  n.rcnt = hi32(b6.y);
-  return n;
-}
-
 // A BVH node in single precision: the double node's child boxes rounded
 // outwards to floats, the same child references.  Layout: fbvh[0].x is
 // the largest |coordinate| of any child box (the scale the slab constants
@@ -571,8 +529,10 @@ __device__ __forceinline__ RayF make_rayf(const RayC& r, float scale) {
   return f;
 }
 
-// box_hit in single precision: never rejects a box that box_hit's exact
-// counterpart accepts (see RayF); tmax is the rounded-up pruning bound.
+// Ray/box entry for BVH culling (padded boxes; not a reference test), in
+// single precision: never rejects a box that the exact ray meets within
+// tmax (see RayF); tmax is the rounded-up pruning bound
+// t * RTB_PRUNE_REL + RTB_PRUNE_ABS.
 __device__ __forceinline__ bool box_hit_f(const float* mn, const float* mx, const RayF& f, float tmax, float* te) {
   float tl = -__int_as_float(0x7f800000), th = __int_as_float(0x7f800000);
 #pragma unroll
@@ -586,27 +546,16 @@ __device__ __forceinline__ bool box_hit_f(const float* mn, const float* mx, cons
   return f.all || (tl <= th && th >= 0.0f && !(tl > tmax));
 }
 
-// Node sources of the BVH walks: a BVH's nodes and one ray's box test, in
-// double (sphere runs) or single precision (meshes).  bound(t) turns a
-// pruning distance into the form test() takes.
-struct DNodes {
-  typedef BNode Node;
-  typedef double T;
-  const double2* bvh;
-  const RayC* r;
-  __device__ __forceinline__ Node load(int k) const { return load_bnode(bvh, k); }
-  __device__ __forceinline__ double bound(double t) const { return t; }
-  __device__ __forceinline__ bool test(const T* mn, const T* mx, double b, T* te) const {
-    return box_hit(mn, mx, *r, b, te);
-  }
-};
+// Node source of the BVH walks (meshes and sphere runs): a BVH's FP32
+// nodes and one ray's box test.  bound(t) turns a pruning distance into
+// the form test() takes.
 struct FNodes {
   typedef FNode Node;
   typedef float T;
   const float4* fbvh;
   RayF f;
   __device__ __forceinline__ Node load(int k) const { return load_fnode(fbvh, k); }
-  // box_hit's t * RTB_PRUNE_REL + RTB_PRUNE_ABS, rounded up
+  // the pruning bound t * RTB_PRUNE_REL + RTB_PRUNE_ABS, rounded up
   __device__ __forceinline__ float bound(double t) const {
     return __double2float_ru(t * RTB_PRUNE_REL + RTB_PRUNE_ABS);
   }
