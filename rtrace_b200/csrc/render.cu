@@ -1493,7 +1493,8 @@ rt_status render_impl(rt_ctx* ctx, const rt_scene* sc, const rt_render_params* P
         }
         for (long long c = 0; c < nchunks; c++) {
           long long c0 = c * chunk;
-          k_emit<<<blocks(chunk, 128, 16), 128, 0, s>>>(F, l, c0);
+          // 64 blocks per SM as for k_trace: emit stage 0.97 ms against 1.03 ms at 16
+          k_emit<<<blocks(chunk, 128, 64), 128, 0, s>>>(F, l, c0);
           Lc.after(RT_STAGE_EMIT);
           if (K > 0) {
             if (count) k_shadow<true><<<blocks(chunk * K, 128, 128), 128, 0, s>>>(F, l, c0);
