@@ -23,6 +23,7 @@ cores, on bounded row bands of the same frame.
 """
 import argparse
 import ctypes
+import datetime
 import json
 import math
 import os
@@ -68,22 +69,30 @@ def make_workload(directory):
 
 
 class ClockSampler:
-    """nvidia-smi clocks and throttle reasons sampled every 200 ms."""
+    """nvidia-smi clocks and throttle reasons sampled every 20 ms, with
+    timestamps.  Started well before the timed region (nvidia-smi takes a
+    moment to start); mark() brackets the region, and stop() keeps the
+    samples taken inside it."""
 
-    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+    FIELDS = ("timestamp,index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
               "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
               "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
 
     def __init__(self, gpu_index):
         self.path = tempfile.mktemp(prefix="rtb_clocks_", suffix=".csv")
         self.proc = None
+        self.window = [None, None]
         try:
             self.fh = open(self.path, "w")
             self.proc = subprocess.Popen(
                 ["nvidia-smi", "-i", str(gpu_index), "--query-gpu=" + self.FIELDS, "--format=csv,noheader,nounits",
-                 "-lms", "200"], stdout=self.fh, stderr=subprocess.DEVNULL)
+                 "-lms", "20"], stdout=self.fh, stderr=subprocess.DEVNULL)
         except (OSError, FileNotFoundError):
             self.proc = None
+
+    def mark(self):
+        """Call at the start and at the end of the timed region."""
+        self.window[0 if self.window[0] is None else 1] = datetime.datetime.now()
 
     def stop(self):
         if self.proc is None:
@@ -96,22 +105,26 @@ class ClockSampler:
         self.fh.close()
         sm, smax, reasons = [], None, set()
         names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        t0, t1 = self.window
         for line in open(self.path):
             parts = [p.strip() for p in line.split(",")]
-            if len(parts) < 9:
+            if len(parts) < 10:
                 continue
             try:
-                sm.append(float(parts[1]))
-                smax = float(parts[2])
+                ts = datetime.datetime.strptime(parts[0], "%Y/%m/%d %H:%M:%S.%f")
+                if t0 is not None and t1 is not None and not (t0 <= ts <= t1):
+                    continue
+                sm.append(float(parts[2]))
+                smax = float(parts[3])
             except ValueError:
                 continue
-            for n, v in zip(names, parts[5:9]):
+            for n, v in zip(names, parts[6:10]):
                 if v.lower().startswith("active"):
                     reasons.add(n)
         os.unlink(self.path)
         sm.sort()
         return {"sm_mhz": sm[len(sm) // 2] if sm else None, "sm_max_mhz": smax, "reasons": sorted(reasons),
-                "samples": len(sm)}
+                "samples": len(sm), "interval_ms": 20}
 
 
 TARGET_RAYS = 1024  # reference visibility for the PSNR: its own noise caps the PSNR near 49 dB
@@ -429,6 +442,7 @@ def main():
     out = torch.empty(W * H * 3, dtype=torch.uint8, device=dev)
     flush = torch.empty(512 * 1024 * 1024, dtype=torch.uint8, device=dev)  # > L2 (126 MB)
 
+    clocks = ClockSampler(local)  # running well before the timed region
     for _ in range(args.warmup):
         r.render(scene, device_ptr=out.data_ptr())
     # profiling renders (not timed): the work counters come from a render
@@ -451,11 +465,11 @@ def main():
     r.flags = _capi.RT_FLAG_CUDA_GRAPH
     r.render(scene, device_ptr=out.data_ptr())
 
-    clocks = ClockSampler(local)
     if world > 1:
         dist.barrier()
     torch.cuda.synchronize(dev)
     dev_ms, rays, launches = 0.0, 0, 0
+    clocks.mark()
     wall0 = time.perf_counter()
     for _ in range(args.steps):
         flush.zero_()
@@ -469,6 +483,7 @@ def main():
     if world > 1:
         dist.barrier()
     wall_s = time.perf_counter() - wall0
+    clocks.mark()
     clk = clocks.stop()
 
     # end to end through the public API: upload the host scene, render into
