@@ -633,8 +633,11 @@ std::string derive_mesh_device(const double2* d_bvh, int nb, const double2* d_bt
   KdArena& A = *arena;
   A.reset();
   const int BS = 256;
-  cudaError_t e = cudaMemsetAsync(fbvh, 0, sizeof(float4), s);
-  if (e == cudaSuccess && nb > 0) k_prep_fbvh<<<grid_for(nb, BS), BS, 0, s>>>(d_bvh, nb, fbvh);
+  cudaError_t e = cudaSuccess;
+  if (d_bvh && fbvh && nb > 0) {
+    e = cudaMemsetAsync(fbvh, 0, sizeof(float4), s);
+    if (e == cudaSuccess) k_prep_fbvh<<<grid_for(nb, BS), BS, 0, s>>>(d_bvh, nb, fbvh);
+  }
   if (e == cudaSuccess && n_kd_nodes > 0)
     k_prep_cells<<<grid_for(n_kd_nodes, BS), BS, 0, s>>>(d_kd_nodes, n_kd_nodes, d_leaf_path, cells);
   if (e == cudaSuccess && n > 0) k_prep_unpermute<<<grid_for(n, BS), BS, 0, s>>>(d_btris, n, brute, normals);

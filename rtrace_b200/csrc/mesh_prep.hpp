@@ -49,8 +49,9 @@ std::string prep_mesh_device(const double* h_vertices, int n, const double2* d_k
 // order, the normals and the k-d occurrence lists.  d_btris: 5n double2
 // (each record's triangle id in [0, n)); d_kd_nodes, d_leaf_tris,
 // d_leaf_path as for prep_mesh_device.  Destinations as in MeshPrepOut
-// (fbvh 1 + 4 nb float4).  Queues the work on stream s (scratch from
-// arena) and returns without waiting.
+// (fbvh 1 + 4 nb float4; with d_bvh or fbvh null the single-precision BVH
+// is not made).  Queues the work on stream s (scratch from arena) and
+// returns without waiting.
 std::string derive_mesh_device(const double2* d_bvh, int nb, const double2* d_btris, int n,
                                const double2* d_kd_nodes, int n_kd_nodes, const int* d_leaf_tris,
                                const int2* d_leaf_path, int n_index, cudaStream_t s, KdArena* arena, float4* fbvh,

@@ -609,6 +609,7 @@ void put_fbvh(const std::vector<BvhNode>& nodes, std::vector<float4>* out) {
 // from them (derive_mesh_device), so only prep_mesh(full = true) fills those.
 struct MeshPrep {
   std::vector<double2> bvh, btris, brute, nodes;
+  std::vector<float4> fbvh;  // the BVH in single precision (put_fbvh), which uploads copy
   std::vector<double4> normals;
   std::vector<int> leaf_tris, occ_off;
   std::vector<int2> leaf_path, occ;
@@ -618,7 +619,7 @@ struct MeshPrep {
   // and occurrence arrays are not on the host (only the k-d part is).
   bool device_made = false;
   // Kept by a host scene, the five uploaded arrays are packed into one
-  // pinned buffer (each at a 256-byte aligned offset; bvh, btris, nodes,
+  // pinned buffer (each at a 256-byte aligned offset; fbvh, btris, nodes,
   // leaf_tris, leaf_path) and the vectors released: uploads then copy the
   // image straight from pinned memory.
   static const int kImageArrays = 5;
@@ -634,8 +635,8 @@ struct MeshPrep {
 // it is if pinned memory cannot be had.
 void pack_prep(MeshPrep* P) {
   const int K = MeshPrep::kImageArrays;
-  const void* src[K] = {P->bvh.data(), P->btris.data(), P->nodes.data(), P->leaf_tris.data(), P->leaf_path.data()};
-  size_t n[K] = {P->bvh.size() * sizeof(double2), P->btris.size() * sizeof(double2), P->nodes.size() * sizeof(double2),
+  const void* src[K] = {P->fbvh.data(), P->btris.data(), P->nodes.data(), P->leaf_tris.data(), P->leaf_path.data()};
+  size_t n[K] = {P->fbvh.size() * sizeof(float4), P->btris.size() * sizeof(double2), P->nodes.size() * sizeof(double2),
                  P->leaf_tris.size() * sizeof(int), P->leaf_path.size() * sizeof(int2)};
   size_t total = 0;
   for (int k = 0; k < K; k++) {
@@ -653,6 +654,7 @@ void pack_prep(MeshPrep* P) {
   P->image = img;
   P->image_bytes = total;
   P->bvh = {};
+  P->fbvh = {};
   P->btris = {};
   P->brute = {};
   P->normals = {};
@@ -836,7 +838,8 @@ std::string prep_mesh(const rt_mesh_desc& md, MeshPrep* P, bool sah = true, bool
   else
     build_bvh(tmin, tmax, kMeshLeaf, 1e-7 * (1.0 + scale), &bnodes, &order);
   std::vector<double2> bvh, btris((size_t)nt * 5);
-  put_bvh(bnodes, &bvh);
+  if (full) put_bvh(bnodes, &bvh);
+  put_fbvh(bnodes, &P->fbvh);
   parallel_ranges(nt, [&](long long k0, long long k1, int) {
     for (long long k = k0; k < k1; k++)
       for (int j = 0; j < 5; j++) btris[5 * k + j] = brute[5 * (size_t)order[k] + j];
@@ -888,9 +891,9 @@ rt_status upload_now(rt_ctx* ctx, rt_scene* sc, const std::vector<T>& h, const T
 }
 
 // Prepares a large mesh on the device straight into the scene's block: P
-// holds the k-d part (prep_mesh_kd).  keep_host: also copies the BVH and
-// the BVH-order records back into P, so that later uploads copy them
-// (upload_prep).
+// holds the k-d part (prep_mesh_kd).  keep_host: also copies the
+// single-precision BVH and the BVH-order records back into P, so that
+// later uploads copy them (upload_prep).
 rt_status upload_prep_device(rt_ctx* ctx, rt_scene* sc, const rt_mesh_desc& md, MeshPrep* P, bool keep_host,
                              DMesh* out) {
   DMesh M{};
@@ -933,9 +936,9 @@ rt_status upload_prep_device(rt_ctx* ctx, rt_scene* sc, const rt_mesh_desc& md, 
   M.occ_off = occ_off;
   if (keep_host) {
     // what upload_prep copies; it derives the rest
-    P->bvh.resize(7 * (size_t)nb);
+    P->fbvh.resize(1 + 4 * (size_t)nb);
     P->btris.resize(5 * (size_t)n);
-    CK(cudaMemcpy(P->bvh.data(), bvh, P->bvh.size() * sizeof(double2), cudaMemcpyDeviceToHost));
+    CK(cudaMemcpy(P->fbvh.data(), fbvh, P->fbvh.size() * sizeof(float4), cudaMemcpyDeviceToHost));
     CK(cudaMemcpy(P->btris.data(), btris, P->btris.size() * sizeof(double2), cudaMemcpyDeviceToHost));
     P->device_made = false;
   }
@@ -957,35 +960,32 @@ rt_status upload_prep(rt_ctx* ctx, rt_scene* sc, const MeshPrep& P, DMesh* out) 
   if (P.image) {
     char* base = nullptr;
     if ((st = upload_direct(ctx, sc, P.image, P.image_bytes, &base)) != RT_OK) return st;
-    M.bvh = reinterpret_cast<const double2*>(base + P.off[0]);
+    M.fbvh = reinterpret_cast<const float4*>(base + P.off[0]);
     M.btris = reinterpret_cast<const double2*>(base + P.off[1]);
     M.nodes = reinterpret_cast<const double2*>(base + P.off[2]);
     M.leaf_tris = reinterpret_cast<const int*>(base + P.off[3]);
     M.leaf_path = reinterpret_cast<const int2*>(base + P.off[4]);
   } else {
     // not packed: each array straight from P's own memory (P outlives the flush)
-    if ((st = upload_array(ctx, sc, P.bvh, &M.bvh)) != RT_OK || (st = upload_array(ctx, sc, P.btris, &M.btris)) != RT_OK ||
+    if ((st = upload_array(ctx, sc, P.fbvh, &M.fbvh)) != RT_OK || (st = upload_array(ctx, sc, P.btris, &M.btris)) != RT_OK ||
         (st = upload_array(ctx, sc, P.nodes, &M.nodes)) != RT_OK ||
         (st = upload_array(ctx, sc, P.leaf_tris, &M.leaf_tris)) != RT_OK ||
         (st = upload_array(ctx, sc, P.leaf_path, &M.leaf_path)) != RT_OK)
       return st;
   }
   const int n = P.n_tris;
-  const int nb = (int)((P.image ? P.len[0] : P.bvh.size() * sizeof(double2)) / (7 * sizeof(double2)));
-  float4* fbvh;
   double2 *cells, *brute;
   double4* normals;
   int2* occ;
   int* occ_off;
-  if ((st = reserve(ctx, sc, 1 + 4 * (size_t)nb, &fbvh)) != RT_OK ||
-      (st = reserve(ctx, sc, 3 * (size_t)P.n_nodes, &cells)) != RT_OK ||
+  if ((st = reserve(ctx, sc, 3 * (size_t)P.n_nodes, &cells)) != RT_OK ||
       (st = reserve(ctx, sc, 5 * (size_t)n, &brute)) != RT_OK || (st = reserve(ctx, sc, (size_t)n, &normals)) != RT_OK ||
       (st = reserve(ctx, sc, (size_t)P.n_index, &occ)) != RT_OK ||
       (st = reserve(ctx, sc, (size_t)n + 1, &occ_off)) != RT_OK)
     return st;
-  sc->derive.push_back(MeshDerive{M.bvh, nb, fbvh, M.btris, n, M.nodes, P.n_nodes, M.leaf_tris, M.leaf_path,
+  // the single-precision BVH is copied as it is: nothing to convert
+  sc->derive.push_back(MeshDerive{nullptr, 0, nullptr, M.btris, n, M.nodes, P.n_nodes, M.leaf_tris, M.leaf_path,
                                   P.n_index, cells, brute, normals, occ, occ_off});
-  M.fbvh = fbvh;
   M.cells = cells;
   M.brute = brute;
   M.normals = normals;
