@@ -56,6 +56,15 @@ B_RAY, B_NODE, B_TRI, B_SPH, B_VERIFY = 57, 64, 80, 40, 16
 F_NODE, F_TRI, F_SPH, F_VERIFY = 0, 40, 22, 2
 
 
+def frame_config(world, split):
+    """The workload, identical in both arms' JSON lines (the reference arm
+    renders the same frame on the CPU)."""
+    return {"workload": WORKLOAD, "width": W, "height": H, "anti_aliasing": "no-jitter", "outline": True,
+            "samples": 1, "max_depth": 10, "seed": 0, "triangles": 81920, "disk_samples": 16,
+            "l2": "GPU arm: 512 MB written before each step (L2 flush)",
+            "parallelism": "single" if world == 1 else ("row bands of one frame" if split else "replicas")}
+
+
 def env_int(name, default):
     try:
         return int(os.environ.get(name, default))
@@ -330,44 +339,68 @@ def large_mesh_run(rt, ctx, directory, reps):
     return out
 
 
-def read_traffic():
-    """Per-launch DRAM bytes of the shadow kernel from the committed ncu summary."""
+def read_profile(path):
+    """The `name: value` figure lines of a committed ncu summary (DRAM
+    traffic per frame, issue-slot and cache hit rates of the kernel)."""
+    out = {}
     try:
-        for line in open(TRAFFIC_FILE):
-            if line.startswith("traffic_bytes_per_frame:"):
-                return float(line.split(":", 1)[1])
+        for line in open(path):
+            name, sep, val = line.partition(":")
+            if sep and name.strip() in ("traffic_bytes_per_frame", "issue_slots_busy", "l2_hit_rate",
+                                        "l1_hit_rate", "tensor_pipe_active", "dram_throughput"):
+                try:
+                    out[name.strip()] = float(val)
+                except ValueError:
+                    pass
     except OSError:
         pass
-    return None
+    return out
 
 
-def cpu_baseline(scene_path, budget_s, threads, kind_outline=True):
-    """Mrays/s of the CPU restatement of the reference on a row band."""
+def cpu_baseline(scene_path, budget_s, threads, centre=None):
+    """Mrays/s of the CPU restatement of the reference on a band of rows
+    centred on row `centre` (default: the middle) and sized to take about
+    budget_s seconds.  Also returns the band's pixels ("img": the full
+    frame's array with only those rows rendered, "rows": (y0, y1)) for the
+    parity check against the GPU frame."""
     from tests import oracle_lib
     import numpy as np
     L = oracle_lib.load()
     err = ctypes.create_string_buffer(512)
 
-    def band(y0, y1):
-        out = np.zeros((H, W, 3), np.uint8)
+    def band(y0, y1, out):
         cnt = np.zeros(6, np.uint64)
         t = time.perf_counter()
-        rc = L.oracle_render_rows(scene_path.encode(), None, W, H, 0, 1, 10, 0, 1, 1 if kind_outline else 0,
-                                  threads, y0, y1, out.ctypes.data, None, cnt.ctypes.data, err, 512)
+        rc = L.oracle_render_rows(scene_path.encode(), None, W, H, 0, 1, 10, 0, 1, 1, threads, y0, y1,
+                                  out.ctypes.data, None, cnt.ctypes.data, err, 512)
         if rc:
             raise RuntimeError(err.value.decode())
         return time.perf_counter() - t, int(cnt[0] + cnt[1] + cnt[2])
 
-    mid = H // 2
-    dt, rays = band(mid, mid + 2)  # calibration
+    mid = H // 2 if centre is None else min(max(int(centre), 1), H - 1)
+    out = np.zeros((H, W, 3), np.uint8)
+    dt, rays = band(mid - 1, mid + 1, out)  # calibration
     per_row = max(dt / 2.0, 1e-4)
-    rows = int(max(2, min(H, budget_s / per_row)))
-    y0 = max(0, mid - rows // 2)
-    dt, rays = band(y0, y0 + rows)
+    rows = int(max(4, min(H, budget_s / per_row)))
+    y0 = min(max(0, mid - rows // 2), H - rows)
+    dt, rays = band(y0, y0 + rows, out)
     return {"value": rays / dt / 1e6, "unit": "Mrays/s", "cores": threads, "kind": "port",
             "sample": "rows %d-%d of the %dx%d frame (%d rays, %.1f s), CPU restatement of the reference, "
                       "%d threads" % (y0, y0 + rows, W, H, rays, dt, threads),
-            "rays": rays, "seconds": dt}
+            "rays": rays, "seconds": dt, "img": out, "rows": (y0, y0 + rows)}
+
+
+def band_parity(frame, band, rows, halo=1):
+    """RGB8 agreement of the GPU frame with the oracle's band of the same
+    frame.  The oracle renders only the band, so the outline stencil at its
+    first and last `halo` rows lacks the neighbours' G-buffer: those rows
+    are left out."""
+    import numpy as np
+    y0, y1 = rows[0] + halo, rows[1] - halo
+    diff = np.abs(frame[y0:y1].astype(np.int16) - band[y0:y1].astype(np.int16)).max(2)
+    n, bad = int(diff.size), int((diff > 0).sum())
+    return {"rows": "%d-%d" % (y0, y1), "pixels": n, "identical_px_frac": (n - bad) / n if n else None,
+            "max_lsb": int(diff.max()) if n else None, "checker": "oracle (CPU restatement of the reference)"}
 
 
 def run_reference(args, rank, world):
@@ -376,25 +409,28 @@ def run_reference(args, rank, world):
     d = tempfile.mkdtemp(prefix="rtb_ref_")
     path = make_workload(d)
     threads = os.cpu_count() or 1
-    # each step: a row band sized so that warm-up + steps take ~2 minutes
+    # each step: a row band sized so that warm-up + steps take ~2 minutes;
+    # step k's band is centred at row (k + 0.5) H / steps, so that the
+    # steps together sample the whole frame, top to bottom
     per_step = max(2.0, 120.0 / max(1, args.steps + args.warmup))
     for _ in range(args.warmup):
         cpu_baseline(path, min(per_step, 5.0), threads)
     tot_rays, tot_s, samples = 0, 0.0, []
-    for _ in range(args.steps):
-        r = cpu_baseline(path, per_step, threads)
+    for k in range(args.steps):
+        r = cpu_baseline(path, per_step, threads, centre=(k + 0.5) * H / args.steps)
         tot_rays += r["rays"]
         tot_s += r["seconds"]
-        samples.append(r["sample"])
+        samples.append("%d-%d" % r["rows"])
     value = tot_rays / tot_s / 1e6
     line = {
         "impl": "reference", "metric": METRIC, "value": value, "unit": "Mrays/s", "n_gpus": args.gpus,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * tot_s / args.steps,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-        "config": {"workload": WORKLOAD, "width": W, "height": H, "anti_aliasing": "no-jitter", "samples": 1,
-                   "max_depth": 10, "outline": True, "step": "row band of the frame, CPU"},
+        "config": frame_config(world, args.split == "rows"),
+        "step": "a band of rows of the frame on the CPU (%.0f s each), bands spread over the frame" % per_step,
         "cpu_baseline": {"value": value, "unit": "Mrays/s", "cores": threads, "kind": "port",
-                         "sample": "; ".join(samples[:2]) + ("; ..." if len(samples) > 2 else "")},
+                         "sample": "rows %s of the %dx%d frame (%d rays, %.1f s), CPU restatement of the "
+                                   "reference, %d threads" % (", ".join(samples), W, H, tot_rays, tot_s, threads)},
         "e2e": {"value": value, "unit": "Mrays/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line), flush=True)
@@ -412,6 +448,9 @@ def main():
     ap.add_argument("--no-learned", action="store_true", help="skip the learned-vs-plain shadow comparison")
     ap.add_argument("--no-batch", action="store_true", help="skip the 256-job batch measurement")
     ap.add_argument("--no-large", action="store_true", help="skip the 2-million-triangle terrain measurement")
+    ap.add_argument("--split", default="replicas", choices=["replicas", "rows"],
+                    help="N > 1: every rank renders its own frame (replicas, weak scaling) or one frame is "
+                         "split into row bands gathered to rank 0 (rows, strong scaling)")
     args = ap.parse_args()
     args.warmup = max(3, args.warmup)
     rank, world, local = env_int("RANK", 0), env_int("WORLD_SIZE", 1), env_int("LOCAL_RANK", 0)
@@ -465,18 +504,34 @@ def main():
     r.flags = _capi.RT_FLAG_CUDA_GRAPH
     r.render(scene, device_ptr=out.data_ptr())
 
+    split = world > 1 and args.split == "rows"
+    if split:
+        from rtrace_b200.distributed import render_frame
+        for _ in range(2):  # warm-up of the band render and the gather
+            render_frame(r, scene)
     if world > 1:
         dist.barrier()
     torch.cuda.synchronize(dev)
     dev_ms, rays, launches = 0.0, 0, 0
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     clocks.mark()
     wall0 = time.perf_counter()
     for _ in range(args.steps):
         flush.zero_()
         torch.cuda.synchronize(dev)
-        r.render(scene, device_ptr=out.data_ptr())
+        if split:
+            # this rank's band (rendered on the context's stream, which the
+            # call waits for) and the gather to rank 0, between two events
+            # on the current stream
+            ev0.record()
+            render_frame(r, scene)
+            ev1.record()
+            ev1.synchronize()
+            dev_ms += ev0.elapsed_time(ev1)
+        else:
+            r.render(scene, device_ptr=out.data_ptr())
+            dev_ms += r.last_stats.device_ms
         st = r.last_stats
-        dev_ms += st.device_ms
         rays += st.rays
         launches += st.kernel_launches
     torch.cuda.synchronize(dev)
@@ -485,25 +540,34 @@ def main():
     wall_s = time.perf_counter() - wall0
     clocks.mark()
     clk = clocks.stop()
+    frame = out.cpu().numpy().reshape(H, W, 3) if not split else None
 
     # end to end through the public API: upload the host scene, render into
     # pinned host memory, free
     host = rt.HostScene.from_json_file(path)
     pinned = torch.empty((H, W, 3), dtype=torch.uint8, pin_memory=True)
     pin_np = pinned.numpy()
-    for _ in range(2):
+
+    def e2e_step():
         sc = rt.Scene.upload(host, ctx)
-        r.render(sc, out=pin_np)
+        if split:
+            img = render_frame(r, sc)  # this rank's band, gathered to rank 0 (host array there)
+            if rank == 0:
+                pin_np[...] = img
+        else:
+            r.render(sc, out=pin_np)
+        nbytes = sc.device_bytes
         sc.close()
+        return nbytes
+
+    for _ in range(2):
+        e2e_step()
     e2e_s, e2e_rays, h2d = 0.0, 0, 0
     if world > 1:
         dist.barrier()
     for _ in range(args.steps):
         t = time.perf_counter()
-        sc = rt.Scene.upload(host, ctx)
-        r.render(sc, out=pin_np)
-        h2d = sc.device_bytes
-        sc.close()
+        h2d = e2e_step()
         e2e_s += time.perf_counter() - t
         e2e_rays += r.last_stats.rays
 
@@ -529,21 +593,35 @@ def main():
         except (OSError, KeyError, ValueError):
             hbm, peak_src = 6650.0, "fallback"
         fp64 = rt.fp64_rate(ctx)
+        l2 = max(rt.l2_read_bandwidth(ctx, mb, 40) for mb in (24, 48))
         achieved = sh_bytes / sh_s / 1e9 if sh_s > 0 else None
-        roofline = {"kernel": "k_shadow", "bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s",
-                    "frac": achieved / hbm if achieved else None, "peak_source": peak_src,
-                    "traffic": read_traffic(), "traffic_unit": "bytes per frame (all k_shadow launches)",
+        pf = read_profile(TRAFFIC_FILE)
+        traffic = pf.get("traffic_bytes_per_frame")
+        roofline = {"kernel": "k_shadow", "bound": "l2", "achieved": achieved, "peak": l2, "unit": "GB/s",
+                    "frac": achieved / l2 if achieved else None,
+                    "peak_source": "measured in this run: L2-resident read bandwidth (rt_debug_l2_read_bandwidth, "
+                                   "24 and 48 MB buffers, the larger figure)",
+                    "frac_l2": achieved / l2 if achieved else None,
+                    "peak_hbm": hbm, "peak_hbm_source": peak_src,
+                    "frac_hbm": achieved / hbm if achieved else None,
+                    "dram_frac_hbm": traffic / sh_s / 1e9 / hbm if traffic and sh_s > 0 else None,
+                    "issue_busy": pf.get("issue_slots_busy"), "l2_hit_rate": pf.get("l2_hit_rate"),
+                    "l1_hit_rate": pf.get("l1_hit_rate"),
+                    "limiter": "latency of the chained BVH node loads (ncu: issue slots about half busy, "
+                               "long-scoreboard stalls dominate); the working set is L2-resident",
+                    "traffic": traffic, "traffic_unit": "DRAM bytes per frame (all k_shadow launches)",
                     "algorithmic_bytes_per_frame": sh_bytes, "kernel_ms_per_frame": stages["shadow"],
                     "dominant_stage": dom,
                     "fp64": {"achieved_gops": sh_flops / sh_s / 1e9 if sh_s > 0 else None,
                              "peak_gops": fp64, "peak_source": "measured FP64 add/mul issue rate (k_fp64_rate)",
                              "frac": (sh_flops / sh_s / 1e9) / fp64 if sh_s > 0 and fp64 else None}}
-        cpu = None
+        cpu, parity = None, None
         if world == 1 and not args.no_cpu_baseline:
             try:
                 cpu = cpu_baseline(path, args.cpu_seconds, os.cpu_count() or 1)
                 cpu.pop("rays", None)
                 cpu.pop("seconds", None)
+                parity = band_parity(frame, cpu.pop("img"), cpu.pop("rows"))
             except Exception as e:  # the oracle is test infrastructure; report, do not fail
                 cpu = {"value": None, "unit": "Mrays/s", "cores": os.cpu_count(), "kind": "port",
                        "sample": "failed: %s" % e}
@@ -574,13 +652,13 @@ def main():
         line = {
             "metric": METRIC, "value": value, "unit": "Mrays/s", "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": dev_ms_max / args.steps, "higher_is_better": True,
-            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-            "config": {"workload": WORKLOAD, "width": W, "height": H, "anti_aliasing": "no-jitter (outline on)",
-                       "samples": 1, "max_depth": 10, "seed": 0, "triangles": 81920,
-                       "rays_per_frame": rays_all / world / args.steps, "l2": "flushed (512 MB write) before each step",
-                       "parallelism": "replicas" if world > 1 else "single",
-                       "launch": "CUDA graph replay of the frame's kernels (RT_FLAG_CUDA_GRAPH)"},
+            "scaling": "strong" if split else "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": frame_config(world, split),
+            "rays_per_frame": rays_all / (1 if split else world) / args.steps,
+            "launch": ("each rank's band of the frame, then a gather to rank 0 (NCCL)" if split else
+                       "CUDA graph replay of the frame's kernels (RT_FLAG_CUDA_GRAPH)"),
             "ms_per_frame": dev_ms_max / args.steps,
+            "parity": parity,
             "wall_ms_per_step": 1e3 * wall_s / args.steps,
             "gpu_launches": launches,
             "e2e": {"value": e2e_value, "unit": "Mrays/s", "ms_per_frame": 1e3 * e2e_s_max / args.steps,

@@ -486,6 +486,12 @@ rt_status rt_debug_disk_offsets(rt_ctx* ctx, const uint64_t* light_seeds, int64_
 /* Measured issue rate of separate FP64 add and multiply instructions (the
  * operations the render path uses; it never fuses them), in Gop/s. */
 rt_status rt_debug_fp64_rate(rt_ctx* ctx, double* gops);
+/* Measured read bandwidth, in GB/s, of a device buffer of about `bytes`
+ * bytes (rounded down to whole passes of the probe's grid; at most 2 GiB)
+ * that stays in L2: `reps` passes of 16-byte loads cached in L2 only,
+ * after a warm-up pass, timed with CUDA events.  The ceiling of kernels
+ * whose working set is L2-resident. */
+rt_status rt_debug_l2_read_bandwidth(rt_ctx* ctx, uint64_t bytes, int32_t reps, double* gbs);
 /* MeshObject::hit (src/ray.rs:614-675) of mesh `mesh_object` of a loaded
  * scene for n rays (6 doubles each: origin, direction).  out: 8 doubles per
  * ray [hit, t, point xyz, normal xyz].  use_kdtree: bit 0 the Renderer

@@ -22,7 +22,7 @@ from . import _capi
 __all__ = [
     "AntiAliasingMode", "OutlineConfig", "Scene", "Renderer", "RtraceError", "SceneError",
     "RenderError", "DeviceError", "Context", "RenderStats", "default_context", "write_png", "HostScene",
-    "fp64_rate", "auto_cameras", "Job", "BatchStats", "render_batch", "batch_autotune", "batch_assign",
+    "fp64_rate", "l2_read_bandwidth", "auto_cameras", "Job", "BatchStats", "render_batch", "batch_autotune", "batch_assign",
     "camera_config",
 ]
 
@@ -322,6 +322,17 @@ def fp64_rate(ctx=None):
     ctx = ctx or default_context()
     v = ctypes.c_double()
     st = _capi.lib().rt_debug_fp64_rate(ctx.handle, ctypes.byref(v))
+    if st != _capi.RT_OK:
+        _raise(st, ctx.handle)
+    return v.value
+
+
+def l2_read_bandwidth(ctx=None, mbytes=32, reps=50):
+    """Measured read bandwidth (GB/s) of an L2-resident buffer of about
+    mbytes MB: the ceiling of kernels whose working set stays in L2."""
+    ctx = ctx or default_context()
+    v = ctypes.c_double()
+    st = _capi.lib().rt_debug_l2_read_bandwidth(ctx.handle, int(mbytes * 1e6), int(reps), ctypes.byref(v))
     if st != _capi.RT_OK:
         _raise(st, ctx.handle)
     return v.value

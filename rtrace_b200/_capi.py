@@ -219,6 +219,8 @@ def lib():
         "rt_host_scene_free": (None, [_vp]),
         "rt_scene_device_bytes": (ctypes.c_int, [_vp, _vp, ctypes.POINTER(ctypes.c_uint64)]),
         "rt_debug_fp64_rate": (ctypes.c_int, [_vp, ctypes.POINTER(ctypes.c_double)]),
+        "rt_debug_l2_read_bandwidth": (ctypes.c_int, [_vp, ctypes.c_uint64, ctypes.c_int32,
+                                                      ctypes.POINTER(ctypes.c_double)]),
         "rt_outline_apply": (ctypes.c_int, [_vp, ctypes.c_uint32, ctypes.c_uint32, _vp, _vp, _vp, _vp, _vp, _vp,
                                             _vp, _vp, ctypes.POINTER(rt_outline_config), _vp]),
         "rt_outline_apply_noalloc": (ctypes.c_int, [_vp, ctypes.c_uint32, ctypes.c_uint32, _vp, _vp, _vp, _vp,

@@ -9,6 +9,7 @@ import os
 import shutil
 import subprocess
 import sys
+from concurrent.futures import ThreadPoolExecutor
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 CSRC = os.path.join(HERE, "csrc")
@@ -53,22 +54,25 @@ def build(force=False, verbose=False):
     os.makedirs(OUT_DIR, exist_ok=True)
     os.makedirs(BUILD_DIR, exist_ok=True)
     nvcc = _nvcc()
-    objs = []
-    log = []
+    cmds, objs = [], []
     for src in sorted(os.listdir(CSRC)):
         path = os.path.join(CSRC, src)
         obj = os.path.join(BUILD_DIR, src + ".o")
         if src.endswith(".cu"):
-            cmd = [nvcc, *NVCC_FLAGS, "-c", path, "-o", obj]
+            cmds.append([nvcc, *NVCC_FLAGS, "-c", path, "-o", obj])
         elif src.endswith(".cpp"):
-            cmd = ["g++", *CXX_FLAGS, "-c", path, "-o", obj]
+            cmds.append(["g++", *CXX_FLAGS, "-c", path, "-o", obj])
         else:
             continue
-        r = subprocess.run(cmd, capture_output=True, text=True)
+        objs.append(obj)
+    # translation units compile independently: one process each, in parallel
+    with ThreadPoolExecutor(max_workers=max(1, min(len(cmds), os.cpu_count() or 1))) as pool:
+        results = list(pool.map(lambda c: subprocess.run(c, capture_output=True, text=True), cmds))
+    log = []
+    for cmd, r in zip(cmds, results):
         log.append(r.stdout + r.stderr)
         if r.returncode != 0:
             raise RuntimeError("compile failed: %s\n%s%s" % (" ".join(cmd), r.stdout, r.stderr))
-        objs.append(obj)
     tmp = LIB + ".tmp"
     cmd = [nvcc, "-shared", "-gencode", "arch=compute_100a,code=sm_100a", "-o", tmp, *objs,
            "-Xcompiler", "-fPIC", "-lz"]

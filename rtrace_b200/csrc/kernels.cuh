@@ -893,6 +893,23 @@ __global__ void k_fp64_rate(double* out, int iters, double a, double b) {
   for (int k = 0; k < 8; k++) s += x[k] + y[k];
   if (s == 12345.678) out[0] = s;  // keeps the chains live
 }
+// Read bandwidth of a buffer small enough to stay in L2: 16-byte loads
+// with ld.global.cg (cached in L2, not L1, so no pass is served by L1),
+// four independent loads per thread in flight, `reps` passes over the
+// buffer.  n16 is the buffer's size in 16-byte vectors, a multiple of
+// 4 * gridDim.x * blockDim.x.
+__global__ void k_l2_read(const uint4* __restrict__ buf, long long n16, int reps, unsigned* out) {
+  const long long stride = (long long)gridDim.x * blockDim.x;
+  unsigned acc = 0;
+  for (int r = 0; r < reps; r++) {
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n16; i += 4 * stride) {
+      uint4 a = __ldcg(buf + i), b = __ldcg(buf + i + stride), c = __ldcg(buf + i + 2 * stride),
+            d = __ldcg(buf + i + 3 * stride);
+      acc ^= a.x ^ a.y ^ a.z ^ a.w ^ b.x ^ b.y ^ b.z ^ b.w ^ c.x ^ c.y ^ c.z ^ c.w ^ d.x ^ d.y ^ d.z ^ d.w;
+    }
+  }
+  if (acc == 0x9E3779B9u) out[0] = acc;  // keeps the loads live
+}
 __global__ void k_debug_rng(const uint64_t* seeds, long long n, int nw, uint32_t* out) {
   for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
     StdRng r;

@@ -1914,6 +1914,33 @@ rt_status rt_debug_fp64_rate(rt_ctx* ctx, double* gops) {
   return RT_OK;
 }
 
+rt_status rt_debug_l2_read_bandwidth(rt_ctx* ctx, uint64_t bytes, int32_t reps, double* gbs) {
+  if (!ctx || !gbs || reps <= 0) return fail(ctx, RT_ERR_INVALID_ARGUMENT, "null argument or reps <= 0");
+  CK(cudaSetDevice(ctx->device));
+  const int threads = 512, blocks = ctx->num_sms * 4;
+  const uint64_t unit = 16ull * 4 * threads * blocks;  // one pass of every thread's four loads
+  uint64_t n_units = bytes / unit;
+  if (n_units == 0 || bytes > (1ull << 31)) return fail(ctx, RT_ERR_INVALID_ARGUMENT, "buffer size out of range");
+  std::vector<void*> tmp;
+  uint4* buf;
+  unsigned* sink;
+  CK(dalloc(tmp, &buf, n_units * unit / 16));
+  CK(dalloc(tmp, &sink, 1));
+  CK(cudaMemsetAsync(buf, 1, n_units * unit, ctx->stream));
+  long long n16 = (long long)(n_units * unit / 16);
+  k_l2_read<<<blocks, threads, 0, ctx->stream>>>(buf, n16, 2, sink);  // warm-up: the buffer enters L2
+  CK(cudaEventRecord(ctx->ev0, ctx->stream));
+  k_l2_read<<<blocks, threads, 0, ctx->stream>>>(buf, n16, reps, sink);
+  CK(cudaEventRecord(ctx->ev1, ctx->stream));
+  CK(cudaGetLastError());
+  CK(cudaStreamSynchronize(ctx->stream));
+  float ms = 0.f;
+  CK(cudaEventElapsedTime(&ms, ctx->ev0, ctx->ev1));
+  free_all(tmp);
+  *gbs = (double)n_units * unit * reps / (ms * 1e-3) / 1e9;
+  return RT_OK;
+}
+
 namespace {
 // Checks the arguments of the outline entry points and fills the frame
 // fields the outline kernels read.

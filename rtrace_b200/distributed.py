@@ -6,7 +6,7 @@ are seeded by their grid position), so rank r renders a contiguous band of
 rows with `Renderer.render_rows`, which traces the outline stencil's extra
 rows itself, and the bands are gathered to the root.  No data moves between
 ranks while they render; the only collective is the final gather of RGB8
-rows (width * rows * 3 bytes per rank).
+rows to the root (width * rows * 3 bytes per rank).
 
 With the NCCL backend the bands are rendered straight into CUDA tensors and
 gathered over NVLink; with gloo (CPU tests) they are host tensors.
@@ -50,7 +50,9 @@ def gather_bands(band, bands, width, group=None, root=0):
     """Gathers every rank's band (a (rows, width, 3) uint8 tensor, rows =
     that rank's band height) to `root`, which returns the (height, width, 3)
     image as a numpy array; other ranks return None.  Bands are padded to the
-    tallest band so that one all-gather of equal-sized buffers moves them."""
+    tallest band so that one gather of equal-sized buffers moves them; only
+    the root receives (world - 1 bands cross the links, not world^2 as an
+    all-gather would move)."""
     rank = dist.get_rank(group)
     world = dist.get_world_size(group)
     if len(bands) != world:
@@ -61,12 +63,13 @@ def gather_bands(band, bands, width, group=None, root=0):
     tallest = max(e - b for b, e in bands)
     padded = torch.zeros((tallest, width, 3), dtype=torch.uint8, device=band.device)
     padded[:rows] = band
-    out = torch.empty((world * tallest, width, 3), dtype=torch.uint8, device=band.device)
-    dist.all_gather_into_tensor(out, padded, group=group)
+    root_global = root if group is None else dist.get_global_rank(group, root)
     if rank != root:
+        dist.gather(padded, None, dst=root_global, group=group)
         return None
-    parts = [out[r * tallest:r * tallest + (e - b)] for r, (b, e) in enumerate(bands)]
-    return torch.cat(parts, 0).cpu().numpy()
+    parts = [torch.empty_like(padded) for _ in range(world)]
+    dist.gather(padded, parts, dst=root_global, group=group)
+    return torch.cat([parts[r][:e - b] for r, (b, e) in enumerate(bands)], 0).cpu().numpy()
 
 
 def render_frame(renderer, scene, group=None, root=0, row_costs=None, band_renderer=None):
