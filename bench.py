@@ -136,17 +136,68 @@ class ClockSampler:
                 "samples": len(sm), "interval_ms": 20}
 
 
-TARGET_RAYS = 1024  # reference visibility for the PSNR: its own noise caps the PSNR near 49 dB
+PLAIN_RAYS = 64        # the configuration's plain arm: two area lights sampled 8x8
+NOISE_CAP_RAYS = 1024  # a near-noise-free reference, reported beside the 64-ray one
 
 
-def learned_vs_plain(rt, torch, ctx, directory, steps):
-    """The metric's second half: the 1,000-sphere ring scene (two disk
-    lights) at 1920x1080, stochastic, 4 samples per pixel, rendered with the
-    reference's 16 shadow rays per disk light ("plain") and with one ray per
-    disk light at the primary hits plus the learned denoiser ("learned").
-    Both are timed (device events, L2 flushed per frame) and their primary
-    hits' visibility is compared, as PSNR over hit pixels of each present
-    light, with a 64-ray-per-light render of the same frame."""
+def denoiser_roofline(rt, torch, ctx, feat, hbm, tflops):
+    """The network alone on the frame's feature image: CUDA-event time of
+    rt_denoiser_run, algorithmic bytes (every op's FP16 input and output
+    once, FP32 outputs of the last op) and FLOPs (2 x 9 x cin x cout per
+    output pixel of each convolution), against HBM and the FP16/BF16 tensor
+    peak."""
+    from rtrace_b200 import denoiser
+    net = denoiser.unpack_net(denoiser.read_blob())
+    P, H, W, _ = feat.shape
+    dims = lambda lv: (-(-H // (1 << lv)), -(-W // (1 << lv)))
+    ch, lv = [16], [0]
+    nbytes, flops = 0.0, 0.0
+    for i, (kind, cin, cout, dil, src, src2) in enumerate(net.ops):
+        level = lv[src] + 1 if kind == "pool" else (lv[src2] if kind == "upadd" else lv[src])
+        h, w = dims(level)
+        hs, ws = dims(lv[src])
+        last = i + 1 == len(net.ops)
+        nbytes += P * hs * ws * ch[src] * 2 + (P * h * w * 16 if last else P * h * w * cout * 2)
+        if kind == "upadd":
+            nbytes += P * h * w * ch[src2] * 2
+        if kind == "conv":
+            flops += 2.0 * 9 * cin * cout * P * h * w
+        ch.append(cout)
+        lv.append(level)
+    vis = torch.empty((P, 2, H, W), dtype=torch.float32, device=feat.device)
+    conf = torch.empty_like(vis)
+    L = rt._capi.lib()
+    ms = []
+    for _ in range(8):
+        d = ctypes.c_double()
+        st = L.rt_denoiser_run(ctx.handle, feat.data_ptr(), P, H, W, vis.data_ptr(), conf.data_ptr(), ctypes.byref(d))
+        if st != 0:
+            raise RuntimeError(L.rt_last_error(ctx.handle))
+        ms.append(d.value)
+    t = sorted(ms[2:])[len(ms[2:]) // 2] * 1e-3
+    return {"kernel": "denoiser network (k_conv3x3_tc x %d, k_pool2, k_upadd)" % sum(o[0] == "conv" for o in net.ops),
+            "bound": "hbm", "achieved": nbytes / t / 1e9, "peak": hbm, "unit": "GB/s", "frac": nbytes / t / 1e9 / hbm,
+            "algorithmic_bytes": nbytes, "ms": t * 1e3, "params": net.param_count,
+            "tensor": {"achieved_tflops": flops / t / 1e12, "peak_tflops": tflops,
+                       "frac": flops / t / 1e12 / tflops if tflops else None}}
+
+
+def learned_vs_plain(rt, torch, ctx, directory, steps, hbm=6650.0, tflops=1590.0):
+    """The metric's second half, on the 1,000-sphere ring scene (two disk
+    lights) at 1920x1080, stochastic, 4 samples per pixel:
+      plain_64  every shading point casts 64 rays per disk light (the
+                configuration's 8x8 plain arm);
+      plain_16  the reference's 16 rays per disk light;
+      learned   primary hits cast 1 ray per disk light and the denoiser
+                estimates the visibility; hits whose estimated error exceeds
+                the network's threshold fall back to the plain path with 64
+                rays; reflection hits cast the reference's 16;
+      learned_refl64  the same with 64 rays at the reflection hits too.
+    Visibility of the primary samples (every hit sample x present light)
+    against the plain 64-ray render of the same frame (PSNR and max abs
+    error), and against a 1,024-ray render beside it; the network's raw
+    input (its 1 ray) and the network without the fallback are scored too.
+    Frames are timed with device events, L2 flushed before each."""
     from rtrace_b200 import denoiser, workloads
     if not os.path.exists(denoiser.DEFAULT_WEIGHTS):
         return {"unavailable": "no trained denoiser weights in the package"}
@@ -154,49 +205,107 @@ def learned_vs_plain(rt, torch, ctx, directory, steps):
     scene = rt.Scene.from_json_file(path, ctx)
     dev = torch.device("cuda", ctx.device)
     spp = 4
-    r = rt.Renderer(W, H)
-    r.anti_aliasing_mode = rt.AntiAliasingMode.Stochastic
-    r.samples = spp
-    vis = {k: torch.empty((spp, 2, H, W), dtype=torch.float32, device=dev) for k in ("target", "plain", "learned")}
-    feat = torch.empty((spp, H, W, 16), dtype=torch.float16, device=dev)
-    # visibility of the primary hits only: depth 1 is enough for the AOVs
-    r.max_depth = 1
-    r.disk_samples = TARGET_RAYS
-    r.render_shadow_aov(scene, vis["target"].data_ptr(), feat.data_ptr())
-    r.disk_samples = 16
-    r.render_shadow_aov(scene, vis["plain"].data_ptr(), None)
     ctx.load_denoiser()
-    r.learned_shadows = True
-    r.render_shadow_aov(scene, vis["learned"].data_ptr(), None)
-    r.max_depth = 10
-    present = torch.stack([feat[..., 8], feat[..., 12]], 1) > 0
-    mask = (feat[..., 0] > 0).unsqueeze(1) & present
-    out = {"workload": "ring_spheres_1000_1080p_4spp", "target": "%d rays per disk light, same frame" % TARGET_RAYS,
-           "psnr_over": "primary-hit samples x present disk lights"}
+
+    def renderer(mode):
+        r = rt.Renderer(W, H)
+        r.anti_aliasing_mode = rt.AntiAliasingMode.Stochastic
+        r.samples = spp
+        r.disk_samples = {"plain_64": PLAIN_RAYS, "learned_refl64": PLAIN_RAYS}.get(mode, 16)
+        if mode.startswith("learned"):
+            r.learned_shadows = True
+            r.fallback_samples = PLAIN_RAYS
+        if mode == "network_only":
+            r.learned_shadows = True
+            r.confidence_threshold = -1.0
+        return r
+
+    vis = {k: torch.zeros((spp, 2, H, W), dtype=torch.float32, device=dev)
+           for k in ("t64", "t1024", "plain_16", "learned", "network_only")}
+    feat = torch.zeros((spp, H, W, 16), dtype=torch.float16, device=dev)
+    lfeat = torch.zeros((spp, H, W, 16), dtype=torch.float16, device=dev)
+    torch.cuda.synchronize(dev)
+    # visibility of the primary hits only: depth 1 is enough for the AOVs
+    for key, mode, rays, fp in (("t64", "plain_64", PLAIN_RAYS, feat), ("t1024", "plain_64", NOISE_CAP_RAYS, None),
+                                ("plain_16", "plain_16", 16, None), ("learned", "learned", None, lfeat),
+                                ("network_only", "network_only", None, None)):
+        r = renderer(mode)
+        r.max_depth = 1
+        if rays:
+            r.disk_samples = rays
+        r.render_shadow_aov(scene, vis[key].data_ptr(), None if fp is None else fp.data_ptr())
+        if key == "learned":
+            fb_hits, hits = r.last_stats.fallback_hits, r.last_stats.hits
+    mask = denoiser.masks(feat)
+    raw = torch.stack([lfeat[..., 5], lfeat[..., 9]], 1).float()
+
+    def score(v):
+        out = {}
+        for tk, name in (("t64", "vs_64"), ("t1024", "vs_1024")):
+            d = (v[mask] - vis[tk][mask]).abs()
+            out[name] = {"psnr_db": denoiser.psnr(v, vis[tk], mask), "max_abs_err": float(d.max().item()),
+                         "mean_abs_err": float(d.mean().item())}
+        return out
+
+    out = {"workload": "ring_spheres_1000_1080p_4spp", "network": denoiser.unpack_net(denoiser.read_blob()).param_count,
+           "target": "visibility of the plain path with %d rays per disk light, same frame and samples" % PLAIN_RAYS,
+           "scored_over": "primary-hit samples x present disk lights (%d)" % int(mask.sum().item()),
+           "visibility": {"plain_16": score(vis["plain_16"]), "learned": score(vis["learned"]),
+                          "network_only": score(vis["network_only"]), "raw_1_ray": score(raw),
+                          "plain_64_vs_1024": score(vis["t64"])["vs_1024"]},
+           "fallback_share": fb_hits / max(1, hits), "fallback_rays_per_light": PLAIN_RAYS}
     img = torch.empty(W * H * 3, dtype=torch.uint8, device=dev)
     flush = torch.empty(512 * 1024 * 1024, dtype=torch.uint8, device=dev)
-    for mode in ("plain", "learned"):
-        r.learned_shadows = mode == "learned"
+    for mode in ("plain_64", "plain_16", "learned", "learned_refl64"):
+        r = renderer(mode)
         for _ in range(3):
             r.render(scene, device_ptr=img.data_ptr())
-        ms, rays = 0.0, 0
+        ms, rays = [], 0
         for _ in range(steps):
             flush.zero_()
             torch.cuda.synchronize(dev)
             r.render(scene, device_ptr=img.data_ptr())
-            ms += r.last_stats.device_ms
+            ms.append(r.last_stats.device_ms)
             rays += r.last_stats.rays
-        out[mode] = {"ms_per_frame": ms / steps, "mrays_per_s": rays / (ms * 1e-3) / 1e6,
-                     "rays_per_frame": rays // steps,
-                     "vis_psnr_db": denoiser.psnr(vis[mode], vis["target"], mask)}
-    r.learned_shadows = True
-    r.flags = 1  # stage times
-    r.render(scene, device_ptr=img.data_ptr())
-    out["learned"]["denoise_ms"] = r.last_stats.stage_ms.get("denoise")
-    out["learned"]["rays_per_light_at_primary_hits"] = denoiser.unpack(denoiser.read_blob(), with_rays=True)[1]
-    out["speedup"] = out["plain"]["ms_per_frame"] / out["learned"]["ms_per_frame"]
+        m = sum(ms) / steps
+        out[mode] = {"ms_per_frame": m, "mrays_per_s": rays / (sum(ms) * 1e-3) / 1e6, "rays_per_frame": rays // steps}
+        r.flags = 1  # stage times of one more frame
+        r.render(scene, device_ptr=img.data_ptr())
+        out[mode]["stage_ms"] = {k: round(v, 3) for k, v in r.last_stats.stage_ms.items() if v}
+    out["speedup_vs_plain_64"] = out["plain_64"]["ms_per_frame"] / out["learned"]["ms_per_frame"]
+    out["speedup_vs_plain_16"] = out["plain_16"]["ms_per_frame"] / out["learned"]["ms_per_frame"]
+    out["speedup_refl64_vs_plain_64"] = out["plain_64"]["ms_per_frame"] / out["learned_refl64"]["ms_per_frame"]
+    try:
+        out["roofline"] = denoiser_roofline(rt, torch, ctx, lfeat, hbm, tflops)
+    except Exception as e:
+        out["roofline"] = {"unavailable": str(e)}
     scene.close()
     return out
+
+
+def ring_parity(rt, directory, rows=4):
+    """RGB8 agreement of the 1080p ring-scene frame (plain path, 16 rays,
+    stochastic 4 spp) with the oracle's render of a band of its rows."""
+    import numpy as np
+    from rtrace_b200 import workloads
+    from tests import oracle_lib
+    path = workloads.write_scene(directory, "ring_spheres.json", workloads.ring_spheres_scene(seed=0))
+    scene = rt.Scene.from_json_file(path)
+    r = rt.Renderer(W, H)
+    r.anti_aliasing_mode = rt.AntiAliasingMode.Stochastic
+    r.samples = 4
+    frame = r.render(scene)
+    scene.close()
+    y0 = H // 2 - rows // 2
+    L = oracle_lib.load()
+    band = np.zeros((H, W, 3), np.uint8)
+    err = ctypes.create_string_buffer(512)
+    if L.oracle_render_rows(path.encode(), None, W, H, 2, 4, 10, 0, 1, 0, os.cpu_count() or 1, y0, y0 + rows,
+                            band.ctypes.data, None, None, err, 512):
+        raise RuntimeError(err.value.decode())
+    p = band_parity(frame, band, (y0, y0 + rows), halo=0)
+    p["workload"] = "ring_spheres_1000_1080p_4spp (plain, 16 rays)"
+    return p
 
 
 def batch_run(rt, ctx, directory, steps):
@@ -628,9 +737,19 @@ def main():
         learned = None
         if world == 1 and not args.no_learned:
             try:
-                learned = learned_vs_plain(rt, torch, ctx, d, min(args.steps, 10))
+                tf = None
+                try:
+                    tf = float(json.load(open(PEAKS)).get("bf16_tflops"))
+                except (OSError, TypeError, ValueError):
+                    tf = 1590.0
+                learned = learned_vs_plain(rt, torch, ctx, d, min(args.steps, 10), hbm, tf)
             except Exception as e:  # report, do not lose the headline line
                 learned = {"unavailable": "failed: %s" % e}
+        if world == 1 and not args.no_cpu_baseline and parity is not None:
+            try:
+                parity = {"headline_frame": parity, "ring_scene": ring_parity(rt, d)}
+            except Exception as e:
+                parity = {"headline_frame": parity, "ring_scene": {"unavailable": "failed: %s" % e}}
         small = None
         if world == 1:
             try:

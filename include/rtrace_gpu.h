@@ -99,7 +99,16 @@ typedef struct rt_render_params {
   /* learned_shadows: rays per disk light at the primary hits (1..16); 0
    * uses the count the loaded network was trained on. */
   uint32_t learned_rays;
-  uint32_t reserved2;
+  /* learned_shadows with a network that estimates its own error (blob
+   * version 3): a primary hit whose estimated visibility error exceeds
+   * confidence_threshold on one of its disk lights is shaded by the plain
+   * path instead, with fallback_samples rays per disk light (0: as
+   * disk_samples), the first samples of the reference's StdRng stream.
+   * confidence_threshold 0 uses the threshold stored with the weights; a
+   * negative value turns the fallback off. */
+  uint32_t fallback_samples;
+  float confidence_threshold;
+  uint32_t reserved3;
 } rt_render_params;
 
 /* Profiling flags: per-stage CUDA-event times, and device work counters
@@ -136,6 +145,7 @@ typedef struct rt_stats {
   double device_ms; /* CUDA-event time of the device pipeline */
   double total_ms;  /* host wall time of the whole call */
   double stage_ms[RT_STAGE_COUNT]; /* RT_FLAG_STAGE_TIMES */
+  uint64_t fallback_hits; /* learned shadows: primary hits shaded by the plain fallback */
 } rt_stats;
 
 /* ------------------------------------------------------------------ */
@@ -447,20 +457,75 @@ rt_status rt_batch_assign(const double* costs, uint32_t n, uint32_t lanes, uint3
 /* ------------------------------------------------------------------ */
 
 /* Loads the denoiser's weights into the context (replacing earlier ones).
- * Blob layout, little endian: "RTDN", u32 version (1 or 2), u32 n_layers,
- * (version 2) u32 rays per disk light the network was trained on, then per
- * layer u32 cin, cout, dilation (1..64), activation (0 ReLU; 2 sigmoid,
- * last layer only); then per layer FP16 weights [cout][3][3][cin] and FP32
- * bias [cout].  Channel counts are 16 or 32; the first layer reads the 16
- * feature channels, the last writes 16 of which the first two are the
- * visibility of disk-light slots 0 and 1. */
+ * Blob layout, little endian: "RTDN", u32 version, u32 n_ops, then
+ *   version 1: per op u32 cin, cout, dilation, activation;
+ *   version 2: u32 rays per disk light the network was trained on, then as
+ *     version 1;
+ *   version 3: u32 rays, f32 default confidence threshold, then per op u32
+ *     kind (0 3x3 convolution, 1 2x2 average pooling, 2 nearest 2x
+ *     upsampling of buffer src added to buffer src2), cin, cout, dilation,
+ *     activation, src, src2 (0xFFFFFFFF: none).
+ * Versions 1 and 2 are chains of convolutions (op i reads op i - 1).  In
+ * version 3, buffer 0 is the feature image and op i writes buffer i + 1;
+ * pooling halves the resolution (rounding up), upsampling joins adjacent
+ * resolutions.  Then per convolution FP16 weights [cout][3][3][cin] and
+ * FP32 bias [cout].  Convolutions have 16, 32 or 64 input and output
+ * channels (16->64 and 64->16 excepted), dilation 1..64 and ReLU
+ * (activation 0), except the last op: a full-resolution convolution to 16
+ * channels with activation 2 (sigmoid) whose channels 0, 1 are the
+ * visibility of disk-light slots 0 and 1 and, in version 3, channels 2, 3
+ * the network's estimate of its own absolute error on them. */
 rt_status rt_denoiser_load(rt_ctx* ctx, const void* blob, size_t bytes);
 
 /* Runs the loaded denoiser on a feature image ([planes][height][width][16]
  * FP16, device) and writes the visibility estimates ([planes][2][height]
- * [width] float, device). */
+ * [width] float, device) and, if confidence is not NULL and the network has
+ * them, its error estimates (same layout).  device_ms (optional): CUDA-event
+ * time of the network's kernels. */
 rt_status rt_denoiser_run(rt_ctx* ctx, const uint16_t* features, uint32_t planes, uint32_t height, uint32_t width,
-                          float* visibility);
+                          float* visibility, float* confidence, double* device_ms);
+
+/* ------------------------------------------------------------------ */
+/* Denoiser training (extension; no counterpart in the reference)     */
+/* ------------------------------------------------------------------ */
+
+/* A trainer holds FP32 master weights, Adam moments and the activations and
+ * gradients of one batch shape: planes feature images of height x width.
+ * It starts from a version 3 blob (rt_denoiser_load's format).  A step runs
+ * the network's forward pass on the inference kernels (masters rounded to
+ * FP16), the loss, the backward pass (weight gradients as tcgen05 implicit
+ * GEMMs, data gradients as the forward convolution with mirrored,
+ * transposed weights) and Adam.  The loss, over the samples whose primary
+ * ray hit and whose slot's light exists (features' valid and slot-present
+ * channels), is sum (v - t)^2 + (c - |v - t|)^2 with v the visibility
+ * output, t the target and c the error output (not differentiated through
+ * v).  features: [planes][height][width][16] FP16, targets:
+ * [planes][2][height][width] FP16, both device pointers. */
+typedef struct rt_dn_trainer rt_dn_trainer;
+rt_status rt_dn_train_create(rt_ctx* ctx, const void* blob, size_t bytes, uint32_t planes, uint32_t height,
+                             uint32_t width, rt_dn_trainer** out);
+/* One optimisation step (Adam with bias correction on the mean loss
+ * gradient); loss (optional, host, 3 floats): masked sample count, sum of
+ * the visibility term, sum of the error term. */
+rt_status rt_dn_train_step(rt_dn_trainer* t, const uint16_t* features, const uint16_t* targets, float lr,
+                           float beta1, float beta2, float eps, float* loss);
+/* The gradient of the summed loss with respect to every parameter (host,
+ * FP32, per convolution its weights [cout][3][3][cin] then bias, in op
+ * order), without an update; loss as in rt_dn_train_step. */
+rt_status rt_dn_train_grads(rt_dn_trainer* t, const uint16_t* features, const uint16_t* targets, float* grads,
+                            float* loss);
+/* The current weights as a version 3 blob.  blob_out NULL: *bytes receives
+ * the size. */
+rt_status rt_dn_train_export(rt_dn_trainer* t, void* blob_out, size_t* bytes);
+/* The default confidence threshold written by rt_dn_train_export. */
+rt_status rt_dn_train_set_threshold(rt_dn_trainer* t, float threshold);
+void rt_dn_train_free(rt_dn_trainer* t);
+/* Weight and bias gradients of one 3x3 convolution (dilation dil) on the
+ * tensor cores: dw[cout][3][3][cin] += sum_q dz[q][co] x[q + tap][ci], db[co]
+ * += sum_q dz[q][co]; x [planes][height][width][cin] and dz [..][cout]
+ * FP16, dw and db FP32, all device pointers. */
+rt_status rt_debug_conv_wgrad(rt_ctx* ctx, const uint16_t* x, const uint16_t* dz, uint32_t planes, uint32_t height,
+                              uint32_t width, uint32_t cin, uint32_t cout, uint32_t dil, float* dw, float* db);
 
 /* rt_render plus, for the primary samples (plane = sample index within
  * the pixel, so planes = samples), the shadow visibility each of the first

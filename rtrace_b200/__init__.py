@@ -89,6 +89,7 @@ class RenderStats:
     stage_ms: dict = field(default_factory=dict)
     work: dict = field(default_factory=dict)
     graph: int = 0  # RT_FLAG_CUDA_GRAPH: 1 captured by this render, 2 replayed
+    fallback_hits: int = 0  # learned shadows: primary hits shaded by the plain fallback
 
     @property
     def rays(self):
@@ -101,7 +102,8 @@ class RenderStats:
             "shadow_triangles", "shadow_spheres", "shadow_verifications")}
         stages = {name: float(st.stage_ms[i]) for i, name in enumerate(_capi.STAGES)}
         return cls(int(st.primary_rays), int(st.reflection_rays), int(st.shadow_rays), float(st.device_ms),
-                   float(st.total_ms), int(st.hits), int(st.kernel_launches), stages, work, int(st.graph))
+                   float(st.total_ms), int(st.hits), int(st.kernel_launches), stages, work, int(st.graph),
+                   int(st.fallback_hits))
 
 
 class Context:
@@ -356,6 +358,12 @@ class Renderer:
         self.disk_samples = 16
         self.learned_shadows = False  # needs Context.load_denoiser first
         self.learned_rays = 0  # rays per disk light at primary hits; 0: what the network was trained on
+        # learned shadows: a primary hit whose estimated visibility error
+        # exceeds confidence_threshold falls back to the plain path with
+        # fallback_samples rays per disk light (0: disk_samples); threshold 0
+        # takes the one stored with the weights, a negative one disables it
+        self.confidence_threshold = 0.0
+        self.fallback_samples = 0
         self.last_stats = RenderStats()
 
     @classmethod
@@ -398,6 +406,8 @@ class Renderer:
         p.disk_samples = int(self.disk_samples)
         p.learned_shadows = 1 if self.learned_shadows else 0
         p.learned_rays = int(self.learned_rays)
+        p.confidence_threshold = float(self.confidence_threshold)
+        p.fallback_samples = int(self.fallback_samples)
         oc = self.outline_config
         if oc is not None:
             p.outline.enabled = 1

@@ -76,7 +76,9 @@ class rt_render_params(ctypes.Structure):
         ("disk_samples", ctypes.c_uint32),
         ("learned_shadows", ctypes.c_int32),
         ("learned_rays", ctypes.c_uint32),
-        ("reserved2", ctypes.c_uint32),
+        ("fallback_samples", ctypes.c_uint32),
+        ("confidence_threshold", ctypes.c_float),
+        ("reserved3", ctypes.c_uint32),
     ]
 
 
@@ -106,6 +108,7 @@ class rt_stats(ctypes.Structure):
         ("device_ms", ctypes.c_double),
         ("total_ms", ctypes.c_double),
         ("stage_ms", ctypes.c_double * 8),
+        ("fallback_hits", ctypes.c_uint64),
     ]
 
 
@@ -202,7 +205,18 @@ def lib():
                                              ctypes.POINTER(ctypes.c_uint32)]),
         "rt_batch_assign": (ctypes.c_int, [_vp, ctypes.c_uint32, ctypes.c_uint32, _vp]),
         "rt_denoiser_load": (ctypes.c_int, [_vp, _vp, ctypes.c_size_t]),
-        "rt_denoiser_run": (ctypes.c_int, [_vp, _vp, ctypes.c_uint32, ctypes.c_uint32, ctypes.c_uint32, _vp]),
+        "rt_denoiser_run": (ctypes.c_int, [_vp, _vp, ctypes.c_uint32, ctypes.c_uint32, ctypes.c_uint32, _vp, _vp,
+                                           _vp]),
+        "rt_dn_train_create": (ctypes.c_int, [_vp, _vp, ctypes.c_size_t, ctypes.c_uint32, ctypes.c_uint32,
+                                              ctypes.c_uint32, _vp]),
+        "rt_dn_train_step": (ctypes.c_int, [_vp, _vp, _vp, ctypes.c_float, ctypes.c_float, ctypes.c_float,
+                                            ctypes.c_float, _vp]),
+        "rt_dn_train_grads": (ctypes.c_int, [_vp, _vp, _vp, _vp, _vp]),
+        "rt_dn_train_export": (ctypes.c_int, [_vp, _vp, ctypes.POINTER(ctypes.c_size_t)]),
+        "rt_dn_train_set_threshold": (ctypes.c_int, [_vp, ctypes.c_float]),
+        "rt_dn_train_free": (None, [_vp]),
+        "rt_debug_conv_wgrad": (ctypes.c_int, [_vp, _vp, _vp, ctypes.c_uint32, ctypes.c_uint32, ctypes.c_uint32,
+                                               ctypes.c_uint32, ctypes.c_uint32, ctypes.c_uint32, _vp, _vp]),
         "rt_render_shadow_aov": (ctypes.c_int, [_vp, _vp, ctypes.POINTER(rt_render_params), _vp, _vp, _vp,
                                                 ctypes.POINTER(rt_stats)]),
         "rt_render_linear": (ctypes.c_int, [_vp, _vp, ctypes.POINTER(rt_render_params), _vp, _vp,

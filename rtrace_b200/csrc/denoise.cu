@@ -94,6 +94,15 @@ __device__ __forceinline__ void tmem_ld<16>(uint32_t taddr, uint32_t (&r)[16]) {
 }
 
 template <>
+__device__ __forceinline__ void tmem_ld<32>(uint32_t taddr, uint32_t (&r)[32]);
+
+template <>
+__device__ __forceinline__ void tmem_ld<64>(uint32_t taddr, uint32_t (&r)[64]) {
+  tmem_ld<32>(taddr, *reinterpret_cast<uint32_t(*)[32]>(&r[0]));
+  tmem_ld<32>(taddr + 32u, *reinterpret_cast<uint32_t(*)[32]>(&r[32]));
+}
+
+template <>
 __device__ __forceinline__ void tmem_ld<32>(uint32_t taddr, uint32_t (&r)[32]) {
   asm volatile(
       "tcgen05.ld.sync.aligned.32x32b.x32.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15,"
@@ -106,8 +115,10 @@ __device__ __forceinline__ void tmem_ld<32>(uint32_t taddr, uint32_t (&r)[32]) {
 }
 
 constexpr int TILE_M = 128;
-constexpr int TMEM_COLS = 32;  // >= COUT, power of two >= 32
 constexpr int MAX_DIL = 64;    // 128 + 2 * dilation pixels must fit one TMA box (<= 256)
+// TMEM columns of one accumulator (>= COUT, at least 32) and of a CTA's
+// allocation (NACC accumulators, a power of two >= 32)
+__host__ __device__ constexpr int acc_cols(int cout) { return cout < 32 ? 32 : cout; }
 
 // Shared memory of one CTA: a ring of NROW staged input rows (TILE_M +
 // 2 * dil pixels each, one block of 16-byte rows per 8 channels), the
@@ -124,7 +135,7 @@ struct ConvSmem {
   static constexpr int B_BYTES = 9 * CPT * COUT * 16;     // weights
   static constexpr int TAIL = 256;                        // barriers, TMEM slot, abort flag
   static_assert(8 * (2 * NROW + 2 * NACC) + 8 <= TAIL, "the mbarriers, TMEM slot and abort flag overflow TAIL");
-  static constexpr int BIAS = 128;                        // COUT floats
+  static constexpr int BIAS = 256;                        // COUT floats
   static constexpr int OUT = 4 * 32 * COUT * 2;           // epilogue staging: 32 pixels per warp
   static int row_bytes(int dil) { return CPT * halo_block(dil); }
   static int total(int dil) { return 1024 + NROW * row_bytes(dil) + B_BYTES + TAIL + BIAS + OUT; }
@@ -171,8 +182,16 @@ __device__ __forceinline__ void mbar_arrive(uint32_t mbar) {
   asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(mbar) : "memory");
 }
 
-// MODE 0: ReLU, FP16 output [plane][H][W][COUT].  MODE 2: sigmoid of the
-// first DN_MAX_SLOTS channels, float output [plane][slot][H][W].
+// Epilogue modes.  FP16 NHWC output [plane][H][W][COUT]:
+//   MODE 0: bias + ReLU (forward hidden layers);
+//   MODE 1: the accumulator times (aux > 0), aux an FP16 NHWC tensor of the
+//           output's shape, no bias (backward data through a ReLU: aux is
+//           the forward activation the gradient flows into);
+//   MODE 3: the accumulator alone (backward data into a linear tensor).
+// MODE 2: float outputs: sigmoid(channel j + bias) for j < DN_MAX_SLOTS
+// into vis [plane][slot][H][W] (visibility of disk-light slot j) and
+// sigmoid(channel DN_MAX_SLOTS + j + bias) into conf (the network's
+// estimate of its own error on slot j), if conf is not null.
 //
 // A step is one 128-pixel run of one output row; the CTA walks segments
 // blockIdx.x, blockIdx.x + gridDim.x, ... (see ConvSeg), a segment's steps
@@ -199,8 +218,10 @@ __global__ void __launch_bounds__(CONV_THREADS) k_conv3x3_tc(const __grid_consta
                                                               int H, int W, int dil, const uint4* __restrict__ wl,
                                                               const float* __restrict__ bias,
                                                               __half* __restrict__ out, float* __restrict__ vis,
-                                                              int* err) {
-  static_assert(CIN % 16 == 0 && COUT % 16 == 0 && COUT <= TMEM_COLS, "unsupported channel counts");
+                                                              float* __restrict__ conf,
+                                                              const __half* __restrict__ aux, int* err) {
+  static_assert(CIN % 16 == 0 && COUT % 16 == 0 && COUT <= 64, "unsupported channel counts");
+  constexpr int ACC = acc_cols(COUT), TMEM_ALLOC = NACC * ACC;
   using SM = ConvSmem<CIN, COUT>;
   constexpr int CPT = SM::CPT;
   extern __shared__ unsigned char smem_raw[];
@@ -244,7 +265,7 @@ __global__ void __launch_bounds__(CONV_THREADS) k_conv3x3_tc(const __grid_consta
   if (warp == 5) {
     __syncwarp();
     asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(tslot)),
-                 "r"(NACC * TMEM_COLS)
+                 "r"(TMEM_ALLOC)
                  : "memory");
     asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
   }
@@ -310,7 +331,7 @@ __global__ void __launch_bounds__(CONV_THREADS) k_conv3x3_tc(const __grid_consta
             break;
           }
           asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-          const uint32_t acc = tmem + (uint32_t)(a * TMEM_COLS);
+          const uint32_t acc = tmem + (uint32_t)(a * ACC);
 #pragma unroll
           for (int tap = 0; tap < 9; tap++) {
             const int ky = tap / 3, kx = tap % 3;
@@ -367,13 +388,21 @@ __global__ void __launch_bounds__(CONV_THREADS) k_conv3x3_tc(const __grid_consta
         }
         asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
         uint32_t accv[COUT];
-        tmem_ld<COUT>(tmem + (uint32_t)(a * TMEM_COLS) + ((uint32_t)(warp * 32) << 16), accv);
+        tmem_ld<COUT>(tmem + (uint32_t)(a * ACC) + ((uint32_t)(warp * 32) << 16), accv);
         asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
         asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
         if (lane == 0) mbar_arrive(acce_bar(a));
         const int tx = c.tx, p = c.p, y = c.r + (c.k0 + t) * dil;
         const int x = tx * TILE_M + tid;
-        if (MODE == 0) {
+        if (MODE != 2) {
+          constexpr int CPX0 = COUT / 8;
+          // MODE 1: the ReLU mask of this pixel's forward activation
+          uint4 mk[CPX0];
+          if (MODE == 1 && x < W) {
+            const uint4* ap = reinterpret_cast<const uint4*>(aux + (((long long)p * H + y) * (long long)W + x) * COUT);
+  #pragma unroll
+            for (int c = 0; c < CPX0; c++) mk[c] = ap[c];
+          }
           // Each warp stages its 32 pixels (COUT halves each) in shared
           // memory, 16-byte chunks XOR-swizzled so that both the writes and
           // the read-back are free of bank conflicts, then writes them out as
@@ -387,8 +416,17 @@ __global__ void __launch_bounds__(CONV_THREADS) k_conv3x3_tc(const __grid_consta
             __align__(16) __half h[8];
   #pragma unroll
             for (int e = 0; e < 8; e++) {
-              float v = __uint_as_float(accv[8 * c + e]) + s_bias[8 * c + e];
-              h[e] = __float2half_rn(v > 0.f ? v : 0.f);
+              float v = __uint_as_float(accv[8 * c + e]);
+              if (MODE == 0) {
+                v += s_bias[8 * c + e];
+                v = v > 0.f ? v : 0.f;
+              } else if (MODE == 1) {
+                const uint32_t word = (&mk[c].x)[e >> 1];
+                const uint16_t bits = (uint16_t)((e & 1) ? (word >> 16) : (word & 0xFFFFu));
+                // FP16 > 0: sign clear and not +0 (NaN cannot occur in a ReLU output)
+                v = ((bits & 0x8000u) == 0 && bits != 0) ? v : 0.f;
+              }
+              h[e] = __float2half_rn(v);
             }
             const int phys = c ^ ((lane / PPL) & (CPX - 1));
             *reinterpret_cast<uint4*>(wb + lane * ROWB + phys * 16) = *reinterpret_cast<const uint4*>(h);
@@ -408,8 +446,13 @@ __global__ void __launch_bounds__(CONV_THREADS) k_conv3x3_tc(const __grid_consta
         } else if (x < W) {
   #pragma unroll
           for (int j = 0; j < DN_MAX_SLOTS; j++) {
+            const long long o = (((long long)p * DN_MAX_SLOTS + j) * H + y) * (long long)W + x;
             float v = __uint_as_float(accv[j]) + s_bias[j];
-            vis[(((long long)p * DN_MAX_SLOTS + j) * H + y) * (long long)W + x] = 1.f / (1.f + __expf(-v));
+            vis[o] = 1.f / (1.f + __expf(-v));
+            if (conf) {
+              float c = __uint_as_float(accv[DN_MAX_SLOTS + j]) + s_bias[DN_MAX_SLOTS + j];
+              conf[o] = 1.f / (1.f + __expf(-c));
+            }
           }
         }
       }
@@ -420,7 +463,7 @@ __global__ void __launch_bounds__(CONV_THREADS) k_conv3x3_tc(const __grid_consta
   if (warp == 5) {
     __syncwarp();
     asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(NACC * TMEM_COLS)
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(TMEM_ALLOC)
                  : "memory");
   }
 }
@@ -455,10 +498,11 @@ cudaError_t make_in_map(CUtensorMap* map, const __half* in, int planes, int H, i
 
 template <int CIN, int COUT, int MODE>
 cudaError_t launch_conv(const __half* in, int planes, int H, int W, int dil, const void* w, const float* b, __half* out,
-                        float* vis, int* err, cudaStream_t s, int num_sms) {
+                        float* vis, float* conf, const __half* aux, int* err, cudaStream_t s, int num_sms) {
   using SM = ConvSmem<CIN, COUT>;
   if (dil < 1 || dil > MAX_DIL) return cudaErrorInvalidValue;
   const int smem = SM::total(dil);
+  if (smem > 227 * 1024) return cudaErrorInvalidValue;
   static int attr_bytes[64] = {};  // per device ordinal: the largest size set so far
   static std::mutex attr_mu;       // batch lanes launch from several host threads
   int dev = 0;
@@ -475,17 +519,83 @@ cudaError_t launch_conv(const __half* in, int planes, int H, int W, int dil, con
   CUtensorMap map;
   e = make_in_map(&map, in, planes, H, W, CIN, dil);
   if (e != cudaSuccess) return e;
-  // 4 CTAs per SM (each holds 64 of the SM's 512 TMEM columns; shared
-  // memory allows 2-6 resident); CTAs beyond the resident ones start as
-  // others finish, which balances the segments better than one resident
+  // 4 CTAs per SM (each holds at most 128 of the SM's 512 TMEM columns;
+  // shared memory allows 1-6 resident); CTAs beyond the resident ones start
+  // as others finish, which balances the segments better than one resident
   // wave (1.8x slower) or one CTA per segment (1.2x slower)
   const long long rows_per_col = (H + dil - 1) / dil;
   const long long nsegs = (long long)planes * ((W + TILE_M - 1) / TILE_M) * dil * ((rows_per_col + SEG - 1) / SEG);
   long long grid = std::min<long long>(nsegs, (long long)num_sms * 4);
   if (grid < 1) grid = 1;
   k_conv3x3_tc<CIN, COUT, MODE><<<(int)grid, CONV_THREADS, smem, s>>>(map, planes, H, W, dil, (const uint4*)w, b,
-                                                                      out, vis, err);
+                                                                      out, vis, conf, aux, err);
   return cudaGetLastError();
+}
+
+// 2x2 average pooling, [P][H][W][C] -> [P][ceil(H/2)][ceil(W/2)][C] FP16;
+// an output pixel averages the input pixels of its 2x2 block that exist.
+// One thread per 8 channels of one output pixel.
+__global__ void k_pool2(const __half* __restrict__ in, __half* __restrict__ out, int P, int H, int W, int C) {
+  const int Ho = (H + 1) / 2, Wo = (W + 1) / 2, CC = C / 8;
+  const long long n = (long long)P * Ho * Wo * CC;
+  for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < n; t += (long long)gridDim.x * blockDim.x) {
+    const int cc = (int)(t % CC);
+    long long q = t / CC;
+    const int x = (int)(q % Wo);
+    q /= Wo;
+    const int y = (int)(q % Ho);
+    const long long p = q / Ho;
+    float acc[8] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
+    int cnt = 0;
+    for (int dy = 0; dy < 2; dy++)
+      for (int dx = 0; dx < 2; dx++) {
+        const int yy = 2 * y + dy, xx = 2 * x + dx;
+        if (yy >= H || xx >= W) continue;
+        const uint4 v = reinterpret_cast<const uint4*>(in + ((p * H + yy) * (long long)W + xx) * C)[cc];
+        const __half2* h = reinterpret_cast<const __half2*>(&v);
+#pragma unroll
+        for (int k = 0; k < 4; k++) {
+          float2 f = __half22float2(h[k]);
+          acc[2 * k] += f.x;
+          acc[2 * k + 1] += f.y;
+        }
+        cnt++;
+      }
+    const float inv = 1.f / (float)cnt;
+    uint4 o;
+    __half2* oh = reinterpret_cast<__half2*>(&o);
+#pragma unroll
+    for (int k = 0; k < 4; k++) oh[k] = __floats2half2_rn(acc[2 * k] * inv, acc[2 * k + 1] * inv);
+    reinterpret_cast<uint4*>(out + ((p * Ho + y) * (long long)Wo + x) * C)[cc] = o;
+  }
+}
+
+// Nearest 2x upsampling of `low` ([P][ceil(H/2)][ceil(W/2)][C]) added to
+// `skip` ([P][H][W][C]): out(y, x) = low(y / 2, x / 2) + skip(y, x), FP16.
+__global__ void k_upadd(const __half* __restrict__ low, const __half* __restrict__ skip, __half* __restrict__ out,
+                        int P, int H, int W, int C) {
+  const int Hl = (H + 1) / 2, Wl = (W + 1) / 2, CC = C / 8;
+  const long long n = (long long)P * H * W * CC;
+  for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < n; t += (long long)gridDim.x * blockDim.x) {
+    const int cc = (int)(t % CC);
+    long long q = t / CC;
+    const int x = (int)(q % W);
+    q /= W;
+    const int y = (int)(q % H);
+    const long long p = q / H;
+    const uint4 a = reinterpret_cast<const uint4*>(low + ((p * Hl + y / 2) * (long long)Wl + x / 2) * C)[cc];
+    const uint4 b = reinterpret_cast<const uint4*>(skip)[t];
+    uint4 o;
+    const __half2* ah = reinterpret_cast<const __half2*>(&a);
+    const __half2* bh = reinterpret_cast<const __half2*>(&b);
+    __half2* oh = reinterpret_cast<__half2*>(&o);
+#pragma unroll
+    for (int k = 0; k < 4; k++) {
+      float2 fa = __half22float2(ah[k]), fb = __half22float2(bh[k]);
+      oh[k] = __floats2half2_rn(fa.x + fb.x, fa.y + fb.y);
+    }
+    reinterpret_cast<uint4*>(out)[t] = o;
+  }
 }
 
 float half_to_float_host(uint16_t h) {
@@ -494,124 +604,260 @@ float half_to_float_host(uint16_t h) {
   return __half2float(__half(r));
 }
 
+int level_dim(int n, int level) { return (n + (1 << level) - 1) >> level; }
+
 }  // namespace
 
-std::string denoise_load(const void* blob, size_t bytes, DenoiseNet* net) {
-  denoise_free(net);
-  const unsigned char* p = static_cast<const unsigned char*>(blob);
+// Dispatch of the convolution shapes and epilogue modes the networks use
+// (forward layers, and the transposed shapes of their backward data passes).
+cudaError_t conv_launch(int cin, int cout, int mode, const __half* in, int planes, int H, int W, int dil,
+                        const void* w, const float* b, __half* out, float* vis, float* conf, const __half* aux,
+                        int* err, cudaStream_t s, int num_sms) {
+#define RTB_CONV_CASE(CI, CO, M)                                                                         \
+  if (cin == CI && cout == CO && mode == M)                                                              \
+    return launch_conv<CI, CO, M>(in, planes, H, W, dil, w, b, out, vis, conf, aux, err, s, num_sms);
+#define RTB_CONV_SHAPE(CI, CO) RTB_CONV_CASE(CI, CO, 0) RTB_CONV_CASE(CI, CO, 1) RTB_CONV_CASE(CI, CO, 3)
+  RTB_CONV_SHAPE(16, 16)
+  RTB_CONV_SHAPE(16, 32)
+  RTB_CONV_SHAPE(32, 16)
+  RTB_CONV_SHAPE(32, 32)
+  RTB_CONV_SHAPE(32, 64)
+  RTB_CONV_SHAPE(64, 32)
+  RTB_CONV_SHAPE(64, 64)
+  RTB_CONV_CASE(16, 16, 2)
+  RTB_CONV_CASE(32, 16, 2)
+#undef RTB_CONV_SHAPE
+#undef RTB_CONV_CASE
+  return cudaErrorInvalidValue;
+}
+
+bool conv_shape_supported(int cin, int cout) {
+  static const int shapes[][2] = {{16, 16}, {16, 32}, {32, 16}, {32, 32}, {32, 64}, {64, 32}, {64, 64}};
+  for (auto& sh : shapes)
+    if (sh[0] == cin && sh[1] == cout) return true;
+  return false;
+}
+
+cudaError_t pool2_launch(const __half* in, __half* out, int P, int H, int W, int C, cudaStream_t s, int num_sms) {
+  const long long n = (long long)P * ((H + 1) / 2) * ((W + 1) / 2) * (C / 8);
+  const int blocks = (int)std::max<long long>(1, std::min<long long>((n + 255) / 256, (long long)num_sms * 16));
+  k_pool2<<<blocks, 256, 0, s>>>(in, out, P, H, W, C);
+  return cudaGetLastError();
+}
+
+cudaError_t upadd_launch(const __half* low, const __half* skip, __half* out, int P, int H, int W, int C,
+                         cudaStream_t s, int num_sms) {
+  const long long n = (long long)P * H * W * (C / 8);
+  const int blocks = (int)std::max<long long>(1, std::min<long long>((n + 255) / 256, (long long)num_sms * 16));
+  k_upadd<<<blocks, 256, 0, s>>>(low, skip, out, P, H, W, C);
+  return cudaGetLastError();
+}
+
+namespace {
+// Reads version 1/2 blobs (a chain of convolutions) and version 3 blobs
+// (an op list); fills ops (weights still on the host, in the blob's
+// [cout][3][3][cin] FP16 layout, at w_off) or returns the reason.
+struct ParsedOp {
+  DnOp op;
+  size_t w_off = 0;
+};
+std::string parse_blob(const unsigned char* p, size_t bytes, std::vector<ParsedOp>* out, int* rays, float* thr) {
   auto u32 = [&](size_t off) {
     uint32_t v;
     memcpy(&v, p + off, 4);
     return v;
   };
-  if (!blob || bytes < 12 || memcmp(p, "RTDN", 4) != 0) return "not a denoiser weight blob (magic RTDN)";
+  if (!p || bytes < 12 || memcmp(p, "RTDN", 4) != 0) return "not a denoiser weight blob (magic RTDN)";
   const uint32_t ver = u32(4);
-  if (ver != 1 && ver != 2) return "unsupported denoiser blob version";
-  uint32_t n = u32(8);
-  if (n < 1 || n > 32) return "denoiser layer count must be 1..32";
-  size_t head = ver == 1 ? 12 : 16;  // version 2 adds the rays per disk light the network was trained on
-  int rays = 1;
-  if (ver == 2) {
-    if (bytes < 16) return "truncated denoiser blob";
-    rays = (int)u32(12);
-    if (rays < 1 || rays > 16) return "denoiser rays per light must be 1..16";
-  }
-  size_t off = head + 16 * (size_t)n;
+  if (ver < 1 || ver > 3) return "unsupported denoiser blob version";
+  const uint32_t n = u32(8);
+  if (n < 1 || n > 64) return "denoiser op count must be 1..64";
+  size_t head = ver == 1 ? 12 : (ver == 2 ? 16 : 20);
+  if (bytes < head) return "truncated denoiser blob";
+  *rays = ver == 1 ? 1 : (int)u32(12);
+  if (*rays < 1 || *rays > 16) return "denoiser rays per light must be 1..16";
+  *thr = 1.0f;
+  if (ver == 3) memcpy(thr, p + 16, 4);
+  if (!(*thr >= 0.0f)) return "denoiser confidence threshold must be >= 0";
+  const size_t rec = ver == 3 ? 28 : 16;
+  size_t off = head + rec * n;
   if (bytes < off) return "truncated denoiser blob";
-  std::vector<DnLayer> L(n);
+  std::vector<int> ch(1, FEAT_CHANNELS), lv(1, 0);  // per buffer
+  out->assign(n, ParsedOp());
   for (uint32_t i = 0; i < n; i++) {
-    L[i].cin = (int)u32(head + 16 * i);
-    L[i].cout = (int)u32(head + 4 + 16 * i);
-    L[i].dil = (int)u32(head + 8 + 16 * i);
-    L[i].act = (int)u32(head + 12 + 16 * i);
-    bool last = i + 1 == n;
-    if ((L[i].cin != 16 && L[i].cin != 32) || (L[i].cout != 16 && L[i].cout != 32))
-      return "denoiser layers must have 16 or 32 input and output channels";
-    if (L[i].dil < 1 || L[i].dil > MAX_DIL) return "denoiser dilation must be 1..64";
-    if (L[i].act != (last ? 2 : 0)) return "denoiser layers must be ReLU, the last one sigmoid";
-    if (last && L[i].cout != 16) return "the last denoiser layer must have 16 output channels";
-    if (i == 0 && L[i].cin != FEAT_CHANNELS) return "the first denoiser layer must read 16 feature channels";
-    if (i > 0 && L[i].cin != L[i - 1].cout) return "denoiser layer channel counts do not chain";
+    DnOp& o = (*out)[i].op;
+    const size_t r = head + rec * i;
+    if (ver == 3) {
+      o.kind = (int)u32(r);
+      o.cin = (int)u32(r + 4);
+      o.cout = (int)u32(r + 8);
+      o.dil = (int)u32(r + 12);
+      o.act = (int)u32(r + 16);
+      o.src = (int)u32(r + 20);
+      o.src2 = (int)u32(r + 24);
+    } else {
+      o.kind = DN_CONV;
+      o.cin = (int)u32(r);
+      o.cout = (int)u32(r + 4);
+      o.dil = (int)u32(r + 8);
+      o.act = (int)u32(r + 12);
+      o.src = (int)i;
+      o.src2 = -1;
+    }
+    const bool last = i + 1 == n;
+    if (o.src < 0 || o.src > (int)i) return "denoiser op reads a buffer not yet written";
+    if (o.kind == DN_CONV) {
+      if (!conv_shape_supported(o.cin, o.cout)) return "unsupported denoiser convolution channel counts";
+      if (o.cin != ch[o.src]) return "denoiser layer channel counts do not chain";
+      if (o.dil < 1 || o.dil > MAX_DIL) return "denoiser dilation must be 1..64";
+      if (o.act != (last ? 2 : 0)) return "denoiser layers must be ReLU, the last one sigmoid";
+      o.level = lv[o.src];
+    } else if (o.kind == DN_POOL) {
+      if (o.cin != ch[o.src] || o.cout != o.cin) return "denoiser pooling must keep its channel count";
+      if (lv[o.src] >= 4) return "denoiser pooling beyond level 4";
+      o.level = lv[o.src] + 1;
+    } else if (o.kind == DN_UPADD) {
+      if (o.src2 < 0 || o.src2 > (int)i) return "denoiser op reads a buffer not yet written";
+      if (lv[o.src] != lv[o.src2] + 1) return "denoiser upsampling must join adjacent levels";
+      if (o.cin != ch[o.src] || o.cin != ch[o.src2] || o.cout != o.cin)
+        return "denoiser upsampling must add equal channel counts";
+      o.level = lv[o.src2];
+    } else {
+      return "unknown denoiser op kind";
+    }
+    if (last && (o.kind != DN_CONV || o.cout != 16 || o.level != 0))
+      return "the last denoiser op must be a convolution writing 16 channels at full resolution";
+    if (i == 0 && o.kind == DN_CONV && o.cin != FEAT_CHANNELS)
+      return "the first denoiser layer must read 16 feature channels";
+    ch.push_back(o.cout);
+    lv.push_back(o.level);
   }
+  for (uint32_t i = 0; i < n; i++) {
+    ParsedOp& po = (*out)[i];
+    if (po.op.kind != DN_CONV) continue;
+    const size_t wbytes = (size_t)po.op.cout * 9 * po.op.cin * 2, bbytes = (size_t)po.op.cout * 4;
+    if (bytes < off + wbytes + bbytes) return "truncated denoiser blob";
+    po.w_off = off;
+    off += wbytes + bbytes;
+  }
+  if (off != bytes) return "denoiser blob has trailing bytes";
+  return std::string();
+}
+}  // namespace
+
+std::string denoise_load(const void* blob, size_t bytes, DenoiseNet* net) {
+  denoise_free(net);
+  const unsigned char* p = static_cast<const unsigned char*>(blob);
+  std::vector<ParsedOp> ops;
+  int rays = 1;
+  float thr = 1.0f;
+  std::string perr = parse_blob(p, bytes, &ops, &rays, &thr);
+  if (!perr.empty()) return perr;
   std::vector<void*> allocs;
   auto fail = [&](const std::string& m) {
     for (void* a : allocs) cudaFree(a);
     return m;
   };
   size_t params = 0;
-  for (uint32_t i = 0; i < n; i++) {
-    const int cin = L[i].cin, cout = L[i].cout, K = 9 * cin;
-    size_t wbytes = (size_t)cout * K * 2, bbytes = (size_t)cout * 4;
-    if (bytes < off + wbytes + bbytes) return fail("truncated denoiser blob");
-    const uint16_t* w = reinterpret_cast<const uint16_t*>(p + off);
-    // [cout][ky][kx][cin] -> operand layout: K chunk k/8 at k/8 * (cout*16),
-    // row n at n * 16, element k%8 at 2 * (k%8); k = (ky*3 + kx) * cin + c
-    std::vector<uint16_t> lay((size_t)cout * K, 0);
-    for (int nn = 0; nn < cout; nn++)
-      for (int k = 0; k < K; k++) {
-        uint16_t v;
-        memcpy(&v, w + (size_t)nn * K + k, 2);
-        size_t dst = ((size_t)(k / 8) * (cout * 16) + (size_t)nn * 16 + (size_t)(k % 8) * 2) / 2;
-        lay[dst] = v;
-        if (half_to_float_host(v) != half_to_float_host(v)) return fail("NaN in denoiser weights");
-      }
-    void* dw = nullptr;
-    float* db = nullptr;
-    if (cudaMalloc(&dw, wbytes) != cudaSuccess) return fail("cudaMalloc(denoiser weights) failed");
-    allocs.push_back(dw);
-    if (cudaMalloc((void**)&db, bbytes) != cudaSuccess) return fail("cudaMalloc(denoiser bias) failed");
-    allocs.push_back(db);
-    if (cudaMemcpy(dw, lay.data(), wbytes, cudaMemcpyHostToDevice) != cudaSuccess ||
-        cudaMemcpy(db, p + off + wbytes, bbytes, cudaMemcpyHostToDevice) != cudaSuccess)
-      return fail("uploading denoiser weights failed");
-    L[i].w = dw;
-    L[i].b = db;
-    off += wbytes + bbytes;
-    params += (size_t)cout * K + cout;
+  std::vector<DnOp> L;
+  for (ParsedOp& po : ops) {
+    DnOp o = po.op;
+    if (o.kind == DN_CONV) {
+      const int cin = o.cin, cout = o.cout, K = 9 * cin;
+      const size_t wbytes = (size_t)cout * K * 2, bbytes = (size_t)cout * 4;
+      const uint16_t* w = reinterpret_cast<const uint16_t*>(p + po.w_off);
+      // [cout][ky][kx][cin] -> operand layout: K chunk k/8 at k/8 * (cout*16),
+      // row n at n * 16, element k%8 at 2 * (k%8); k = (ky*3 + kx) * cin + c
+      std::vector<uint16_t> lay((size_t)cout * K, 0);
+      for (int nn = 0; nn < cout; nn++)
+        for (int k = 0; k < K; k++) {
+          uint16_t v;
+          memcpy(&v, w + (size_t)nn * K + k, 2);
+          size_t dst = ((size_t)(k / 8) * (cout * 16) + (size_t)nn * 16 + (size_t)(k % 8) * 2) / 2;
+          lay[dst] = v;
+          if (half_to_float_host(v) != half_to_float_host(v)) return fail("NaN in denoiser weights");
+        }
+      void* dw = nullptr;
+      float* db = nullptr;
+      if (cudaMalloc(&dw, wbytes) != cudaSuccess) return fail("cudaMalloc(denoiser weights) failed");
+      allocs.push_back(dw);
+      if (cudaMalloc((void**)&db, bbytes) != cudaSuccess) return fail("cudaMalloc(denoiser bias) failed");
+      allocs.push_back(db);
+      if (cudaMemcpy(dw, lay.data(), wbytes, cudaMemcpyHostToDevice) != cudaSuccess ||
+          cudaMemcpy(db, p + po.w_off + wbytes, bbytes, cudaMemcpyHostToDevice) != cudaSuccess)
+        return fail("uploading denoiser weights failed");
+      o.w = dw;
+      o.b = db;
+      params += (size_t)cout * K + cout;
+    }
+    L.push_back(o);
   }
-  if (off != bytes) return fail("denoiser blob has trailing bytes");
-  net->layers = L;
+  net->ops = L;
   net->allocs = allocs;
   net->param_count = params;
   net->rays_per_light = rays;
+  net->conf_threshold = thr;
+  // version 3 networks output an error estimate per slot (channels 2, 3)
+  net->has_conf = memcmp(p + 4, "\x03\x00\x00\x00", 4) == 0;
   return std::string();
 }
 
 void denoise_free(DenoiseNet* net) {
   for (void* a : net->allocs) cudaFree(a);
   net->allocs.clear();
-  net->layers.clear();
+  net->ops.clear();
   net->param_count = 0;
   net->rays_per_light = 1;
+  net->has_conf = false;
+  net->conf_threshold = 1.0f;
 }
 
-int denoise_run(const DenoiseNet& net, const __half* feat, int planes, int H, int W, __half* act0, __half* act1,
-                float* vis, int* err, cudaStream_t s, int num_sms, cudaError_t* launch_err) {
-  const __half* cur = feat;
+size_t denoise_scratch_halves(const DenoiseNet& net, int planes, int H, int W) {
+  size_t n = 0;
+  for (size_t i = 0; i + 1 < net.ops.size(); i++) {
+    const DnOp& o = net.ops[i];
+    n += (size_t)planes * level_dim(H, o.level) * level_dim(W, o.level) * o.cout;
+    n = (n + 127) & ~(size_t)127;  // 256-byte aligned buffers
+  }
+  return std::max<size_t>(n, 128);
+}
+
+int denoise_run(const DenoiseNet& net, const __half* feat, int planes, int H, int W, __half* arena, float* vis,
+                float* conf, int* err, cudaStream_t s, int num_sms, cudaError_t* launch_err) {
+  std::vector<const __half*> buf(net.ops.size() + 1, nullptr);
+  buf[0] = feat;
+  size_t off = 0;
   int launches = 0;
   *launch_err = cudaSuccess;
-  for (size_t i = 0; i < net.layers.size(); i++) {
-    const DnLayer& l = net.layers[i];
-    __half* out = (i % 2 == 0) ? act0 : act1;
-    cudaError_t e = cudaErrorInvalidValue;
-    if (l.act == 2) {
-      if (l.cin == 16) e = launch_conv<16, 16, 2>(cur, planes, H, W, l.dil, l.w, l.b, nullptr, vis, err, s, num_sms);
-      else e = launch_conv<32, 16, 2>(cur, planes, H, W, l.dil, l.w, l.b, nullptr, vis, err, s, num_sms);
-    } else if (l.cin == 16 && l.cout == 16) {
-      e = launch_conv<16, 16, 0>(cur, planes, H, W, l.dil, l.w, l.b, out, nullptr, err, s, num_sms);
-    } else if (l.cin == 16 && l.cout == 32) {
-      e = launch_conv<16, 32, 0>(cur, planes, H, W, l.dil, l.w, l.b, out, nullptr, err, s, num_sms);
-    } else if (l.cin == 32 && l.cout == 16) {
-      e = launch_conv<32, 16, 0>(cur, planes, H, W, l.dil, l.w, l.b, out, nullptr, err, s, num_sms);
+  for (size_t i = 0; i < net.ops.size(); i++) {
+    const DnOp& o = net.ops[i];
+    const int h = level_dim(H, o.level), w = level_dim(W, o.level);
+    __half* out = nullptr;
+    if (i + 1 < net.ops.size()) {
+      out = arena + off;
+      off += (size_t)planes * h * w * o.cout;
+      off = (off + 127) & ~(size_t)127;
+    }
+    cudaError_t e;
+    if (o.kind == DN_CONV) {
+      if (o.act == 2)
+        e = conv_launch(o.cin, o.cout, 2, buf[o.src], planes, h, w, o.dil, o.w, o.b, nullptr, vis,
+                        net.has_conf ? conf : nullptr, nullptr, err, s, num_sms);
+      else
+        e = conv_launch(o.cin, o.cout, 0, buf[o.src], planes, h, w, o.dil, o.w, o.b, out, nullptr, nullptr, nullptr,
+                        err, s, num_sms);
+    } else if (o.kind == DN_POOL) {
+      e = pool2_launch(buf[o.src], out, planes, level_dim(H, o.level - 1), level_dim(W, o.level - 1), o.cin, s,
+                       num_sms);
     } else {
-      e = launch_conv<32, 32, 0>(cur, planes, H, W, l.dil, l.w, l.b, out, nullptr, err, s, num_sms);
+      e = upadd_launch(buf[o.src], buf[o.src2], out, planes, h, w, o.cin, s, num_sms);
     }
     launches++;
     if (e != cudaSuccess) {
       *launch_err = e;
       return launches;
     }
-    cur = out;
+    buf[i + 1] = out;
   }
   return launches;
 }

@@ -32,18 +32,27 @@ enum {
 // error word; its other bits are the ERR_* of dscene.cuh).
 constexpr int DN_ERR_WAIT = 16;
 
-struct DnLayer {
-  int cin = 0, cout = 0, dil = 1, act = 0;  // act: 0 ReLU, 2 sigmoid (last layer)
-  void* w = nullptr;                        // weights in the tensor-core operand layout
+// One operation of the network.  Buffer 0 is the feature image; op i
+// writes buffer i + 1.  Resolution level l has ceil(H / 2^l) x ceil(W / 2^l)
+// pixels per plane; every buffer is FP16 NHWC.
+enum { DN_CONV = 0, DN_POOL = 1, DN_UPADD = 2 };
+struct DnOp {
+  int kind = DN_CONV;
+  int cin = 0, cout = 0, dil = 1, act = 0;  // conv act: 0 ReLU, 2 sigmoid outputs (last op only)
+  int src = 0, src2 = -1;                   // input buffer(s); upadd: src is the coarse one, src2 the skip
+  int level = 0;                            // level of the output
+  void* w = nullptr;                        // conv: weights in the tensor-core operand layout
   float* b = nullptr;
 };
 
 struct DenoiseNet {
-  std::vector<DnLayer> layers;
+  std::vector<DnOp> ops;
   std::vector<void*> allocs;
   size_t param_count = 0;
   int rays_per_light = 1;  // disk-light rays per primary hit the network was trained on
-  bool loaded() const { return !layers.empty(); }
+  bool has_conf = false;   // the output holds an error estimate per slot (channels 2, 3)
+  float conf_threshold = 1.0f;  // default fallback threshold stored with the weights
+  bool loaded() const { return !ops.empty(); }
 };
 
 // Parses and uploads a weight blob (format in include/rtrace_gpu.h next to
@@ -51,11 +60,28 @@ struct DenoiseNet {
 std::string denoise_load(const void* blob, size_t bytes, DenoiseNet* net);
 void denoise_free(DenoiseNet* net);
 
+// Halves of activation scratch denoise_run needs for planes x H x W.
+size_t denoise_scratch_halves(const DenoiseNet& net, int planes, int H, int W);
+
 // Runs the network on feat ([planes][H][W][16] FP16) and writes the
-// visibility estimate of each slot to vis ([planes][2][H][W] float).
-// act0/act1 hold planes*H*W*32 halves each.  err receives a nonzero code if
-// a wait on the tensor cores ran out.  Returns the number of launches.
-int denoise_run(const DenoiseNet& net, const __half* feat, int planes, int H, int W, __half* act0, __half* act1,
-                float* vis, int* err, cudaStream_t s, int num_sms, cudaError_t* launch_err);
+// visibility estimate of each slot to vis ([planes][2][H][W] float) and,
+// when the network has them and conf is not null, its error estimates to
+// conf (same layout).  arena holds denoise_scratch_halves() halves.  err
+// receives a nonzero code if a wait on the tensor cores ran out.  Returns
+// the number of launches.
+int denoise_run(const DenoiseNet& net, const __half* feat, int planes, int H, int W, __half* arena, float* vis,
+                float* conf, int* err, cudaStream_t s, int num_sms, cudaError_t* launch_err);
+
+// The building blocks, also used by training (rtrace_b200/csrc/dn_train.cu).
+// conv_launch: one 3x3 convolution (see k_conv3x3_tc for the epilogue
+// modes) of an FP16 NHWC tensor [planes][H][W][cin]; w in the tensor-core
+// operand layout.  cudaErrorInvalidValue for an unsupported shape or mode.
+cudaError_t conv_launch(int cin, int cout, int mode, const __half* in, int planes, int H, int W, int dil,
+                        const void* w, const float* b, __half* out, float* vis, float* conf, const __half* aux,
+                        int* err, cudaStream_t s, int num_sms);
+bool conv_shape_supported(int cin, int cout);
+cudaError_t pool2_launch(const __half* in, __half* out, int P, int H, int W, int C, cudaStream_t s, int num_sms);
+cudaError_t upadd_launch(const __half* low, const __half* skip, __half* out, int P, int H, int W, int C,
+                         cudaStream_t s, int num_sms);
 
 }  // namespace rtb

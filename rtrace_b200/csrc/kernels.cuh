@@ -61,6 +61,17 @@ struct DFrame {
   float* vhat;          // denoised visibility, read by k_resolve at level 0
   float* vis_aov;       // optional: per slot visible/dsamp of level-0 hits
   int n_slots;          // disk lights that are denoiser slots (<= DN_MAX_SLOTS)
+  // Confidence-gated fallback (learned shadows): a level-0 hit whose
+  // estimated visibility error (vconf, layout of vhat) exceeds conf_thr on
+  // any slot is shaded by the plain path.  k_fb_select lists such hits in
+  // fb_list (count *fbn) and flags them in fb_flag; launches with fb_mode
+  // set walk fb_list instead of the level's hit list.
+  float* vconf;
+  float conf_thr;
+  int fb_mode;
+  int* fb_list;
+  int* fbn;
+  unsigned char* fb_flag;
   uint64_t seed;
   long long n_primary;
   long long n_corner;  // quincunx corner rays, (W+1)(H+1)
@@ -143,6 +154,7 @@ __global__ void k_frame_init(DFrame F, int levels) {
   for (int i = threadIdx.x; i < levels + 1; i += blockDim.x) F.nhits[i] = 0;
   if (threadIdx.x < 16) F.stats[threadIdx.x] = 0;
   if (threadIdx.x == 0) *F.err = 0;
+  if (threadIdx.x == 0 && F.fbn) *F.fbn = 0;
 }
 
 __global__ void k_raygen(DFrame F) {
@@ -334,14 +346,14 @@ __device__ __forceinline__ HitRec load_hit(const DFrame& F, int level, int h, Ra
 // Light sampling for hits [c0, c1) of the level's hit list.
 __global__ void __launch_bounds__(128) k_emit(DFrame F, int level, long long c0) {
   const DScene& S = F.S;
-  long long nh = F.nhits[level];
+  long long nh = F.fb_mode ? *F.fbn : F.nhits[level];
   long long c1 = c0 + F.chunk_hits < nh ? c0 + F.chunk_hits : nh;
   V3 campos = ld3(F.C.campos);
   for (long long h = c0 + blockIdx.x * (long long)blockDim.x + threadIdx.x; h < c1;
        h += (long long)gridDim.x * blockDim.x) {
     RayC rc;
     uint64_t seed;
-    HitRec hr = load_hit(F, level, (int)h, &rc, &seed);
+    HitRec hr = load_hit(F, level, F.fb_mode ? F.fb_list[h] : (int)h, &rc, &seed);
     V3 so = hr.p + 0.001 * hr.n;
     long long hl = h - c0;
     F.sh.ox[hl] = so.x;
@@ -430,7 +442,7 @@ __global__ void __launch_bounds__(128) k_emit(DFrame F, int level, long long c0)
 // 8 (64 registers, more spills) or 6.
 template <bool COUNT>
 __global__ void __launch_bounds__(128, 7) k_shadow(DFrame F, int level, long long c0) {
-  long long nh = F.nhits[level];
+  long long nh = F.fb_mode ? *F.fbn : F.nhits[level];
   long long c1 = c0 + F.chunk_hits < nh ? c0 + F.chunk_hits : nh;
   const int K = F.K;
   long long nhc = c1 > c0 ? c1 - c0 : 0;
@@ -476,7 +488,7 @@ __global__ void __launch_bounds__(128, 7) k_shadow(DFrame F, int level, long lon
 // 7.0 ms against 7.23 ms at 128 registers; 6, 10 and 12 blocks were slower).
 __global__ void __launch_bounds__(128, 8) k_resolve(DFrame F, int level, long long c0) {
   const DScene& S = F.S;
-  long long nh = F.nhits[level];
+  long long nh = F.fb_mode ? *F.fbn : F.nhits[level];
   long long c1 = c0 + F.chunk_hits < nh ? c0 + F.chunk_hits : nh;
   RayBuf qn = F.q[(level + 1) & 1];
   LevelBuf L = F.levels[level];
@@ -486,6 +498,10 @@ __global__ void __launch_bounds__(128, 8) k_resolve(DFrame F, int level, long lo
   for (long long base = c0 + blockIdx.x * (long long)blockDim.x; base < c1; base += stride) {
     long long h = base + threadIdx.x;
     bool active = h < c1;
+    // the hit in the level's list (fallback launches walk fb_list); a
+    // learned launch leaves the hits the fallback shades
+    const int hi = active ? (F.fb_mode ? F.fb_list[h] : (int)h) : 0;
+    if (active && F.learned && level == 0 && F.fb_flag && F.fb_flag[hi]) active = false;
     bool emit = false;
     V3 ro = mk(0, 0, 0), rd = mk(0, 0, 0);
     uint64_t seed = 0;
@@ -494,8 +510,8 @@ __global__ void __launch_bounds__(128, 8) k_resolve(DFrame F, int level, long lo
     double refl = 0.0;
     if (active) {
       RayC rc;
-      HitRec hr = load_hit(F, level, (int)h, &rc, &seed);
-      i = F.hit_ray[h];
+      HitRec hr = load_hit(F, level, hi, &rc, &seed);
+      i = F.hit_ray[hi];
       const DMat& mat = S.mat[hr.mat];
       SMat m = effective_material(mat, hr);
       color = m.ka * S.amb_int * cmul(ld3(S.amb_color), m.c);
@@ -504,7 +520,7 @@ __global__ void __launch_bounds__(128, 8) k_resolve(DFrame F, int level, long lo
       long long s = h - c0;  // advances by CH per shadow ray
       const bool learned = level == 0 && F.learned;
       long long vix = 0;
-      if (learned) {
+      if (learned || (level == 0 && F.fb_mode)) {
         long long pix = i / F.S_per_px;
         vix = ((long long)(i % F.S_per_px) * DN_MAX_SLOTS * F.H) * F.W + pix;  // slot 0 of this sample
       }
@@ -538,6 +554,11 @@ __global__ void __launch_bounds__(128, 8) k_resolve(DFrame F, int level, long lo
           }
           const double n = (double)F.dsamp;  // 16.0 in the reference
           contrib = (total / n) * ((double)visible / n);
+          // fallback of a learned render: the plain visibility replaces the
+          // estimate in the visibility output
+          if (F.fb_mode && level == 0 && slot < F.n_slots && F.vhat)
+            F.vhat[vix + (long long)slot * F.H * F.W] = (float)visible / (float)F.dsamp;
+          slot++;
         }
         color = color + contrib;
       }
@@ -583,6 +604,27 @@ __global__ void __launch_bounds__(128, 8) k_resolve(DFrame F, int level, long lo
         qn.seed[slot] = seed;
       }
     }
+  }
+}
+
+// Confidence gate of learned shadows: every level-0 hit with an estimated
+// visibility error above conf_thr on one of its slots goes to fb_list (and
+// is flagged in fb_flag), to be shaded by the plain path.
+__global__ void __launch_bounds__(128) k_fb_select(DFrame F) {
+  const long long nh = F.nhits[0];
+  const long long plane_px = (long long)F.H * F.W;
+  for (long long base = blockIdx.x * (long long)blockDim.x; base < nh; base += (long long)gridDim.x * blockDim.x) {
+    const long long h = base + threadIdx.x;
+    bool want = false;
+    if (h < nh) {
+      const int i = F.hit_ray[h];
+      const long long pix = i / F.S_per_px, plane = i % F.S_per_px;
+      for (int j = 0; j < F.n_slots; j++)
+        want |= F.vconf[(plane * DN_MAX_SLOTS + j) * plane_px + pix] > F.conf_thr;
+      F.fb_flag[h] = want ? 1 : 0;
+    }
+    const int at = warp_alloc(F.fbn, want);  // every lane of the warp takes part
+    if (want) F.fb_list[at] = (int)h;
   }
 }
 

@@ -121,8 +121,13 @@ struct rt_ctx {
   DenoiseNet net;
   std::vector<void*> dn_scratch;
   long long dn_cap = 0;  // primary samples the buffers hold
-  __half *d_feat = nullptr, *d_act0 = nullptr, *d_act1 = nullptr;
-  float* d_vhat = nullptr;
+  __half* d_feat = nullptr;
+  float *d_vhat = nullptr, *d_vconf = nullptr;  // visibility estimates and their error estimates
+  int *d_fb_list = nullptr, *d_fbn = nullptr;   // confidence-gated fallback: hits and their count
+  unsigned char* d_fb_flag = nullptr;
+  std::vector<void*> dn_arena_alloc;  // the network's activations (grown on demand)
+  __half* d_dn_arena = nullptr;
+  size_t dn_arena_cap = 0;  // halves
   // batched rendering: lanes are child contexts (own stream and scratch)
   std::vector<rt_ctx*> lanes;
   uint32_t tuned_lanes = 0;
@@ -258,8 +263,8 @@ cudaError_t outline_smem_attr(int bytes) {
   return e;
 }
 
-// Feature image, two activation buffers and the visibility estimate for n
-// primary samples (32 + 2 * 64 + 8 bytes each).
+// Feature image, visibility and error estimates and the fallback lists for
+// n primary samples (32 + 8 + 8 + 4 + 1 bytes each).
 rt_status ensure_dn_scratch(rt_ctx* ctx, long long n) {
   if (n <= ctx->dn_cap) return RT_OK;
   CK(cudaStreamSynchronize(ctx->stream));
@@ -268,10 +273,24 @@ rt_status ensure_dn_scratch(rt_ctx* ctx, long long n) {
   ctx->dn_cap = 0;
   auto& o = ctx->dn_scratch;
   CK(dalloc(o, &ctx->d_feat, n * FEAT_CHANNELS));
-  CK(dalloc(o, &ctx->d_act0, n * 32));
-  CK(dalloc(o, &ctx->d_act1, n * 32));
   CK(dalloc(o, &ctx->d_vhat, n * DN_MAX_SLOTS));
+  CK(dalloc(o, &ctx->d_vconf, n * DN_MAX_SLOTS));
+  CK(dalloc(o, &ctx->d_fb_list, n));
+  CK(dalloc(o, &ctx->d_fb_flag, n));
+  CK(dalloc(o, &ctx->d_fbn, 1));
   ctx->dn_cap = n;
+  return RT_OK;
+}
+
+// The network's activation buffers for one run (denoise_scratch_halves).
+rt_status ensure_dn_arena(rt_ctx* ctx, size_t halves) {
+  if (halves <= ctx->dn_arena_cap) return RT_OK;
+  CK(cudaStreamSynchronize(ctx->stream));
+  drop_graphs(ctx);
+  free_all(ctx->dn_arena_alloc);
+  ctx->dn_arena_cap = 0;
+  CK(dalloc(ctx->dn_arena_alloc, &ctx->d_dn_arena, halves));
+  ctx->dn_arena_cap = halves;
   return RT_OK;
 }
 
@@ -1373,18 +1392,34 @@ rt_status render_impl(rt_ctx* ctx, const rt_scene* sc, const rt_render_params* P
     if (!ctx->net.loaded()) return fail(ctx, RT_ERR_INVALID_ARGUMENT, "learned shadows need rt_denoiser_load first");
   }
   if (P->learned_rays > 16) return fail(ctx, RT_ERR_INVALID_ARGUMENT, "learned_rays above 16 is not supported");
+  if (P->fallback_samples > 4096)
+    return fail(ctx, RT_ERR_INVALID_ARGUMENT, "fallback_samples above 4096 is not supported");
+  if (!(P->confidence_threshold == P->confidence_threshold))
+    return fail(ctx, RT_ERR_INVALID_ARGUMENT, "confidence_threshold is NaN");
   const int lrays = learned ? (P->learned_rays ? (int)P->learned_rays : ctx->net.rays_per_light) : 0;
   const int K_full = sc->n_point_lights + sc->n_disk_lights * dsamp;
   const int K_0 = learned ? sc->n_point_lights + sc->n_disk_lights * lrays : K_full;
+  // Confidence-gated fallback: level-0 hits whose estimated visibility error
+  // exceeds the threshold are shaded by the plain path with fb_dsamp rays
+  // per disk light.  Threshold 0: the one stored with the weights; < 0: off.
+  const bool fallback = learned && ctx->net.has_conf && P->confidence_threshold >= 0.0f;
+  const float conf_thr = P->confidence_threshold > 0.0f ? P->confidence_threshold : ctx->net.conf_threshold;
+  const int fb_dsamp = P->fallback_samples ? (int)P->fallback_samples : dsamp;
+  const int K_fb = sc->n_point_lights + sc->n_disk_lights * fb_dsamp;
   auto chunk_for = [&](int K) { return K > 0 ? std::max(1LL, std::min(nprim, kShadowCap / K)) : nprim; };
-  const long long chunk_0 = chunk_for(K_0), chunk_n = chunk_for(K_full);
+  const long long chunk_0 = chunk_for(K_0), chunk_n = chunk_for(K_full), chunk_fb = fallback ? chunk_for(K_fb) : 1;
   if (learned && chunk_0 < nprim)
     return fail(ctx, RT_ERR_INVALID_ARGUMENT, "too many primary samples for learned shadows in one pass");
   long long n_shadow = std::max(1LL, std::max(chunk_0 * std::max(K_0, 1), chunk_n * std::max(K_full, 1)));
-  rt_status st = ensure_scratch(ctx, nprim, levels, npix, n_shadow, std::max(chunk_0, chunk_n));
+  if (fallback) n_shadow = std::max(n_shadow, chunk_fb * std::max(K_fb, 1));
+  rt_status st = ensure_scratch(ctx, nprim, levels, npix, n_shadow, std::max(std::max(chunk_0, chunk_n), chunk_fb));
   if (st != RT_OK) return st;
   if (learned || want_aov) {
     st = ensure_dn_scratch(ctx, nprim);
+    if (st != RT_OK) return st;
+  }
+  if (learned) {
+    st = ensure_dn_arena(ctx, denoise_scratch_halves(ctx->net, spp, H, W));
     if (st != RT_OK) return st;
   }
 
@@ -1428,6 +1463,12 @@ rt_status render_impl(rt_ctx* ctx, const rt_scene* sc, const rt_render_params* P
   F.vhat = (aov && aov->vis) ? aov->vis : ctx->d_vhat;
   F.vis_aov = (aov && aov->vis && !learned) ? aov->vis : nullptr;
   F.n_slots = std::min(sc->n_disk_lights, (int)DN_MAX_SLOTS);
+  F.vconf = learned ? ctx->d_vconf : nullptr;
+  F.conf_thr = conf_thr;
+  F.fb_mode = 0;
+  F.fb_list = fallback ? ctx->d_fb_list : nullptr;
+  F.fbn = fallback ? ctx->d_fbn : nullptr;
+  F.fb_flag = fallback ? ctx->d_fb_flag : nullptr;
   F.stats = ctx->d_stats;
   F.err = ctx->d_err;
   F.linear = nullptr;
@@ -1511,9 +1552,34 @@ rt_status render_impl(rt_ctx* ctx, const rt_scene* sc, const rt_render_params* P
         }
         if (l == 0 && learned) {
           cudaError_t le = cudaSuccess;
-          int nl = denoise_run(ctx->net, F.feat, spp, H, W, ctx->d_act0, ctx->d_act1, F.vhat, F.err, s, nsm, &le);
+          int nl = denoise_run(ctx->net, F.feat, spp, H, W, ctx->d_dn_arena, F.vhat, F.vconf, F.err, s, nsm, &le);
           for (int k = 0; k < nl; k++) Lc.after(RT_STAGE_DENOISE);
           if (le != cudaSuccess) return cuda_fail(ctx, le, "denoiser launch");
+          if (fallback) {
+            // the hits the network is not confident about: plain shading
+            // with fb_dsamp rays per disk light, over the compacted list
+            k_fb_select<<<blocks(nprim, 128, 16), 128, 0, s>>>(F);
+            Lc.after(RT_STAGE_DENOISE);
+            DFrame Fb = F;
+            Fb.fb_mode = 1;
+            Fb.learned = 0;
+            Fb.dsamp = fb_dsamp;
+            Fb.K = K_fb;
+            Fb.chunk_hits = chunk_fb;
+            const long long nfb_chunks = (nprim + chunk_fb - 1) / chunk_fb;  // the list holds at most nprim hits
+            for (long long c = 0; c < nfb_chunks; c++) {
+              const long long c0 = c * chunk_fb;
+              k_emit<<<blocks(chunk_fb, 128, 64), 128, 0, s>>>(Fb, 0, c0);
+              Lc.after(RT_STAGE_EMIT);
+              if (K_fb > 0) {
+                if (count) k_shadow<true><<<blocks(chunk_fb * K_fb, 128, 128), 128, 0, s>>>(Fb, 0, c0);
+                else k_shadow<false><<<blocks(chunk_fb * K_fb, 128, 128), 128, 0, s>>>(Fb, 0, c0);
+                Lc.after(RT_STAGE_SHADOW);
+              }
+              k_resolve<<<blocks(chunk_fb, 128, 16), 128, 0, s>>>(Fb, 0, c0);
+              Lc.after(RT_STAGE_RESOLVE);
+            }
+          }
           k_resolve<<<blocks(chunk, 128, 16), 128, 0, s>>>(F, l, 0);
           Lc.after(RT_STAGE_RESOLVE);
         }
@@ -1545,14 +1611,14 @@ rt_status render_impl(rt_ctx* ctx, const rt_scene* sc, const rt_render_params* P
     };
     put(&F, sizeof F);
     const long long kl[] = {nprim, npix, chunk_0, chunk_n, levels, max_depth, K_0, K_full, lrays, dsamp,
-                            learned, count, nsm, spp, H, W, (long long)o_shm};
+                            learned, count, nsm, spp, H, W, (long long)o_shm, fallback, fb_dsamp, K_fb, chunk_fb};
     put(kl, sizeof kl);
     if (learned) {
-      const void* ap[] = {ctx->d_act0, ctx->d_act1};
+      const void* ap[] = {ctx->d_dn_arena};
       put(ap, sizeof ap);
-      for (const DnLayer& dl : ctx->net.layers) {
-        const void* lp[] = {dl.w, dl.b};
-        const int li[] = {dl.cin, dl.cout, dl.dil, dl.act};
+      for (const DnOp& o : ctx->net.ops) {
+        const void* lp[] = {o.w, o.b};
+        const int li[] = {o.kind, o.cin, o.cout, o.dil, o.act, o.src, o.src2, o.level};
         put(lp, sizeof lp);
         put(li, sizeof li);
       }
@@ -1610,6 +1676,8 @@ rt_status render_impl(rt_ctx* ctx, const rt_scene* sc, const rt_render_params* P
   CK(cudaMemcpyAsync(nh.data(), ctx->d_nhits, (levels + 1) * sizeof(int), cudaMemcpyDeviceToHost, s));
   CK(cudaMemcpyAsync(hstats, ctx->d_stats, sizeof hstats, cudaMemcpyDeviceToHost, s));
   CK(cudaMemcpyAsync(&herr, ctx->d_err, sizeof(int), cudaMemcpyDeviceToHost, s));
+  int hfb = 0;
+  if (fallback) CK(cudaMemcpyAsync(&hfb, ctx->d_fbn, sizeof(int), cudaMemcpyDeviceToHost, s));
   cudaError_t se = cudaStreamSynchronize(s);
   free_all(tmp);
   if (se != cudaSuccess) return cuda_fail(ctx, se, "render");
@@ -1630,7 +1698,9 @@ rt_status render_impl(rt_ctx* ctx, const rt_scene* sc, const rt_render_params* P
       for (int l = 0; l < levels; l++) hits += (uint64_t)nh[l];
       stats->reflection_rays = refl;
       stats->hits = hits;
-      stats->shadow_rays = (uint64_t)nh[0] * (uint64_t)K_0 + (hits - (uint64_t)nh[0]) * (uint64_t)K_full;
+      stats->shadow_rays = (uint64_t)nh[0] * (uint64_t)K_0 + (hits - (uint64_t)nh[0]) * (uint64_t)K_full +
+                           (uint64_t)hfb * (uint64_t)K_fb;
+      stats->fallback_hits = (uint64_t)hfb;
       stats->trace_nodes = hstats[2];
       stats->trace_triangles = hstats[3];
       stats->trace_spheres = hstats[4];
@@ -1707,6 +1777,7 @@ void rt_ctx_destroy(rt_ctx* ctx) {
   drop_graphs(ctx);
   free_all(ctx->scratch);
   free_all(ctx->dn_scratch);
+  free_all(ctx->dn_arena_alloc);
   if (ctx->kd_arena) kd_arena_free(ctx->kd_arena);
   if (!ctx->borrowed_net) denoise_free(&ctx->net);
   for (cudaEvent_t e : ctx->stage_ev) cudaEventDestroy(e);
@@ -1914,6 +1985,18 @@ rt_status rt_debug_fp64_rate(rt_ctx* ctx, double* gops) {
   return RT_OK;
 }
 
+}  // extern "C"
+
+namespace rtb {
+// Context access for the training entry points (dn_train.cu).
+cudaStream_t ctx_stream(rt_ctx* ctx) { return ctx->stream; }
+int ctx_device(rt_ctx* ctx) { return ctx->device; }
+int ctx_num_sms(rt_ctx* ctx) { return ctx->num_sms; }
+rt_status ctx_fail(rt_ctx* ctx, rt_status st, const std::string& msg) { return fail(ctx, st, msg); }
+}  // namespace rtb
+
+extern "C" {
+
 rt_status rt_debug_l2_read_bandwidth(rt_ctx* ctx, uint64_t bytes, int32_t reps, double* gbs) {
   if (!ctx || !gbs || reps <= 0) return fail(ctx, RT_ERR_INVALID_ARGUMENT, "null argument or reps <= 0");
   CK(cudaSetDevice(ctx->device));
@@ -2098,9 +2181,11 @@ rt_status rt_render_batch(rt_ctx* ctx, rt_job* jobs, uint32_t n, uint32_t lanes,
   }
   for (uint32_t k = 0; k < lanes; k++) {
     rt_ctx* l = ctx->lanes[k];
-    l->net.layers = ctx->net.layers;
+    l->net.ops = ctx->net.ops;
     l->net.param_count = ctx->net.param_count;
     l->net.rays_per_light = ctx->net.rays_per_light;
+    l->net.has_conf = ctx->net.has_conf;
+    l->net.conf_threshold = ctx->net.conf_threshold;
     l->net.allocs.clear();
   }
   // estimated rays per job -> lanes, longest first
@@ -2214,7 +2299,7 @@ rt_status rt_denoiser_load(rt_ctx* ctx, const void* blob, size_t bytes) {
 }
 
 rt_status rt_denoiser_run(rt_ctx* ctx, const uint16_t* features, uint32_t planes, uint32_t height, uint32_t width,
-                          float* visibility) {
+                          float* visibility, float* confidence, double* device_ms) {
   if (!ctx) return fail(nullptr, RT_ERR_INVALID_ARGUMENT, "null context");
   if (!features || !visibility) return fail(ctx, RT_ERR_INVALID_ARGUMENT, "null argument");
   if (!ctx->net.loaded()) return fail(ctx, RT_ERR_INVALID_ARGUMENT, "no denoiser weights loaded");
@@ -2225,6 +2310,8 @@ rt_status rt_denoiser_run(rt_ctx* ctx, const uint16_t* features, uint32_t planes
   long long n = (long long)planes * height * width;
   rt_status st = ensure_dn_scratch(ctx, n);
   if (st != RT_OK) return st;
+  st = ensure_dn_arena(ctx, denoise_scratch_halves(ctx->net, (int)planes, (int)height, (int)width));
+  if (st != RT_OK) return st;
   // the scratch error word is shared with renders on this context
   if (!ctx->d_err) {
     st = ensure_scratch(ctx, 1, 1, 1, 1, 1);
@@ -2232,12 +2319,19 @@ rt_status rt_denoiser_run(rt_ctx* ctx, const uint16_t* features, uint32_t planes
   }
   CK(cudaMemsetAsync(ctx->d_err, 0, sizeof(int), ctx->stream));
   cudaError_t le = cudaSuccess;
+  CK(cudaEventRecord(ctx->ev0, ctx->stream));
   denoise_run(ctx->net, reinterpret_cast<const __half*>(features), (int)planes, (int)height, (int)width,
-              ctx->d_act0, ctx->d_act1, visibility, ctx->d_err, ctx->stream, ctx->num_sms, &le);
+              ctx->d_dn_arena, visibility, confidence, ctx->d_err, ctx->stream, ctx->num_sms, &le);
   if (le != cudaSuccess) return cuda_fail(ctx, le, "denoiser launch");
+  CK(cudaEventRecord(ctx->ev1, ctx->stream));
   int herr = 0;
   CK(cudaMemcpyAsync(&herr, ctx->d_err, sizeof(int), cudaMemcpyDeviceToHost, ctx->stream));
   CK(cudaStreamSynchronize(ctx->stream));
+  if (device_ms) {
+    float ms = 0.f;
+    CK(cudaEventElapsedTime(&ms, ctx->ev0, ctx->ev1));
+    *device_ms = ms;
+  }
   if (herr & DN_ERR_WAIT) return fail(ctx, RT_ERR_DEVICE_WATCHDOG, "denoiser: a tensor-core wait timed out");
   ctx->err.clear();
   return RT_OK;

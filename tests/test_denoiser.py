@@ -40,7 +40,7 @@ def _run_net(ctx, layers, feat):
     vis = torch.full((planes, 2, H, W), -7.0, dtype=torch.float32, device=feat.device)
     torch.cuda.synchronize()  # torch's fills run on torch's stream, the network on the context's
     L = rt._capi.lib()
-    st = L.rt_denoiser_run(ctx.handle, feat.data_ptr(), planes, H, W, vis.data_ptr())
+    st = L.rt_denoiser_run(ctx.handle, feat.data_ptr(), planes, H, W, vis.data_ptr(), None, None)
     assert st == 0, L.rt_last_error(ctx.handle)
     torch.cuda.synchronize()
     return vis
