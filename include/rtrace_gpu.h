@@ -71,6 +71,12 @@ typedef struct rt_outline_config {
   double threshold;
   double edge_color[3];
   double line_thickness;
+  /* Extension (0 keeps the reference's outline): weight of an edge term
+   * between neighbouring foreground pixels whose nearest samples hit
+   * different World objects, added to the depth and normal terms.  Renders
+   * take the objects from their own hit records; rt_outline_apply has no
+   * object buffer and ignores it. */
+  double object_id_weight;
 } rt_outline_config;
 
 /* Renderer fields (src/renderer.rs:37-47).  thread_count has no device
@@ -394,9 +400,10 @@ rt_status rt_outline_apply(rt_ctx* ctx, uint32_t width, uint32_t height, const d
  * The per-pixel edge-strength scratch lives in one static device array of
  * RT_OUTLINE_NOALLOC_MAX_PIXELS doubles (32 MiB), which every device that
  * loads this library keeps until the process exits; width * height above
- * that limit is rejected with RT_ERR_INVALID_ARGUMENT.  The first call on
- * a device looks up the array's device address (cudaGetSymbolAddress) and
- * remembers it, so make that first call before any stream capture.  All
+ * that limit is rejected with RT_ERR_INVALID_ARGUMENT.  Each call looks up
+ * the array's device address on the context's device (cudaGetSymbolAddress;
+ * the first lookup on a device also sets up the library's device code
+ * there), so make the first call on a device before any stream capture.  All
  * calls share the array: calls whose work overlaps on the GPU (other
  * threads, other contexts on the same device) race on it and must be
  * serialised by the caller.  Nothing in it needs clearing between calls:

@@ -75,6 +75,8 @@ class OutlineConfig:
     edge_color: tuple = (0.0, 0.0, 0.0)
     use_8_neighbors: bool = False
     line_thickness: float = 1.0
+    # extension: edges between different objects (0 keeps the reference's outline)
+    object_id_weight: float = 0.0
 
 
 @dataclass
@@ -189,7 +191,7 @@ class Scene:
         if not oc.enabled:
             return None
         return OutlineConfig(oc.depth_weight, oc.normal_weight, oc.threshold, tuple(oc.edge_color),
-                             bool(oc.use_8_neighbors), oc.line_thickness)
+                             bool(oc.use_8_neighbors), oc.line_thickness, oc.object_id_weight)
 
     @classmethod
     def upload(cls, host_scene, ctx=None):
@@ -418,6 +420,7 @@ class Renderer:
             for k in range(3):
                 p.outline.edge_color[k] = oc.edge_color[k]
             p.outline.line_thickness = oc.line_thickness
+            p.outline.object_id_weight = oc.object_id_weight
         return p
 
     def render(self, scene, out=None, linear=False, device_ptr=None):

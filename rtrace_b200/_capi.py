@@ -39,6 +39,7 @@ class rt_outline_config(ctypes.Structure):
         ("threshold", ctypes.c_double),
         ("edge_color", ctypes.c_double * 3),
         ("line_thickness", ctypes.c_double),
+        ("object_id_weight", ctypes.c_double),
     ]
 
 

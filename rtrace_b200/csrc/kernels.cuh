@@ -86,19 +86,21 @@ struct DFrame {
   int* nhits;        // device [max_depth]
   ShadowBuf sh;
   long long chunk_hits;  // hits whose shadow rays fit the shadow buffer at once
-  // per primary ray outline data
+  // per primary ray outline data (pobj: World index of the hit object)
   double *pdepth, *pnx, *pny, *pnz;
   unsigned char* phit;
+  int* pobj;
   // per pixel
   double *cr, *cg, *cb;
   double *dep, *nx, *ny, *nz;
+  int* oid;  // per pixel: object of the nearest sample (outline object-ID term), or null
   unsigned char* valid;
   double* mask;
   unsigned char* rgb;
   double* linear;  // optional pixel colours (3 per pixel) before quantisation
   unsigned long long* stats;  // [2..5] trace work, [6..9] shadow work (nodes, tris, spheres, verify)
   int* err;
-  double o_wd, o_wn, o_thr, o_color[3], o_thick;
+  double o_wd, o_wn, o_thr, o_color[3], o_thick, o_wid;
   int o_use8, o_radius;
 };
 
@@ -581,6 +583,7 @@ __global__ void __launch_bounds__(128, 8) k_resolve(DFrame F, int level, long lo
       }
       if (level == 0 && F.outline) {
         F.phit[i] = 1;
+        F.pobj[i] = F.hobj[hi];
         F.pdepth[i] = norm(hr.p - campos);
         F.pnx[i] = hr.n.x;
         F.pny[i] = hr.n.y;
@@ -756,6 +759,7 @@ __global__ void k_pixels(DFrame F) {
       bool have = false;
       double pd = 0.0;
       V3 pn = mk(0.0, 0.0, 0.0);
+      int po = -1;
       for (int s = 0; s < F.S_per_px; s++) {
         long long i = p * F.S_per_px + s;
         t = t + mk(L.r[i], L.g[i], L.b[i]);
@@ -765,12 +769,14 @@ __global__ void k_pixels(DFrame F) {
             have = true;
             pd = d;
             pn = mk(F.pnx[i], F.pny[i], F.pnz[i]);
+            po = F.pobj[i];
           }
         }
       }
       c = t / (double)F.S_per_px;
       if (F.outline) {
         F.valid[p] = have ? 1 : 0;
+        if (F.oid) F.oid[p] = po;
         F.dep[p] = pd;
         F.nx[p] = pn.x;
         F.ny[p] = pn.y;
@@ -795,12 +801,15 @@ __global__ void __launch_bounds__(OT_X* OT_Y) k_outline_mask(DFrame F) {
   __shared__ double sd[OT_Y + 2][OT_X + 2];
   __shared__ double snx[OT_Y + 2][OT_X + 2], sny[OT_Y + 2][OT_X + 2], snz[OT_Y + 2][OT_X + 2];
   __shared__ unsigned char sv[OT_Y + 2][OT_X + 2];
+  __shared__ int so[OT_Y + 2][OT_X + 2];
+  const bool ids = F.oid && F.o_wid != 0.0;
   int x0 = blockIdx.x * OT_X - 1, y0 = blockIdx.y * OT_Y - 1;
   for (int k = threadIdx.y * OT_X + threadIdx.x; k < (OT_X + 2) * (OT_Y + 2); k += OT_X * OT_Y) {
     int lx = k % (OT_X + 2), ly = k / (OT_X + 2);
     int gx = x0 + lx, gy = y0 + ly;
     unsigned char v = 0;
     double d = 0, a = 0, b = 0, c = 0;
+    int o = -1;
     if (gx >= 0 && gy >= 0 && gx < F.W && gy < F.H) {
       long long p = (long long)gy * F.W + gx;
       v = F.valid[p];
@@ -808,7 +817,9 @@ __global__ void __launch_bounds__(OT_X* OT_Y) k_outline_mask(DFrame F) {
       a = F.nx[p];
       b = F.ny[p];
       c = F.nz[p];
+      if (ids) o = F.oid[p];
     }
+    so[ly][lx] = o;
     sv[ly][lx] = v;
     sd[ly][lx] = d;
     snx[ly][lx] = a;
@@ -857,6 +868,8 @@ __global__ void __launch_bounds__(OT_X* OT_Y) k_outline_mask(DFrame F) {
       double ndd = dd / rmax(cd * 0.1, 0.1);
       double dp = rclamp(dot(cn, nnv), -1.0, 1.0);
       e = F.o_wd * ndd + F.o_wn * (1.0 - dp);
+      // extension: different objects on either side of the edge
+      if (ids && so[ly][lx] != so[ly + ndy[k]][lx + ndx[k]]) e = e + F.o_wid;
     } else if (cf != nf) {
       e = F.o_wd * 2.0 + F.o_wn * 2.0;
     } else {
@@ -911,6 +924,39 @@ __global__ void __launch_bounds__(OT_X* OT_Y) k_outline_apply(DFrame F) {
            c.z * (1.0 - w) + F.o_color[2] * w);
   }
   store_rgb(F, p, c);
+}
+
+// k_outline_apply for radii whose mask tile does not fit in shared memory
+// (outline thickness above 65): the same dilation, reading the mask from
+// global memory (its neighbourhood stays in L1/L2).  One thread per pixel.
+__global__ void __launch_bounds__(256) k_outline_apply_wide(DFrame F) {
+  const int R = F.o_radius;
+  const double th = F.o_thick;
+  const long long n = (long long)F.W * F.H;
+  for (long long p = blockIdx.x * (long long)blockDim.x + threadIdx.x; p < n; p += (long long)gridDim.x * blockDim.x) {
+    const int gx = (int)(p % F.W), gy = (int)(p / F.W);
+    double ms = F.mask[p];
+    for (int dy = -R; dy <= R; dy++) {
+      const int ny = gy + dy;
+      if (ny < 0 || ny >= F.H) continue;
+      for (int dx = -R; dx <= R; dx++) {
+        const int nx = gx + dx;
+        if (nx < 0 || nx >= F.W) continue;
+        double dist = sqrt((double)(dx * dx + dy * dy));
+        if (dist <= th) {
+          double fo = 1.0 - (dist / th);
+          ms = rmax(ms, __ldg(F.mask + (long long)ny * F.W + nx) * fo);
+        }
+      }
+    }
+    V3 c = mk(F.cr[p], F.cg[p], F.cb[p]);
+    if (ms > 0.0) {
+      double w = rclamp(rmin(ms, 1.0), 0.0, 1.0);
+      c = mk(c.x * (1.0 - w) + F.o_color[0] * w, c.y * (1.0 - w) + F.o_color[1] * w,
+             c.z * (1.0 - w) + F.o_color[2] * w);
+    }
+    store_rgb(F, p, c);
+  }
 }
 
 // --------------------------------------------------------------------------

@@ -233,9 +233,11 @@ rt_status ensure_scratch(rt_ctx* ctx, long long n_rays, int levels, long long n_
   CK(dalloc(o, &F.sh.ox, HS)); CK(dalloc(o, &F.sh.oy, HS)); CK(dalloc(o, &F.sh.oz, HS));
   CK(dalloc(o, &F.pdepth, R)); CK(dalloc(o, &F.pnx, R)); CK(dalloc(o, &F.pny, R)); CK(dalloc(o, &F.pnz, R));
   CK(dalloc(o, &F.phit, R));
+  CK(dalloc(o, &F.pobj, R));
   CK(dalloc(o, &F.cr, P)); CK(dalloc(o, &F.cg, P)); CK(dalloc(o, &F.cb, P));
   CK(dalloc(o, &F.dep, P)); CK(dalloc(o, &F.nx, P)); CK(dalloc(o, &F.ny, P)); CK(dalloc(o, &F.nz, P));
   CK(dalloc(o, &F.valid, P));
+  CK(dalloc(o, &F.oid, P));
   CK(dalloc(o, &F.mask, P));
   CK(dalloc(o, &F.rgb, 3 * P));
   CK(dalloc(o, &ctx->d_stats, 16));
@@ -247,6 +249,14 @@ rt_status ensure_scratch(rt_ctx* ctx, long long n_rays, int levels, long long n_
   ctx->cap_hits_sh = HS;
   return RT_OK;
 }
+
+// Dilation radii (ceil(thickness - 1)) up to kOutlineTileRadius stage their
+// mask tile in shared memory ((32 + 2R) x (8 + 2R) doubles: 174 KB at 64);
+// larger ones read the mask from global memory.  The reference has no
+// limit; radii are capped where one pixel's (2R + 1)^2 loop would run for
+// seconds.
+constexpr int kOutlineTileRadius = 64;
+constexpr double kOutlineMaxRadius = 2048.0;
 
 // Raises k_outline_apply's dynamic shared-memory limit to at least `bytes`
 // (never lowers it: batch lanes render from several host threads).
@@ -1358,7 +1368,8 @@ rt_status render_impl(rt_ctx* ctx, const rt_scene* sc, const rt_render_params* P
   int o_radius = 0;
   if (outline && P->outline.line_thickness > 1.0) {
     double rr = std::ceil(P->outline.line_thickness - 1.0);
-    if (rr > 64.0) return fail(ctx, RT_ERR_INVALID_ARGUMENT, "outline thickness above 65 is not supported");
+    if (!(rr <= kOutlineMaxRadius))
+      return fail(ctx, RT_ERR_INVALID_ARGUMENT, "outline thickness above 2049 is not supported");
     o_radius = (int)rr;
   }
   const int halo = outline ? 1 + o_radius : 0;
@@ -1477,6 +1488,7 @@ rt_status render_impl(rt_ctx* ctx, const rt_scene* sc, const rt_render_params* P
   F.o_thr = P->outline.threshold;
   for (int k = 0; k < 3; k++) F.o_color[k] = P->outline.edge_color[k];
   F.o_thick = P->outline.line_thickness;
+  F.o_wid = P->outline.object_id_weight;
   F.o_use8 = P->outline.use_8_neighbors ? 1 : 0;
   F.o_radius = o_radius;
   double* d_linear = nullptr;
@@ -1499,7 +1511,8 @@ rt_status render_impl(rt_ctx* ctx, const rt_scene* sc, const rt_render_params* P
     long long cap = (long long)nsm * per_sm;
     return (int)std::max<long long>(1, std::min(b, cap));
   };
-  const size_t o_shm = (size_t)(OT_X + 2 * o_radius) * (OT_Y + 2 * o_radius) * sizeof(double);
+  const bool o_wide = o_radius > kOutlineTileRadius;  // mask tile beyond shared memory: global-memory dilation
+  const size_t o_shm = o_wide ? 0 : (size_t)(OT_X + 2 * o_radius) * (OT_Y + 2 * o_radius) * sizeof(double);
   if (F.outline && o_shm > 48 * 1024) CK(outline_smem_attr((int)o_shm));
   // The frame's device work, from queue reset to outline: launched directly,
   // or captured into a CUDA graph.  Every argument it passes comes from F
@@ -1595,7 +1608,8 @@ rt_status render_impl(rt_ctx* ctx, const rt_scene* sc, const rt_render_params* P
       dim3 ob(OT_X, OT_Y), og((W + OT_X - 1) / OT_X, (H + OT_Y - 1) / OT_Y);
       k_outline_mask<<<og, ob, 0, s>>>(F);
       Lc.after(RT_STAGE_POST);
-      k_outline_apply<<<og, ob, o_shm, s>>>(F);
+      if (o_wide) k_outline_apply_wide<<<blocks(npix, 256, 8), 256, 0, s>>>(F);
+      else k_outline_apply<<<og, ob, o_shm, s>>>(F);
       Lc.after(RT_STAGE_POST);
     }
     CK(cudaGetLastError());
@@ -2053,11 +2067,14 @@ rt_status outline_frame(rt_ctx* ctx, uint32_t width, uint32_t height, const doub
   F->o_thr = cfg->threshold;
   for (int k = 0; k < 3; k++) F->o_color[k] = cfg->edge_color[k];
   F->o_thick = cfg->line_thickness;
+  F->o_wid = 0.0;  // no object buffer here
+  F->oid = nullptr;
   F->o_use8 = cfg->use_8_neighbors ? 1 : 0;
   F->o_radius = 0;
   if (cfg->line_thickness > 1.0) {
     double rr = std::ceil(cfg->line_thickness - 1.0);
-    if (rr > 64.0) return fail(ctx, RT_ERR_INVALID_ARGUMENT, "outline thickness above 65 is not supported");
+    if (!(rr <= kOutlineMaxRadius))
+      return fail(ctx, RT_ERR_INVALID_ARGUMENT, "outline thickness above 2049 is not supported");
     F->o_radius = (int)rr;
   }
   return RT_OK;
@@ -2066,10 +2083,15 @@ rt_status outline_frame(rt_ctx* ctx, uint32_t width, uint32_t height, const doub
 rt_status launch_outline(rt_ctx* ctx, const DFrame& F) {
   dim3 ob(OT_X, OT_Y), og((F.W + OT_X - 1) / OT_X, (F.H + OT_Y - 1) / OT_Y);
   k_outline_mask<<<og, ob, 0, ctx->stream>>>(F);
-  size_t shm = (size_t)(OT_X + 2 * F.o_radius) * (OT_Y + 2 * F.o_radius) * sizeof(double);
-  if (shm > 48 * 1024)
-    CK(outline_smem_attr((int)shm));
-  k_outline_apply<<<og, ob, shm, ctx->stream>>>(F);
+  if (F.o_radius > kOutlineTileRadius) {
+    const long long n = (long long)F.W * F.H;
+    const int nb = (int)std::max<long long>(1, std::min<long long>((n + 255) / 256, (long long)ctx->num_sms * 8));
+    k_outline_apply_wide<<<nb, 256, 0, ctx->stream>>>(F);
+  } else {
+    size_t shm = (size_t)(OT_X + 2 * F.o_radius) * (OT_Y + 2 * F.o_radius) * sizeof(double);
+    if (shm > 48 * 1024) CK(outline_smem_attr((int)shm));
+    k_outline_apply<<<og, ob, shm, ctx->stream>>>(F);
+  }
   CK(cudaGetLastError());
   CK(cudaStreamSynchronize(ctx->stream));
   return RT_OK;
@@ -2098,21 +2120,15 @@ rt_status rt_outline_apply(rt_ctx* ctx, uint32_t width, uint32_t height, const d
 static __device__ __align__(256) double g_outline_mask[RT_OUTLINE_NOALLOC_MAX_PIXELS];
 
 namespace {
-const int kMaxDevices = 64;
-std::mutex g_mask_mu;
-double* g_mask_addr[kMaxDevices] = {};  // device address of g_outline_mask, per device ordinal
-
-// Set-up, once per device, with that device current.
+// The device address of g_outline_mask on the current device (ctx's, made
+// current by the caller).  Looked up on every call rather than cached, so
+// that an address never outlives the context it came from (a device reset
+// or a new primary context gives the array a new address).
 rt_status noalloc_mask(rt_ctx* ctx, double** out) {
-  if (ctx->device < 0 || ctx->device >= kMaxDevices) return fail(ctx, RT_ERR_INVALID_ARGUMENT, "device ordinal too large");
-  std::lock_guard<std::mutex> g(g_mask_mu);
-  if (!g_mask_addr[ctx->device]) {
-    double* p = nullptr;
-    CK(cudaGetSymbolAddress((void**)&p, g_outline_mask));
-    if (!p) return fail(ctx, RT_ERR_CUDA, "cudaGetSymbolAddress returned a null address");
-    g_mask_addr[ctx->device] = p;
-  }
-  *out = g_mask_addr[ctx->device];
+  double* p = nullptr;
+  CK(cudaGetSymbolAddress((void**)&p, g_outline_mask));
+  if (!p) return fail(ctx, RT_ERR_CUDA, "cudaGetSymbolAddress returned a null address");
+  *out = p;
   return RT_OK;
 }
 }  // namespace

@@ -1037,6 +1037,8 @@ bool load_scene_json(const std::string& text, const std::string& base_dir, HostS
       if (const J* v = o->get("color")) ocol = str(*v);
       if (const J* v = o->get("thickness")) oc.line_thickness = f64(*v);
       if (const J* v = o->get("use_8_neighbors")) oc.use_8_neighbors = boolean(*v) ? 1 : 0;
+      // extension, no key of the reference's schema (serde ignores it there)
+      if (const J* v = o->get("object_id_weight")) oc.object_id_weight = f64(*v);
       if (en) {
         std::string e2;
         if (hex_to_color(ocol, oc.edge_color, &e2)) {

@@ -300,6 +300,65 @@ def test_outline_entry_point_matches_oracle(gpu_ctx, cfg):
         assert np.array_equal(img, ref), (w, h, int((img != ref).any(2).sum()))
 
 
+@pytest.mark.parametrize("thickness", [65.0, 80.0, 130.5])
+def test_thick_outlines_match_oracle(gpu_ctx, tmp_path, thickness):
+    """Dilation radii beyond the shared-memory tile (thickness above 65)
+    take the global-memory path; the reference dilates at any thickness
+    (src/outline.rs:227-268).  The outline entry point against the oracle's
+    outline, and a whole render with such an outline against the oracle's
+    render."""
+    from tests.gpu_outline import device_outline, gbuffers
+    cfg = {"thickness": thickness, "threshold": 0.3, "edge_color": (0.9, 0.1, 0.2), "use_8_neighbors": True}
+    color, valid, depth, normal = gbuffers(97, 61, 7)
+    st, img = device_outline(gpu_ctx, rt._capi.lib().rt_outline_apply, color, valid, depth, normal, cfg)
+    assert st == 0
+    ref = oracle_lib.outline(color, valid, depth, normal, 1.0, 1.0, 0.3, (0.9, 0.1, 0.2), True, thickness)
+    assert np.array_equal(img, ref), int((img != ref).any(2).sum())
+    path = workloads.make_noisy_icosphere(str(tmp_path), level=3, seed=5)
+    s = json.load(open(path))
+    s["scene_settings"]["outline"]["thickness"] = thickness
+    p2 = workloads.write_scene(str(tmp_path), "thick.json", s)
+    got, _ = gpu_render(p2, 64, 40, "no-jitter", 1, outline=True)
+    want = oracle_lib.render(p2, width=64, height=40, aa="no-jitter", outline=True)
+    assert np.array_equal(got, want), int((got != want).any(2).sum())
+
+
+def test_object_id_outline_term(gpu_ctx):
+    """Extension: with object_id_weight > 0 the outline also marks edges
+    between different objects.  Two unit cubes touch along x = 0 with
+    coplanar tops; seen from above, depth and normal are continuous across
+    the seam, so the reference's outline (weight 0, the oracle's render)
+    draws nothing there, and the object term draws the seam."""
+    cube = lambda x: {"kind": "cube", "center": [x, 0, 0], "size": [1, 1, 1],
+                      "material": {"color": "#D0D0D0", "ambient": 0.3, "diffuse": 0.7, "specular": 0.0,
+                                   "shininess": 8}}
+    scene = {"camera": {"kind": "ortho", "position": [0.013, 0.007, 10], "target": [0.013, 0.007, 0],
+                        "up": [0, 1, 0], "width": 4, "height": 2},
+             "objects": [cube(-0.5), cube(0.5)],
+             "lights": [{"position": [2, 3, 8], "color": "#FFFFFF", "intensity": 1.0}],
+             "scene_settings": {"ambient_illumination": {"color": "#FFFFFF", "intensity": 0.2},
+                                "background_color": "#000000",
+                                "outline": {"enabled": True, "color": "#FF00FF", "threshold": 0.1}}}
+    js = json.dumps(scene)
+    sc = rt.Scene.from_json_str(js)
+    W, H = 80, 40
+    r = rt.Renderer(W, H)
+    r.anti_aliasing_mode = rt.AntiAliasingMode.NoJitter
+    r.outline_config = sc.get_outline_config()
+    assert r.outline_config.object_id_weight == 0.0
+    base = r.render(sc)
+    assert np.array_equal(base, oracle_lib.render(json_text=js, width=W, height=H, aa="no-jitter", outline=True))
+    magenta = (base == [255, 0, 255]).all(2)
+    r.outline_config.object_id_weight = 1.0
+    ids = r.render(sc)
+    changed = (ids != base).any(2)
+    cols = np.nonzero(changed.any(0))[0]
+    # only the two columns on either side of the seam change, to the edge colour
+    assert changed.sum() > 10 and set(cols.tolist()) <= {W // 2 - 1, W // 2}
+    assert (ids[changed] == [255, 0, 255]).all()
+    assert not magenta[:, W // 2 - 1:W // 2 + 1][changed[:, W // 2 - 1:W // 2 + 1]].any()
+
+
 @pytest.mark.gpu
 def test_host_scene_uploads_render_the_same(gpu_ctx, tmp_path):
     """A host scene's first upload prepares its meshes and keeps them packed
