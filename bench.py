@@ -313,25 +313,25 @@ def batch_run(rt, ctx, directory, steps):
     0-3 noisy-icosphere meshes of 1,280-81,920 triangles, 0-200 spheres, a
     grid plane) x their 4 auto-camera views = 256 jobs at resolutions drawn
     from 128x128 .. 1920x1080, quincunx (the CLI's default), depth 10.
-    Renders the whole batch with the autotuned lane count, with one lane,
-    and autotuned with every job replayed as a CUDA graph; rays counted as
-    the reference casts them."""
-    from rtrace_b200 import _capi, workloads
+    The autotuner picks the lane count, the fused group's size limit and the
+    fused kernels' grid budgets; the batch is then timed as tuned, without
+    the fused group, and on one lane without it (the per-job pipelines run
+    one after another); rays counted as the reference casts them."""
+    from rtrace_b200 import workloads
     wl = workloads.batch_workload(os.path.join(directory, "batch"), n_scenes=64, seed=0)
     jobs = []
     for path, views in wl:
         scene = rt.Scene.from_json_file(path, ctx)
         for _, cam, (w, h) in views:
             jobs.append(rt.Job(scene, rt.Renderer(w, h), cam))
-    best = rt.batch_autotune(jobs, ctx=ctx)
+    tuned = rt.batch_autotune_ex(jobs, ctx=ctx)
     out = {"workload": "batch_64_scenes_x_4_auto_views", "jobs": len(jobs),
-           "pixels": int(sum(j.renderer.width * j.renderer.height for j in jobs))}
-    for name, lanes in (("tuned", 0), ("one_lane", 1), ("tuned_graph", 0)):
-        if name == "tuned_graph":
-            # every job replays its CUDA graph (captured by the untimed batch)
-            for j in jobs:
-                j.renderer.flags = _capi.RT_FLAG_CUDA_GRAPH
-            rt.render_batch(jobs, lanes=lanes, ctx=ctx)
+           "pixels": int(sum(j.renderer.width * j.renderer.height for j in jobs)), "tuning": tuned,
+           "fused_jobs": sum(1 for j in jobs if j.renderer.width * j.renderer.height <= tuned["fuse_pixels"])}
+    variants = (("tuned", 0, tuned["fuse_pixels"]), ("unfused", 0, 0), ("one_lane_unfused", 1, 0))
+    for name, lanes, fuse in variants:
+        rt.batch_tuning(ctx, fuse_pixels=fuse)
+        rt.render_batch(jobs, lanes=lanes, ctx=ctx)  # captures the fused group's graph
         ms, rays = [], 0
         for _ in range(steps):
             _, st = rt.render_batch(jobs, lanes=lanes, ctx=ctx)
@@ -339,11 +339,10 @@ def batch_run(rt, ctx, directory, steps):
             rays = st.rays
         ms.sort()
         med = ms[len(ms) // 2]
-        out[name] = {"lanes": best if lanes == 0 else 1, "ms_per_batch": med, "mrays_per_s": rays / (med * 1e-3) / 1e6,
-                     "rays_per_batch": rays}
-    for j in jobs:
-        j.renderer.flags = 0
-    out["speedup_vs_one_lane"] = out["one_lane"]["ms_per_batch"] / out["tuned"]["ms_per_batch"]
+        out[name] = {"lanes": st.lanes, "fuse_pixels": fuse, "ms_per_batch": med,
+                     "mrays_per_s": rays / (med * 1e-3) / 1e6, "rays_per_batch": rays}
+    rt.batch_tuning(ctx, fuse_pixels=tuned["fuse_pixels"])
+    out["speedup_vs_one_lane_unfused"] = out["one_lane_unfused"]["ms_per_batch"] / out["tuned"]["ms_per_batch"]
     out["timing"] = "host wall time of rt_render_batch (median of %d), scenes resident" % steps
     return out
 

@@ -440,18 +440,47 @@ typedef struct rt_batch_stats {
 } rt_batch_stats;
 
 /* Renders n jobs on `lanes` concurrent streams of the context's device
- * (0: the count rt_batch_autotune chose for this context, else 4).  Jobs
- * are assigned to lanes longest first by their estimated rays (width *
- * height * samples * (1 + shadow rays per hit)) and each lane renders its
- * jobs in that order, so small jobs run beside large ones.  Every job's
+ * (0: the count rt_batch_autotune chose for this context, else 4).  The
+ * fused group (rt_batch_tuning.fuse_pixels) goes to lane 0 first; the other
+ * jobs are assigned to lanes longest first by their estimated rays (width *
+ * height * samples * (1 + shadow rays per hit)) onto the least-loaded lane,
+ * so small jobs run beside large ones.  Every job's
  * image is byte for byte the one rt_render gives for the same scene,
  * camera and params.  Returns RT_OK when every job rendered, else the
  * first failing job's status (each job's own status is in jobs[i].status;
  * rt_last_error names the job). */
 rt_status rt_render_batch(rt_ctx* ctx, rt_job* jobs, uint32_t n, uint32_t lanes, rt_batch_stats* stats);
 
-/* Renders the batch with 1, 2, 4 and 8 lanes, keeps the fastest for later
- * rt_render_batch calls with lanes = 0, and returns it in *best_lanes. */
+/* Launch parameters of rt_render_batch (per context):
+ *   lanes: concurrent streams when rt_render_batch gets lanes = 0;
+ *   fuse_pixels: frames of at most this many pixels (plain path, no
+ *     outline pass, one shadow chunk, no profiling flags) form the fused
+ *     group: each wavefront kernel is launched once for all of them over a
+ *     device table of their launch blocks, the sequence captured as a CUDA
+ *     graph and replayed when the same group comes again (0: no group);
+ *   blocks_per_sm: grid budget of each fused kernel kind (ray generation,
+ *     closest hit, light sampling, shadow rays, shading, reflection fold,
+ *     pixels) in blocks per SM, shared out between the group's frames in
+ *     proportion to their work bounds.
+ * Defaults: 4 lanes, 640 x 480, {16, 64, 64, 128, 16, 16, 16}. */
+typedef struct rt_batch_tuning {
+  uint32_t lanes;
+  uint32_t fuse_pixels;
+  int32_t blocks_per_sm[7];
+  uint32_t trials;  /* out (autotune): batches timed */
+  double best_ms;   /* out (autotune): wall time of the chosen parameters */
+} rt_batch_tuning;
+rt_status rt_batch_get_tuning(rt_ctx* ctx, rt_batch_tuning* out);
+rt_status rt_batch_set_tuning(rt_ctx* ctx, const rt_batch_tuning* tuning);
+
+/* Autotuner: renders the batch (twice per candidate: the first run of a new
+ * fused group captures its graph) and keeps what is fastest in wall time,
+ * one parameter at a time: lanes in {1, 2, 4, 8}; fuse_pixels in {0, 256^2,
+ * 640 x 480, 1280 x 720}; then, with a fused group, the blocks per SM of
+ * the closest-hit, shadow, light-sampling and shading kernels.  The chosen
+ * parameters stay on the context and are returned in *out (may be NULL). */
+rt_status rt_batch_autotune_ex(rt_ctx* ctx, rt_job* jobs, uint32_t n, rt_batch_tuning* out);
+/* rt_batch_autotune_ex returning only the lane count. */
 rt_status rt_batch_autotune(rt_ctx* ctx, rt_job* jobs, uint32_t n, uint32_t* best_lanes);
 
 /* The assignment rt_render_batch makes: job i (estimated cost costs[i])

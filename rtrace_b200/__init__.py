@@ -22,7 +22,7 @@ from . import _capi
 __all__ = [
     "AntiAliasingMode", "OutlineConfig", "Scene", "Renderer", "RtraceError", "SceneError",
     "RenderError", "DeviceError", "Context", "RenderStats", "default_context", "write_png", "HostScene",
-    "fp64_rate", "l2_read_bandwidth", "auto_cameras", "Job", "BatchStats", "render_batch", "batch_autotune", "batch_assign",
+    "fp64_rate", "l2_read_bandwidth", "batch_autotune_ex", "batch_tuning", "auto_cameras", "Job", "BatchStats", "render_batch", "batch_autotune", "batch_assign",
     "camera_config",
 ]
 
@@ -573,16 +573,53 @@ def render_batch(jobs, lanes=0, ctx=None):
 
 
 def batch_autotune(jobs, ctx=None):
-    """rt_batch_autotune: the fastest lane count for this batch (kept by the
-    context for render_batch(lanes=0))."""
+    """rt_batch_autotune: the fastest lane count for this batch (the context
+    keeps every tuned parameter for render_batch(lanes=0))."""
+    return batch_autotune_ex(jobs, ctx)["lanes"]
+
+
+_KINDS = ("raygen", "trace", "emit", "shadow", "resolve", "fold", "pixels")
+
+
+def _tuning_dict(t):
+    return {"lanes": int(t.lanes), "fuse_pixels": int(t.fuse_pixels),
+            "blocks_per_sm": {k: int(t.blocks_per_sm[i]) for i, k in enumerate(_KINDS)},
+            "trials": int(t.trials), "best_ms": float(t.best_ms)}
+
+
+def batch_autotune_ex(jobs, ctx=None):
+    """rt_batch_autotune_ex: searches lanes, the fused group's size limit and
+    its kernels' grid budgets on this batch; returns the chosen parameters."""
     ctx = ctx or jobs[0].scene._ctx
     outs = [np.empty((j.renderer.height, j.renderer.width, 3), np.uint8) for j in jobs]
     arr, keep = _jobs_array(jobs, outs)
-    best = ctypes.c_uint32()
-    st = _capi.lib().rt_batch_autotune(ctx.handle, arr, len(jobs), ctypes.byref(best))
+    t = _capi.rt_batch_tuning()
+    st = _capi.lib().rt_batch_autotune_ex(ctx.handle, arr, len(jobs), ctypes.byref(t))
     if st != _capi.RT_OK:
         _raise(st, ctx.handle)
-    return int(best.value)
+    return _tuning_dict(t)
+
+
+def batch_tuning(ctx=None, **changes):
+    """The context's batch parameters (rt_batch_get_tuning); keyword
+    arguments (lanes, fuse_pixels, blocks_per_sm={kind: n}) change them."""
+    ctx = ctx or default_context()
+    t = _capi.rt_batch_tuning()
+    L = _capi.lib()
+    st = L.rt_batch_get_tuning(ctx.handle, ctypes.byref(t))
+    if st != _capi.RT_OK:
+        _raise(st, ctx.handle)
+    if changes:
+        if "lanes" in changes:
+            t.lanes = int(changes["lanes"])
+        if "fuse_pixels" in changes:
+            t.fuse_pixels = int(changes["fuse_pixels"])
+        for k, v in changes.get("blocks_per_sm", {}).items():
+            t.blocks_per_sm[_KINDS.index(k)] = int(v)
+        st = L.rt_batch_set_tuning(ctx.handle, ctypes.byref(t))
+        if st != _capi.RT_OK:
+            _raise(st, ctx.handle)
+    return _tuning_dict(t)
 
 
 def batch_assign(costs, lanes):

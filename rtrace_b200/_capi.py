@@ -113,6 +113,16 @@ class rt_stats(ctypes.Structure):
     ]
 
 
+class rt_batch_tuning(ctypes.Structure):
+    _fields_ = [
+        ("lanes", ctypes.c_uint32),
+        ("fuse_pixels", ctypes.c_uint32),
+        ("blocks_per_sm", ctypes.c_int32 * 7),
+        ("trials", ctypes.c_uint32),
+        ("best_ms", ctypes.c_double),
+    ]
+
+
 class rt_job(ctypes.Structure):
     _fields_ = [
         ("scene", ctypes.c_void_p),
@@ -205,6 +215,10 @@ def lib():
         "rt_batch_autotune": (ctypes.c_int, [_vp, ctypes.POINTER(rt_job), ctypes.c_uint32,
                                              ctypes.POINTER(ctypes.c_uint32)]),
         "rt_batch_assign": (ctypes.c_int, [_vp, ctypes.c_uint32, ctypes.c_uint32, _vp]),
+        "rt_batch_autotune_ex": (ctypes.c_int, [_vp, ctypes.POINTER(rt_job), ctypes.c_uint32,
+                                                ctypes.POINTER(rt_batch_tuning)]),
+        "rt_batch_get_tuning": (ctypes.c_int, [_vp, ctypes.POINTER(rt_batch_tuning)]),
+        "rt_batch_set_tuning": (ctypes.c_int, [_vp, ctypes.POINTER(rt_batch_tuning)]),
         "rt_denoiser_load": (ctypes.c_int, [_vp, _vp, ctypes.c_size_t]),
         "rt_denoiser_run": (ctypes.c_int, [_vp, _vp, ctypes.c_uint32, ctypes.c_uint32, ctypes.c_uint32, _vp, _vp,
                                            _vp]),

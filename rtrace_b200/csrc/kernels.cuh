@@ -146,23 +146,47 @@ __device__ __forceinline__ void camera_ray(const DCam& c, double u, double v, V3
   }
 }
 
+// Several frames in one launch (batched small jobs): T holds the frames,
+// and job j owns blocks [b0[j], b0[j + 1]) of the grid (b0[nj] = the grid
+// size).  The job of this block, by binary search.
+__device__ __forceinline__ int job_of_block(const int* __restrict__ b0, int nj) {
+  int lo = 0, hi = nj - 1;
+  const int b = (int)blockIdx.x;
+  while (lo < hi) {
+    const int mid = (lo + hi + 1) >> 1;
+    if (b0[mid] <= b) lo = mid;
+    else hi = mid - 1;
+  }
+  return lo;
+}
+// queue levels of a frame: max_depth clamped to [1, RTB_MAX_LEVELS]
+__device__ __forceinline__ int frame_levels(const DFrame& F) {
+  return F.max_depth < 1 ? 1 : (F.max_depth > RTB_MAX_LEVELS ? RTB_MAX_LEVELS : F.max_depth);
+}
+
 // Start of a frame: queue sizes and hit counts to zero except the level-0
 // queue, which holds the primary rays; work counters and the error word
 // cleared.  One block of 128 threads (levels <= RTB_MAX_LEVELS).  A kernel
 // rather than memsets and a host copy, so that the whole frame is device
 // work a CUDA graph can hold.
-__global__ void k_frame_init(DFrame F, int levels) {
+__device__ __forceinline__ void frame_init_body(const DFrame& F, int levels) {
   for (int i = threadIdx.x; i < levels + 2; i += blockDim.x) F.counts[i] = i == 0 ? (int)F.n_primary : 0;
   for (int i = threadIdx.x; i < levels + 1; i += blockDim.x) F.nhits[i] = 0;
   if (threadIdx.x < 16) F.stats[threadIdx.x] = 0;
   if (threadIdx.x == 0) *F.err = 0;
   if (threadIdx.x == 0 && F.fbn) *F.fbn = 0;
 }
+__global__ void k_frame_init(const __grid_constant__ DFrame F, int levels) { frame_init_body(F, levels); }
+// one block per frame
+__global__ void k_frame_init_multi(const DFrame* __restrict__ T) {
+  const DFrame& F = T[blockIdx.x];
+  frame_init_body(F, frame_levels(F));
+}
 
-__global__ void k_raygen(DFrame F) {
+__device__ __forceinline__ void raygen_body(const DFrame& F, int bid, int nblk) {
   const uint64_t GOLD = 0x9E3779B97F4A7C15ULL;
   long long n = F.n_primary;
-  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
+  for (long long i = bid * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)nblk * blockDim.x) {
     double u, v;
     uint64_t seed;
     if (F.aa == RT_AA_QUINCUNX) {
@@ -234,6 +258,15 @@ __global__ void k_raygen(DFrame F) {
     q.seed[i] = seed;
   }
 }
+__global__ void k_raygen(const __grid_constant__ DFrame F) {
+  raygen_body(F, blockIdx.x, gridDim.x);
+}
+__global__ void k_raygen_multi(const DFrame* __restrict__ T, const int* __restrict__ b0, int nj) {
+  const int j = job_of_block(b0, nj);
+  const DFrame& F = T[j];
+  raygen_body(F, blockIdx.x - b0[j], b0[j + 1] - b0[j]);
+}
+
 
 // --------------------------------------------------------------------------
 // Closest hit + hit compaction; misses resolve to their background here.
@@ -241,13 +274,13 @@ __global__ void k_raygen(DFrame F) {
 // 0.75-0.78 ms unbounded (96 registers) on the bench frame.
 // --------------------------------------------------------------------------
 template <bool COUNT>
-__global__ void __launch_bounds__(128, 6) k_trace(DFrame F, int level) {
+__device__ __forceinline__ void trace_body(const DFrame& F, int level, int bid, int nblk) {
   int n = F.counts[level];
   RayBuf q = F.q[level & 1];
   LevelBuf L = F.levels[level];
-  int stride = gridDim.x * blockDim.x;
+  int stride = nblk * blockDim.x;
   Work w{0, 0, 0, 0};
-  for (int base = blockIdx.x * blockDim.x; base < n; base += stride) {
+  for (int base = bid * blockDim.x; base < n; base += stride) {
     int i = base + threadIdx.x;
     bool active = i < n;
     bool hit = false;
@@ -281,6 +314,18 @@ __global__ void __launch_bounds__(128, 6) k_trace(DFrame F, int level) {
   }
   if (COUNT) flush_work(F, w, 0);
 }
+template <bool COUNT>
+__global__ void __launch_bounds__(128, 6) k_trace(const __grid_constant__ DFrame F, int level) {
+  trace_body<COUNT>(F, level, blockIdx.x, gridDim.x);
+}
+template <bool COUNT>
+__global__ void __launch_bounds__(128, 6) k_trace_multi(const DFrame* __restrict__ T, const int* __restrict__ b0, int nj, int level) {
+  const int j = job_of_block(b0, nj);
+  const DFrame& F = T[j];
+  if (level >= frame_levels(F)) return;
+  trace_body<COUNT>(F, level, blockIdx.x - b0[j], b0[j + 1] - b0[j]);
+}
+
 
 // --------------------------------------------------------------------------
 // Shading
@@ -346,13 +391,13 @@ __device__ __forceinline__ HitRec load_hit(const DFrame& F, int level, int h, Ra
 }
 
 // Light sampling for hits [c0, c1) of the level's hit list.
-__global__ void __launch_bounds__(128) k_emit(DFrame F, int level, long long c0) {
+__device__ __forceinline__ void emit_body(const DFrame& F, int level, long long c0, int bid, int nblk) {
   const DScene& S = F.S;
   long long nh = F.fb_mode ? *F.fbn : F.nhits[level];
   long long c1 = c0 + F.chunk_hits < nh ? c0 + F.chunk_hits : nh;
   V3 campos = ld3(F.C.campos);
-  for (long long h = c0 + blockIdx.x * (long long)blockDim.x + threadIdx.x; h < c1;
-       h += (long long)gridDim.x * blockDim.x) {
+  for (long long h = c0 + bid * (long long)blockDim.x + threadIdx.x; h < c1;
+       h += (long long)nblk * blockDim.x) {
     RayC rc;
     uint64_t seed;
     HitRec hr = load_hit(F, level, F.fb_mode ? F.fb_list[h] : (int)h, &rc, &seed);
@@ -438,12 +483,22 @@ __global__ void __launch_bounds__(128) k_emit(DFrame F, int level, long long c0)
     }
   }
 }
+__global__ void __launch_bounds__(128) k_emit(const __grid_constant__ DFrame F, int level, long long c0) {
+  emit_body(F, level, c0, blockIdx.x, gridDim.x);
+}
+__global__ void __launch_bounds__(128) k_emit_multi(const DFrame* __restrict__ T, const int* __restrict__ b0, int nj, int level, long long c0) {
+  const int j = job_of_block(b0, nj);
+  const DFrame& F = T[j];
+  if (level >= frame_levels(F)) return;
+  emit_body(F, level, c0, blockIdx.x - b0[j], b0[j + 1] - b0[j]);
+}
+
 
 // world.hit(&shadow_ray, 0.001, distance).is_some() per shadow ray.  Seven
 // blocks of 128 per SM (72 registers): 1-2% faster on the bench frame than
 // 8 (64 registers, more spills) or 6.
 template <bool COUNT>
-__global__ void __launch_bounds__(128, 7) k_shadow(DFrame F, int level, long long c0) {
+__device__ __forceinline__ void shadow_body(const DFrame& F, int level, long long c0, int bid, int nblk) {
   long long nh = F.fb_mode ? *F.fbn : F.nhits[level];
   long long c1 = c0 + F.chunk_hits < nh ? c0 + F.chunk_hits : nh;
   const int K = F.K;
@@ -456,8 +511,8 @@ __global__ void __launch_bounds__(128, 7) k_shadow(DFrame F, int level, long lon
   // collective).  Hit-major order: the K rays of one hit point sit in
   // adjacent lanes, so a warp holds a bundle of rays from one or two points
   // towards one light, which the packet traversal shares out.
-  const long long stride = (long long)gridDim.x * blockDim.x;
-  for (long long base = blockIdx.x * (long long)blockDim.x + (threadIdx.x & ~31); base < ns; base += stride) {
+  const long long stride = (long long)nblk * blockDim.x;
+  for (long long base = bid * (long long)blockDim.x + (threadIdx.x & ~31); base < ns; base += stride) {
     const long long t = base + (threadIdx.x & 31);
     const bool have = t < ns;
     long long hl = 0, s = 0;
@@ -482,13 +537,25 @@ __global__ void __launch_bounds__(128, 7) k_shadow(DFrame F, int level, long lon
   }
   if (COUNT) flush_work(F, w, 1);
 }
+template <bool COUNT>
+__global__ void __launch_bounds__(128, 7) k_shadow(const __grid_constant__ DFrame F, int level, long long c0) {
+  shadow_body<COUNT>(F, level, c0, blockIdx.x, gridDim.x);
+}
+template <bool COUNT>
+__global__ void __launch_bounds__(128, 7) k_shadow_multi(const DFrame* __restrict__ T, const int* __restrict__ b0, int nj, int level, long long c0) {
+  const int j = job_of_block(b0, nj);
+  const DFrame& F = T[j];
+  if (level >= frame_levels(F)) return;
+  shadow_body<COUNT>(F, level, c0, blockIdx.x - b0[j], b0[j + 1] - b0[j]);
+}
+
 
 // phong_lighting's sum, fog and the reflection ray (src/lighting.rs:220-288,
 // 297-319, 437-496) for hits [c0, c1).  Eight blocks of 128 per SM (64
 // registers, some spilled): the kernel streams the shadow buffer, and the
 // extra warps hide more of its latency than the spills cost (bench frame
 // 7.0 ms against 7.23 ms at 128 registers; 6, 10 and 12 blocks were slower).
-__global__ void __launch_bounds__(128, 8) k_resolve(DFrame F, int level, long long c0) {
+__device__ __forceinline__ void resolve_body(const DFrame& F, int level, long long c0, int bid, int nblk) {
   const DScene& S = F.S;
   long long nh = F.fb_mode ? *F.fbn : F.nhits[level];
   long long c1 = c0 + F.chunk_hits < nh ? c0 + F.chunk_hits : nh;
@@ -496,8 +563,8 @@ __global__ void __launch_bounds__(128, 8) k_resolve(DFrame F, int level, long lo
   LevelBuf L = F.levels[level];
   bool can_reflect = (F.max_depth - level) > 1;
   V3 campos = ld3(F.C.campos);
-  long long stride = (long long)gridDim.x * blockDim.x;
-  for (long long base = c0 + blockIdx.x * (long long)blockDim.x; base < c1; base += stride) {
+  long long stride = (long long)nblk * blockDim.x;
+  for (long long base = c0 + bid * (long long)blockDim.x; base < c1; base += stride) {
     long long h = base + threadIdx.x;
     bool active = h < c1;
     // the hit in the level's list (fallback launches walk fb_list); a
@@ -609,6 +676,16 @@ __global__ void __launch_bounds__(128, 8) k_resolve(DFrame F, int level, long lo
     }
   }
 }
+__global__ void __launch_bounds__(128, 8) k_resolve(const __grid_constant__ DFrame F, int level, long long c0) {
+  resolve_body(F, level, c0, blockIdx.x, gridDim.x);
+}
+__global__ void __launch_bounds__(128, 8) k_resolve_multi(const DFrame* __restrict__ T, const int* __restrict__ b0, int nj, int level, long long c0) {
+  const int j = job_of_block(b0, nj);
+  const DFrame& F = T[j];
+  if (level >= frame_levels(F)) return;
+  resolve_body(F, level, c0, blockIdx.x - b0[j], b0[j + 1] - b0[j]);
+}
+
 
 // Confidence gate of learned shadows: every level-0 hit with an estimated
 // visibility error above conf_thr on one of its slots goes to fb_list (and
@@ -695,11 +772,11 @@ __global__ void __launch_bounds__(128) k_features(DFrame F, long long c0) {
 }
 
 // color * (1 - r) + reflected * r, deepest level first
-__global__ void k_fold(DFrame F, int level) {
+__device__ __forceinline__ void fold_body(const DFrame& F, int level, int bid, int nblk) {
   int n = F.counts[level];
   LevelBuf L = F.levels[level];
   LevelBuf C = F.levels[level + 1];
-  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+  for (int i = bid * blockDim.x + threadIdx.x; i < n; i += nblk * blockDim.x) {
     int c = L.child[i];
     if (c < 0) continue;
     double r = L.refl[i];
@@ -709,6 +786,16 @@ __global__ void k_fold(DFrame F, int level) {
     L.b[i] = L.b[i] * k + C.b[c] * r;
   }
 }
+__global__ void k_fold(const __grid_constant__ DFrame F, int level) {
+  fold_body(F, level, blockIdx.x, gridDim.x);
+}
+__global__ void k_fold_multi(const DFrame* __restrict__ T, const int* __restrict__ b0, int nj, int level) {
+  const int j = job_of_block(b0, nj);
+  const DFrame& F = T[j];
+  if (level > frame_levels(F) - 2) return;
+  fold_body(F, level, blockIdx.x - b0[j], b0[j + 1] - b0[j]);
+}
+
 
 // --------------------------------------------------------------------------
 // Per-pixel resolve, outline, quantise
@@ -724,10 +811,10 @@ __device__ __forceinline__ void store_rgb(const DFrame& F, long long p, V3 c) {
   }
 }
 
-__global__ void k_pixels(DFrame F) {
+__device__ __forceinline__ void pixels_body(const DFrame& F, int bid, int nblk) {
   long long np = (long long)F.W * F.H;
   LevelBuf L = F.levels[0];
-  for (long long p = blockIdx.x * (long long)blockDim.x + threadIdx.x; p < np; p += (long long)gridDim.x * blockDim.x) {
+  for (long long p = bid * (long long)blockDim.x + threadIdx.x; p < np; p += (long long)nblk * blockDim.x) {
     V3 c;
     if (F.max_depth <= 0) {
       // ray_color returns black before any World::hit (src/lighting.rs:450-452)
@@ -792,6 +879,15 @@ __global__ void k_pixels(DFrame F) {
     }
   }
 }
+__global__ void k_pixels(const __grid_constant__ DFrame F) {
+  pixels_body(F, blockIdx.x, gridDim.x);
+}
+__global__ void k_pixels_multi(const DFrame* __restrict__ T, const int* __restrict__ b0, int nj) {
+  const int j = job_of_block(b0, nj);
+  const DFrame& F = T[j];
+  pixels_body(F, blockIdx.x - b0[j], b0[j + 1] - b0[j]);
+}
+
 
 // detect_edges / compute_edge_strength (src/outline.rs:113-182): one tile of
 // OT_X x OT_Y pixels with a one-pixel halo staged in shared memory.

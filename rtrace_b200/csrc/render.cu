@@ -131,6 +131,15 @@ struct rt_ctx {
   // batched rendering: lanes are child contexts (own stream and scratch)
   std::vector<rt_ctx*> lanes;
   uint32_t tuned_lanes = 0;
+  // the fused group of a batch: frames of at most fuse_pixels pixels are
+  // rendered together, each kernel launched once for all of them; slots
+  // hold their scratch (child contexts), group_buf their frame table.
+  std::vector<rt_ctx*> slots;
+  uint32_t fuse_pixels = 640 * 480;
+  int tune_bpsm[7] = {16, 64, 64, 128, 16, 16, 16};  // blocks per SM: raygen trace emit shadow resolve fold pixels
+  bool tuned = false;
+  void* group_buf = nullptr;
+  size_t group_cap = 0;
   char* pin = nullptr;  // pinned staging of scene uploads
   size_t pin_cap = 0;
   bool borrowed_net = false;  // a lane's net points at its parent's weights
@@ -1341,9 +1350,25 @@ struct AovOut {
   __half* feat = nullptr; // [plane][H][W][FEAT_CHANNELS]
 };
 
+// A frame set up for a fused multi-frame launch (rt_render_batch): its
+// arguments, validated as rt_render validates them, with the context's
+// scratch sized and the frame's launch block filled, but nothing launched.
+struct FramePlan {
+  DFrame F;
+  int levels = 1;
+  long long nprim = 0, npix = 0, chunk = 0;
+  int K = 0;
+  uint8_t* rgb_out = nullptr;  // where the image goes
+  int on_device = 0;
+  bool direct = false;         // the kernels write rgb_out themselves
+  uint8_t* d_rgb = nullptr;    // else the image in the context's scratch
+  std::chrono::steady_clock::time_point t0;
+};
+
 rt_status render_impl(rt_ctx* ctx, const rt_scene* sc, const rt_render_params* P, uint32_t row_begin,
                       uint32_t row_end, uint8_t* rgb_out, int on_device, double* linear_out, rt_stats* stats,
-                      const AovOut* aov = nullptr, const rt_camera_config* camera = nullptr) {
+                      const AovOut* aov = nullptr, const rt_camera_config* camera = nullptr,
+                      FramePlan* plan = nullptr) {
   auto t0 = std::chrono::steady_clock::now();
   if (!ctx || !sc || !P) return fail(ctx, RT_ERR_INVALID_ARGUMENT, "null argument");
   if (!rgb_out && !linear_out) return fail(ctx, RT_ERR_INVALID_ARGUMENT, "no output buffer");
@@ -1501,6 +1526,25 @@ rt_status render_impl(rt_ctx* ctx, const rt_scene* sc, const rt_render_params* P
   uint8_t* d_rgb = F.rgb;
   const bool direct = rgb_out && on_device && keep_off == 0 && keep_pix == npix;
   if (direct) F.rgb = rgb_out;
+  if (plan) {
+    // one launch block for every level (no learned level 0), one shadow
+    // chunk, whole frame, no outline pass, no linear copy
+    if (learned || want_aov || linear_out || F.outline || !full_frame || max_depth <= 0 || chunk_n < nprim ||
+        !rgb_out)
+      return fail(ctx, RT_ERR_INVALID_ARGUMENT, "this frame cannot join a fused batch group");
+    plan->F = F;
+    plan->levels = levels;
+    plan->nprim = nprim;
+    plan->npix = npix;
+    plan->chunk = chunk_n;
+    plan->K = K_full;
+    plan->rgb_out = rgb_out;
+    plan->on_device = on_device;
+    plan->direct = direct;
+    plan->d_rgb = d_rgb;
+    plan->t0 = t0;
+    return RT_OK;
+  }
 
   const bool count = (P->flags & RT_FLAG_COUNT_WORK) != 0;
   Launcher Lc{ctx, (P->flags & RT_FLAG_STAGE_TIMES) != 0};
@@ -1734,6 +1778,220 @@ rt_status render_impl(rt_ctx* ctx, const rt_scene* sc, const rt_render_params* P
   return RT_OK;
 }
 
+// Kernel kinds of a fused launch, their block sizes and the work that sizes
+// their grids.
+enum { FK_RAYGEN, FK_TRACE, FK_EMIT, FK_SHADOW, FK_RESOLVE, FK_FOLD, FK_PIXELS, FK_COUNT };
+const int kFusedBlock[FK_COUNT] = {256, 128, 128, 128, 128, 256, 256};
+
+// The fused group of a batch on `lane`: every frame is planned on its own
+// slot (scratch; render_impl's checks), then each kernel of the wavefront is
+// launched once for all frames over a device table of their launch blocks.
+// Kernel kind k gets about nsm * tune_bpsm[k] blocks in all, shared out in
+// proportion to each frame's work bound; each frame's blocks stride over its
+// own rays.  The sequence is captured as a CUDA graph and replayed when the
+// same group (frames, buffers, grid split) comes again.  Frames that cannot
+// join (rare: the eligibility test in rt_render_batch mirrors render_impl's)
+// render on their slot the usual way.
+rt_status run_fused(rt_ctx* parent, rt_ctx* lane, rt_job* jobs, const std::vector<uint32_t>& idx,
+                    std::vector<std::string>& errs, double* group_ms) {
+  rt_ctx* ctx = lane;  // CK reports failures on the lane
+  *group_ms = 0.0;
+  const size_t n = idx.size();
+  while (parent->slots.size() < n) {
+    rt_ctx* l = nullptr;
+    rt_status st = rt_ctx_create(parent->device, &l);
+    if (st != RT_OK) return fail(parent, st, "creating a batch slot: " + std::string(rt_last_error(nullptr)));
+    l->borrowed_net = true;
+    parent->slots.push_back(l);
+  }
+  std::vector<FramePlan> plans(n);
+  std::vector<size_t> ok;
+  for (size_t k = 0; k < n; k++) {
+    rt_job& J = jobs[idx[k]];
+    rt_ctx* sl = parent->slots[k];
+    memset(&J.stats, 0, sizeof J.stats);
+    if (!J.scene || !J.rgb_out) {
+      J.status = RT_ERR_INVALID_ARGUMENT;
+      errs[idx[k]] = "null scene or output";
+      continue;
+    }
+    J.status = render_impl(sl, J.scene, &J.params, 0, J.params.height, J.rgb_out, J.out_on_device, nullptr, nullptr,
+                           nullptr, J.camera, &plans[k]);
+    if (J.status == RT_OK) {
+      ok.push_back(k);
+    } else if (sl->err == "this frame cannot join a fused batch group") {
+      J.status = render_impl(sl, J.scene, &J.params, 0, J.params.height, J.rgb_out, J.out_on_device, nullptr,
+                             &J.stats, nullptr, J.camera);
+      if (J.status != RT_OK) errs[idx[k]] = sl->err;
+    } else {
+      errs[idx[k]] = sl->err;
+    }
+  }
+  if (ok.empty()) return RT_OK;
+  const int nj = (int)ok.size();
+  CK(cudaSetDevice(lane->device));
+  // host image of the table: frames, then (nj + 1) first blocks per kind
+  const size_t frames_bytes = ((sizeof(DFrame) * nj + 255) / 256) * 256;
+  const size_t bytes = frames_bytes + sizeof(int) * (size_t)FK_COUNT * (nj + 1);
+  std::vector<unsigned char> host(bytes, 0);
+  DFrame* T = reinterpret_cast<DFrame*>(host.data());
+  int* b0 = reinterpret_cast<int*>(host.data() + frames_bytes);
+  int Lmax = 1;
+  for (int j = 0; j < nj; j++) {
+    T[j] = plans[ok[j]].F;
+    Lmax = std::max(Lmax, plans[ok[j]].levels);
+  }
+  const int nsm = lane->num_sms;
+  int total[FK_COUNT];
+  for (int k = 0; k < FK_COUNT; k++) {
+    std::vector<double> w(nj);
+    double sum = 0.0;
+    for (int j = 0; j < nj; j++) {
+      const FramePlan& pl = plans[ok[j]];
+      const double v = k == FK_SHADOW ? (double)pl.chunk * std::max(pl.K, 1)
+                       : (k == FK_EMIT || k == FK_RESOLVE) ? (double)pl.chunk
+                       : k == FK_PIXELS ? (double)pl.npix : (double)pl.nprim;
+      w[j] = v;
+      sum += v;
+    }
+    const double budget = (double)nsm * parent->tune_bpsm[k];
+    int at = 0;
+    for (int j = 0; j < nj; j++) {
+      b0[k * (nj + 1) + j] = at;
+      const long long most = std::max(1LL, (long long)((w[j] + kFusedBlock[k] - 1) / kFusedBlock[k]));
+      const long long want = std::max(1LL, (long long)std::llround(budget * w[j] / std::max(sum, 1.0)));
+      at += (int)std::min(most, want);
+    }
+    b0[k * (nj + 1) + nj] = at;
+    total[k] = at;
+  }
+  if (bytes > parent->group_cap) {
+    CK(cudaStreamSynchronize(lane->stream));
+    if (parent->group_buf) cudaFree(parent->group_buf);
+    parent->group_buf = nullptr;
+    parent->group_cap = 0;
+    cudaError_t e = cudaMalloc(&parent->group_buf, bytes * 2);
+    if (e != cudaSuccess) return cuda_fail(parent, e, "cudaMalloc(batch group table)");
+    parent->group_cap = bytes * 2;
+  }
+  const DFrame* dT = reinterpret_cast<const DFrame*>(parent->group_buf);
+  const int* db0 = reinterpret_cast<const int*>(static_cast<unsigned char*>(parent->group_buf) + frames_bytes);
+  auto B = [&](int k) { return db0 + k * (nj + 1); };
+  cudaStream_t s = lane->stream;
+  CK(cudaMemcpyAsync(parent->group_buf, host.data(), bytes, cudaMemcpyHostToDevice, s));
+  uint32_t launches = 0;
+  auto enqueue = [&]() -> rt_status {
+    k_frame_init_multi<<<nj, 128, 0, s>>>(dT);
+    k_raygen_multi<<<total[FK_RAYGEN], 256, 0, s>>>(dT, B(FK_RAYGEN), nj);
+    launches = 2;
+    for (int l = 0; l < Lmax; l++) {
+      k_trace_multi<false><<<total[FK_TRACE], 128, 0, s>>>(dT, B(FK_TRACE), nj, l);
+      k_emit_multi<<<total[FK_EMIT], 128, 0, s>>>(dT, B(FK_EMIT), nj, l, 0);
+      k_shadow_multi<false><<<total[FK_SHADOW], 128, 0, s>>>(dT, B(FK_SHADOW), nj, l, 0);
+      k_resolve_multi<<<total[FK_RESOLVE], 128, 0, s>>>(dT, B(FK_RESOLVE), nj, l, 0);
+      launches += 4;
+    }
+    for (int l = Lmax - 2; l >= 0; l--) {
+      k_fold_multi<<<total[FK_FOLD], 256, 0, s>>>(dT, B(FK_FOLD), nj, l);
+      launches++;
+    }
+    k_pixels_multi<<<total[FK_PIXELS], 256, 0, s>>>(dT, B(FK_PIXELS), nj);
+    launches++;
+    CK(cudaGetLastError());
+    return RT_OK;
+  };
+  // graph: keyed by the table image (frames with their buffers, grid split)
+  std::vector<unsigned char> key(host.begin(), host.end());
+  const char tag[] = "fused";
+  key.insert(key.end(), tag, tag + sizeof tag);
+  GraphEntry* hit = nullptr;
+  for (GraphEntry& g : lane->graphs)
+    if (g.key == key) hit = &g;
+  uint32_t graph_state = 2;
+  if (!hit) {
+    cudaGraph_t g = nullptr;
+    CK(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
+    rt_status es = enqueue();
+    cudaError_t ce = cudaStreamEndCapture(s, &g);
+    if (es != RT_OK) {
+      if (g) cudaGraphDestroy(g);
+      return es;
+    }
+    if (ce != cudaSuccess) return cuda_fail(lane, ce, "cudaStreamEndCapture");
+    cudaGraphExec_t ex = nullptr;
+    ce = cudaGraphInstantiate(&ex, g, 0);
+    cudaGraphDestroy(g);
+    if (ce != cudaSuccess) return cuda_fail(lane, ce, "cudaGraphInstantiate");
+    if (lane->graphs.size() >= kMaxGraphs) {
+      auto lru = std::min_element(lane->graphs.begin(), lane->graphs.end(),
+                                  [](const GraphEntry& a, const GraphEntry& b) { return a.used < b.used; });
+      cudaGraphExecDestroy(lru->exec);
+      lane->graphs.erase(lru);
+    }
+    lane->graphs.push_back(GraphEntry{std::move(key), ex, launches, 0});
+    hit = &lane->graphs.back();
+    graph_state = 1;
+  }
+  hit->used = ++lane->graph_tick;
+  CK(cudaEventRecord(lane->ev0, s));
+  CK(cudaGraphLaunch(hit->exec, s));
+  CK(cudaEventRecord(lane->ev1, s));
+  // per frame: image, queue sizes, hit counts, error word
+  struct Back {
+    std::vector<int> counts, nh;
+    int err = 0;
+  };
+  std::vector<Back> back(nj);
+  for (int j = 0; j < nj; j++) {
+    const FramePlan& pl = plans[ok[j]];
+    rt_ctx* sl = parent->slots[ok[j]];
+    if (!pl.direct)
+      CK(cudaMemcpyAsync(pl.rgb_out, pl.d_rgb, 3 * pl.npix,
+                         pl.on_device ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost, s));
+    back[j].counts.assign(pl.levels + 2, 0);
+    back[j].nh.assign(pl.levels + 1, 0);
+    CK(cudaMemcpyAsync(back[j].counts.data(), sl->d_counts, (pl.levels + 2) * sizeof(int), cudaMemcpyDeviceToHost, s));
+    CK(cudaMemcpyAsync(back[j].nh.data(), sl->d_nhits, (pl.levels + 1) * sizeof(int), cudaMemcpyDeviceToHost, s));
+    CK(cudaMemcpyAsync(&back[j].err, sl->d_err, sizeof(int), cudaMemcpyDeviceToHost, s));
+  }
+  cudaError_t se = cudaStreamSynchronize(s);
+  if (se != cudaSuccess) return cuda_fail(lane, se, "fused batch group");
+  float ms = 0.f;
+  cudaEventElapsedTime(&ms, lane->ev0, lane->ev1);
+  *group_ms = ms;
+  for (int j = 0; j < nj; j++) {
+    const FramePlan& pl = plans[ok[j]];
+    rt_job& J = jobs[idx[ok[j]]];
+    const int herr = back[j].err;
+    std::string msg;
+    rt_status st = RT_OK;
+    if (herr & ERR_EMPTY_RANGE) st = RT_ERR_RENDER, msg = "cannot sample empty range";
+    else if (herr & ERR_RANGE_OVERFLOW) st = RT_ERR_RENDER, msg = "UniformSampler::sample_single: range overflow";
+    else if (herr & (ERR_WATCHDOG | ERR_STACK))
+      st = RT_ERR_DEVICE_WATCHDOG,
+      msg = herr & ERR_STACK ? "traversal stack exhausted" : "rejection sampling did not terminate";
+    J.status = st;
+    if (st != RT_OK) {
+      errs[idx[ok[j]]] = msg;
+      continue;
+    }
+    rt_stats& S = J.stats;
+    memset(&S, 0, sizeof S);
+    S.primary_rays = (uint64_t)back[j].counts[0];
+    uint64_t refl = 0, hits = 0;
+    for (int l = 1; l < pl.levels; l++) refl += (uint64_t)back[j].counts[l];
+    for (int l = 0; l < pl.levels; l++) hits += (uint64_t)back[j].nh[l];
+    S.reflection_rays = refl;
+    S.hits = hits;
+    S.shadow_rays = hits * (uint64_t)pl.K;
+    S.kernel_launches = launches;  // shared by the group
+    S.graph = graph_state;
+    S.device_ms = ms;  // the group's time, shared by its frames
+    S.total_ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - pl.t0).count();
+  }
+  return RT_OK;
+}
+
 }  // namespace
 
 // Meshes from this many triangles up build their k-d tree on the device when
@@ -1786,6 +2044,10 @@ void rt_ctx_destroy(rt_ctx* ctx) {
   if (ctx->stream) cudaStreamSynchronize(ctx->stream);
   for (rt_ctx* l : ctx->lanes) rt_ctx_destroy(l);
   ctx->lanes.clear();
+  for (rt_ctx* l : ctx->slots) rt_ctx_destroy(l);
+  ctx->slots.clear();
+  if (ctx->group_buf) cudaFree(ctx->group_buf);
+  ctx->group_buf = nullptr;
   if (ctx->pin) cudaFreeHost(ctx->pin);
   ctx->pin = nullptr;
   drop_graphs(ctx);
@@ -2204,8 +2466,11 @@ rt_status rt_render_batch(rt_ctx* ctx, rt_job* jobs, uint32_t n, uint32_t lanes,
     l->net.conf_threshold = ctx->net.conf_threshold;
     l->net.allocs.clear();
   }
-  // estimated rays per job -> lanes, longest first
+  // estimated rays per job -> lanes, longest first; small frames that can
+  // share launches form the fused group, which lane 0 renders first
   std::vector<double> cost(n, 0.0);
+  std::vector<uint32_t> fused;
+  std::vector<char> in_group(n, 0);
   for (uint32_t i = 0; i < n; i++) {
     const rt_render_params& P = jobs[i].params;
     const rt_scene* sc = jobs[i].scene;
@@ -2213,21 +2478,53 @@ rt_status rt_render_batch(rt_ctx* ctx, rt_job* jobs, uint32_t n, uint32_t lanes,
     int ds = P.disk_samples ? (int)P.disk_samples : 16;
     double K = sc ? (double)(sc->n_point_lights + sc->n_disk_lights * ds) : 0.0;
     cost[i] = (double)P.width * P.height * spp * (1.0 + K);
+    // fused group: whole small frames on the plain path, one shadow chunk,
+    // no outline pass, no profiling
+    const double nprim = P.anti_aliasing_mode == RT_AA_QUINCUNX
+                             ? (double)(P.width + 1) * (P.height + 1) + (double)P.width * P.height
+                             : (double)P.width * P.height * std::max(1u, P.samples);
+    const bool outline = P.outline.enabled && P.anti_aliasing_mode != RT_AA_QUINCUNX;
+    if (ctx->fuse_pixels && sc && jobs[i].rgb_out && (uint64_t)P.width * P.height <= ctx->fuse_pixels &&
+        !P.learned_shadows && !outline && P.max_depth > 0 && P.max_depth <= RTB_MAX_LEVELS && P.samples > 0 &&
+        !(P.flags & (RT_FLAG_STAGE_TIMES | RT_FLAG_COUNT_WORK)) && nprim * std::max(K, 1.0) <= (double)kShadowCap) {
+      fused.push_back(i);
+      in_group[i] = 1;
+    }
   }
-  std::vector<uint32_t> lane_of(n, 0);
-  rt_status st = rt_batch_assign(cost.data(), n, lanes, lane_of.data());
-  if (st != RT_OK) return fail(ctx, st, "rt_batch_assign failed");
+  if (fused.size() < 2) {  // one frame gains nothing from fusion
+    fused.clear();
+    std::fill(in_group.begin(), in_group.end(), 0);
+  }
   std::vector<std::vector<uint32_t>> per_lane(lanes);
   {
-    std::vector<uint32_t> order(n);
-    for (uint32_t i = 0; i < n; i++) order[i] = i;
+    // longest processing time first onto the least-loaded lane; lane 0
+    // starts with the fused group's estimated cost
+    std::vector<double> load(lanes, 0.0);
+    for (uint32_t i : fused) load[0] += cost[i];
+    std::vector<uint32_t> order;
+    for (uint32_t i = 0; i < n; i++)
+      if (!in_group[i]) order.push_back(i);
     std::stable_sort(order.begin(), order.end(), [&](uint32_t a, uint32_t b) { return cost[a] > cost[b]; });
-    for (uint32_t i : order) per_lane[lane_of[i]].push_back(i);
+    for (uint32_t i : order) {
+      uint32_t best = 0;
+      for (uint32_t k = 1; k < lanes; k++)
+        if (load[k] < load[best]) best = k;
+      per_lane[best].push_back(i);
+      load[best] += cost[i];
+    }
   }
   std::vector<std::string> errs(n);
   std::vector<double> lane_ms(lanes, 0.0);
+  rt_status group_st = RT_OK;
+  std::string group_err;
+  double group_ms = 0.0;  // device time of the fused group (shared by its frames)
   auto run_lane = [&](uint32_t k) {
     rt_ctx* l = ctx->lanes[k];
+    if (k == 0 && !fused.empty()) {
+      group_st = run_fused(ctx, l, jobs, fused, errs, &group_ms);
+      if (group_st != RT_OK) group_err = l->err.empty() ? ctx->err : l->err;
+      lane_ms[0] += group_ms;
+    }
     for (uint32_t i : per_lane[k]) {
       rt_job& J = jobs[i];
       memset(&J.stats, 0, sizeof J.stats);
@@ -2246,6 +2543,7 @@ rt_status rt_render_batch(rt_ctx* ctx, rt_job* jobs, uint32_t n, uint32_t lanes,
   for (uint32_t k = 1; k < lanes; k++) threads.emplace_back(run_lane, k);
   run_lane(0);
   for (auto& t : threads) t.join();
+  if (group_st != RT_OK) return fail(ctx, group_st, "fused batch group: " + group_err);
   rt_status first = RT_OK;
   std::string msg;
   uint64_t rays = 0;
@@ -2256,8 +2554,9 @@ rt_status rt_render_batch(rt_ctx* ctx, rt_job* jobs, uint32_t n, uint32_t lanes,
       msg = "job " + std::to_string(i) + ": " + errs[i];
     }
     rays += jobs[i].stats.primary_rays + jobs[i].stats.reflection_rays + jobs[i].stats.shadow_rays;
-    dev += jobs[i].stats.device_ms;
+    if (!in_group[i]) dev += jobs[i].stats.device_ms;
   }
+  dev += group_ms;
   if (stats) {
     memset(stats, 0, sizeof *stats);
     stats->jobs = n;
@@ -2272,31 +2571,104 @@ rt_status rt_render_batch(rt_ctx* ctx, rt_job* jobs, uint32_t n, uint32_t lanes,
   return RT_OK;
 }
 
-rt_status rt_batch_autotune(rt_ctx* ctx, rt_job* jobs, uint32_t n, uint32_t* best_lanes) {
+rt_status rt_batch_get_tuning(rt_ctx* ctx, rt_batch_tuning* out) {
+  if (!ctx || !out) return fail(ctx, RT_ERR_INVALID_ARGUMENT, "null argument");
+  memset(out, 0, sizeof *out);
+  out->lanes = ctx->tuned_lanes ? ctx->tuned_lanes : 4;
+  out->fuse_pixels = ctx->fuse_pixels;
+  for (int k = 0; k < 7; k++) out->blocks_per_sm[k] = ctx->tune_bpsm[k];
+  return RT_OK;
+}
+
+rt_status rt_batch_set_tuning(rt_ctx* ctx, const rt_batch_tuning* t) {
+  if (!ctx || !t) return fail(ctx, RT_ERR_INVALID_ARGUMENT, "null argument");
+  if (t->lanes < 1 || t->lanes > 16) return fail(ctx, RT_ERR_INVALID_ARGUMENT, "lanes must be 1..16");
+  for (int k = 0; k < 7; k++)
+    if (t->blocks_per_sm[k] < 1 || t->blocks_per_sm[k] > 1024)
+      return fail(ctx, RT_ERR_INVALID_ARGUMENT, "blocks_per_sm must be 1..1024");
+  ctx->tuned_lanes = t->lanes;
+  ctx->fuse_pixels = t->fuse_pixels;
+  for (int k = 0; k < 7; k++) ctx->tune_bpsm[k] = t->blocks_per_sm[k];
+  return RT_OK;
+}
+
+rt_status rt_batch_autotune_ex(rt_ctx* ctx, rt_job* jobs, uint32_t n, rt_batch_tuning* out) {
   if (!ctx) return fail(nullptr, RT_ERR_INVALID_ARGUMENT, "null context");
-  const uint32_t cand[4] = {1, 2, 4, 8};
-  double best_ms = 1e300;
-  uint32_t best = 4;
-  {
-    // warm-up with the most lanes: creates them and sizes their scratch for
-    // the largest jobs (the longest jobs go to the first lanes), so that the
-    // timed runs below allocate nothing
+  rt_batch_tuning cur;
+  rt_status st = rt_batch_get_tuning(ctx, &cur);
+  if (st != RT_OK) return st;
+  uint32_t trials = 0;
+  auto measure = [&](const rt_batch_tuning& t, double* ms) -> rt_status {
+    rt_status s2 = rt_batch_set_tuning(ctx, &t);
+    if (s2 != RT_OK) return s2;
     rt_batch_stats bs;
-    rt_status st = rt_render_batch(ctx, jobs, n, cand[3], &bs);
+    s2 = rt_render_batch(ctx, jobs, n, t.lanes, &bs);  // first run with a new group captures its graph
+    if (s2 != RT_OK) return s2;
+    s2 = rt_render_batch(ctx, jobs, n, t.lanes, &bs);
+    if (s2 != RT_OK) return s2;
+    trials++;
+    *ms = bs.wall_ms;
+    return RT_OK;
+  };
+  {
+    // warm-up with the most lanes: creates the lanes and slots and sizes
+    // their scratch, so that the timed runs allocate nothing
+    rt_batch_tuning w = cur;
+    w.lanes = 8;
+    double ms;
+    st = measure(w, &ms);
     if (st != RT_OK) return st;
   }
-  for (uint32_t c : cand) {
-    rt_batch_stats bs;
-    rt_status st = rt_render_batch(ctx, jobs, n, c, &bs);
-    if (st != RT_OK) return st;
-    if (bs.wall_ms < best_ms) {
-      best_ms = bs.wall_ms;
-      best = c;
+  double best_ms;
+  st = measure(cur, &best_ms);
+  if (st != RT_OK) return st;
+  // coordinate search: lanes, then the fused group's size limit, then the
+  // grid budget (blocks per SM) of each fused kernel kind
+  auto try_values = [&](auto set, std::initializer_list<long long> vals) -> rt_status {
+    for (long long v : vals) {
+      rt_batch_tuning t = cur;
+      set(t, v);
+      if (memcmp(&t, &cur, sizeof t) == 0) continue;
+      double ms;
+      rt_status s2 = measure(t, &ms);
+      if (s2 != RT_OK) return s2;
+      if (ms < best_ms) {
+        best_ms = ms;
+        cur = t;
+      }
+    }
+    return RT_OK;
+  };
+  st = try_values([](rt_batch_tuning& t, long long v) { t.lanes = (uint32_t)v; }, {1, 2, 4, 8});
+  if (st != RT_OK) return st;
+  st = try_values([](rt_batch_tuning& t, long long v) { t.fuse_pixels = (uint32_t)v; },
+                  {0, 256 * 256, 640 * 480, 1280 * 720});
+  if (st != RT_OK) return st;
+  const std::initializer_list<long long> grid_vals[7] = {{8, 16, 32}, {16, 32, 64, 128}, {16, 32, 64, 128},
+                                                         {32, 64, 128, 256}, {8, 16, 32, 64}, {8, 16, 32},
+                                                         {8, 16, 32}};
+  if (cur.fuse_pixels) {
+    for (int k : {1, 3, 2, 4}) {  // the walks first, then emit and resolve
+      st = try_values([k](rt_batch_tuning& t, long long v) { t.blocks_per_sm[k] = (int32_t)v; }, grid_vals[k]);
+      if (st != RT_OK) return st;
     }
   }
-  ctx->tuned_lanes = best;
-  if (best_lanes) *best_lanes = best;
+  st = rt_batch_set_tuning(ctx, &cur);
+  if (st != RT_OK) return st;
+  ctx->tuned = true;
+  if (out) {
+    *out = cur;
+    out->best_ms = best_ms;
+    out->trials = trials;
+  }
   return RT_OK;
+}
+
+rt_status rt_batch_autotune(rt_ctx* ctx, rt_job* jobs, uint32_t n, uint32_t* best_lanes) {
+  rt_batch_tuning t;
+  rt_status st = rt_batch_autotune_ex(ctx, jobs, n, &t);
+  if (st == RT_OK && best_lanes) *best_lanes = t.lanes;
+  return st;
 }
 
 rt_status rt_denoiser_load(rt_ctx* ctx, const void* blob, size_t bytes) {

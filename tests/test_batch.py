@@ -98,3 +98,69 @@ def test_batch_reports_the_failing_job(gpu_ctx, tmp_path):
     jobs = [rt.Job(scene, good, views[0][1]), rt.Job(scene, bad, views[1][1]), rt.Job(scene, good, views[2][1])]
     with pytest.raises(rt.RenderError, match="job 1: Samples must be greater than 0"):
         rt.render_batch(jobs, lanes=2, ctx=gpu_ctx)
+
+
+@pytest.mark.gpu
+def test_fused_group_equals_separate_renders(gpu_ctx, tmp_path):
+    """Small frames of a batch render as one fused launch sequence over a
+    table of frames (then replayed as a graph); every image must equal the
+    unfused batch's and rt_render's, and a frame with the outline on (not
+    fusable) renders beside the group."""
+    wl = workloads.batch_workload(str(tmp_path), n_scenes=4, seed=7)
+    jobs = []
+    sizes = [(64, 48), (96, 64), (40, 40), (128, 72)]
+    for k, (path, views) in enumerate(wl):
+        scene = rt.Scene.from_json_file(path, gpu_ctx)
+        for v, (name, cam, _) in enumerate(views):
+            w, h = sizes[(k + v) % 4]
+            r = rt.Renderer(w, h)
+            if v == 1:
+                r.anti_aliasing_mode = rt.AntiAliasingMode.Stochastic
+                r.samples = 3
+            if v == 2:
+                r.anti_aliasing_mode = rt.AntiAliasingMode.NoJitter
+                r.max_depth = 2 + k
+            if k == 3 and v == 3:
+                r.anti_aliasing_mode = rt.AntiAliasingMode.NoJitter
+                r.outline_config = rt.OutlineConfig()
+            jobs.append(rt.Job(scene, r, cam))
+    saved = rt.batch_tuning(gpu_ctx)
+    try:
+        rt.batch_tuning(gpu_ctx, fuse_pixels=0)
+        want, _ = rt.render_batch(jobs, lanes=2, ctx=gpu_ctx)
+        rt.batch_tuning(gpu_ctx, fuse_pixels=1 << 20, blocks_per_sm={"trace": 8, "shadow": 16})
+        for rep in range(2):  # capture, then replay
+            got, st = rt.render_batch(jobs, lanes=2, ctx=gpu_ctx)
+            assert st.jobs == len(jobs)
+            for a, b in zip(got, want):
+                assert np.array_equal(a, b), rep
+        fused = [j for j in jobs if j.renderer.outline_config is None]
+        assert all(j.renderer.last_stats.graph == 2 for j in fused)
+        assert jobs[-1].renderer.last_stats.graph == 0
+        # against rt_render of the same camera written into the scene
+        for idx in (0, 5, 10):
+            path, cam, r = wl[idx // 4][0], jobs[idx].camera, jobs[idx].renderer
+            p2 = tmp_path / "single.json"
+            p2.write_text(json.dumps(_with_camera(path, cam)))
+            s2 = rt.Scene.from_json_file(str(p2), gpu_ctx)
+            assert np.array_equal(got[idx], r.render(s2))
+            s2.close()
+    finally:
+        rt.batch_tuning(gpu_ctx, lanes=saved["lanes"], fuse_pixels=saved["fuse_pixels"],
+                        blocks_per_sm=saved["blocks_per_sm"])
+
+
+@pytest.mark.gpu
+def test_autotuner_reports_its_choice(gpu_ctx, tmp_path):
+    wl = workloads.batch_workload(str(tmp_path), n_scenes=2, seed=9)
+    jobs = []
+    for path, views in wl:
+        scene = rt.Scene.from_json_file(path, gpu_ctx)
+        for _, cam, _ in views:
+            jobs.append(rt.Job(scene, rt.Renderer(80, 60), cam))
+    t = rt.batch_autotune_ex(jobs, ctx=gpu_ctx)
+    assert t["lanes"] in (1, 2, 4, 8) and t["fuse_pixels"] in (0, 256 * 256, 640 * 480, 1280 * 720)
+    assert t["trials"] >= 5 and t["best_ms"] > 0
+    assert rt.batch_tuning(gpu_ctx)["lanes"] == t["lanes"]
+    with pytest.raises(ValueError):
+        rt.batch_tuning(gpu_ctx, lanes=0)
