@@ -612,7 +612,9 @@ rt_status rt_debug_mesh_hit(rt_ctx* ctx, const rt_scene* scene, int32_t object_i
  * 4 k-d occurrences, 5 occurrence offsets).  Bit 6: the arrays that an
  * upload of a host-prepared mesh derives on the device from its BVH-order
  * records and k-d tree (records in mesh order, normals, occurrences) differ
- * from the host's.  More than 4 triangles (the BVH leaf size). */
+ * from the host's.  Bit 7: the single-precision BVH the walks test (the
+ * device's conversion against the host's, which host-prepared uploads
+ * copy) differs.  More than 4 triangles (the BVH leaf size). */
 rt_status rt_debug_mesh_prep(rt_ctx* ctx, const rt_mesh_desc* mesh, uint32_t* mismatch);
 
 #ifdef __cplusplus

@@ -63,8 +63,11 @@ struct DCube {
 // (split, int2 meta): internal {right child, axis}, leaf {first, -1-count}.
 struct DMesh {
   double bmin[3], bmax[3];
-  const double2* bvh;      // triangle BVH nodes
-  const float4* fbvh;      // the same BVH in single precision (FNode), which the walks test
+  // triangle BVH nodes in double precision: set only for meshes prepared on
+  // the device (null for host-prepared ones) and read by no walk; the
+  // walks test fbvh
+  const double2* bvh;
+  const float4* fbvh;      // the BVH in single precision (FNode), which the walks test
   const double2* btris;    // triangle records in BVH leaf order
   const double2* brute;    // triangle records in original order
   const double4* normals;  // normalize(e1 x e2) per triangle
@@ -80,8 +83,7 @@ struct DMesh {
 
 // A run of consecutive spheres [first_obj, first_obj + count) in the World.
 struct DSphGroup {
-  const double2* bvh;  // BVH nodes over the run; leaves index `order`
-  const float4* fbvh;  // the same BVH in single precision (FNode), which the walks test
+  const float4* fbvh;  // BVH over the run in single precision (FNode); leaves index `order`
   const int* order;    // BVH position -> position in the run
   int first_sphere;    // index of the run's first sphere in DScene::sph
   int first_obj;       // World index of the run's first sphere

@@ -1180,22 +1180,17 @@ rt_status do_upload(rt_ctx* ctx, const rt_scene_desc* d, rt_scene** out,
       // leaves of 4 spheres: 47.6 ms for the 1,000-sphere ring frame (1080p,
       // 4 spp) against 49.4 ms with 8 or 12
       build_bvh(bmin, bmax, 4, 1e-6 * (1.0 + scale), &bn, &order);
-      std::vector<double2> bvh;
-      put_bvh(bn, &bvh);
       std::vector<float4> fbvh;
-      put_fbvh(bn, &fbvh);
+      put_fbvh(bn, &fbvh);  // the walks test single-precision boxes only
       DSphGroup G{};
-      const double2* pb;
       const float4* pf;
-      rt_status st = upload(ctx, sc.get(), bvh, &pb);
+      rt_status st = upload(ctx, sc.get(), fbvh, &pf);
       if (st != RT_OK) return st;
-      if ((st = upload(ctx, sc.get(), fbvh, &pf)) != RT_OK) return st;
       G.fbvh = pf;
       std::vector<int> ord(order.begin(), order.end());
       const int* po;
       st = upload(ctx, sc.get(), ord, &po);
       if (st != RT_OK) return st;
-      G.bvh = pb;
       G.order = po;
       G.first_sphere = first_sph;
       G.first_obj = obj[k].w;
@@ -2843,6 +2838,9 @@ rt_status rt_debug_mesh_prep(rt_ctx* ctx, const rt_mesh_desc* md, uint32_t* mism
   if (!same(normals, H.normals.data(), H.normals.size() * sizeof(double4))) m |= 8;
   if (!same(occ, H.occ.data(), H.occ.size() * sizeof(int2))) m |= 16;
   if (!same(occ_off, H.occ_off.data(), H.occ_off.size() * sizeof(int))) m |= 32;
+  // the single-precision BVH the walks test: the device's conversion
+  // (k_prep_fbvh) against the host's (put_fbvh), scale element included
+  if (H.fbvh.size() != 1 + 4 * (size_t)nb || !same(fbvh, H.fbvh.data(), H.fbvh.size() * sizeof(float4))) m |= 128;
   // the arrays an upload of the host preparation derives on the device,
   // from the host's BVH-order records, into the same buffers
   cudaStream_t s = ctx->stream;
