@@ -24,6 +24,8 @@ enum {
                          //   +1 max(n . l, 0) towards the light centre
                          //   +2 light radius / centre distance, clamped to [0, 1]
                          //   +3 1 (slot present)
+  FEAT_PIXEL_VIS = 13,   // per slot j, FEAT_PIXEL_VIS + j: the mean cast-ray visibility over
+                         // the pixel's samples that hit (every sample plane of the pixel)
   FEAT_CHANNELS = 16,
   DN_MAX_SLOTS = 2,
 };

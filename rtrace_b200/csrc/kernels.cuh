@@ -771,6 +771,35 @@ __global__ void __launch_bounds__(128) k_features(DFrame F, long long c0) {
   }
 }
 
+// Pixel-level feature: for each slot, the mean cast-ray visibility over the
+// samples of the pixel whose primary ray hit, written into every hit
+// sample's FEAT_PIXEL_VIS + slot channel, so that the network of each
+// sample plane sees the pixel's other samples too.  One thread per pixel.
+__global__ void __launch_bounds__(128) k_feat_pixel_mean(DFrame F) {
+  const long long plane_px = (long long)F.H * F.W;
+  for (long long pix = blockIdx.x * (long long)blockDim.x + threadIdx.x; pix < plane_px;
+       pix += (long long)gridDim.x * blockDim.x) {
+    float sum[DN_MAX_SLOTS] = {0.f, 0.f};
+    int n = 0;
+    for (int s = 0; s < F.S_per_px; s++) {
+      const __half* f = F.feat + ((long long)s * plane_px + pix) * FEAT_CHANNELS;
+      if (__half2float(f[FEAT_VALID]) > 0.f) {
+        n++;
+#pragma unroll
+        for (int j = 0; j < DN_MAX_SLOTS; j++) sum[j] += __half2float(f[FEAT_SLOT0 + FEAT_SLOT_STRIDE * j]);
+      }
+    }
+    if (n == 0) continue;
+    for (int s = 0; s < F.S_per_px; s++) {
+      __half* f = F.feat + ((long long)s * plane_px + pix) * FEAT_CHANNELS;
+      if (__half2float(f[FEAT_VALID]) > 0.f) {
+#pragma unroll
+        for (int j = 0; j < DN_MAX_SLOTS; j++) f[FEAT_PIXEL_VIS + j] = __float2half_rn(sum[j] / (float)n);
+      }
+    }
+  }
+}
+
 // color * (1 - r) + reflected * r, deepest level first
 __device__ __forceinline__ void fold_body(const DFrame& F, int level, int bid, int nblk) {
   int n = F.counts[level];

@@ -1602,6 +1602,10 @@ rt_status render_impl(rt_ctx* ctx, const rt_scene* sc, const rt_render_params* P
           k_resolve<<<blocks(chunk, 128, 16), 128, 0, s>>>(F, l, c0);
           Lc.after(RT_STAGE_RESOLVE);
         }
+        if (feat) {
+          k_feat_pixel_mean<<<blocks(npix, 128, 16), 128, 0, s>>>(F);
+          Lc.after(RT_STAGE_DENOISE);
+        }
         if (l == 0 && learned) {
           cudaError_t le = cudaSuccess;
           int nl = denoise_run(ctx->net, F.feat, spp, H, W, ctx->d_dn_arena, F.vhat, F.vconf, F.err, s, nsm, &le);

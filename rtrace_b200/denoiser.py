@@ -335,26 +335,26 @@ def training_scene(seed):
     return sc
 
 
-def render_pair(ctx, scene_path, width, height, rays=1, target_samples=64, seed=0):
-    """(features [1,H,W,16] half, target visibility [1,2,H,W] float) on the
-    GPU for one jittered sample per pixel (stochastic anti-aliasing, as the
-    learned render's sample planes): the feature image of `rays` rays per
-    disk light (what learned mode casts at primary hits) and the plain
-    path's visibility with target_samples rays per disk light (the first
-    samples of the same StdRng streams)."""
+def render_pair(ctx, scene_path, width, height, rays=1, target_samples=64, seed=0, spp=4):
+    """(features [spp,H,W,16] half, target visibility [spp,2,H,W] float) on
+    the GPU for spp stochastic samples per pixel (the learned render's
+    sample planes): the feature image of `rays` rays per disk light (what
+    learned mode casts at primary hits) and the plain path's visibility
+    with target_samples rays per disk light (the first samples of the same
+    StdRng streams)."""
     import torch
     import rtrace_b200 as rt
     scene = rt.Scene.from_json_file(scene_path, ctx)
     dev = torch.device("cuda", ctx.device)
     r = rt.Renderer(width, height)
     r.anti_aliasing_mode = rt.AntiAliasingMode.Stochastic
-    r.samples = 1
+    r.samples = spp
     r.seed = seed
     r.max_depth = 1
-    feat = torch.empty((1, height, width, FEAT_CHANNELS), dtype=torch.float16, device=dev)
+    feat = torch.empty((spp, height, width, FEAT_CHANNELS), dtype=torch.float16, device=dev)
     r.disk_samples = rays
     r.render_shadow_aov(scene, feat_ptr=feat.data_ptr())
-    vis = torch.empty((1, SLOTS, height, width), dtype=torch.float32, device=dev)
+    vis = torch.empty((spp, SLOTS, height, width), dtype=torch.float32, device=dev)
     r.disk_samples = target_samples
     r.render_shadow_aov(scene, vis_ptr=vis.data_ptr())
     scene.close()
@@ -430,9 +430,10 @@ def make_dataset(ctx, n_scenes, first_seed, width=1920, height=1080, rays=1, tar
         f, v = render_pair(ctx, path, width, height, rays=rays, target_samples=target_samples, seed=first_seed + k)
         ys = torch.randint(0, height - crop + 1, (crops,), generator=g).tolist()
         xs = torch.randint(0, width - crop + 1, (crops,), generator=g).tolist()
-        for y, x in zip(ys, xs):
-            feats.append(f[0, y:y + crop, x:x + crop].clone())
-            targs.append(v[0, :, y:y + crop, x:x + crop].half())
+        ps = torch.randint(0, f.shape[0], (crops,), generator=g).tolist()  # one sample plane per crop
+        for y, x, q in zip(ys, xs, ps):
+            feats.append(f[q, y:y + crop, x:x + crop].clone())
+            targs.append(v[q, :, y:y + crop, x:x + crop].half())
         if (k + 1) % 250 == 0:
             log("rendered %d/%d scenes (%.0f s)" % (k + 1, n_scenes, time.time() - t0))
     return torch.stack(feats), torch.stack(targs)

@@ -211,3 +211,29 @@ def test_confidence_fallback_uses_the_plain_path(gpu_ctx):
     assert torch.equal(vis[fb], pv[fb])
     keep = m & ~fb
     assert torch.equal(vis[keep], gv[keep])
+
+
+@pytest.mark.gpu
+def test_pixel_mean_visibility_feature(gpu_ctx):
+    """Channels 13 and 14 of each hit sample hold the mean cast-ray
+    visibility of slots 0 and 1 over the pixel's samples that hit."""
+    import torch
+    import rtrace_b200 as rt
+    scene = rt.Scene.from_json_str(_disk_scene_json(), gpu_ctx)
+    dev = torch.device("cuda", gpu_ctx.device)
+    S, H, W = 3, 40, 64
+    r = rt.Renderer(W, H)
+    r.anti_aliasing_mode = rt.AntiAliasingMode.Stochastic
+    r.samples = S
+    r.disk_samples = 2
+    feat = torch.zeros((S, H, W, 16), dtype=torch.float16, device=dev)
+    torch.cuda.synchronize()
+    r.render_shadow_aov(scene, None, feat.data_ptr())
+    f = feat.float()
+    valid = f[..., 0] > 0
+    n = valid.sum(0)
+    for j, ch in ((0, 5), (1, 9)):
+        mean = torch.where(n > 0, (f[..., ch] * valid).sum(0) / n.clamp_min(1), torch.zeros_like(n, dtype=f.dtype))
+        want = mean.unsqueeze(0).expand_as(valid)[valid].half().float()
+        assert torch.equal(f[..., 13 + j][valid], want)
+    assert (f[..., 13:15][~valid] == 0).all()
