@@ -811,6 +811,8 @@ def main():
                 learned = learned_vs_plain(rt, torch, ctx, d, min(args.steps, 10), hbm, tf)
             except Exception as e:  # report, do not lose the headline line
                 learned = {"unavailable": "failed: %s" % e}
+        if isinstance(learned, dict) and isinstance(learned.get("roofline"), dict):
+            roofline["conv"] = learned["roofline"]  # the learned form's tensor-core network
         if world == 1 and not args.no_cpu_baseline and parity is not None:
             try:
                 parity = {"headline_frame": parity, "ring_scene": ring_parity(rt, d)}
