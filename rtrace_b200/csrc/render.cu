@@ -1817,6 +1817,10 @@ rt_status run_fused(rt_ctx* parent, rt_ctx* lane, rt_job* jobs, const std::vecto
     J.status = render_impl(sl, J.scene, &J.params, 0, J.params.height, J.rgb_out, J.out_on_device, nullptr, nullptr,
                            nullptr, J.camera, &plans[k]);
     if (J.status == RT_OK) {
+      // whatever set-up the plan queued on the slot's stream precedes the
+      // fused launch, which runs on the lane's stream
+      cudaError_t se = cudaStreamSynchronize(sl->stream);
+      if (se != cudaSuccess) return cuda_fail(parent, se, "batch slot set-up");
       ok.push_back(k);
     } else if (sl->err == "this frame cannot join a fused batch group") {
       J.status = render_impl(sl, J.scene, &J.params, 0, J.params.height, J.rgb_out, J.out_on_device, nullptr,
