@@ -3,6 +3,7 @@
     python -m rtrace_b200.profile_render --workload noisy_icosphere --width 960 --height 540 --reps 1
     python -m rtrace_b200.profile_render --workload ring_spheres --width 1920 --height 1080 --learned
     python -m rtrace_b200.profile_render --kd-build terrain --reps 2
+    python -m rtrace_b200.profile_render --train-steps 3
 
 Workloads (see rtrace_b200.workloads): sphere_grid (quincunx), noisy_icosphere
 (no-jitter + outline, the bench.py scene), ring_spheres (stochastic, 4 spp).
@@ -12,6 +13,8 @@ heightfield, 2,093,058 triangles; icosphere: the level-6 noisy icosphere)
 on the device --reps times after one warm-up build of 1,000 of its
 triangles, checks it against the host build, then uploads the scene once
 (the mesh's search data prepared on the device).
+--train-steps runs that many steps of the denoiser's training on the
+library's kernels, on a batch of 16 seeded random 256x256 feature crops.
 """
 import argparse
 import json
@@ -32,10 +35,13 @@ def main(argv=None):
     ap.add_argument("--disk-samples", type=int, default=16, help="shadow rays per disk light (16: the reference)")
     ap.add_argument("--learned", action="store_true", help="learned soft shadows with the shipped denoiser weights")
     ap.add_argument("--kd-build", default=None, choices=["terrain", "icosphere"])
+    ap.add_argument("--train-steps", type=int, default=0)
     a = ap.parse_args(argv)
     d = a.dir or tempfile.mkdtemp(prefix="rtb_prof_")
     if a.kd_build:
         return kd_build(rt, workloads, a.kd_build, d, a.reps)
+    if a.train_steps:
+        return train_steps(rt, a.train_steps)
     if a.workload == "sphere_grid":
         path, aa, spp = workloads.write_scene(d, "sphere_grid.json", workloads.sphere_grid_scene()), 1, 1
     elif a.workload == "noisy_icosphere":
@@ -57,6 +63,31 @@ def main(argv=None):
     st = r.last_stats
     print(json.dumps({"workload": a.workload, "width": a.width, "height": a.height, "rays": st.rays,
                       "device_ms": st.device_ms}))
+    return 0
+
+
+def train_steps(rt, steps):
+    import time
+    import torch
+    from rtrace_b200 import denoiser
+    from rtrace_b200.dn_train import Trainer
+    ctx = rt.default_context(0)
+    dev = torch.device("cuda", 0)
+    g = torch.Generator(device="cpu").manual_seed(0)
+    f = torch.rand((16, 256, 256, 16), generator=g) * 2 - 0.5
+    f[..., 0] = 1.0
+    f[..., 8] = 1.0
+    f[..., 12] = 1.0
+    feats = f.half().to(dev)
+    targs = torch.rand((16, 2, 256, 256), generator=g).half().to(dev)
+    tr = Trainer(ctx, denoiser.random_net(0), 16, 256, 256)
+    tr.step(feats, targs, 1e-3, want_loss=True)
+    t = time.perf_counter()
+    for _ in range(steps):
+        loss = tr.step(feats, targs, 1e-3, want_loss=True)
+    print(json.dumps({"train_steps": steps, "ms_per_step": (time.perf_counter() - t) * 1e3 / steps,
+                      "loss": list(loss)}))
+    tr.close()
     return 0
 
 
