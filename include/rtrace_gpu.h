@@ -106,10 +106,10 @@ typedef struct rt_render_params {
    * uses the count the loaded network was trained on. */
   uint32_t learned_rays;
   /* learned_shadows with a network that estimates its own error (blob
-   * version 3): a primary hit whose estimated visibility error exceeds
-   * confidence_threshold on one of its disk lights is shaded by the plain
-   * path instead, with fallback_samples rays per disk light (0: as
-   * disk_samples), the first samples of the reference's StdRng stream.
+   * version 3): a primary hit's disk light whose estimated visibility error
+   * exceeds confidence_threshold is shaded by the plain path instead, with
+   * fallback_samples rays (0: as disk_samples), the first samples of the
+   * reference's StdRng stream.
    * confidence_threshold 0 uses the threshold stored with the weights; a
    * negative value turns the fallback off. */
   uint32_t fallback_samples;
@@ -151,7 +151,7 @@ typedef struct rt_stats {
   double device_ms; /* CUDA-event time of the device pipeline */
   double total_ms;  /* host wall time of the whole call */
   double stage_ms[RT_STAGE_COUNT]; /* RT_FLAG_STAGE_TIMES */
-  uint64_t fallback_hits; /* learned shadows: primary hits shaded by the plain fallback */
+  uint64_t fallback_hits; /* learned shadows: primary hits with a light shaded by the plain fallback */
 } rt_stats;
 
 /* ------------------------------------------------------------------ */
@@ -458,14 +458,18 @@ rt_status rt_render_batch(rt_ctx* ctx, rt_job* jobs, uint32_t n, uint32_t lanes,
  *     group: each wavefront kernel is launched once for all of them over a
  *     device table of their launch blocks, the sequence captured as a CUDA
  *     graph and replayed when the same group comes again (0: no group);
+ *   fuse_bytes: the group's frames hold their scratch together, so the
+ *     group takes the smallest eligible frames while their estimated
+ *     scratch stays within this many bytes (the others render on lanes);
  *   blocks_per_sm: grid budget of each fused kernel kind (ray generation,
  *     closest hit, light sampling, shadow rays, shading, reflection fold,
  *     pixels) in blocks per SM, shared out between the group's frames in
  *     proportion to their work bounds.
- * Defaults: 4 lanes, 640 x 480, {16, 64, 64, 128, 16, 16, 16}. */
+ * Defaults: 4 lanes, 640 x 480, 16 GiB, {16, 64, 64, 128, 16, 16, 16}. */
 typedef struct rt_batch_tuning {
   uint32_t lanes;
   uint32_t fuse_pixels;
+  uint64_t fuse_bytes;
   int32_t blocks_per_sm[7];
   uint32_t trials;  /* out (autotune): batches timed */
   double best_ms;   /* out (autotune): wall time of the chosen parameters */

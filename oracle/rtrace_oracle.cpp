@@ -1788,14 +1788,24 @@ struct OutlineCfg {
   bool use8;
   double thickness;
 };
+// Applied to rows [ya, yb) of the image (the whole image in the reference's
+// render; a band of rows for bounded samples, whose first and last
+// 1 + ceil(thickness - 1) rows then lack their neighbours' G-buffers).  The
+// edge mask is computed only where the band's blend reads it.
 static void apply_outline(std::vector<V3>& img, const std::vector<uint8_t>& valid, const std::vector<double>& depth,
-                          const std::vector<V3>& normal, uint32_t W, uint32_t H, const OutlineCfg& cfg) {
+                          const std::vector<V3>& normal, uint32_t W, uint32_t H, const OutlineCfg& cfg,
+                          uint32_t ya = 0, uint32_t yb = UINT32_MAX) {
+  yb = std::min(yb, H);
   auto fg = [&](int64_t x, int64_t y) -> bool {
     if (x < 0 || y < 0 || x >= (int64_t)W || y >= (int64_t)H) return false;
     return valid[(size_t)y * W + x];
   };
+  int32_t radius = 0;
+  if (cfg.thickness > 1.0) radius = std::max(0, sat_i32(std::ceil(cfg.thickness - 1.0)));
+  const uint32_t my0 = ya > (uint32_t)radius ? ya - (uint32_t)radius : 0;
+  const uint32_t my1 = (uint32_t)std::min<int64_t>((int64_t)H, (int64_t)yb + radius);
   std::vector<double> mask((size_t)W * H, 0.0);
-  for (uint32_t y = 0; y < H; y++)
+  for (uint32_t y = my0; y < my1; y++)
     for (uint32_t x = 0; x < W; x++) {
       std::vector<std::pair<int64_t, int64_t>> nb;
       if (cfg.use8) {
@@ -1834,9 +1844,8 @@ static void apply_outline(std::vector<V3>& img, const std::vector<uint8_t>& vali
     }
   std::vector<double> fin = mask;
   if (cfg.thickness > 1.0) {
-    int32_t radius = sat_i32(std::ceil(cfg.thickness - 1.0));
     if (radius > 0) {
-      for (uint32_t y = 0; y < H; y++)
+      for (uint32_t y = ya; y < yb; y++)
         for (uint32_t x = 0; x < W; x++) {
           size_t idx = (size_t)y * W + x;
           double ms = mask[idx];
@@ -1856,7 +1865,7 @@ static void apply_outline(std::vector<V3>& img, const std::vector<uint8_t>& vali
         }
     }
   }
-  for (size_t i = 0; i < img.size(); i++) {
+  for (size_t i = (size_t)ya * W; i < (size_t)yb * W; i++) {
     if (fin[i] > 0.0) {
       double w = rclamp(rmin(fin[i], 1.0), 0.0, 1.0);
       img[i] = v3(img[i].x * (1.0 - w) + cfg.color.x * w, img[i].y * (1.0 - w) + cfg.color.y * w,
@@ -2103,7 +2112,7 @@ static void render(const Scene& s, const RenderOpts& o, std::vector<V3>* out, Co
       (*out)[i] = tot / (double)o.samples;
       if (outline && have) { valid[i] = 1; depth[i] = pd; nrm[i] = pn; }
     }, ct);
-    if (outline && ya == 0 && yb == H) apply_outline(*out, valid, depth, nrm, W, H, ocfg);
+    if (outline) apply_outline(*out, valid, depth, nrm, W, H, ocfg, ya, yb);
   }
 }
 
@@ -2154,9 +2163,10 @@ int oracle_render(const char* scene_path, const char* scene_json, uint32_t width
 }
 
 // As oracle_render, restricted to image rows [y0, y1): the pixels of other
-// rows stay black and the outline pass (which needs whole-image buffers) is
-// skipped unless the band is the whole image.  Used to time bounded samples
-// of a frame for the CPU baseline.
+// rows stay black.  The outline pass runs on the band's rows; its first and
+// last 1 + ceil(thickness - 1) rows lack the neighbouring rows' depth and
+// normals, so only the rows inside them are the reference's.  Used to time
+// bounded samples of a frame (CPU baseline) and to check full-size frames.
 int oracle_render_ex(const char* scene_path, const char* scene_json, uint32_t width, uint32_t height, int aa,
                      uint32_t samples, int max_depth, uint64_t seed, int use_kdtree, int outline, int threads,
                      uint32_t y0, uint32_t y1, uint32_t disk_samples, uint8_t* out_rgb, double* out_linear,

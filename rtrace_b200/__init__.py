@@ -582,7 +582,7 @@ _KINDS = ("raygen", "trace", "emit", "shadow", "resolve", "fold", "pixels")
 
 
 def _tuning_dict(t):
-    return {"lanes": int(t.lanes), "fuse_pixels": int(t.fuse_pixels),
+    return {"lanes": int(t.lanes), "fuse_pixels": int(t.fuse_pixels), "fuse_bytes": int(t.fuse_bytes),
             "blocks_per_sm": {k: int(t.blocks_per_sm[i]) for i, k in enumerate(_KINDS)},
             "trials": int(t.trials), "best_ms": float(t.best_ms)}
 
@@ -602,7 +602,8 @@ def batch_autotune_ex(jobs, ctx=None):
 
 def batch_tuning(ctx=None, **changes):
     """The context's batch parameters (rt_batch_get_tuning); keyword
-    arguments (lanes, fuse_pixels, blocks_per_sm={kind: n}) change them."""
+    arguments (lanes, fuse_pixels, fuse_bytes, blocks_per_sm={kind: n})
+    change them."""
     ctx = ctx or default_context()
     t = _capi.rt_batch_tuning()
     L = _capi.lib()
@@ -614,6 +615,8 @@ def batch_tuning(ctx=None, **changes):
             t.lanes = int(changes["lanes"])
         if "fuse_pixels" in changes:
             t.fuse_pixels = int(changes["fuse_pixels"])
+        if "fuse_bytes" in changes:
+            t.fuse_bytes = int(changes["fuse_bytes"])
         for k, v in changes.get("blocks_per_sm", {}).items():
             t.blocks_per_sm[_KINDS.index(k)] = int(v)
         st = L.rt_batch_set_tuning(ctx.handle, ctypes.byref(t))

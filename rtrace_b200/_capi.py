@@ -117,6 +117,7 @@ class rt_batch_tuning(ctypes.Structure):
     _fields_ = [
         ("lanes", ctypes.c_uint32),
         ("fuse_pixels", ctypes.c_uint32),
+        ("fuse_bytes", ctypes.c_uint64),
         ("blocks_per_sm", ctypes.c_int32 * 7),
         ("trials", ctypes.c_uint32),
         ("best_ms", ctypes.c_double),

@@ -61,11 +61,12 @@ struct DFrame {
   float* vhat;          // denoised visibility, read by k_resolve at level 0
   float* vis_aov;       // optional: per slot visible/dsamp of level-0 hits
   int n_slots;          // disk lights that are denoiser slots (<= DN_MAX_SLOTS)
-  // Confidence-gated fallback (learned shadows): a level-0 hit whose
+  // Confidence-gated fallback (learned shadows): for a level-0 hit whose
   // estimated visibility error (vconf, layout of vhat) exceeds conf_thr on
-  // any slot is shaded by the plain path.  k_fb_select lists such hits in
-  // fb_list (count *fbn) and flags them in fb_flag; launches with fb_mode
-  // set walk fb_list instead of the level's hit list.
+  // some slot, those slots are shaded by the plain path.  k_fb_select lists
+  // such hits in fb_list (count fbn[0]; fbn[1] counts their slots) and
+  // keeps each hit's slot bits in fb_flag; launches with fb_mode set walk
+  // fb_list instead of the level's hit list.
   float* vconf;
   float conf_thr;
   int fb_mode;
@@ -174,7 +175,7 @@ __device__ __forceinline__ void frame_init_body(const DFrame& F, int levels) {
   for (int i = threadIdx.x; i < levels + 1; i += blockDim.x) F.nhits[i] = 0;
   if (threadIdx.x < 16) F.stats[threadIdx.x] = 0;
   if (threadIdx.x == 0) *F.err = 0;
-  if (threadIdx.x == 0 && F.fbn) *F.fbn = 0;
+  if (threadIdx.x < 2 && F.fbn) F.fbn[threadIdx.x] = 0;
 }
 __global__ void k_frame_init(const __grid_constant__ DFrame F, int levels) { frame_init_body(F, levels); }
 // one block per frame
@@ -400,7 +401,11 @@ __device__ __forceinline__ void emit_body(const DFrame& F, int level, long long 
        h += (long long)nblk * blockDim.x) {
     RayC rc;
     uint64_t seed;
-    HitRec hr = load_hit(F, level, F.fb_mode ? F.fb_list[h] : (int)h, &rc, &seed);
+    const int hidx = F.fb_mode ? F.fb_list[h] : (int)h;
+    HitRec hr = load_hit(F, level, hidx, &rc, &seed);
+    // fallback launches sample only the slots that fall back
+    const unsigned fbmask = F.fb_mode ? (unsigned)F.fb_flag[hidx] : ~0u;
+    int dslot = 0;
     V3 so = hr.p + 0.001 * hr.n;
     long long hl = h - c0;
     F.sh.ox[hl] = so.x;
@@ -436,6 +441,9 @@ __device__ __forceinline__ void emit_body(const DFrame& F, int level, long long 
           atomicOr(F.err, ERR_RANGE_OVERFLOW);
           ok = false;
         }
+        // a slot the network is confident about: placeholder rays, never traced
+        if (dslot < F.n_slots && !((fbmask >> dslot) & 1u)) ok = false;
+        dslot++;
         V3 cdir = normalize(lp - hr.p);
         V3 up = fabs(cdir.x) < 0.9 ? mk(1.0, 0.0, 0.0) : mk(0.0, 1.0, 0.0);
         V3 bu = normalize(cross(up, cdir));
@@ -571,6 +579,9 @@ __device__ __forceinline__ void resolve_body(const DFrame& F, int level, long lo
     // learned launch leaves the hits the fallback shades
     const int hi = active ? (F.fb_mode ? F.fb_list[h] : (int)h) : 0;
     if (active && F.learned && level == 0 && F.fb_flag && F.fb_flag[hi]) active = false;
+    // fallback launch: the slots that fall back take the plain sum, the
+    // others keep the network's estimate
+    const unsigned fbmask = (active && F.fb_mode) ? (unsigned)F.fb_flag[hi] : ~0u;
     bool emit = false;
     V3 ro = mk(0, 0, 0), rd = mk(0, 0, 0);
     uint64_t seed = 0;
@@ -602,7 +613,7 @@ __device__ __forceinline__ void resolve_body(const DFrame& F, int level, long lo
           contrib = F.sh.vis[s] ? light_term(m, hr, mk(F.sh.dx[s], F.sh.dy[s], F.sh.dz[s]), lc, L0.intensity, view)
                                 : mk(0.0, 0.0, 0.0);
           s += CH;
-        } else if (learned) {
+        } else if (learned || (F.fb_mode && level == 0 && slot < F.n_slots && !((fbmask >> slot) & 1u))) {
           // extension: the light-centre term times the squared visibility
           // estimate, the expectation of the reference's
           // (sum of visible terms / n) * (visible / n)
@@ -688,23 +699,29 @@ __global__ void __launch_bounds__(128, 8) k_resolve_multi(const DFrame* __restri
 
 
 // Confidence gate of learned shadows: every level-0 hit with an estimated
-// visibility error above conf_thr on one of its slots goes to fb_list (and
-// is flagged in fb_flag), to be shaded by the plain path.
+// visibility error above conf_thr on one of its slots goes to fb_list, with
+// those slots' bits in fb_flag, to be shaded by the plain path.
 __global__ void __launch_bounds__(128) k_fb_select(DFrame F) {
   const long long nh = F.nhits[0];
   const long long plane_px = (long long)F.H * F.W;
   for (long long base = blockIdx.x * (long long)blockDim.x; base < nh; base += (long long)gridDim.x * blockDim.x) {
     const long long h = base + threadIdx.x;
     bool want = false;
+    unsigned slots = 0;
     if (h < nh) {
       const int i = F.hit_ray[h];
       const long long pix = i / F.S_per_px, plane = i % F.S_per_px;
+      unsigned mask = 0;
       for (int j = 0; j < F.n_slots; j++)
-        want |= F.vconf[(plane * DN_MAX_SLOTS + j) * plane_px + pix] > F.conf_thr;
-      F.fb_flag[h] = want ? 1 : 0;
+        if (F.vconf[(plane * DN_MAX_SLOTS + j) * plane_px + pix] > F.conf_thr) mask |= 1u << j;
+      F.fb_flag[h] = (unsigned char)mask;
+      want = mask != 0;
+      slots = __popc(mask);
     }
     const int at = warp_alloc(F.fbn, want);  // every lane of the warp takes part
     if (want) F.fb_list[at] = (int)h;
+    slots = __reduce_add_sync(0xffffffffu, slots);
+    if ((threadIdx.x & 31) == 0 && slots) atomicAdd(F.fbn + 1, slots);
   }
 }
 

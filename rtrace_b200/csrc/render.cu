@@ -136,6 +136,7 @@ struct rt_ctx {
   // hold their scratch (child contexts), group_buf their frame table.
   std::vector<rt_ctx*> slots;
   uint32_t fuse_pixels = 640 * 480;
+  uint64_t fuse_bytes = 16ull << 30;  // scratch the group's frames may hold together (estimated)
   int tune_bpsm[7] = {16, 64, 64, 128, 16, 16, 16};  // blocks per SM: raygen trace emit shadow resolve fold pixels
   bool tuned = false;
   void* group_buf = nullptr;
@@ -296,7 +297,7 @@ rt_status ensure_dn_scratch(rt_ctx* ctx, long long n) {
   CK(dalloc(o, &ctx->d_vconf, n * DN_MAX_SLOTS));
   CK(dalloc(o, &ctx->d_fb_list, n));
   CK(dalloc(o, &ctx->d_fb_flag, n));
-  CK(dalloc(o, &ctx->d_fbn, 1));
+  CK(dalloc(o, &ctx->d_fbn, 2));
   ctx->dn_cap = n;
   return RT_OK;
 }
@@ -1733,8 +1734,8 @@ rt_status render_impl(rt_ctx* ctx, const rt_scene* sc, const rt_render_params* P
   CK(cudaMemcpyAsync(nh.data(), ctx->d_nhits, (levels + 1) * sizeof(int), cudaMemcpyDeviceToHost, s));
   CK(cudaMemcpyAsync(hstats, ctx->d_stats, sizeof hstats, cudaMemcpyDeviceToHost, s));
   CK(cudaMemcpyAsync(&herr, ctx->d_err, sizeof(int), cudaMemcpyDeviceToHost, s));
-  int hfb = 0;
-  if (fallback) CK(cudaMemcpyAsync(&hfb, ctx->d_fbn, sizeof(int), cudaMemcpyDeviceToHost, s));
+  int hfb[2] = {0, 0};  // fallback hits, fallback slots
+  if (fallback) CK(cudaMemcpyAsync(hfb, ctx->d_fbn, sizeof hfb, cudaMemcpyDeviceToHost, s));
   cudaError_t se = cudaStreamSynchronize(s);
   free_all(tmp);
   if (se != cudaSuccess) return cuda_fail(ctx, se, "render");
@@ -1755,9 +1756,11 @@ rt_status render_impl(rt_ctx* ctx, const rt_scene* sc, const rt_render_params* P
       for (int l = 0; l < levels; l++) hits += (uint64_t)nh[l];
       stats->reflection_rays = refl;
       stats->hits = hits;
+      // fallback hits recast their point lights and fb_dsamp rays per slot
+      // that falls back
       stats->shadow_rays = (uint64_t)nh[0] * (uint64_t)K_0 + (hits - (uint64_t)nh[0]) * (uint64_t)K_full +
-                           (uint64_t)hfb * (uint64_t)K_fb;
-      stats->fallback_hits = (uint64_t)hfb;
+                           (uint64_t)hfb[0] * (uint64_t)sc->n_point_lights + (uint64_t)hfb[1] * (uint64_t)fb_dsamp;
+      stats->fallback_hits = (uint64_t)hfb[0];
       stats->trace_nodes = hstats[2];
       stats->trace_triangles = hstats[3];
       stats->trace_spheres = hstats[4];
@@ -2474,6 +2477,7 @@ rt_status rt_render_batch(rt_ctx* ctx, rt_job* jobs, uint32_t n, uint32_t lanes,
   std::vector<double> cost(n, 0.0);
   std::vector<uint32_t> fused;
   std::vector<char> in_group(n, 0);
+  std::vector<double> scratch(n, 0.0);  // estimated scratch bytes of a fused frame
   for (uint32_t i = 0; i < n; i++) {
     const rt_render_params& P = jobs[i].params;
     const rt_scene* sc = jobs[i].scene;
@@ -2490,9 +2494,23 @@ rt_status rt_render_batch(rt_ctx* ctx, rt_job* jobs, uint32_t n, uint32_t lanes,
     if (ctx->fuse_pixels && sc && jobs[i].rgb_out && (uint64_t)P.width * P.height <= ctx->fuse_pixels &&
         !P.learned_shadows && !outline && P.max_depth > 0 && P.max_depth <= RTB_MAX_LEVELS && P.samples > 0 &&
         !(P.flags & (RT_FLAG_STAGE_TIMES | RT_FLAG_COUNT_WORK)) && nprim * std::max(K, 1.0) <= (double)kShadowCap) {
+      // a fused frame keeps all its scratch at once: per primary ray the
+      // queues, hit records, per-level colours and outline data, its whole
+      // shadow buffer (K rays of 33 bytes, 24 bytes of origin per hit), and
+      // about 80 bytes per pixel
+      const double levels = std::max(1, std::min(P.max_depth, RTB_MAX_LEVELS));
+      scratch[i] = nprim * (173.0 + 36.0 * levels + 33.0 * K + 24.0) + (double)P.width * P.height * 80.0;
       fused.push_back(i);
-      in_group[i] = 1;
     }
+  }
+  // the smallest frames first, while the estimated scratch fits the budget
+  std::stable_sort(fused.begin(), fused.end(), [&](uint32_t a, uint32_t b) { return scratch[a] < scratch[b]; });
+  {
+    double used = 0.0;
+    size_t keep = 0;
+    while (keep < fused.size() && used + scratch[fused[keep]] <= (double)ctx->fuse_bytes) used += scratch[fused[keep++]];
+    fused.resize(keep);
+    for (uint32_t i : fused) in_group[i] = 1;
   }
   if (fused.size() < 2) {  // one frame gains nothing from fusion
     fused.clear();
@@ -2579,6 +2597,7 @@ rt_status rt_batch_get_tuning(rt_ctx* ctx, rt_batch_tuning* out) {
   memset(out, 0, sizeof *out);
   out->lanes = ctx->tuned_lanes ? ctx->tuned_lanes : 4;
   out->fuse_pixels = ctx->fuse_pixels;
+  out->fuse_bytes = ctx->fuse_bytes;
   for (int k = 0; k < 7; k++) out->blocks_per_sm[k] = ctx->tune_bpsm[k];
   return RT_OK;
 }
@@ -2591,6 +2610,7 @@ rt_status rt_batch_set_tuning(rt_ctx* ctx, const rt_batch_tuning* t) {
       return fail(ctx, RT_ERR_INVALID_ARGUMENT, "blocks_per_sm must be 1..1024");
   ctx->tuned_lanes = t->lanes;
   ctx->fuse_pixels = t->fuse_pixels;
+  ctx->fuse_bytes = t->fuse_bytes;
   for (int k = 0; k < 7; k++) ctx->tune_bpsm[k] = t->blocks_per_sm[k];
   return RT_OK;
 }

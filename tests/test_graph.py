@@ -129,17 +129,24 @@ def test_replay_to_device_output_and_in_batches(gpu_ctx):
     assert states == [1, 2, 1]  # a new output pointer is a new sequence
     for buf in bufs:
         assert np.array_equal(buf.cpu().numpy(), want)
-    # batch jobs with the flag: each lane captures its jobs, a second batch
-    # replays them (every job shares `r`, whose stats are the last job's)
+    # batch jobs with the flag, outside a fused group (a fused group is always
+    # one captured sequence, tests/test_batch.py): each lane captures its
+    # jobs, a second batch replays them (every job shares `r`, whose stats
+    # are the last job's)
     cams = list(rt.auto_cameras(json_text=json.dumps(js)).values())[:3]
-    r.flags = 0
-    plain, _ = rt.render_batch([rt.Job(scene, r, cam) for cam in cams], lanes=2, ctx=gpu_ctx)
-    r.flags = _capi.RT_FLAG_CUDA_GRAPH
-    jobs = [rt.Job(scene, r, cam) for cam in cams]
-    for k in range(2):
-        imgs, _ = rt.render_batch(jobs, lanes=2, ctx=gpu_ctx)
-        assert r.last_stats.graph == k + 1
-        assert all(np.array_equal(a, b) for a, b in zip(imgs, plain))
+    saved = rt.batch_tuning(gpu_ctx)["fuse_pixels"]
+    rt.batch_tuning(gpu_ctx, fuse_pixels=0)
+    try:
+        r.flags = 0
+        plain, _ = rt.render_batch([rt.Job(scene, r, cam) for cam in cams], lanes=2, ctx=gpu_ctx)
+        r.flags = _capi.RT_FLAG_CUDA_GRAPH
+        jobs = [rt.Job(scene, r, cam) for cam in cams]
+        for k in range(2):
+            imgs, _ = rt.render_batch(jobs, lanes=2, ctx=gpu_ctx)
+            assert r.last_stats.graph == k + 1
+            assert all(np.array_equal(a, b) for a, b in zip(imgs, plain))
+    finally:
+        rt.batch_tuning(gpu_ctx, fuse_pixels=saved)
     scene.close()
 
 
