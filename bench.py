@@ -235,7 +235,7 @@ def learned_vs_plain(rt, torch, ctx, directory, steps, hbm=6650.0, tflops=1590.0
             r.disk_samples = rays
         r.render_shadow_aov(scene, vis[key].data_ptr(), None if fp is None else fp.data_ptr())
         if key == "learned":
-            fb_hits, hits = r.last_stats.fallback_hits, r.last_stats.hits
+            fb_hits, fb_lights, hits = r.last_stats.fallback_hits, r.last_stats.fallback_lights, r.last_stats.hits
     mask = denoiser.masks(feat)
     raw = torch.stack([lfeat[..., 5], lfeat[..., 9]], 1).float()
 
@@ -253,7 +253,9 @@ def learned_vs_plain(rt, torch, ctx, directory, steps, hbm=6650.0, tflops=1590.0
            "visibility": {"plain_16": score(vis["plain_16"]), "learned": score(vis["learned"]),
                           "network_only": score(vis["network_only"]), "raw_1_ray": score(raw),
                           "plain_64_vs_1024": score(vis["t64"])["vs_1024"]},
-           "fallback_share": fb_hits / max(1, hits), "fallback_rays_per_light": PLAIN_RAYS}
+           "fallback_share": {"hit_samples": fb_hits / max(1, hits),
+                              "sample_lights": fb_lights / max(1, int(mask.sum().item()))},
+           "fallback_rays_per_light": PLAIN_RAYS}
     img = torch.empty(W * H * 3, dtype=torch.uint8, device=dev)
     flush = torch.empty(512 * 1024 * 1024, dtype=torch.uint8, device=dev)
     for mode in ("plain_64", "plain_16", "learned", "learned_refl64"):
@@ -506,7 +508,8 @@ def terrain_learned(rt, ctx, scene, cams, reps):
         torch.cuda.synchronize(dev)
         r.render_shadow_aov(scene, vis[key].data_ptr(), feat.data_ptr() if key == "t64" else None)
         if key == "learned":
-            out["fallback_share"] = r.last_stats.fallback_hits / max(1, r.last_stats.hits)
+            out["fallback_share"] = {"hit_samples": r.last_stats.fallback_hits / max(1, r.last_stats.hits),
+                                     "fallback_lights": r.last_stats.fallback_lights}
     m = denoiser.masks(feat)
     out["vis_psnr_db_vs_64"] = denoiser.psnr(vis["learned"], vis["t64"], m)
     out["vis_max_abs_err_vs_64"] = float((vis["learned"][m] - vis["t64"][m]).abs().max().item())

@@ -113,6 +113,7 @@ pub mod ffi {
         pub total_ms: f64,
         pub stage_ms: [f64; RT_STAGE_COUNT],
         pub fallback_hits: u64,
+        pub fallback_lights: u64,
     }
 
     extern "C" {

@@ -151,7 +151,8 @@ typedef struct rt_stats {
   double device_ms; /* CUDA-event time of the device pipeline */
   double total_ms;  /* host wall time of the whole call */
   double stage_ms[RT_STAGE_COUNT]; /* RT_FLAG_STAGE_TIMES */
-  uint64_t fallback_hits; /* learned shadows: primary hits with a light shaded by the plain fallback */
+  uint64_t fallback_hits;   /* learned shadows: primary hits with a light shaded by the plain fallback */
+  uint64_t fallback_lights; /* learned shadows: (primary hit, disk light) pairs shaded by the fallback */
 } rt_stats;
 
 /* ------------------------------------------------------------------ */

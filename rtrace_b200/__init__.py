@@ -91,7 +91,8 @@ class RenderStats:
     stage_ms: dict = field(default_factory=dict)
     work: dict = field(default_factory=dict)
     graph: int = 0  # RT_FLAG_CUDA_GRAPH: 1 captured by this render, 2 replayed
-    fallback_hits: int = 0  # learned shadows: primary hits shaded by the plain fallback
+    fallback_hits: int = 0  # learned shadows: primary hits with a light shaded by the plain fallback
+    fallback_lights: int = 0  # learned shadows: (primary hit, disk light) pairs shaded by it
 
     @property
     def rays(self):
@@ -105,7 +106,7 @@ class RenderStats:
         stages = {name: float(st.stage_ms[i]) for i, name in enumerate(_capi.STAGES)}
         return cls(int(st.primary_rays), int(st.reflection_rays), int(st.shadow_rays), float(st.device_ms),
                    float(st.total_ms), int(st.hits), int(st.kernel_launches), stages, work, int(st.graph),
-                   int(st.fallback_hits))
+                   int(st.fallback_hits), int(st.fallback_lights))
 
 
 class Context:

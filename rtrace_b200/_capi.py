@@ -110,6 +110,7 @@ class rt_stats(ctypes.Structure):
         ("total_ms", ctypes.c_double),
         ("stage_ms", ctypes.c_double * 8),
         ("fallback_hits", ctypes.c_uint64),
+        ("fallback_lights", ctypes.c_uint64),
     ]
 
 

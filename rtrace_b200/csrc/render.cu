@@ -1761,6 +1761,7 @@ rt_status render_impl(rt_ctx* ctx, const rt_scene* sc, const rt_render_params* P
       stats->shadow_rays = (uint64_t)nh[0] * (uint64_t)K_0 + (hits - (uint64_t)nh[0]) * (uint64_t)K_full +
                            (uint64_t)hfb[0] * (uint64_t)sc->n_point_lights + (uint64_t)hfb[1] * (uint64_t)fb_dsamp;
       stats->fallback_hits = (uint64_t)hfb[0];
+      stats->fallback_lights = (uint64_t)hfb[1];
       stats->trace_nodes = hstats[2];
       stats->trace_triangles = hstats[3];
       stats->trace_spheres = hstats[4];

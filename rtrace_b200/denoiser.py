@@ -381,18 +381,18 @@ def psnr(est, ref, mask):
 
 
 def gated(vis, conf, target, mask, threshold):
-    """The visibility a render with the confidence-gated fallback uses: the
-    network's estimate, or at a sample whose estimated error exceeds the
-    threshold on a present slot the plain path's (= target, same samples).
-    Returns (visibility, fraction of hit samples that fall back)."""
+    """The visibility a render with the confidence-gated fallback uses: per
+    sample and present light, the network's estimate, or where its estimated
+    error exceeds the threshold the plain path's (= target: the same
+    samples).  Returns (visibility, fraction of the sample-light pairs that
+    fall back)."""
     import torch
-    fb = ((conf > threshold) & mask).any(1, keepdim=True)
-    hit = mask.any(1, keepdim=True)
-    share = (fb & hit).sum().item() / max(1, hit.sum().item())
-    return torch.where(fb.expand_as(vis), target, vis), share
+    fb = (conf > threshold) & mask
+    share = fb.sum().item() / max(1, mask.sum().item())
+    return torch.where(fb, target, vis), share
 
 
-def choose_threshold(vis, conf, target, mask, target_db=41.0, max_share=0.35):
+def choose_threshold(vis, conf, target, mask, target_db=40.5, max_share=0.35):
     """The largest threshold whose gated visibility reaches target_db PSNR
     against the target on these (validation) samples, among the error
     estimates' quantiles; if none does within max_share fallback, the
@@ -490,7 +490,7 @@ def evaluate(net, feats, targs, batch=32):
 
 
 def train(out_path, n_scenes=2000, n_val=60, width=1920, height=1080, iters=8000, batch=16, crop=256, seed=0, rays=1,
-          target_samples=64, engine="native", target_db=41.0, log=print):
+          target_samples=64, engine="native", target_db=40.5, log=print):
     """Renders the training set (n_scenes scenes) and a validation set
     (n_val other scenes), fits UNET (engine "native": the library's own
     tensor-core training kernels; "torch": PyTorch autograd), picks the
@@ -514,8 +514,8 @@ def train(out_path, n_scenes=2000, n_val=60, width=1920, height=1080, iters=8000
     m = masks(vf)
     thr, p, share = choose_threshold(vis, conf, vt, m, target_db)
     net.threshold = thr
-    log("validation: visibility PSNR %.2f dB without fallback; threshold %.4f -> %.2f dB with %.1f%% of hit "
-        "samples falling back" % (psnr(vis, vt, m), thr, p, 100 * share))
+    log("validation: visibility PSNR %.2f dB without fallback; threshold %.4f -> %.2f dB with %.1f%% of the "
+        "hit-sample lights falling back" % (psnr(vis, vt, m), thr, p, 100 * share))
     blob = pack_net(net)
     with open(out_path, "wb") as f:
         f.write(blob)
@@ -537,7 +537,7 @@ def main(argv=None):
     ap.add_argument("--target-samples", type=int, default=64)
     ap.add_argument("--engine", choices=["native", "torch"], default="native",
                     help="native: the library's tcgen05 training kernels; torch: PyTorch autograd")
-    ap.add_argument("--target-db", type=float, default=41.0)
+    ap.add_argument("--target-db", type=float, default=40.5)
     ap.add_argument("--log", default=None)
     a = ap.parse_args(argv)
     logf = open(a.log, "w") if a.log else None
