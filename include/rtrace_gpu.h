@@ -546,8 +546,10 @@ typedef struct rt_dn_trainer rt_dn_trainer;
 rt_status rt_dn_train_create(rt_ctx* ctx, const void* blob, size_t bytes, uint32_t planes, uint32_t height,
                              uint32_t width, rt_dn_trainer** out);
 /* One optimisation step (Adam with bias correction on the mean loss
- * gradient); loss (optional, host, 3 floats): masked sample count, sum of
- * the visibility term, sum of the error term. */
+ * gradient); loss (optional, host, 4 floats): masked sample count, sum of
+ * the visibility term, sum of the error term, and the gradient entries that
+ * were not finite (an FP16 activation gradient overflowed; the step is then
+ * skipped and the weights keep their values). */
 rt_status rt_dn_train_step(rt_dn_trainer* t, const uint16_t* features, const uint16_t* targets, float lr,
                            float beta1, float beta2, float eps, float* loss);
 /* The gradient of the summed loss with respect to every parameter (host,

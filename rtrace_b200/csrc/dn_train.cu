@@ -452,10 +452,21 @@ __global__ void k_loss(const float* vis, const float* conf, const __half* target
   }
 }
 
+// Non-finite gradient entries (an FP16 activation gradient that overflowed
+// the loss scale) into acc[3].
+__global__ void k_grad_check(const float* grad, long long n, float* acc) {
+  float bad = 0.f;
+  RTB_GRID_STRIDE(i, n) bad += isfinite(grad[i]) ? 0.f : 1.f;
+  for (int off = 16; off > 0; off >>= 1) bad += __shfl_down_sync(0xffffffffu, bad, off);
+  if ((threadIdx.x & 31) == 0 && bad > 0.f) atomicAdd(&acc[3], bad);
+}
+
 // Adam on the FP32 masters (weights [cout][3][3][cin] then bias, per
-// convolution, concatenated): g = grad / (loss scale * masked count).
+// convolution, concatenated): g = grad / (loss scale * masked count).  A
+// step whose gradient has a non-finite entry (acc[3] > 0) is skipped.
 __global__ void k_adam(float* w, float* m, float* v, const float* grad, long long n, const float* acc, float lr,
                        float b1, float b2, float eps, float bc1, float bc2) {
+  if (acc[3] > 0.f) return;
   const float denom = kLossScale * fmaxf(acc[0], 1.f);
   RTB_GRID_STRIDE(i, n) {
     const float g = grad[i] / denom;
@@ -809,6 +820,7 @@ rt_status rt_dn_train_step(rt_dn_trainer* t, const uint16_t* features, const uin
   cudaStream_t s = ctx_stream(t->ctx);
   t->steps++;
   const float bc1 = 1.f - std::pow(beta1, (float)t->steps), bc2 = 1.f - std::pow(beta2, (float)t->steps);
+  k_grad_check<<<grid_for(t->n_params, ctx_num_sms(t->ctx)), 256, 0, s>>>(t->grad, t->n_params, t->acc);
   k_adam<<<grid_for(t->n_params, ctx_num_sms(t->ctx)), 256, 0, s>>>(t->master, t->m1, t->m2, t->grad, t->n_params,
                                                                      t->acc, lr, beta1, beta2, eps, bc1, bc2);
   if (loss) {
@@ -823,6 +835,7 @@ rt_status rt_dn_train_step(rt_dn_trainer* t, const uint16_t* features, const uin
     loss[0] = hacc[0];
     loss[1] = hacc[1];
     loss[2] = hacc[2];
+    loss[3] = hacc[3];
   } else if (cudaGetLastError() != cudaSuccess) {
     return ctx_fail(t->ctx, RT_ERR_CUDA, "training step launch failed");
   }

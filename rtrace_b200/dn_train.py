@@ -49,9 +49,10 @@ class Trainer:
 
     def step(self, feats, targs, lr, beta1=0.9, beta2=0.999, eps=1e-8, want_loss=False):
         """One Adam step on a batch (device tensors).  With want_loss, returns
-        (masked count, visibility loss sum, error loss sum)."""
+        (masked count, visibility loss sum, error loss sum, non-finite
+        gradient entries: the step was skipped when this is not 0)."""
         f, t = self._args(feats, targs)
-        loss = (ctypes.c_float * 3)() if want_loss else None
+        loss = (ctypes.c_float * 4)() if want_loss else None
         self._check(_capi.lib().rt_dn_train_step(self.handle, f, t, lr, beta1, beta2, eps, loss))
         return tuple(loss) if want_loss else None
 
@@ -94,7 +95,7 @@ class Trainer:
             pass
 
 
-def fit_native(ctx, net, feats, targs, iters=8000, batch=16, lr=2e-3, seed=0, log=print):
+def fit_native(ctx, net, feats, targs, iters=8000, batch=16, lr=1e-3, seed=0, log=print):
     """Adam on the library's training kernels with a one-cycle learning-rate
     schedule (5% warm-up, cosine decay); returns the fitted Net."""
     import torch
@@ -115,9 +116,10 @@ def fit_native(ctx, net, feats, targs, iters=8000, batch=16, lr=2e-3, seed=0, lo
         report = it % 500 == 0 or it == iters - 1
         loss = tr.step(fb, tb, a, want_loss=report)
         if report:
-            cnt, lv, lc = loss
-            log("iter %d loss %.6f vis-mse %.6f (%.1f s, native kernels)" %
-                (it, (lv + lc) / max(cnt, 1), lv / max(cnt, 1), time.time() - t0))
+            cnt, lv, lc, bad = loss
+            log("iter %d loss %.6f vis-mse %.6f%s (%.1f s, native kernels)" %
+                (it, (lv + lc) / max(cnt, 1), lv / max(cnt, 1), " (step skipped: non-finite gradient)" if bad else "",
+                 time.time() - t0))
     out = tr.export()
     tr.close()
     return out
