@@ -490,7 +490,7 @@ def evaluate(net, feats, targs, batch=32):
 
 
 def train(out_path, n_scenes=2000, n_val=60, width=1920, height=1080, iters=8000, batch=16, crop=256, seed=0, rays=1,
-          target_samples=64, engine="native", target_db=40.5, log=print):
+          target_samples=64, engine="native", target_db=40.5, lr=None, log=print):
     """Renders the training set (n_scenes scenes) and a validation set
     (n_val other scenes), fits UNET (engine "native": the library's own
     tensor-core training kernels; "torch": PyTorch autograd), picks the
@@ -505,10 +505,10 @@ def train(out_path, n_scenes=2000, n_val=60, width=1920, height=1080, iters=8000
     log("rendered %d training and %d validation crops in %.1f s" % (len(feats), len(vf), time.time() - t0))
     net = random_net(seed, UNET, rays=rays)
     if engine == "torch":
-        net = fit_torch(net, feats, targs, iters, batch, seed=seed, log=log)
+        net = fit_torch(net, feats, targs, iters, batch, lr=lr or 2e-3, seed=seed, log=log)
     else:
         from . import dn_train
-        net = dn_train.fit_native(ctx, net, feats, targs, iters, batch, seed=seed, log=log)
+        net = dn_train.fit_native(ctx, net, feats, targs, iters, batch, lr=lr or 1e-3, seed=seed, log=log)
     vis, conf = evaluate(net, vf, vt)
     vt = vt.float()
     m = masks(vf)
@@ -538,6 +538,7 @@ def main(argv=None):
     ap.add_argument("--engine", choices=["native", "torch"], default="native",
                     help="native: the library's tcgen05 training kernels; torch: PyTorch autograd")
     ap.add_argument("--target-db", type=float, default=40.5)
+    ap.add_argument("--lr", type=float, default=None, help="peak learning rate (native: 1e-3, torch: 2e-3)")
     ap.add_argument("--log", default=None)
     a = ap.parse_args(argv)
     logf = open(a.log, "w") if a.log else None
@@ -550,7 +551,7 @@ def main(argv=None):
 
     train(a.out, n_scenes=a.scenes, n_val=a.val_scenes, width=a.width, height=a.height, iters=a.iters,
           batch=a.batch, rays=a.rays, target_samples=a.target_samples, engine=a.engine, target_db=a.target_db,
-          log=log)
+          lr=a.lr, log=log)
     return 0
 
 
