@@ -856,6 +856,7 @@ def main():
             "roofline": roofline,
             "stage_ms": {k: round(v, 4) for k, v in stages.items()},
             "work_per_frame": w,
+            "shadow_rays_untraced_per_frame": prof.shadow_rays_untraced,
             "cpu_baseline": cpu,
             "learned_vs_plain": learned,
             "batch": batch,

@@ -114,6 +114,7 @@ pub mod ffi {
         pub stage_ms: [f64; RT_STAGE_COUNT],
         pub fallback_hits: u64,
         pub fallback_lights: u64,
+        pub shadow_rays_untraced: u64,
     }
 
     extern "C" {

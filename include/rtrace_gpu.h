@@ -153,6 +153,11 @@ typedef struct rt_stats {
   double stage_ms[RT_STAGE_COUNT]; /* RT_FLAG_STAGE_TIMES */
   uint64_t fallback_hits;   /* learned shadows: primary hits with a light shaded by the plain fallback */
   uint64_t fallback_lights; /* learned shadows: (primary hit, disk light) pairs shaded by the fallback */
+  /* Shadow rays (counted in shadow_rays, which counts the rays the
+   * reference casts) that were not traced because the surface faces away
+   * from the light: the reference's contribution of that light is exactly
+   * zero whatever they hit. */
+  uint64_t shadow_rays_untraced;
 } rt_stats;
 
 /* ------------------------------------------------------------------ */

@@ -93,6 +93,7 @@ class RenderStats:
     graph: int = 0  # RT_FLAG_CUDA_GRAPH: 1 captured by this render, 2 replayed
     fallback_hits: int = 0  # learned shadows: primary hits with a light shaded by the plain fallback
     fallback_lights: int = 0  # learned shadows: (primary hit, disk light) pairs shaded by it
+    shadow_rays_untraced: int = 0  # counted shadow rays not traced: the surface faces away from the light
 
     @property
     def rays(self):
@@ -106,7 +107,7 @@ class RenderStats:
         stages = {name: float(st.stage_ms[i]) for i, name in enumerate(_capi.STAGES)}
         return cls(int(st.primary_rays), int(st.reflection_rays), int(st.shadow_rays), float(st.device_ms),
                    float(st.total_ms), int(st.hits), int(st.kernel_launches), stages, work, int(st.graph),
-                   int(st.fallback_hits), int(st.fallback_lights))
+                   int(st.fallback_hits), int(st.fallback_lights), int(st.shadow_rays_untraced))
 
 
 class Context:

@@ -111,6 +111,7 @@ class rt_stats(ctypes.Structure):
         ("stage_ms", ctypes.c_double * 8),
         ("fallback_hits", ctypes.c_uint64),
         ("fallback_lights", ctypes.c_uint64),
+        ("shadow_rays_untraced", ctypes.c_uint64),
     ]
 
 

@@ -397,6 +397,7 @@ __device__ __forceinline__ void emit_body(const DFrame& F, int level, long long 
   long long nh = F.fb_mode ? *F.fbn : F.nhits[level];
   long long c1 = c0 + F.chunk_hits < nh ? c0 + F.chunk_hits : nh;
   V3 campos = ld3(F.C.campos);
+  unsigned long long culled = 0;  // shadow rays not traced (lights facing away)
   for (long long h = c0 + bid * (long long)blockDim.x + threadIdx.x; h < c1;
        h += (long long)nblk * blockDim.x) {
     RayC rc;
@@ -406,6 +407,16 @@ __device__ __forceinline__ void emit_body(const DFrame& F, int level, long long 
     // fallback launches sample only the slots that fall back
     const unsigned fbmask = F.fb_mode ? (unsigned)F.fb_flag[hidx] : ~0u;
     int dslot = 0;
+    // Lights the surface faces away from: the reference's light term is
+    // exactly zero there (diffuse max(n . l, 0) = 0, specular only when
+    // n . l > 0), so their shadow rays cannot change the image and are not
+    // traced (distance -1).  A disk light qualifies when every point of the
+    // disk is behind the surface: n . (centre - p) + radius < 0, with a
+    // margin far above the rounding of the sample directions' dot products.
+    // Not where the rays' visibility is itself an output (the denoiser's
+    // features and visibility images at level 0, the fallback).
+    const bool may_cull = !F.fb_mode && !(level == 0 && F.feat_on);
+    const double pscale = norm(hr.p) + 1.0;
     V3 so = hr.p + 0.001 * hr.n;
     long long hl = h - c0;
     F.sh.ox[hl] = so.x;
@@ -421,10 +432,12 @@ __device__ __forceinline__ void emit_body(const DFrame& F, int level, long long 
         V3 lv = lp - hr.p;
         double dist = norm(lv);
         V3 ldir = lv / dist;
+        const bool cull = may_cull && dot(hr.n, lv) < -1e-9 * (norm(lp) + pscale);
+        culled += cull ? 1 : 0;
         F.sh.dx[s] = ldir.x;
         F.sh.dy[s] = ldir.y;
         F.sh.dz[s] = ldir.z;
-        F.sh.dist[s] = dist;
+        F.sh.dist[s] = cull ? -1.0 : dist;
         s += CH;
       } else {
         // calculate_diffuse_light_contribution (src/lighting.rs:145-217),
@@ -444,6 +457,10 @@ __device__ __forceinline__ void emit_body(const DFrame& F, int level, long long 
         // a slot the network is confident about: placeholder rays, never traced
         if (dslot < F.n_slots && !((fbmask >> dslot) & 1u)) ok = false;
         dslot++;
+        if (ok && may_cull && dot(hr.n, lp - hr.p) + radius < -1e-9 * (norm(lp) + pscale + radius)) {
+          ok = false;  // facing away from the whole disk
+          culled += (unsigned long long)F.dsamp;
+        }
         V3 cdir = normalize(lp - hr.p);
         V3 up = fabs(cdir.x) < 0.9 ? mk(1.0, 0.0, 0.0) : mk(0.0, 1.0, 0.0);
         V3 bu = normalize(cross(up, cdir));
@@ -490,6 +507,7 @@ __device__ __forceinline__ void emit_body(const DFrame& F, int level, long long 
       }
     }
   }
+  warp_sum_add(F.stats + 10, culled);
 }
 __global__ void __launch_bounds__(128) k_emit(const __grid_constant__ DFrame F, int level, long long c0) {
   emit_body(F, level, c0, blockIdx.x, gridDim.x);

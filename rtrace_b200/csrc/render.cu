@@ -1762,6 +1762,7 @@ rt_status render_impl(rt_ctx* ctx, const rt_scene* sc, const rt_render_params* P
                            (uint64_t)hfb[0] * (uint64_t)sc->n_point_lights + (uint64_t)hfb[1] * (uint64_t)fb_dsamp;
       stats->fallback_hits = (uint64_t)hfb[0];
       stats->fallback_lights = (uint64_t)hfb[1];
+      stats->shadow_rays_untraced = hstats[10];
       stats->trace_nodes = hstats[2];
       stats->trace_triangles = hstats[3];
       stats->trace_spheres = hstats[4];
@@ -1947,6 +1948,7 @@ rt_status run_fused(rt_ctx* parent, rt_ctx* lane, rt_job* jobs, const std::vecto
   struct Back {
     std::vector<int> counts, nh;
     int err = 0;
+    unsigned long long untraced = 0;
   };
   std::vector<Back> back(nj);
   for (int j = 0; j < nj; j++) {
@@ -1960,6 +1962,7 @@ rt_status run_fused(rt_ctx* parent, rt_ctx* lane, rt_job* jobs, const std::vecto
     CK(cudaMemcpyAsync(back[j].counts.data(), sl->d_counts, (pl.levels + 2) * sizeof(int), cudaMemcpyDeviceToHost, s));
     CK(cudaMemcpyAsync(back[j].nh.data(), sl->d_nhits, (pl.levels + 1) * sizeof(int), cudaMemcpyDeviceToHost, s));
     CK(cudaMemcpyAsync(&back[j].err, sl->d_err, sizeof(int), cudaMemcpyDeviceToHost, s));
+    CK(cudaMemcpyAsync(&back[j].untraced, sl->d_stats + 10, sizeof(unsigned long long), cudaMemcpyDeviceToHost, s));
   }
   cudaError_t se = cudaStreamSynchronize(s);
   if (se != cudaSuccess) return cuda_fail(lane, se, "fused batch group");
@@ -1991,6 +1994,7 @@ rt_status run_fused(rt_ctx* parent, rt_ctx* lane, rt_job* jobs, const std::vecto
     S.reflection_rays = refl;
     S.hits = hits;
     S.shadow_rays = hits * (uint64_t)pl.K;
+    S.shadow_rays_untraced = back[j].untraced;
     S.kernel_launches = launches;  // shared by the group
     S.graph = graph_state;
     S.device_ms = ms;  // the group's time, shared by its frames

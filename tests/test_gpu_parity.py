@@ -243,6 +243,18 @@ def test_modes_match_oracle(gpu_ctx, tmp_path, aa, samples):
         assert (st.primary_rays, st.reflection_rays, st.shadow_rays) == (int(cnt[0]), int(cnt[1]), int(cnt[2])), name
 
 
+def test_facing_away_lights_are_not_traced(gpu_ctx, tmp_path):
+    """Shadow rays toward a light the surface faces away from are not traced
+    (the reference's light term is exactly zero there); the image stays the
+    reference's and the rays are still counted as the reference casts them."""
+    paths = _synthetic_scenes(tmp_path)
+    for name in ("icosphere", "rings", "mixed"):
+        img, st = gpu_render(paths[name], 80, 50, "no-jitter")
+        ref, cnt = oracle_lib.render(paths[name], width=80, height=50, aa="no-jitter", counts=True)
+        assert np.array_equal(img, ref), name
+        assert st.shadow_rays == int(cnt[2]) and 0 < st.shadow_rays_untraced < st.shadow_rays, name
+
+
 def test_brute_force_and_seed(gpu_ctx, tmp_path):
     path = _synthetic_scenes(tmp_path)["icosphere"]
     for kd in (True, False):
