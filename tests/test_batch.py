@@ -145,9 +145,14 @@ def test_fused_group_equals_separate_renders(gpu_ctx, tmp_path):
             s2 = rt.Scene.from_json_file(str(p2), gpu_ctx)
             assert np.array_equal(got[idx], r.render(s2))
             s2.close()
+        # a scratch budget no frame fits: no group, the same images
+        rt.batch_tuning(gpu_ctx, fuse_bytes=1)
+        got, _ = rt.render_batch(jobs, lanes=2, ctx=gpu_ctx)
+        assert all(j.renderer.last_stats.graph == 0 for j in jobs)
+        assert all(np.array_equal(a, b) for a, b in zip(got, want))
     finally:
         rt.batch_tuning(gpu_ctx, lanes=saved["lanes"], fuse_pixels=saved["fuse_pixels"],
-                        blocks_per_sm=saved["blocks_per_sm"])
+                        fuse_bytes=saved["fuse_bytes"], blocks_per_sm=saved["blocks_per_sm"])
 
 
 @pytest.mark.gpu
