@@ -297,16 +297,23 @@ def ring_parity(rt, directory, rows=4):
     r.anti_aliasing_mode = rt.AntiAliasingMode.Stochastic
     r.samples = 4
     frame = r.render(scene)
+    st_rays, st_ms = r.last_stats.rays, r.last_stats.device_ms
     scene.close()
     y0 = H // 2 - rows // 2
     L = oracle_lib.load()
     band = np.zeros((H, W, 3), np.uint8)
+    cnt = np.zeros(6, np.uint64)
     err = ctypes.create_string_buffer(512)
+    t = time.perf_counter()
     if L.oracle_render_rows(path.encode(), None, W, H, 2, 4, 10, 0, 1, 0, os.cpu_count() or 1, y0, y0 + rows,
-                            band.ctypes.data, None, None, err, 512):
+                            band.ctypes.data, None, cnt.ctypes.data, err, 512):
         raise RuntimeError(err.value.decode())
+    dt = time.perf_counter() - t
     p = band_parity(frame, band, (y0, y0 + rows), halo=0)
     p["workload"] = "ring_spheres_1000_1080p_4spp (plain, 16 rays)"
+    rays = int(cnt[0] + cnt[1] + cnt[2])
+    p["cpu_port"] = {"mrays_per_s": rays / dt / 1e6, "rays": rays, "seconds": dt, "cores": os.cpu_count() or 1,
+                     "gpu_rays_per_frame": st_rays, "gpu_ms_per_frame": st_ms}
     return p
 
 
