@@ -274,8 +274,8 @@ def net_forward(net, feat, round_fp16=True, weights=None):
                 wt, bt = weights[k]
             else:
                 w, b = net.params[k]
-                wt = torch.as_tensor(np.asarray(w, np.float32), device=x.device).permute(0, 3, 1, 2).contiguous()
-                bt = torch.as_tensor(np.asarray(b, np.float32), device=x.device)
+                wt = torch.as_tensor(np.array(w, np.float32), device=x.device).permute(0, 3, 1, 2).contiguous()
+                bt = torch.as_tensor(np.array(b, np.float32), device=x.device)
             k += 1
             y = Fn.conv2d(x, wt, bt, padding=dil, dilation=dil)
             if i + 1 < n:
