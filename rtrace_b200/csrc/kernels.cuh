@@ -29,13 +29,20 @@ struct LevelBuf {
   double *r, *g, *b, *refl;
   int* child;
 };
+// One shadow ray: unit direction to the light sample and its distance
+// (-1: not traced), one 32-byte sector.
+struct __align__(32) SRay {
+  double dx, dy, dz, dist;
+};
 // Shadow rays of a chunk, sample-major: ray k of hit h (h relative to the
 // chunk) lives at k * chunk_hits + h, so that k_emit and k_resolve (one
-// thread per hit) read and write coalesced.
+// thread per hit) write and read it coalesced; k_shadow's hit-major
+// packets read each ray as one sector.  The visibility bytes are
+// hit-major (h * K + k), so that a packet stores them contiguously.
 struct ShadowBuf {
-  double *dx, *dy, *dz, *dist;  // per shadow ray: unit direction to the light sample, distance
+  SRay* ray;
   unsigned char* vis;
-  double *ox, *oy, *oz;         // per hit: shadow-ray origin p + 0.001 n
+  double *ox, *oy, *oz;  // per hit: shadow-ray origin p + 0.001 n
 };
 
 #define RTB_MAX_LEVELS 64
@@ -434,10 +441,7 @@ __device__ __forceinline__ void emit_body(const DFrame& F, int level, long long 
         V3 ldir = lv / dist;
         const bool cull = may_cull && dot(hr.n, lv) < -1e-9 * (norm(lp) + pscale);
         culled += cull ? 1 : 0;
-        F.sh.dx[s] = ldir.x;
-        F.sh.dy[s] = ldir.y;
-        F.sh.dz[s] = ldir.z;
-        F.sh.dist[s] = cull ? -1.0 : dist;
+        F.sh.ray[s] = SRay{ldir.x, ldir.y, ldir.z, cull ? -1.0 : dist};
         s += CH;
       } else {
         // calculate_diffuse_light_contribution (src/lighting.rs:145-217),
@@ -486,10 +490,7 @@ __device__ __forceinline__ void emit_body(const DFrame& F, int level, long long 
             V3 sv = sp - hr.p;
             double dist = norm(sv);
             V3 sdir = sv / dist;
-            F.sh.dx[s] = sdir.x;
-            F.sh.dy[s] = sdir.y;
-            F.sh.dz[s] = sdir.z;
-            F.sh.dist[s] = dist;
+            F.sh.ray[s] = SRay{sdir.x, sdir.y, sdir.z, dist};
             s += CH;
             smp++;
             it = 0;
@@ -499,10 +500,7 @@ __device__ __forceinline__ void emit_body(const DFrame& F, int level, long long 
         for (; smp < F.dsamp; smp++, s += CH) {
           V3 sv = lp - hr.p;
           V3 sdir = sv / norm(sv);
-          F.sh.dx[s] = sdir.x;
-          F.sh.dy[s] = sdir.y;
-          F.sh.dz[s] = sdir.z;
-          F.sh.dist[s] = -1.0;
+          F.sh.ray[s] = SRay{sdir.x, sdir.y, sdir.z, -1.0};
         }
       }
     }
@@ -542,24 +540,25 @@ __device__ __forceinline__ void shadow_body(const DFrame& F, int level, long lon
     const long long t = base + (threadIdx.x & 31);
     const bool have = t < ns;
     long long hl = 0, s = 0;
-    double dist = -1.0;
+    SRay sr{0.0, 0.0, 1.0, -1.0};
     if (have) {
       hl = t / K;
       long long k = t - hl * K;
       s = k * F.chunk_hits + hl;
-      dist = F.sh.dist[s];
+      sr = F.sh.ray[s];
     }
+    const double dist = sr.dist;
     const bool valid = have && (dist >= 0.0 || dist != dist);
     RayC r;
     if (valid) {
       // Ray::new normalises the (already unit) light direction once more
-      r = make_rayc(mk(F.sh.ox[hl], F.sh.oy[hl], F.sh.oz[hl]), normalize(mk(F.sh.dx[s], F.sh.dy[s], F.sh.dz[s])));
+      r = make_rayc(mk(F.sh.ox[hl], F.sh.oy[hl], F.sh.oz[hl]), normalize(mk(sr.dx, sr.dy, sr.dz)));
     } else {
       r = make_rayc(mk(0.0, 0.0, 0.0), mk(0.0, 0.0, 1.0));
     }
     bool blocked = world_any_warp(F.S, r, 0.001, valid ? dist : 0.0, valid, F.use_kd != 0, stack, F.err,
                                   COUNT ? &w : nullptr);
-    if (have) F.sh.vis[s] = (valid && !blocked) ? 1 : 0;
+    if (have) F.sh.vis[t] = (valid && !blocked) ? 1 : 0;
   }
   if (COUNT) flush_work(F, w, 1);
 }
@@ -616,6 +615,7 @@ __device__ __forceinline__ void resolve_body(const DFrame& F, int level, long lo
       V3 view = normalize(campos - hr.p);
       const long long CH = F.chunk_hits;
       long long s = h - c0;  // advances by CH per shadow ray
+      long long v = s * F.K;  // the ray's visibility byte
       const bool learned = level == 0 && F.learned;
       long long vix = 0;
       if (learned || (level == 0 && F.fb_mode)) {
@@ -628,9 +628,14 @@ __device__ __forceinline__ void resolve_body(const DFrame& F, int level, long lo
         V3 lc = ld3(L0.color);
         V3 contrib;
         if (!L0.disk) {
-          contrib = F.sh.vis[s] ? light_term(m, hr, mk(F.sh.dx[s], F.sh.dy[s], F.sh.dz[s]), lc, L0.intensity, view)
-                                : mk(0.0, 0.0, 0.0);
+          if (F.sh.vis[v]) {
+            const SRay sr = F.sh.ray[s];
+            contrib = light_term(m, hr, mk(sr.dx, sr.dy, sr.dz), lc, L0.intensity, view);
+          } else {
+            contrib = mk(0.0, 0.0, 0.0);
+          }
           s += CH;
+          v++;
         } else if (learned || (F.fb_mode && level == 0 && slot < F.n_slots && !((fbmask >> slot) & 1u))) {
           // extension: the light-centre term times the squared visibility
           // estimate, the expectation of the reference's
@@ -641,13 +646,15 @@ __device__ __forceinline__ void resolve_body(const DFrame& F, int level, long lo
           contrib = light_term(m, hr, cdir, lc, L0.intensity, view) * (v * v);
           slot++;
           s += (long long)F.dsamp * CH;
+          v += F.dsamp;
         } else {
           V3 total = mk(0.0, 0.0, 0.0);
           unsigned visible = 0;
-          for (int smp = 0; smp < F.dsamp; smp++, s += CH) {
-            if (F.sh.vis[s]) {
+          for (int smp = 0; smp < F.dsamp; smp++, s += CH, v++) {
+            if (F.sh.vis[v]) {
               visible++;
-              total = total + light_term(m, hr, mk(F.sh.dx[s], F.sh.dy[s], F.sh.dz[s]), lc, L0.intensity, view);
+              const SRay sr = F.sh.ray[s];
+              total = total + light_term(m, hr, mk(sr.dx, sr.dy, sr.dz), lc, L0.intensity, view);
             }
           }
           const double n = (double)F.dsamp;  // 16.0 in the reference
@@ -751,7 +758,6 @@ __global__ void __launch_bounds__(128) k_features(DFrame F, long long c0) {
   long long nh = F.nhits[0];
   long long c1 = c0 + F.chunk_hits < nh ? c0 + F.chunk_hits : nh;
   V3 campos = ld3(F.C.campos);
-  const long long CH = F.chunk_hits;
   const long long plane_px = (long long)F.H * F.W;
   for (long long h = c0 + blockIdx.x * (long long)blockDim.x + threadIdx.x; h < c1;
        h += (long long)gridDim.x * blockDim.x) {
@@ -770,16 +776,16 @@ __global__ void __launch_bounds__(128) k_features(DFrame F, long long c0) {
     f[FEAT_NX] = (float)hr.n.x;
     f[FEAT_NX + 1] = (float)hr.n.y;
     f[FEAT_NX + 2] = (float)hr.n.z;
-    long long s = h - c0;
+    long long v = (h - c0) * F.K;  // the hit's first visibility byte
     int slot = 0;
     for (int li = 0; li < S.n_lights; li++) {
       const DLight& L0 = S.lights[li];
       if (!L0.disk) {
-        s += CH;
+        v++;
         continue;
       }
       unsigned visible = 0;
-      for (int smp = 0; smp < F.dsamp; smp++, s += CH) visible += F.sh.vis[s];
+      for (int smp = 0; smp < F.dsamp; smp++, v++) visible += F.sh.vis[v];
       if (slot < DN_MAX_SLOTS) {
         float v = (float)visible / (float)F.dsamp;
         V3 lp = ld3(L0.pos);

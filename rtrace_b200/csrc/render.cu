@@ -237,8 +237,7 @@ rt_status ensure_scratch(rt_ctx* ctx, long long n_rays, int levels, long long n_
   CK(cudaMemcpy(ctx->d_levels, ctx->h_levels.data(), (Lv + 1) * sizeof(LevelBuf), cudaMemcpyHostToDevice));
   CK(dalloc(o, &ctx->d_counts, Lv + 2));
   CK(dalloc(o, &ctx->d_nhits, Lv + 1));
-  CK(dalloc(o, &F.sh.dx, SH)); CK(dalloc(o, &F.sh.dy, SH)); CK(dalloc(o, &F.sh.dz, SH));
-  CK(dalloc(o, &F.sh.dist, SH));
+  CK(dalloc(o, &F.sh.ray, SH));
   CK(dalloc(o, &F.sh.vis, SH));
   CK(dalloc(o, &F.sh.ox, HS)); CK(dalloc(o, &F.sh.oy, HS)); CK(dalloc(o, &F.sh.oz, HS));
   CK(dalloc(o, &F.pdepth, R)); CK(dalloc(o, &F.pnx, R)); CK(dalloc(o, &F.pny, R)); CK(dalloc(o, &F.pnz, R));
