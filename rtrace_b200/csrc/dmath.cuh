@@ -12,6 +12,11 @@
 
 #define RTB_HD __host__ __device__ __forceinline__
 
+// float4 elements before node 0 of a single-precision BVH (the header
+// holds the slab scale in element 0): 64 bytes, so that every 64-byte
+// node lies in one 128-byte line of a 128-byte aligned array.
+#define RTB_FBVH_HEAD 4
+
 namespace rtb {
 
 struct V3 {

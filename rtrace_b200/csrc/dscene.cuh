@@ -472,14 +472,15 @@ __device__ bool mesh_kd_walk(const DMesh& M, const RayC& r, double tmin, double&
 // A BVH node in single precision: the double node's child boxes rounded
 // outwards to floats, the same child references.  Layout: fbvh[0].x is
 // the largest |coordinate| of any child box (the scale the slab constants
-// below need); node k is fbvh[1 + 4k .. 4 + 4k] = {lmn.xyz, lmx.x},
+// below need; elements 1-3 unused); node k is fbvh[H + 4k .. H + 3 + 4k]
+// (H = RTB_FBVH_HEAD) = {lmn.xyz, lmx.x},
 // {lmx.yz, rmn.xy}, {rmn.z, rmx.xyz}, {lidx, lcnt, ridx, rcnt as int bits}.
 struct FNode {
   float lmn[3], lmx[3], rmn[3], rmx[3];
   int lidx, lcnt, ridx, rcnt;
 };
 __device__ __forceinline__ FNode load_fnode(const float4* fbvh, int node) {
-  const float4* N = fbvh + 1 + 4 * (size_t)node;
+  const float4* N = fbvh + RTB_FBVH_HEAD + 4 * (size_t)node;
   const float4 a = __ldg(N + 0), b = __ldg(N + 1), c = __ldg(N + 2), d = __ldg(N + 3);
   FNode n;
   n.lmn[0] = a.x; n.lmn[1] = a.y; n.lmn[2] = a.z;

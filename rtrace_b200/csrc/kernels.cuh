@@ -527,7 +527,9 @@ __device__ __forceinline__ void shadow_body(const DFrame& F, int level, long lon
   long long c1 = c0 + F.chunk_hits < nh ? c0 + F.chunk_hits : nh;
   const int K = F.K;
   long long nhc = c1 > c0 ? c1 - c0 : 0;
-  long long ns = nhc * K;
+  // a chunk holds at most 2^26 shadow rays (the host's cap): 32-bit indices
+  const int ns = (int)(nhc * K);
+  const int CH = (int)F.chunk_hits;
   Work w{0, 0, 0, 0};
   __shared__ int s_stack[4][RTB_STACK];  // one traversal stack per warp (128 threads)
   volatile int* stack = s_stack[threadIdx.x >> 5];
@@ -535,17 +537,16 @@ __device__ __forceinline__ void shadow_body(const DFrame& F, int level, long lon
   // collective).  Hit-major order: the K rays of one hit point sit in
   // adjacent lanes, so a warp holds a bundle of rays from one or two points
   // towards one light, which the packet traversal shares out.
-  const long long stride = (long long)nblk * blockDim.x;
-  for (long long base = bid * (long long)blockDim.x + (threadIdx.x & ~31); base < ns; base += stride) {
-    const long long t = base + (threadIdx.x & 31);
+  const int stride = nblk * blockDim.x;
+  for (int base = bid * blockDim.x + (threadIdx.x & ~31); base < ns; base += stride) {
+    const int t = base + (threadIdx.x & 31);
     const bool have = t < ns;
-    long long hl = 0, s = 0;
+    int hl = 0;
     SRay sr{0.0, 0.0, 1.0, -1.0};
     if (have) {
-      hl = t / K;
-      long long k = t - hl * K;
-      s = k * F.chunk_hits + hl;
-      sr = F.sh.ray[s];
+      hl = (int)((unsigned)t / (unsigned)K);
+      const int k = t - hl * K;
+      sr = F.sh.ray[k * CH + hl];
     }
     const double dist = sr.dist;
     const bool valid = have && (dist >= 0.0 || dist != dist);

@@ -245,7 +245,7 @@ __global__ void k_prep_fbvh(const double2* __restrict__ bvh, int nb, float4* __r
       // present children only; a NaN coordinate makes the scale NaN
       if (hi32(j < 6 ? refs.x : refs.y) >= 0 && (m > scale || m != m) && scale == scale) scale = m;
     }
-    float4* F = fbvh + 1 + 4 * (long long)k;
+    float4* F = fbvh + RTB_FBVH_HEAD + 4 * (long long)k;
     F[0] = make_float4(f[0], f[1], f[2], f[3]);
     F[1] = make_float4(f[4], f[5], f[6], f[7]);
     F[2] = make_float4(f[8], f[9], f[10], f[11]);
@@ -610,7 +610,7 @@ std::string prep_mesh_device(const double* h_vertices, int n, const double2* d_k
 
   // ---- the single-precision BVH, the k-d leaf cells
   const int nb = bvh_internal_nodes(n, leaf);
-  PCK(cudaMemsetAsync(out.fbvh, 0, sizeof(float4), s));
+  PCK(cudaMemsetAsync(out.fbvh, 0, RTB_FBVH_HEAD * sizeof(float4), s));
   k_prep_fbvh<<<grid_for(nb, BS), BS, 0, s>>>(out.bvh, nb, out.fbvh);
   if (n_kd_nodes > 0)
     k_prep_cells<<<grid_for(n_kd_nodes, BS), BS, 0, s>>>(d_kd_nodes, n_kd_nodes, d_leaf_path, out.cells);
@@ -635,7 +635,7 @@ std::string derive_mesh_device(const double2* d_bvh, int nb, const double2* d_bt
   const int BS = 256;
   cudaError_t e = cudaSuccess;
   if (d_bvh && fbvh && nb > 0) {
-    e = cudaMemsetAsync(fbvh, 0, sizeof(float4), s);
+    e = cudaMemsetAsync(fbvh, 0, RTB_FBVH_HEAD * sizeof(float4), s);
     if (e == cudaSuccess) k_prep_fbvh<<<grid_for(nb, BS), BS, 0, s>>>(d_bvh, nb, fbvh);
   }
   if (e == cudaSuccess && n_kd_nodes > 0)

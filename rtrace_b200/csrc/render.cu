@@ -609,7 +609,7 @@ float float_up(double x) { return -float_down(-x); }
 // element 0 the largest |coordinate| of a present child's box (+inf when
 // one is NaN, which turns the float tests off).
 void put_fbvh(const std::vector<BvhNode>& nodes, std::vector<float4>* out) {
-  out->assign(1 + 4 * nodes.size(), float4{0.f, 0.f, 0.f, 0.f});
+  out->assign(RTB_FBVH_HEAD + 4 * nodes.size(), float4{0.f, 0.f, 0.f, 0.f});
   float scale = 0.0f;
   for (size_t k = 0; k < nodes.size(); k++) {
     const BvhNode& n = nodes[k];
@@ -624,7 +624,7 @@ void put_fbvh(const std::vector<BvhNode>& nodes, std::vector<float4>* out) {
       const float m = std::fabs(f[j]);
       if ((j < 6 ? n.lcnt : n.rcnt) >= 0 && (m > scale || m != m) && scale == scale) scale = m;
     }
-    float4* F = &(*out)[1 + 4 * k];
+    float4* F = &(*out)[RTB_FBVH_HEAD + 4 * k];
     auto bits = [](int v) {
       float x;
       memcpy(&x, &v, sizeof x);
@@ -950,7 +950,7 @@ rt_status upload_prep_device(rt_ctx* ctx, rt_scene* sc, const rt_mesh_desc& md, 
   int* occ_off;
   if ((st = upload_now(ctx, sc, P->nodes, &M.nodes)) != RT_OK || (st = upload_now(ctx, sc, P->leaf_tris, &M.leaf_tris)) != RT_OK ||
       (st = upload_now(ctx, sc, P->leaf_path, &M.leaf_path)) != RT_OK || (st = reserve(ctx, sc, 7 * (size_t)nb, &bvh)) != RT_OK ||
-      (st = reserve(ctx, sc, 1 + 4 * (size_t)nb, &fbvh)) != RT_OK ||
+      (st = reserve(ctx, sc, RTB_FBVH_HEAD + 4 * (size_t)nb, &fbvh)) != RT_OK ||
       (st = reserve(ctx, sc, 3 * (size_t)P->n_nodes, &cells)) != RT_OK ||
       (st = reserve(ctx, sc, 5 * (size_t)n, &btris)) != RT_OK || (st = reserve(ctx, sc, 5 * (size_t)n, &brute)) != RT_OK ||
       (st = reserve(ctx, sc, (size_t)n, &normals)) != RT_OK || (st = reserve(ctx, sc, (size_t)P->n_index, &occ)) != RT_OK ||
@@ -974,7 +974,7 @@ rt_status upload_prep_device(rt_ctx* ctx, rt_scene* sc, const rt_mesh_desc& md, 
   M.occ_off = occ_off;
   if (keep_host) {
     // what upload_prep copies; it derives the rest
-    P->fbvh.resize(1 + 4 * (size_t)nb);
+    P->fbvh.resize(RTB_FBVH_HEAD + 4 * (size_t)nb);
     P->btris.resize(5 * (size_t)n);
     CK(cudaMemcpy(P->fbvh.data(), fbvh, P->fbvh.size() * sizeof(float4), cudaMemcpyDeviceToHost));
     CK(cudaMemcpy(P->btris.data(), btris, P->btris.size() * sizeof(double2), cudaMemcpyDeviceToHost));
@@ -2840,7 +2840,7 @@ rt_status rt_debug_mesh_prep(rt_ctx* ctx, const rt_mesh_desc* md, uint32_t* mism
   if ((ce = dalloc(tmp, &dn, D.nodes.size())) != cudaSuccess || (ce = dalloc(tmp, &dl, D.leaf_tris.size())) != cudaSuccess ||
       (ce = dalloc(tmp, &dp, D.leaf_path.size())) != cudaSuccess ||
       (ce = dalloc(tmp, &cells, 3 * (size_t)D.n_nodes)) != cudaSuccess ||
-      (ce = dalloc(tmp, &bvh, 7 * (size_t)nb)) != cudaSuccess || (ce = dalloc(tmp, &fbvh, 1 + 4 * (size_t)nb)) != cudaSuccess ||
+      (ce = dalloc(tmp, &bvh, 7 * (size_t)nb)) != cudaSuccess || (ce = dalloc(tmp, &fbvh, RTB_FBVH_HEAD + 4 * (size_t)nb)) != cudaSuccess ||
       (ce = dalloc(tmp, &btris, 5 * (size_t)n)) != cudaSuccess ||
       (ce = dalloc(tmp, &brute, 5 * (size_t)n)) != cudaSuccess || (ce = dalloc(tmp, &normals, (size_t)n)) != cudaSuccess ||
       (ce = dalloc(tmp, &occ, (size_t)D.n_index)) != cudaSuccess || (ce = dalloc(tmp, &occ_off, (size_t)n + 1)) != cudaSuccess) {
@@ -2872,7 +2872,7 @@ rt_status rt_debug_mesh_prep(rt_ctx* ctx, const rt_mesh_desc* md, uint32_t* mism
   if (!same(occ_off, H.occ_off.data(), H.occ_off.size() * sizeof(int))) m |= 32;
   // the single-precision BVH the walks test: the device's conversion
   // (k_prep_fbvh) against the host's (put_fbvh), scale element included
-  if (H.fbvh.size() != 1 + 4 * (size_t)nb || !same(fbvh, H.fbvh.data(), H.fbvh.size() * sizeof(float4))) m |= 128;
+  if (H.fbvh.size() != RTB_FBVH_HEAD + 4 * (size_t)nb || !same(fbvh, H.fbvh.data(), H.fbvh.size() * sizeof(float4))) m |= 128;
   // the arrays an upload of the host preparation derives on the device,
   // from the host's BVH-order records, into the same buffers
   cudaStream_t s = ctx->stream;
