@@ -123,7 +123,8 @@ __host__ __device__ constexpr int acc_cols(int cout) { return cout < 32 ? 32 : c
 // Shared memory of one CTA: a ring of NROW staged input rows (TILE_M +
 // 2 * dil pixels each, one block of 16-byte rows per 8 channels), the
 // weights, the pipeline's mbarriers, the TMEM address and an abort flag.
-constexpr int NROW = 6;    // staged input rows (TMA -> MMA); a step reads 3
+constexpr int NROW = 4;    // staged input rows (TMA -> MMA); a step reads 3 (4: 2.75 ms for the
+                           // network at 1080p x 4 against 2.87 with 6, more CTAs fit an SM)
 constexpr int NACC = 2;    // TMEM accumulators (MMA -> epilogue)
 constexpr int SEG = 8;     // output rows a CTA walks down one column at a time (8 measured best of 8-64)
 constexpr int CONV_THREADS = 192;  // warps 0-3 epilogue, warp 4 TMA, warp 5 MMA
@@ -519,13 +520,14 @@ cudaError_t launch_conv(const __half* in, int planes, int H, int W, int dil, con
   CUtensorMap map;
   e = make_in_map(&map, in, planes, H, W, CIN, dil);
   if (e != cudaSuccess) return e;
-  // 4 CTAs per SM (each holds at most 128 of the SM's 512 TMEM columns;
-  // shared memory allows 1-6 resident); CTAs beyond the resident ones start
+  // 6 CTAs per SM (each holds at most 128 of the SM's 512 TMEM columns;
+  // shared memory allows 1-7 resident); CTAs beyond the resident ones start
   // as others finish, which balances the segments better than one resident
-  // wave (1.8x slower) or one CTA per segment (1.2x slower)
+  // wave (1.8x slower) or one CTA per segment (1.2x slower); 2.67 ms for
+  // the network at 1080p x 4 against 2.75 ms with 4
   const long long rows_per_col = (H + dil - 1) / dil;
   const long long nsegs = (long long)planes * ((W + TILE_M - 1) / TILE_M) * dil * ((rows_per_col + SEG - 1) / SEG);
-  long long grid = std::min<long long>(nsegs, (long long)num_sms * 4);
+  long long grid = std::min<long long>(nsegs, (long long)num_sms * 6);
   if (grid < 1) grid = 1;
   k_conv3x3_tc<CIN, COUT, MODE><<<(int)grid, CONV_THREADS, smem, s>>>(map, planes, H, W, dil, (const uint4*)w, b,
                                                                       out, vis, conf, aux, err);

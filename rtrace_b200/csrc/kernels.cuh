@@ -641,10 +641,10 @@ __device__ __forceinline__ void resolve_body(const DFrame& F, int level, long lo
           // extension: the light-centre term times the squared visibility
           // estimate, the expectation of the reference's
           // (sum of visible terms / n) * (visible / n)
-          double v = (double)F.vhat[vix + (long long)slot * F.H * F.W];
-          v = rclamp(v, 0.0, 1.0);
+          double vh = (double)F.vhat[vix + (long long)slot * F.H * F.W];
+          vh = rclamp(vh, 0.0, 1.0);
           V3 cdir = normalize(ld3(L0.pos) - hr.p);
-          contrib = light_term(m, hr, cdir, lc, L0.intensity, view) * (v * v);
+          contrib = light_term(m, hr, cdir, lc, L0.intensity, view) * (vh * vh);
           slot++;
           s += (long long)F.dsamp * CH;
           v += F.dsamp;
