@@ -527,7 +527,7 @@ __device__ __forceinline__ void shadow_body(const DFrame& F, int level, long lon
   long long c1 = c0 + F.chunk_hits < nh ? c0 + F.chunk_hits : nh;
   const int K = F.K;
   long long nhc = c1 > c0 ? c1 - c0 : 0;
-  // a chunk holds at most 2^26 shadow rays (the host's cap): 32-bit indices
+  // a chunk holds at most 2^28 shadow rays (the host's cap): 32-bit indices
   const int ns = (int)(nhc * K);
   const int CH = (int)F.chunk_hits;
   Work w{0, 0, 0, 0};

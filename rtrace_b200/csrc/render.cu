@@ -201,8 +201,12 @@ void drop_graphs(rt_ctx* ctx) {
 // replays instead of cycling through a too-small LRU.
 const size_t kMaxGraphs = 256;
 
-// Shadow-ray entries kept on the device at once (33 B each).
-const long long kShadowCap = 1LL << 26;
+// Shadow-ray entries kept on the device at once (33 B each, 8.9 GB at
+// most).  A 1080p frame with 4 samples and 32 rays per hit fits in one
+// chunk per level: at 2^26 it took four, and at every reflection level the
+// three chunks beyond the level's few hits still cost their launches (about
+// 0.7 ms per frame of the 1,000-sphere ring scene).
+const long long kShadowCap = 1LL << 28;
 
 rt_status ensure_scratch(rt_ctx* ctx, long long n_rays, int levels, long long n_pix, long long n_shadow,
                          long long n_hits_sh) {
