@@ -123,8 +123,12 @@ __host__ __device__ constexpr int acc_cols(int cout) { return cout < 32 ? 32 : c
 // Shared memory of one CTA: a ring of NROW staged input rows (TILE_M +
 // 2 * dil pixels each, one block of 16-byte rows per 8 channels), the
 // weights, the pipeline's mbarriers, the TMEM address and an abort flag.
-constexpr int NROW = 4;    // staged input rows (TMA -> MMA); a step reads 3 (4: 2.75 ms for the
-                           // network at 1080p x 4 against 2.87 with 6, more CTAs fit an SM)
+// A step reads 3 rows, so the TMA warp runs NROW - 3 rows ahead.  Fewer
+// rows let more CTAs share an SM, which hides more than deeper prefetch
+// does (measured on the network at 1080p x 4: 4 rows everywhere 2.68 ms,
+// 6 everywhere 2.87 ms, 6 for the 64-channel shapes 2.71 ms); 64 -> 32 fits
+// two CTAs per SM only with 3 rows (2.62 ms).
+__host__ __device__ constexpr int conv_nrow(int cin, int cout) { return (cin == 64 && cout == 32) ? 3 : 4; }
 constexpr int NACC = 2;    // TMEM accumulators (MMA -> epilogue)
 constexpr int SEG = 8;     // output rows a CTA walks down one column at a time (8 measured best of 8-64)
 constexpr int CONV_THREADS = 192;  // warps 0-3 epilogue, warp 4 TMA, warp 5 MMA
@@ -132,6 +136,7 @@ __host__ __device__ constexpr int halo_px(int dil) { return TILE_M + 2 * dil; }
 __host__ __device__ constexpr int halo_block(int dil) { return ((halo_px(dil) * 16 + 127) / 128) * 128; }
 template <int CIN, int COUT>
 struct ConvSmem {
+  static constexpr int NROW = conv_nrow(CIN, COUT);       // staged input rows (TMA -> MMA)
   static constexpr int CPT = CIN / 8;                     // 16-byte channel chunks per pixel
   static constexpr int B_BYTES = 9 * CPT * COUT * 16;     // weights
   static constexpr int TAIL = 256;                        // barriers, TMEM slot, abort flag
@@ -225,6 +230,7 @@ __global__ void __launch_bounds__(CONV_THREADS) k_conv3x3_tc(const __grid_consta
   constexpr int ACC = acc_cols(COUT), TMEM_ALLOC = NACC * ACC;
   using SM = ConvSmem<CIN, COUT>;
   constexpr int CPT = SM::CPT;
+  constexpr int NROW = SM::NROW;
   extern __shared__ unsigned char smem_raw[];
   uint32_t raw = smem_u32(smem_raw);
   uint32_t pad = (1024u - (raw & 1023u)) & 1023u;

@@ -73,7 +73,10 @@ struct DFrame {
   // some slot, those slots are shaded by the plain path.  k_fb_select lists
   // such hits in fb_list (count fbn[0]; fbn[1] counts their slots) and
   // keeps each hit's slot bits in fb_flag; launches with fb_mode set walk
-  // fb_list instead of the level's hit list.
+  // fb_list instead of the level's hit list (fb_hit).  The list holds the
+  // hits with one falling slot from the front (fbn[2] of them) and those
+  // with more from the back (fbn[3], down from index n_primary - 1), so
+  // that a warp's hits sample and shade the same number of lights.
   float* vconf;
   float conf_thr;
   int fb_mode;
@@ -182,7 +185,7 @@ __device__ __forceinline__ void frame_init_body(const DFrame& F, int levels) {
   for (int i = threadIdx.x; i < levels + 1; i += blockDim.x) F.nhits[i] = 0;
   if (threadIdx.x < 16) F.stats[threadIdx.x] = 0;
   if (threadIdx.x == 0) *F.err = 0;
-  if (threadIdx.x < 2 && F.fbn) F.fbn[threadIdx.x] = 0;
+  if (threadIdx.x < 4 && F.fbn) F.fbn[threadIdx.x] = 0;
 }
 __global__ void k_frame_init(const __grid_constant__ DFrame F, int levels) { frame_init_body(F, levels); }
 // one block per frame
@@ -398,6 +401,12 @@ __device__ __forceinline__ HitRec load_hit(const DFrame& F, int level, int h, Ra
   return finalize_hit(F.S, *rc, w);
 }
 
+// The hit at position h of the fallback list (see DFrame::fb_list).
+__device__ __forceinline__ int fb_hit(const DFrame& F, long long h) {
+  const long long n1 = F.fbn[2];
+  return F.fb_list[h < n1 ? h : F.n_primary - 1 - (h - n1)];
+}
+
 // Light sampling for hits [c0, c1) of the level's hit list.
 __device__ __forceinline__ void emit_body(const DFrame& F, int level, long long c0, int bid, int nblk) {
   const DScene& S = F.S;
@@ -409,7 +418,7 @@ __device__ __forceinline__ void emit_body(const DFrame& F, int level, long long 
        h += (long long)nblk * blockDim.x) {
     RayC rc;
     uint64_t seed;
-    const int hidx = F.fb_mode ? F.fb_list[h] : (int)h;
+    const int hidx = F.fb_mode ? fb_hit(F, h) : (int)h;
     HitRec hr = load_hit(F, level, hidx, &rc, &seed);
     // fallback launches sample only the slots that fall back
     const unsigned fbmask = F.fb_mode ? (unsigned)F.fb_flag[hidx] : ~0u;
@@ -496,11 +505,13 @@ __device__ __forceinline__ void emit_body(const DFrame& F, int level, long long 
             it = 0;
           }
         }
-        // after a failed range check or the watchdog: never traced
-        for (; smp < F.dsamp; smp++, s += CH) {
-          V3 sv = lp - hr.p;
-          V3 sdir = sv / norm(sv);
-          F.sh.ray[s] = SRay{sdir.x, sdir.y, sdir.z, -1.0};
+        // after a failed range check or the watchdog, for a culled light or
+        // a slot the network is confident about: never traced (one
+        // direction, the light centre's, for all of the light's records)
+        if (smp < F.dsamp) {
+          const V3 sv = lp - hr.p;
+          const V3 sdir = sv / norm(sv);
+          for (; smp < F.dsamp; smp++, s += CH) F.sh.ray[s] = SRay{sdir.x, sdir.y, sdir.z, -1.0};
         }
       }
     }
@@ -518,9 +529,10 @@ __global__ void __launch_bounds__(128) k_emit_multi(const DFrame* __restrict__ T
 }
 
 
-// world.hit(&shadow_ray, 0.001, distance).is_some() per shadow ray.  Seven
-// blocks of 128 per SM (72 registers): 1-2% faster on the bench frame than
-// 8 (64 registers, more spills) or 6.
+// world.hit(&shadow_ray, 0.001, distance).is_some() per shadow ray.  MINB
+// blocks of 128 per SM: with meshes 7 (72 registers; the icosphere frame's
+// shadow stage 3.30 ms, against 3.40 at 6 and 3.50 at 8), with spheres and
+// planes only 8 (64 registers; the ring frame's 21.57 -> 20.83 ms).
 template <bool COUNT>
 __device__ __forceinline__ void shadow_body(const DFrame& F, int level, long long c0, int bid, int nblk) {
   long long nh = F.fb_mode ? *F.fbn : F.nhits[level];
@@ -563,8 +575,8 @@ __device__ __forceinline__ void shadow_body(const DFrame& F, int level, long lon
   }
   if (COUNT) flush_work(F, w, 1);
 }
-template <bool COUNT>
-__global__ void __launch_bounds__(128, 7) k_shadow(const __grid_constant__ DFrame F, int level, long long c0) {
+template <bool COUNT, int MINB>
+__global__ void __launch_bounds__(128, MINB) k_shadow(const __grid_constant__ DFrame F, int level, long long c0) {
   shadow_body<COUNT>(F, level, c0, blockIdx.x, gridDim.x);
 }
 template <bool COUNT>
@@ -595,7 +607,7 @@ __device__ __forceinline__ void resolve_body(const DFrame& F, int level, long lo
     bool active = h < c1;
     // the hit in the level's list (fallback launches walk fb_list); a
     // learned launch leaves the hits the fallback shades
-    const int hi = active ? (F.fb_mode ? F.fb_list[h] : (int)h) : 0;
+    const int hi = active ? (F.fb_mode ? fb_hit(F, h) : (int)h) : 0;
     if (active && F.learned && level == 0 && F.fb_flag && F.fb_flag[hi]) active = false;
     // fallback launch: the slots that fall back take the plain sum, the
     // others keep the network's estimate
@@ -732,22 +744,22 @@ __global__ void __launch_bounds__(128) k_fb_select(DFrame F) {
   const long long plane_px = (long long)F.H * F.W;
   for (long long base = blockIdx.x * (long long)blockDim.x; base < nh; base += (long long)gridDim.x * blockDim.x) {
     const long long h = base + threadIdx.x;
-    bool want = false;
-    unsigned slots = 0;
+    unsigned mask = 0;
     if (h < nh) {
       const int i = F.hit_ray[h];
       const long long pix = i / F.S_per_px, plane = i % F.S_per_px;
-      unsigned mask = 0;
       for (int j = 0; j < F.n_slots; j++)
         if (F.vconf[(plane * DN_MAX_SLOTS + j) * plane_px + pix] > F.conf_thr) mask |= 1u << j;
       F.fb_flag[h] = (unsigned char)mask;
-      want = mask != 0;
-      slots = __popc(mask);
     }
-    const int at = warp_alloc(F.fbn, want);  // every lane of the warp takes part
-    if (want) F.fb_list[at] = (int)h;
-    slots = __reduce_add_sync(0xffffffffu, slots);
-    if ((threadIdx.x & 31) == 0 && slots) atomicAdd(F.fbn + 1, slots);
+    const bool want = mask != 0, one = __popc(mask) == 1;
+    // every lane of the warp takes part in each allocation
+    warp_alloc(F.fbn, want);
+    const int at1 = warp_alloc(F.fbn + 2, one);
+    const int at2 = warp_alloc(F.fbn + 3, want && !one);
+    if (want) F.fb_list[one ? at1 : F.n_primary - 1 - at2] = (int)h;
+    const unsigned slots = __reduce_add_sync(0xffffffffu, (unsigned)__popc(mask));
+    if ((threadIdx.x & 31) == 0 && slots) atomicAdd(F.fbn + 1, (int)slots);
   }
 }
 

@@ -300,7 +300,7 @@ rt_status ensure_dn_scratch(rt_ctx* ctx, long long n) {
   CK(dalloc(o, &ctx->d_vconf, n * DN_MAX_SLOTS));
   CK(dalloc(o, &ctx->d_fb_list, n));
   CK(dalloc(o, &ctx->d_fb_flag, n));
-  CK(dalloc(o, &ctx->d_fbn, 2));
+  CK(dalloc(o, &ctx->d_fbn, 4));
   ctx->dn_cap = n;
   return RT_OK;
 }
@@ -1554,6 +1554,18 @@ rt_status render_impl(rt_ctx* ctx, const rt_scene* sc, const rt_render_params* P
     long long cap = (long long)nsm * per_sm;
     return (int)std::max<long long>(1, std::min(b, cap));
   };
+  // k_shadow's register budget: 7 blocks per SM where the walk reaches mesh
+  // leaves (triangle tests, k-d verification), 8 for spheres and planes only
+  const bool mesh_scene = !sc->host_meshes.empty();
+  auto launch_shadow = [&](const DFrame& Fs, int level, long long c0, int grid) {
+    if (count) {
+      if (mesh_scene) k_shadow<true, 7><<<grid, 128, 0, s>>>(Fs, level, c0);
+      else k_shadow<true, 8><<<grid, 128, 0, s>>>(Fs, level, c0);
+    } else {
+      if (mesh_scene) k_shadow<false, 7><<<grid, 128, 0, s>>>(Fs, level, c0);
+      else k_shadow<false, 8><<<grid, 128, 0, s>>>(Fs, level, c0);
+    }
+  };
   const bool o_wide = o_radius > kOutlineTileRadius;  // mask tile beyond shared memory: global-memory dilation
   const size_t o_shm = o_wide ? 0 : (size_t)(OT_X + 2 * o_radius) * (OT_Y + 2 * o_radius) * sizeof(double);
   if (F.outline && o_shm > 48 * 1024) CK(outline_smem_attr((int)o_shm));
@@ -1594,8 +1606,7 @@ rt_status render_impl(rt_ctx* ctx, const rt_scene* sc, const rt_render_params* P
           k_emit<<<blocks(chunk, 128, 64), 128, 0, s>>>(F, l, c0);
           Lc.after(RT_STAGE_EMIT);
           if (K > 0) {
-            if (count) k_shadow<true><<<blocks(chunk * K, 128, 128), 128, 0, s>>>(F, l, c0);
-            else k_shadow<false><<<blocks(chunk * K, 128, 128), 128, 0, s>>>(F, l, c0);
+            launch_shadow(F, l, c0, blocks(chunk * K, 128, 128));
             Lc.after(RT_STAGE_SHADOW);
           }
           if (feat) {
@@ -1632,8 +1643,7 @@ rt_status render_impl(rt_ctx* ctx, const rt_scene* sc, const rt_render_params* P
               k_emit<<<blocks(chunk_fb, 128, 64), 128, 0, s>>>(Fb, 0, c0);
               Lc.after(RT_STAGE_EMIT);
               if (K_fb > 0) {
-                if (count) k_shadow<true><<<blocks(chunk_fb * K_fb, 128, 128), 128, 0, s>>>(Fb, 0, c0);
-                else k_shadow<false><<<blocks(chunk_fb * K_fb, 128, 128), 128, 0, s>>>(Fb, 0, c0);
+                launch_shadow(Fb, 0, c0, blocks(chunk_fb * K_fb, 128, 128));
                 Lc.after(RT_STAGE_SHADOW);
               }
               k_resolve<<<blocks(chunk_fb, 128, 16), 128, 0, s>>>(Fb, 0, c0);
