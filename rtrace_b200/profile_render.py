@@ -1,7 +1,7 @@
 """Renders one of the benchmark workloads a few times, for profiler captures.
 
     python -m rtrace_b200.profile_render --workload noisy_icosphere --width 960 --height 540 --reps 1
-    python -m rtrace_b200.profile_render --workload ring_spheres --width 1920 --height 1080 --learned
+    python -m rtrace_b200.profile_render --workload ring_spheres --width 1920 --height 1080 --learned --fallback-samples 64
     python -m rtrace_b200.profile_render --kd-build terrain --reps 2
     python -m rtrace_b200.profile_render --train-steps 3
 
@@ -34,6 +34,8 @@ def main(argv=None):
     ap.add_argument("--dir", default=None)
     ap.add_argument("--disk-samples", type=int, default=16, help="shadow rays per disk light (16: the reference)")
     ap.add_argument("--learned", action="store_true", help="learned soft shadows with the shipped denoiser weights")
+    ap.add_argument("--fallback-samples", type=int, default=0,
+                    help="rays per disk light where a learned render falls back (0: --disk-samples)")
     ap.add_argument("--kd-build", default=None, choices=["terrain", "icosphere"])
     ap.add_argument("--train-steps", type=int, default=0)
     a = ap.parse_args(argv)
@@ -58,6 +60,7 @@ def main(argv=None):
     if a.learned:
         scene._ctx.load_denoiser()
         r.learned_shadows = True
+        r.fallback_samples = a.fallback_samples
     for _ in range(a.reps):
         r.render(scene)
     st = r.last_stats
