@@ -215,6 +215,69 @@ def test_confidence_fallback_uses_the_plain_path(gpu_ctx):
 
 
 @pytest.mark.gpu
+def test_confidence_fallback_with_point_lights(gpu_ctx):
+    """A point light before and one between the disk lights: each hit's
+    shadow rays are then point, disk (n rays), point, disk (n rays), so the
+    rays of a falling slot start at an offset that is not a multiple of the
+    warp width.  Every light falling back gives the plain render's bytes and
+    visibility; at the stored threshold each slot's visibility is the plain
+    path's where its error estimate exceeds the threshold, the network's
+    elsewhere, in both halves of the bucketed fallback list."""
+    import torch
+    import rtrace_b200 as rt
+    from rtrace_b200 import workloads
+    sc = workloads.ring_spheres_scene(seed=5, n_rings=2, per_ring=6)
+    disks = sc["lights"]
+    sc["lights"] = [{"position": [2.0, -3.0, 7.0], "color": "#FFE0C0", "intensity": 0.4}, disks[0],
+                    {"position": [-4.0, 2.0, 6.0], "color": "#C0E0FF", "intensity": 0.3}, disks[1]]
+    scene = rt.Scene.from_json_str(json.dumps(sc), gpu_ctx)
+    dev = torch.device("cuda", gpu_ctx.device)
+    net = denoiser.random_net(11, threshold=0.5)
+    gpu_ctx.load_denoiser(denoiser.pack_net(net))
+    W, H, S = 120, 64, 2
+    for fb_rays in (5, 16):
+        plain = rt.Renderer(W, H)
+        plain.anti_aliasing_mode = rt.AntiAliasingMode.Stochastic
+        plain.samples = S
+        plain.disk_samples = fb_rays
+        pv = torch.zeros((S, 2, H, W), device=dev)
+        feat = torch.zeros((S, H, W, 16), dtype=torch.float16, device=dev)
+        torch.cuda.synchronize()
+        want = plain.render_shadow_aov(scene, pv.data_ptr(), feat.data_ptr())
+        m = denoiser.masks(feat)
+        r = rt.Renderer(W, H)
+        r.anti_aliasing_mode = rt.AntiAliasingMode.Stochastic
+        r.samples = S
+        r.disk_samples = fb_rays
+        r.learned_shadows = True
+        r.fallback_samples = fb_rays
+        r.confidence_threshold = 1e-30  # every slot of every hit falls back
+        vis = torch.zeros((S, 2, H, W), device=dev)
+        img = r.render_shadow_aov(scene, vis.data_ptr(), None)
+        assert np.array_equal(img, want), fb_rays
+        assert torch.equal(vis[m], pv[m]), fb_rays
+        # the stored threshold: some hits with one falling slot, some with two
+        r.confidence_threshold = 0.0
+        lfeat = torch.zeros((S, H, W, 16), dtype=torch.float16, device=dev)
+        r.render_shadow_aov(scene, vis.data_ptr(), lfeat.data_ptr())
+        gv = torch.zeros_like(vis)
+        gc = torch.zeros_like(vis)
+        torch.cuda.synchronize()
+        L = rt._capi.lib()
+        assert L.rt_denoiser_run(gpu_ctx.handle, lfeat.data_ptr(), S, H, W, gv.data_ptr(), gc.data_ptr(), None) == 0
+        torch.cuda.synchronize()
+        fb = (gc > 0.5) & m
+        both = fb.all(1)
+        one = fb.any(1) & ~both
+        assert int(both.sum().item()) > 0 and int(one.sum().item()) > 0
+        assert r.last_stats.fallback_hits == int(fb.any(1).sum().item())
+        assert r.last_stats.fallback_lights == int(fb.sum().item())
+        assert torch.equal(vis[fb], pv[fb])
+        keep = m & ~fb
+        assert torch.equal(vis[keep], gv[keep])
+
+
+@pytest.mark.gpu
 def test_pixel_mean_visibility_feature(gpu_ctx):
     """Channels 13 and 14 of each hit sample hold the mean cast-ray
     visibility of slots 0 and 1 over the pixel's samples that hit."""
