@@ -4,6 +4,7 @@
     python -m rtrace_b200.profile_render --workload ring_spheres --width 1920 --height 1080 --learned --fallback-samples 64
     python -m rtrace_b200.profile_render --kd-build terrain --reps 2
     python -m rtrace_b200.profile_render --train-steps 3
+    python -m rtrace_b200.profile_render --denoiser-net 3 --width 1920 --height 1080
 
 Workloads (see rtrace_b200.workloads): sphere_grid (quincunx), noisy_icosphere
 (no-jitter + outline, the bench.py scene), ring_spheres (stochastic, 4 spp).
@@ -13,6 +14,9 @@ heightfield, 2,093,058 triangles; icosphere: the level-6 noisy icosphere)
 on the device --reps times after one warm-up build of 1,000 of its
 triangles, checks it against the host build, then uploads the scene once
 (the mesh's search data prepared on the device).
+--denoiser-net runs the shipped denoiser network on seeded features of
+4 sample planes at --width x --height (what a learned render's network pass
+reads), printing its CUDA-event times.
 --train-steps runs that many steps of the denoiser's training on the
 library's kernels, on a batch of 16 seeded random 256x256 feature crops.
 """
@@ -38,12 +42,17 @@ def main(argv=None):
                     help="rays per disk light where a learned render falls back (0: --disk-samples)")
     ap.add_argument("--kd-build", default=None, choices=["terrain", "icosphere"])
     ap.add_argument("--train-steps", type=int, default=0)
+    ap.add_argument("--denoiser-net", type=int, default=0, metavar="REPS",
+                    help="run the shipped denoiser network REPS times on 4 planes of seeded "
+                         "--width x --height features (rt_denoiser_run)")
     a = ap.parse_args(argv)
     d = a.dir or tempfile.mkdtemp(prefix="rtb_prof_")
     if a.kd_build:
         return kd_build(rt, workloads, a.kd_build, d, a.reps)
     if a.train_steps:
         return train_steps(rt, a.train_steps)
+    if a.denoiser_net:
+        return denoiser_net(rt, a.width, a.height, a.denoiser_net)
     if a.workload == "sphere_grid":
         path, aa, spp = workloads.write_scene(d, "sphere_grid.json", workloads.sphere_grid_scene()), 1, 1
     elif a.workload == "noisy_icosphere":
@@ -66,6 +75,34 @@ def main(argv=None):
     st = r.last_stats
     print(json.dumps({"workload": a.workload, "width": a.width, "height": a.height, "rays": st.rays,
                       "device_ms": st.device_ms}))
+    return 0
+
+
+def denoiser_net(rt, W, H, reps, planes=4):
+    import ctypes
+    import torch
+    ctx = rt.default_context(0)
+    ctx.load_denoiser()
+    g = torch.Generator(device="cpu").manual_seed(0)
+    f = torch.rand((planes, H, W, 16), generator=g) * 2 - 0.5
+    f[..., 0] = 1.0
+    feat = f.half().cuda()
+    vis = torch.empty((planes, 2, H, W), device="cuda")
+    conf = torch.empty_like(vis)
+    torch.cuda.synchronize()
+    L = rt._capi.lib()
+    ms = []
+    for _ in range(reps):
+        d = ctypes.c_double()
+        st = L.rt_denoiser_run(ctx.handle, feat.data_ptr(), planes, H, W, vis.data_ptr(), conf.data_ptr(),
+                               ctypes.byref(d))
+        if st != 0:
+            msg = L.rt_last_error(ctx.handle)
+            raise RuntimeError("rt_denoiser_run failed: %s" % (msg.decode() if msg else st))
+        ms.append(d.value)
+    torch.cuda.synchronize()
+    print(json.dumps({"denoiser_net": reps, "planes": planes, "width": W, "height": H,
+                      "ms_min": min(ms), "ms_median": sorted(ms)[len(ms) // 2]}))
     return 0
 
 
