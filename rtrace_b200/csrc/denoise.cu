@@ -526,14 +526,17 @@ cudaError_t launch_conv(const __half* in, int planes, int H, int W, int dil, con
   CUtensorMap map;
   e = make_in_map(&map, in, planes, H, W, CIN, dil);
   if (e != cudaSuccess) return e;
-  // 6 CTAs per SM (each holds at most 128 of the SM's 512 TMEM columns;
-  // shared memory allows 1-7 resident); CTAs beyond the resident ones start
-  // as others finish, which balances the segments better than one resident
-  // wave (1.8x slower) or one CTA per segment (1.2x slower); 2.67 ms for
-  // the network at 1080p x 4 against 2.75 ms with 4
+  // Two waves of the CTAs that fit an SM (shared memory: 228 KB less 1 KB
+  // reserved per CTA; TMEM: 512 columns); CTAs beyond the resident ones
+  // start as others finish, which balances the segments better than one
+  // resident wave (1.8x slower) or one CTA per segment (1.2x slower), and
+  // a CTA loads its weights once for many segments.
+  const int fit_smem = (228 * 1024) / (smem + 1024);
+  const int fit_tmem = 512 / (NACC * acc_cols(COUT));
+  const int resident = std::max(1, std::min(fit_smem, fit_tmem));
   const long long rows_per_col = (H + dil - 1) / dil;
   const long long nsegs = (long long)planes * ((W + TILE_M - 1) / TILE_M) * dil * ((rows_per_col + SEG - 1) / SEG);
-  long long grid = std::min<long long>(nsegs, (long long)num_sms * 6);
+  long long grid = std::min<long long>(nsegs, (long long)num_sms * 2 * resident);
   if (grid < 1) grid = 1;
   k_conv3x3_tc<CIN, COUT, MODE><<<(int)grid, CONV_THREADS, smem, s>>>(map, planes, H, W, dil, (const uint4*)w, b,
                                                                       out, vis, conf, aux, err);
