@@ -132,6 +132,12 @@ __host__ __device__ constexpr int conv_nrow(int cin, int cout) { return (cin == 
 constexpr int NACC = 2;    // TMEM accumulators (MMA -> epilogue)
 constexpr int SEG = 8;     // output rows a CTA walks down one column at a time (8 measured best of 8-64)
 constexpr int CONV_THREADS = 192;  // warps 0-3 epilogue, warp 4 TMA, warp 5 MMA
+// Register cap: the pooling epilogue (MODE 4) of 32 -> 32 keeps 32 running
+// sums per thread; without a cap it takes 128 registers and 2 CTAs per SM
+// where shared memory allows 3.
+__host__ __device__ constexpr int conv_min_blocks(int cin, int cout, int mode) {
+  return (mode == 4 && cin == 32 && cout == 32) ? 3 : 1;
+}
 __host__ __device__ constexpr int halo_px(int dil) { return TILE_M + 2 * dil; }
 __host__ __device__ constexpr int halo_block(int dil) { return ((halo_px(dil) * 16 + 127) / 128) * 128; }
 template <int CIN, int COUT>
@@ -193,7 +199,9 @@ __device__ __forceinline__ void mbar_arrive(uint32_t mbar) {
 //   MODE 1: the accumulator times (aux > 0), aux an FP16 NHWC tensor of the
 //           output's shape, no bias (backward data through a ReLU: aux is
 //           the forward activation the gradient flows into);
-//   MODE 3: the accumulator alone (backward data into a linear tensor).
+//   MODE 3: the accumulator alone (backward data into a linear tensor);
+//   MODE 4: MODE 0, and the output's 2x2 average pool (k_pool2's bytes)
+//           into `pool`, for a layer of dilation 1 that a pooling follows.
 // MODE 2: float outputs: sigmoid(channel j + bias) for j < DN_MAX_SLOTS
 // into vis [plane][slot][H][W] (visibility of disk-light slot j) and
 // sigmoid(channel DN_MAX_SLOTS + j + bias) into conf (the network's
@@ -220,12 +228,13 @@ __device__ __forceinline__ void mbar_arrive(uint32_t mbar) {
 // leave their loops, and the TMA and MMA threads wait (bounded) for their
 // operations still in flight before the tensor memory is released.
 template <int CIN, int COUT, int MODE>
-__global__ void __launch_bounds__(CONV_THREADS) k_conv3x3_tc(const __grid_constant__ CUtensorMap in_map, int planes,
+__global__ void __launch_bounds__(CONV_THREADS, conv_min_blocks(CIN, COUT, MODE)) k_conv3x3_tc(const __grid_constant__ CUtensorMap in_map, int planes,
                                                               int H, int W, int dil, const uint4* __restrict__ wl,
                                                               const float* __restrict__ bias,
                                                               __half* __restrict__ out, float* __restrict__ vis,
                                                               float* __restrict__ conf,
-                                                              const __half* __restrict__ aux, int* err) {
+                                                              const __half* __restrict__ aux,
+                                                              __half* __restrict__ pool, int* err) {
   static_assert(CIN % 16 == 0 && COUT % 16 == 0 && COUT <= 64, "unsupported channel counts");
   constexpr int ACC = acc_cols(COUT), TMEM_ALLOC = NACC * ACC;
   using SM = ConvSmem<CIN, COUT>;
@@ -365,6 +374,10 @@ __global__ void __launch_bounds__(CONV_THREADS) k_conv3x3_tc(const __grid_consta
     // ---- epilogue (warps 0-3: thread tid <-> TMEM lane tid <-> pixel x0 + tid)
     long long i = 0;
     bool stop = false;
+    // MODE 4: the running 2x2 sums of the pooled pixel this lane (even
+    // lanes: pixels x, x + 1; rows y, y + 1 are consecutive steps of a
+    // segment) writes, added in k_pool2's order
+    float pacc[MODE == 4 ? COUT : 1];
     for (long long g = blockIdx.x; g < nsegs && !stop; g += gridDim.x) {
       const ConvSeg c = conv_seg(g, H, dil, tiles_x);
       for (int t = 0; t < c.L; t++, i++) {
@@ -401,6 +414,10 @@ __global__ void __launch_bounds__(CONV_THREADS) k_conv3x3_tc(const __grid_consta
         if (lane == 0) mbar_arrive(acce_bar(a));
         const int tx = c.tx, p = c.p, y = c.r + (c.k0 + t) * dil;
         const int x = tx * TILE_M + tid;
+        // MODE 4 (dilation 1, segments start on even rows): rows y, y + 1 of
+        // a pooled row are steps t, t + 1; an odd count ends at the image's
+        // last row
+        const bool odd_row = (t & 1) != 0, pool_row = odd_row || t + 1 == c.L, pair_x = x + 1 < W;
         if (MODE != 2) {
           constexpr int CPX0 = COUT / 8;
           // MODE 1: the ReLU mask of this pixel's forward activation
@@ -424,7 +441,7 @@ __global__ void __launch_bounds__(CONV_THREADS) k_conv3x3_tc(const __grid_consta
   #pragma unroll
             for (int e = 0; e < 8; e++) {
               float v = __uint_as_float(accv[8 * c + e]);
-              if (MODE == 0) {
+              if (MODE == 0 || MODE == 4) {
                 v += s_bias[8 * c + e];
                 v = v > 0.f ? v : 0.f;
               } else if (MODE == 1) {
@@ -434,6 +451,26 @@ __global__ void __launch_bounds__(CONV_THREADS) k_conv3x3_tc(const __grid_consta
                 v = ((bits & 0x8000u) == 0 && bits != 0) ? v : 0.f;
               }
               h[e] = __float2half_rn(v);
+            }
+            if (MODE == 4) {
+  #pragma unroll
+              for (int e = 0; e < 8; e++) {
+                const float fv = __half2float(h[e]);
+                const float nb = __shfl_xor_sync(0xffffffffu, fv, 1);  // pixel x + 1 (even lanes)
+                float acc = odd_row ? pacc[8 * c + e] + fv : fv;
+                if (pair_x) acc = acc + nb;
+                pacc[8 * c + e] = acc;
+              }
+              if (pool_row && (lane & 1) == 0 && x < W) {
+                const float inv = 1.f / (float)((pair_x ? 2 : 1) * (odd_row ? 2 : 1));
+                uint4 o;
+                __half2* oh = reinterpret_cast<__half2*>(&o);
+  #pragma unroll
+                for (int k = 0; k < 4; k++)
+                  oh[k] = __floats2half2_rn(pacc[8 * c + 2 * k] * inv, pacc[8 * c + 2 * k + 1] * inv);
+                const int Ho = (H + 1) / 2, Wo = (W + 1) / 2;
+                reinterpret_cast<uint4*>(pool + (((long long)p * Ho + y / 2) * (long long)Wo + x / 2) * COUT)[c] = o;
+              }
             }
             const int phys = c ^ ((lane / PPL) & (CPX - 1));
             *reinterpret_cast<uint4*>(wb + lane * ROWB + phys * 16) = *reinterpret_cast<const uint4*>(h);
@@ -505,7 +542,8 @@ cudaError_t make_in_map(CUtensorMap* map, const __half* in, int planes, int H, i
 
 template <int CIN, int COUT, int MODE>
 cudaError_t launch_conv(const __half* in, int planes, int H, int W, int dil, const void* w, const float* b, __half* out,
-                        float* vis, float* conf, const __half* aux, int* err, cudaStream_t s, int num_sms) {
+                        float* vis, float* conf, const __half* aux, __half* pool, int* err, cudaStream_t s,
+                        int num_sms) {
   using SM = ConvSmem<CIN, COUT>;
   if (dil < 1 || dil > MAX_DIL) return cudaErrorInvalidValue;
   const int smem = SM::total(dil);
@@ -539,7 +577,7 @@ cudaError_t launch_conv(const __half* in, int planes, int H, int W, int dil, con
   long long grid = std::min<long long>(nsegs, (long long)num_sms * 2 * resident);
   if (grid < 1) grid = 1;
   k_conv3x3_tc<CIN, COUT, MODE><<<(int)grid, CONV_THREADS, smem, s>>>(map, planes, H, W, dil, (const uint4*)w, b,
-                                                                      out, vis, conf, aux, err);
+                                                                      out, vis, conf, aux, pool, err);
   return cudaGetLastError();
 }
 
@@ -626,7 +664,7 @@ cudaError_t conv_launch(int cin, int cout, int mode, const __half* in, int plane
                         int* err, cudaStream_t s, int num_sms) {
 #define RTB_CONV_CASE(CI, CO, M)                                                                         \
   if (cin == CI && cout == CO && mode == M)                                                              \
-    return launch_conv<CI, CO, M>(in, planes, H, W, dil, w, b, out, vis, conf, aux, err, s, num_sms);
+    return launch_conv<CI, CO, M>(in, planes, H, W, dil, w, b, out, vis, conf, aux, nullptr, err, s, num_sms);
 #define RTB_CONV_SHAPE(CI, CO) RTB_CONV_CASE(CI, CO, 0) RTB_CONV_CASE(CI, CO, 1) RTB_CONV_CASE(CI, CO, 3)
   RTB_CONV_SHAPE(16, 16)
   RTB_CONV_SHAPE(16, 32)
@@ -641,6 +679,21 @@ cudaError_t conv_launch(int cin, int cout, int mode, const __half* in, int plane
 #undef RTB_CONV_CASE
   return cudaErrorInvalidValue;
 }
+
+// A forward layer (bias + ReLU) whose output is also 2x2 average-pooled
+// into `pool` ([planes][ceil(H/2)][ceil(W/2)][cout]), the bytes of
+// pool2_launch on `out`.  Dilation 1 only; the shapes the network pools
+// after (32 -> 32, 64 -> 64).
+cudaError_t conv_pool_launch(int cin, int cout, const __half* in, int planes, int H, int W, const void* w,
+                             const float* b, __half* out, __half* pool, int* err, cudaStream_t s, int num_sms) {
+  if (cin == 32 && cout == 32)
+    return launch_conv<32, 32, 4>(in, planes, H, W, 1, w, b, out, nullptr, nullptr, nullptr, pool, err, s, num_sms);
+  if (cin == 64 && cout == 64)
+    return launch_conv<64, 64, 4>(in, planes, H, W, 1, w, b, out, nullptr, nullptr, nullptr, pool, err, s, num_sms);
+  return cudaErrorInvalidValue;
+}
+
+bool conv_pool_supported(int cin, int cout) { return cin == cout && (cin == 32 || cin == 64); }
 
 bool conv_shape_supported(int cin, int cout) {
   static const int shapes[][2] = {{16, 16}, {16, 32}, {32, 16}, {32, 32}, {32, 64}, {64, 32}, {64, 64}};
@@ -850,6 +903,24 @@ int denoise_run(const DenoiseNet& net, const __half* feat, int planes, int H, in
       off = (off + 127) & ~(size_t)127;
     }
     cudaError_t e;
+    // a forward layer whose output the next op pools: one launch writes both
+    const DnOp* np = i + 1 < net.ops.size() ? &net.ops[i + 1] : nullptr;
+    if (o.kind == DN_CONV && o.act == 0 && o.dil == 1 && np && np->kind == DN_POOL && np->src == (int)i + 1 &&
+        i + 2 < net.ops.size() && conv_pool_supported(o.cin, o.cout)) {
+      __half* pooled = arena + off;
+      off += (size_t)planes * level_dim(H, np->level) * level_dim(W, np->level) * np->cout;
+      off = (off + 127) & ~(size_t)127;
+      e = conv_pool_launch(o.cin, o.cout, buf[o.src], planes, h, w, o.w, o.b, out, pooled, err, s, num_sms);
+      launches++;
+      if (e != cudaSuccess) {
+        *launch_err = e;
+        return launches;
+      }
+      buf[i + 1] = out;
+      buf[i + 2] = pooled;
+      i++;
+      continue;
+    }
     if (o.kind == DN_CONV) {
       if (o.act == 2)
         e = conv_launch(o.cin, o.cout, 2, buf[o.src], planes, h, w, o.dil, o.w, o.b, nullptr, vis,

@@ -51,18 +51,20 @@ def test_unet_forward_matches_torch_fp32(gpu_ctx):
     dev = torch.device("cuda", gpu_ctx.device)
     net = denoiser.random_net(1, scale=1.0)
     gpu_ctx.load_denoiser(denoiser.pack_net(net))
-    # 300 wide: two full 128-pixel tiles and a ragged one; odd heights pool raggedly
-    feat = (torch.rand((2, 37, 300, 16), device=dev) * 2 - 0.5).half()
-    vis = torch.full((2, 2, 37, 300), -7.0, device=dev)
-    conf = torch.full((2, 2, 37, 300), -7.0, device=dev)
-    torch.cuda.synchronize()
     L = rt._capi.lib()
-    st = L.rt_denoiser_run(gpu_ctx.handle, feat.data_ptr(), 2, 37, 300, vis.data_ptr(), conf.data_ptr(), None)
-    assert st == 0, L.rt_last_error(gpu_ctx.handle)
-    torch.cuda.synchronize()
-    rv, rc = denoiser.net_forward(net, feat, round_fp16=True)
-    assert (vis - rv).abs().max().item() < 3e-3
-    assert (conf - rc).abs().max().item() < 3e-3
+    # 300 wide: two full 128-pixel tiles and a ragged one; odd heights pool
+    # raggedly.  301 wide: odd widths at both poolings (301, 151)
+    for H, W in ((37, 300), (35, 301)):
+        feat = (torch.rand((2, H, W, 16), device=dev) * 2 - 0.5).half()
+        vis = torch.full((2, 2, H, W), -7.0, device=dev)
+        conf = torch.full((2, 2, H, W), -7.0, device=dev)
+        torch.cuda.synchronize()
+        st = L.rt_denoiser_run(gpu_ctx.handle, feat.data_ptr(), 2, H, W, vis.data_ptr(), conf.data_ptr(), None)
+        assert st == 0, L.rt_last_error(gpu_ctx.handle)
+        torch.cuda.synchronize()
+        rv, rc = denoiser.net_forward(net, feat, round_fp16=True)
+        assert (vis - rv).abs().max().item() < 3e-3, (H, W)
+        assert (conf - rc).abs().max().item() < 3e-3, (H, W)
 
 
 @pytest.mark.gpu
