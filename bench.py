@@ -143,21 +143,31 @@ NOISE_CAP_RAYS = 1024  # a near-noise-free reference, reported beside the 64-ray
 def denoiser_roofline(rt, torch, ctx, feat, hbm, tflops):
     """The network alone on the frame's feature image: CUDA-event time of
     rt_denoiser_run, algorithmic bytes (every op's FP16 input and output
-    once, FP32 outputs of the last op) and FLOPs (2 x 9 x cin x cout per
-    output pixel of each convolution), against HBM and the FP16/BF16 tensor
-    peak."""
+    once, FP32 outputs of the last op; a pooling that the library fuses into
+    the convolution before it reads nothing) and FLOPs (2 x 9 x cin x cout
+    per output pixel of each convolution), against HBM and the FP16/BF16
+    tensor peak."""
     from rtrace_b200 import denoiser
     net = denoiser.unpack_net(denoiser.read_blob())
     P, H, W, _ = feat.shape
     dims = lambda lv: (-(-H // (1 << lv)), -(-W // (1 << lv)))
     ch, lv = [16], [0]
     nbytes, flops = 0.0, 0.0
+    fused = 0
     for i, (kind, cin, cout, dil, src, src2) in enumerate(net.ops):
         level = lv[src] + 1 if kind == "pool" else (lv[src2] if kind == "upadd" else lv[src])
         h, w = dims(level)
         hs, ws = dims(lv[src])
         last = i + 1 == len(net.ops)
-        nbytes += P * hs * ws * ch[src] * 2 + (P * h * w * 16 if last else P * h * w * cout * 2)
+        prev = net.ops[i - 1] if i > 0 else None
+        # the library's rule (denoise_run): a pooling right after the
+        # dilation-1 32 -> 32 or 64 -> 64 layer it reads runs in its epilogue
+        pooled_in_epilogue = (kind == "pool" and src == i and prev is not None and prev[0] == "conv" and
+                              prev[3] == 1 and prev[1] == prev[2] and prev[1] in (32, 64))
+        fused += pooled_in_epilogue
+        if not pooled_in_epilogue:
+            nbytes += P * hs * ws * ch[src] * 2
+        nbytes += P * h * w * 16 if last else P * h * w * cout * 2
         if kind == "upadd":
             nbytes += P * h * w * ch[src2] * 2
         if kind == "conv":
@@ -175,7 +185,12 @@ def denoiser_roofline(rt, torch, ctx, feat, hbm, tflops):
             raise RuntimeError(L.rt_last_error(ctx.handle))
         ms.append(d.value)
     t = sorted(ms[2:])[len(ms[2:]) // 2] * 1e-3
-    return {"kernel": "denoiser network (k_conv3x3_tc x %d, k_pool2, k_upadd)" % sum(o[0] == "conv" for o in net.ops),
+    n_conv = sum(o[0] == "conv" for o in net.ops)
+    n_pool = sum(o[0] == "pool" for o in net.ops) - fused
+    n_up = sum(o[0] == "upadd" for o in net.ops)
+    name = "denoiser network (k_conv3x3_tc x %d, %d of them pooling in the epilogue; k_pool2 x %d, k_upadd x %d)" % (
+        n_conv, fused, n_pool, n_up)
+    return {"kernel": name,
             "bound": "hbm", "achieved": nbytes / t / 1e9, "peak": hbm, "unit": "GB/s", "frac": nbytes / t / 1e9 / hbm,
             "algorithmic_bytes": nbytes, "ms": t * 1e3, "params": net.param_count,
             "tensor": {"achieved_tflops": flops / t / 1e12, "peak_tflops": tflops,
