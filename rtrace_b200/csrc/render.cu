@@ -72,7 +72,8 @@ struct rt_scene {
   rt_outline_config outline{};
   int has_outline = 0;
   std::string render_error;
-  std::vector<DMesh> host_meshes;       // device pointers, for the debug entry point
+  std::vector<DMesh> host_meshes;       // device pointers, for the debug entry point; empty: k_shadow's
+                                        // mesh-free register budget
   std::vector<int> obj_kind, obj_mesh;  // per World object
   int n_point_lights = 0, n_disk_lights = 0;
   // upload arena: one device block; small arrays are staged in the
